@@ -1,0 +1,347 @@
+/*
+ * relax_b200.h -- C ABI of the B200 (sm_100a) implementation of RELAX's
+ * per-time-step relaxation loop.
+ *
+ * Two layers are exported:
+ *
+ *  1. A context API (relax_*): explicit handle, int status on every call,
+ *     stream-ordered work on one CUDA device.  This is what a new host
+ *     (C, C++, Fortran via iso_c_binding, Python via ctypes) binds.
+ *
+ *  2. A compatibility shim (cu*_ symbols, gfortran naming: lower case and a
+ *     trailing underscore, scalars by value, arrays by reference) that
+ *     replaces the reference CUDA layer symbol for symbol, so that the
+ *     reference Fortran GPU driver links unchanged.  Each declaration below
+ *     cites the reference function it replaces.
+ *
+ * Field layouts at the boundary are RELAX's: Fortran column-major, i1
+ * fastest.  Vector fields are padded to sx1+2 in x1 (in-place real FFT
+ * layout of src/relax.f90:250-252), tensors are arrays of 6-float structs
+ * (TENSOR, src/types.f90:41-44), the physical half-space holds sx3/2 layers.
+ * Inside the library the fields are kept in a structure-of-arrays layout.
+ */
+#ifndef RELAX_B200_H
+#define RELAX_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                       */
+/* ------------------------------------------------------------------ */
+#define RELAX_OK               0
+#define RELAX_ERR_ARG          1   /* invalid argument / size            */
+#define RELAX_ERR_CUDA         2   /* CUDA runtime error                 */
+#define RELAX_ERR_NOMEM        3   /* device or host allocation failed   */
+#define RELAX_ERR_UNSUPPORTED  4   /* grid/feature not implemented       */
+#define RELAX_ERR_STATE        5   /* call out of order / no context     */
+#define RELAX_ERR_FRICTION     6   /* tau/((a-b)sigma) > 20, the abort of
+                                      src/friction3d.f90:204-215         */
+#define RELAX_ERR_POWER        7   /* stress exponent < 0.999999, the abort
+                                      of src/viscoelastic3d.f90:271-276   */
+
+/* ------------------------------------------------------------------ */
+/* data types (binary compatible with the reference)                   */
+/* ------------------------------------------------------------------ */
+
+/* TENSOR, src/types.f90:41-44 (C mirror src/cuinclude.h:204-212) */
+typedef struct relax_tensor {
+    float s11, s12, s13, s22, s23, s33;
+} relax_tensor;
+
+/* TENSOR_LAYER_STRUCT, src/types.f90:52-56 */
+typedef struct relax_tensor_layer {
+    float z, dum;
+    relax_tensor t;
+} relax_tensor_layer;
+
+/* LAYER_STRUCT, src/types.f90:31-34.  For fault-creep structures the
+ * fields are reused as: gammadot0 = V0, stressexponent = (a-b)sigma,
+ * friction = mu_f, cohesion = c (src/friction3d.f90:131-134). */
+typedef struct relax_layer {
+    double z, gammadot0, stressexponent, cohesion, friction, Gk;
+} relax_layer;
+
+/* SOURCE_STRUCT, src/types.f90:26-29, in the internal convention
+ * (after wangconvention, src/input.f90:1780-1800): centre coordinates,
+ * strike/dip/rake in radians, slip sign flipped. */
+typedef struct relax_source {
+    double slip, x, y, z, width, length, strike, dip, rake,
+           period, phase, beta, opening;
+} relax_source;
+
+/* PLANE_STRUCT without its patch array, src/types.f90:92-97 */
+typedef struct relax_plane {
+    double x, y, z, width, length, strike, dip, rake;
+    int px2, px3;
+} relax_plane;
+
+/* SLIPPATCH_STRUCT, src/types.f90:76-90 */
+typedef struct relax_slippatch {
+    double x1, x2, x3, lx, lz, slip, ss, ds, v, vss, vds, taus;
+    relax_tensor sig;
+} relax_slippatch;
+
+/* EVENT_STRUC, src/types.f90:99-106 (shear, tensile, point and load
+ * sources; cuboid/tetrahedron eigenstrain sources are not supported). */
+typedef struct relax_event {
+    double time;
+    int ns, nt, nm, nl;
+    const relax_source *s;    /* shear dislocations                    */
+    const relax_source *ts;   /* tensile cracks                        */
+    const relax_source *m;    /* dilatation point sources              */
+    const relax_source *l;    /* surface loads                         */
+} relax_event;
+
+/* The part of SIMULATION_STRUCT (src/types.f90:118-266) that the time
+ * loop reads.  Depth structures are per physical layer (sx3/2 entries),
+ * i.e. already expanded by relax_viscoelastic_structure /
+ * relax_tensor_structure.  A NULL structure means "mechanism absent"
+ * (Fortran .NOT.ALLOCATED). */
+typedef struct relax_config {
+    int sx1, sx2, sx3;                  /* FFT box                     */
+    double dx1, dx2, dx3, beta, nyquist;
+    double lambda, mu, gam;             /* Lame parameters, gravity    */
+    double interval, odt, tscale;       /* time-step policy            */
+    int skip;                           /* >0: adaptive, skip mode     */
+    const relax_tensor_layer *stressstruc;  /* prestress, NULL = zero  */
+    const relax_layer *linearstruc;
+    const relax_layer *nonlinearstruc;
+    const relax_layer *faultcreepstruc;
+    const float *lineardgammadot0;      /* optional weak-zone fields,  */
+    const float *nonlineardgammadot0;   /* sx1*sx2*(sx3/2), or NULL    */
+    int np;                             /* afterslip planes            */
+    const relax_plane *planes;
+    int ne;                             /* coseismic events            */
+    const relax_event *events;
+    relax_event inter;                  /* interseismic loading rates  */
+} relax_config;
+
+/* One line of RELAX's step log (src/relax.f90:1027-1047, format 1100):
+ * I, Dt, tm(ve), tm(pl), tm(as), t, power, C:E^i. */
+typedef struct relax_step_log {
+    int i;
+    int event;         /* 1 when a coseismic event fired after the step */
+    double dt, tm_ve, tm_pl, tm_as, t, power, cei;
+} relax_step_log;
+
+/* field selectors for relax_get_field / relax_set_field */
+#define RELAX_FIELD_U       1   /* 3 x float (sx1+2, sx2, sx3/2)         */
+#define RELAX_FIELD_SIG     2   /* relax_tensor (sx1, sx2, sx3/2)        */
+#define RELAX_FIELD_TAU     3   /* relax_tensor (sx1, sx2, sx3/2)        */
+#define RELAX_FIELD_MOMENT  4   /* relax_tensor (sx1, sx2, sx3/2)        */
+#define RELAX_FIELD_GAMMA   5   /* float (sx1+2, sx2, sx3/2)             */
+#define RELAX_FIELD_V       6   /* 3 x float (sx1+2, sx2, sx3) work field */
+#define RELAX_FIELD_T       7   /* 3 x float (sx1+2, sx2) surface traction */
+
+/* ------------------------------------------------------------------ */
+/* host helpers (no device work)                                      */
+/* ------------------------------------------------------------------ */
+
+/* viscoelasticstructure, src/elastic3d.f90:732-829: expand interface
+ * list -> per-layer structure (nz = sx3/2 entries). */
+int relax_viscoelastic_structure(const relax_layer *layers, int nlayers,
+                                 double dx3, int nz, relax_layer *out);
+
+/* tensorstructure, src/elastic3d.f90:630-702 */
+int relax_tensor_structure(const relax_tensor_layer *layers, int nlayers,
+                           double dx3, int nz, relax_tensor_layer *out);
+
+/* wangconvention, src/input.f90:1780-1800 (+ rotation :1802-1815) */
+void relax_wang_convention(double *slip, double *x, double *y, double *z,
+                           double length, double width, double *strike,
+                           double *dip, double *rake, double x0, double y0,
+                           double rot);
+
+/* ------------------------------------------------------------------ */
+/* context API                                                        */
+/* ------------------------------------------------------------------ */
+typedef struct relax_ctx relax_ctx;
+
+const char *relax_version(void);
+const char *relax_last_error(void);     /* thread-local message        */
+
+/* Allocates all device state for one RELAX instance on `device`.  The
+ * configuration is deep-copied.  Replaces cuinflags_/cuinit_
+ * (src/cuelastic.cu:736, :476). */
+int relax_create(const relax_config *cfg, int device, relax_ctx **out);
+/* Replaces cudeinit_ (src/cuelastic.cu:1344). */
+int relax_destroy(relax_ctx *ctx);
+
+/* Stream the context's work is ordered on (cudaStream_t as void*). */
+int relax_get_stream(relax_ctx *ctx, void **stream);
+
+/* Coseismic solve of event `e` (0-based) at the current time:
+ * dislocations -> greenfunctioncowling -> u (+)= v, tau update, then
+ * sig = -tau + C:E(u)  (src/relax.f90:318-371 for e=0, :858-890 later). */
+int relax_coseismic(relax_ctx *ctx, int e, relax_step_log *log0);
+
+/* One RK2 predictor/corrector step (src/relax.f90:555-890).  If
+ * dt_override is non-NULL its value replaces the adaptive Dt of
+ * integrationstep (dt-schedule replay).  Returns RELAX_OK with
+ * log->i == 0 when t >= interval (nothing done). */
+int relax_step(relax_ctx *ctx, const double *dt_override, relax_step_log *log);
+
+/* Runs the coseismic solve of event 0 and up to max_steps steps, stopping
+ * at t >= interval; events are fired as the reference does.  logs has
+ * room for max_steps+1 entries (entry 0 = coseismic line). */
+int relax_run(relax_ctx *ctx, int max_steps, const double *dt_schedule,
+              relax_step_log *logs, int *nsteps_done);
+
+/* Host <-> device field copies in the reference layout (see
+ * RELAX_FIELD_*); `bytes` must equal the field size. */
+int relax_get_field(relax_ctx *ctx, int which, void *host, size_t bytes);
+int relax_set_field(relax_ctx *ctx, int which, const void *host, size_t bytes);
+/* Afterslip patch state of plane k (px2*px3 entries, j2 fastest). */
+int relax_get_patches(relax_ctx *ctx, int k, relax_slippatch *host, size_t n);
+/* Current time, step counter, event index. */
+int relax_get_time(relax_ctx *ctx, double *t, int *i, int *e);
+
+/* Per-stage device timing of the last step (ms), for profiling. */
+int relax_synchronize(relax_ctx *ctx);
+
+/* ------------------------------------------------------------------ */
+/* stateless operators on device buffers (reference layout)           */
+/*                                                                    */
+/* Each takes device pointers in RELAX's layout and a CUDA stream      */
+/* (NULL = legacy default stream); the work is enqueued, not waited   */
+/* for.  They are the unit under the per-kernel parity tests.         */
+/* ------------------------------------------------------------------ */
+
+/* stressupdate, src/elastic3d.f90:956-1180: sig += C:E(u).
+ * u1..u3: (sx1+2, sx2, sx3h) float; sig: (sx1, sx2, sx3h) relax_tensor. */
+int relax_op_stressupdate(const float *u1, const float *u2, const float *u3,
+                          double lambda, double mu, double dx1, double dx2,
+                          double dx3, int sx1, int sx2, int sx3h,
+                          relax_tensor *sig, void *stream);
+
+/* equivalentbodyforce, src/elastic3d.f90:1214-1506:
+ * c_i -= div(sig)_i on the first sx3h layers, t_i += sig_i3(x3=0).
+ * c1..c3: (sx1+2, sx2, >=sx3h) float; t1..t3: (sx1+2, sx2) float. */
+int relax_op_bodyforce(const relax_tensor *sig, double dx1, double dx2,
+                       double dx3, int sx1, int sx2, int sx3h,
+                       float *c1, float *c2, float *c3,
+                       float *t1, float *t2, float *t3, void *stream);
+
+/* viscouseigenstress, src/viscoelastic3d.f90:217-314.
+ * structure/prestress: sx3h entries on the HOST (uploaded internally).
+ * moment += ...; *maxwelltime = min(*maxwelltime, min 1/gammadot) when
+ * maxwelltime != NULL; gamma (sx1+2, sx2, sx3h), written where active,
+ * when non-NULL; dgammadot0 optional (sx1, sx2, sx3h).  Synchronous when
+ * maxwelltime is requested. */
+int relax_op_viscouseigenstress(double mu, const relax_layer *structure,
+                                const relax_tensor_layer *prestress,
+                                const relax_tensor *sig, int sx1, int sx2,
+                                int sx3h, relax_tensor *moment,
+                                double *maxwelltime, float *gamma,
+                                const float *dgammadot0, void *stream);
+
+/* frictioneigenstress, src/friction3d.f90:82-241 for one afterslip plane
+ * (x..rake in the internal convention; L = plane width, W = plane length
+ * as the reference call sites pass them).  Synchronous when maxwelltime
+ * is requested. */
+int relax_op_frictioneigenstress(double x, double y, double z, double L,
+                                 double W, double strike, double dip,
+                                 double rake, double beta,
+                                 const relax_tensor *sig, double mu,
+                                 const relax_layer *structure, int sx1,
+                                 int sx2, int sx3h, double dx1, double dx2,
+                                 double dx3, relax_tensor *moment,
+                                 double *maxwelltime, void *stream);
+
+/* greenfunctioncowling, src/green.f90:1008-1129: c1..c3 (sx1+2, sx2, sx3)
+ * body forces in, displacements out (all sx3 layers); t1..t3 (sx1+2, sx2)
+ * surface tractions are consumed (their content is undefined after the
+ * call).  Replaces calfftnelasic_ (src/cugreen.cu:1453). */
+int relax_op_green(float *c1, float *c2, float *c3, float *t1, float *t2,
+                   float *t3, int sx1, int sx2, int sx3, double dx1,
+                   double dx2, double dx3, double lambda, double mu,
+                   double gam, void *stream);
+
+/* 3-D real<->complex FFT in place on a (sx1+2, sx2, sx3) array with
+ * RELAX's normalisation (src/fourier.f90:177-201): direction -1 forward
+ * (x dx1 dx2 dx3), +1 inverse (/ (sx1 dx1 sx2 dx2 sx3 dx3)). */
+int relax_op_fft3(float *data, int sx1, int sx2, int sx3, double dx1,
+                  double dx2, double dx3, int direction, void *stream);
+
+/* tensoramplitude, src/elastic3d.f90:446-466 (synchronous). */
+int relax_op_tensoramplitude(const relax_tensor *t, int sx1, int sx2,
+                             int sx3h, double dx1, double dx2, double dx3,
+                             double *amp, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* compatibility shim: the reference CUDA layer, symbol for symbol     */
+/* (src/cuelastic.cu, src/cugreen.cu).  One implicit default context,  */
+/* single thread, synchronous, as the reference.                      */
+/* ------------------------------------------------------------------ */
+typedef relax_tensor ST_TENSOR_C;
+
+/* src/cuelastic.cu:736 */
+void cuinflags_(int *istransient, int *nlwz, int *nnlwz, int *nltwz,
+                int *nnltwz, int islinear, int isnonlinear,
+                int isltransient, int isnltransient, int *iRet);
+/* src/cuelastic.cu:476 */
+void cuinit_(int sx1, int sx2, int sx3, double dx1, double dx2, double dx3,
+             int *iRet);
+/* src/cuelastic.cu:1344 */
+void cudeinit_(void);
+/* src/cuelastic.cu:1493 -- v = 0, t = 0 */
+void curesetvectors_(void);
+/* src/cuelastic.cu:1596 -- 1: tau, 2: moment, 3: sig <- 0 */
+void cutensormemset_(int eType);
+/* src/cuelastic.cu:1572 -- dir 0: device->host, 1: host->device */
+void copytau_(ST_TENSOR_C *host, int sx1, int sx2, int sx3h, int dir);
+/* src/cuelastic.cu:1330 -- t3 device -> host */
+void cucopytraction_(float *t3, int sx1, int sx2, int *iRet);
+/* src/cuelastic.cu:1483 -- u = v (first sx3h layers) */
+void cufieldrep_(int sx1p2, int sx2, int sx3h);
+/* src/cuelastic.cu:1412 -- 1: u = c1 u + c2 v, 2: v = c1 v + c2 u */
+void cufieldadd_(int eType, float *a, float *b, float *c, float *d,
+                 float *e, float *f, int sx1p2, int sx2, int sx3h,
+                 float c1, float c2);
+/* src/cuelastic.cu:1216 -- enum E_TENSOR_FIELD (src/cuinclude.h:100-111) */
+void cutensorfieldadd_(int eField, int sx1, int sx2, int sx3h, float c1,
+                       float c2);
+/* src/cuelastic.cu:786 -- 1: sig += C:E(u), 2: sig += C:E(v) */
+void custressupdatewrapper_(int eType, double lambda, double mu, double dx1,
+                            double dx2, double dx3, int sx1, int sx2,
+                            int sx3h, float *u1, float *u2, float *u3,
+                            ST_TENSOR_C *sig);
+/* src/cuelastic.cu:838 -- 1: div(sig), 2: div(moment) -> v, t */
+void cubodyforceswrapper_(int eType, double dx1, double dx2, double dx3,
+                          int sx1, int sx2, int sx3h, float *v1, float *v2,
+                          float *v3, float *t1, float *t2, float *t3);
+/* src/cugreen.cu:1453 -- Green's function on the context's v, t */
+void calfftnelasic_(float *c1, float *c2, float *c3, float *t1, float *t2,
+                    float *t3, int sx1, int sx2, int sx3, double dx1,
+                    double dx2, double dx3, double lambda, double mu,
+                    double gam, float *p1, float *p2, float *p3, int *iRet);
+/* src/cuelastic.cu:1122 -- moment += viscous eigenstress of sig */
+void cuviscouseigen_(relax_layer *structure, relax_tensor_layer *prestress,
+                     double mu, int sx1, int sx2, int sx3h, double dx1,
+                     double dx2, double dx3, int bMaxwell, double *tm,
+                     int gammadot0type);
+/* src/cuelastic.cu:1762 */
+void cufrictioneigenstress_(double x, double y, double z, double L, double W,
+                            double strike, double dip, double rake,
+                            double beta, double mu, relax_layer *structure,
+                            int sx1, int sx2, int sx3h, double dx1,
+                            double dx2, double dx3, int bPresent, float *tm,
+                            ST_TENSOR_C *moment, ST_TENSOR_C *sig);
+/* src/cuelastic.cu:1350 -- 1: moment, 2: tau; sum of norms (no dV) */
+void cutensoramp_(int eType, int sx1, int sx2, int sx3h, double *amp);
+/* src/cuelastic.cu:874 -- body force + traction of one shear source */
+void cusource_(double mu, double s, double x, double y, double z, double L,
+               double W, double strike, double dip, double rake,
+               double beta, int sx1, int sx2, int sx3, double dx1,
+               double dx2, double dx3, float *f1, float *f2, float *f3,
+               float *t1, float *t2, float *t3);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RELAX_B200_H */

@@ -1,0 +1,373 @@
+"""Host-side description of one RELAX simulation and its C-ABI mirror.
+
+The ctypes structures below mirror ``include/relax_b200.h`` field for field
+(and therefore RELAX's own types, src/types.f90:26-266).  ``Simulation``
+holds an input deck in RELAX's *input-file* convention (geologic fault
+geometry in degrees, interface lists) and ``Simulation.to_c`` turns it into
+a ``relax_config`` in the internal convention the time loop reads:
+
+* faults and afterslip planes go through ``wang_convention``
+  (src/input.f90:1780-1800) and the afterslip rake flip
+  (src/input.f90:1079-1083);
+* interface lists are expanded to one entry per physical layer by a
+  caller-supplied ``structure_fn`` (the library's
+  ``relax_viscoelastic_structure`` or the oracle's restatement).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+DEG2RAD = 0.01745329251994329547437168059786927
+
+
+class relax_tensor(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("s11", "s12", "s13", "s22", "s23", "s33")]
+
+
+class relax_tensor_layer(C.Structure):
+    _fields_ = [("z", C.c_float), ("dum", C.c_float), ("t", relax_tensor)]
+
+
+class relax_layer(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("z", "gammadot0", "stressexponent", "cohesion", "friction", "Gk")]
+
+
+class relax_source(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("slip", "x", "y", "z", "width", "length", "strike", "dip", "rake",
+                 "period", "phase", "beta", "opening")]
+
+
+class relax_plane(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("x", "y", "z", "width", "length", "strike", "dip", "rake")] + \
+               [("px2", C.c_int), ("px3", C.c_int)]
+
+
+class relax_slippatch(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("x1", "x2", "x3", "lx", "lz", "slip", "ss", "ds", "v", "vss", "vds",
+                 "taus")] + [("sig", relax_tensor)]
+
+
+class relax_event(C.Structure):
+    _fields_ = [("time", C.c_double), ("ns", C.c_int), ("nt", C.c_int), ("nm", C.c_int),
+                ("nl", C.c_int), ("s", C.POINTER(relax_source)),
+                ("ts", C.POINTER(relax_source)), ("m", C.POINTER(relax_source)),
+                ("l", C.POINTER(relax_source))]
+
+
+class relax_config(C.Structure):
+    _fields_ = [("sx1", C.c_int), ("sx2", C.c_int), ("sx3", C.c_int),
+                ("dx1", C.c_double), ("dx2", C.c_double), ("dx3", C.c_double),
+                ("beta", C.c_double), ("nyquist", C.c_double),
+                ("lambda_", C.c_double), ("mu", C.c_double), ("gam", C.c_double),
+                ("interval", C.c_double), ("odt", C.c_double), ("tscale", C.c_double),
+                ("skip", C.c_int),
+                ("stressstruc", C.POINTER(relax_tensor_layer)),
+                ("linearstruc", C.POINTER(relax_layer)),
+                ("nonlinearstruc", C.POINTER(relax_layer)),
+                ("faultcreepstruc", C.POINTER(relax_layer)),
+                ("lineardgammadot0", C.POINTER(C.c_float)),
+                ("nonlineardgammadot0", C.POINTER(C.c_float)),
+                ("np", C.c_int), ("planes", C.POINTER(relax_plane)),
+                ("ne", C.c_int), ("events", C.POINTER(relax_event)),
+                ("inter", relax_event)]
+
+
+class relax_step_log(C.Structure):
+    _fields_ = [("i", C.c_int), ("event", C.c_int)] + \
+               [(n, C.c_double) for n in ("dt", "tm_ve", "tm_pl", "tm_as", "t", "power", "cei")]
+
+    def as_tuple(self):
+        return (self.i, self.dt, self.tm_ve, self.tm_pl, self.tm_as, self.t, self.power,
+                self.cei)
+
+
+TENSOR_DTYPE = np.dtype([(n, np.float32) for n in ("s11", "s12", "s13", "s22", "s23", "s33")])
+
+
+def wang_convention(slip, x, y, z, length, width, strike, dip, rake, x0=0.0, y0=0.0, rot=0.0):
+    """wangconvention + rotation, src/input.f90:1780-1815.
+
+    Geologic description (upper end of the top edge, strike/dip/rake in
+    degrees) -> internal convention (centre, radians, slip sign flipped).
+    """
+    slip = -slip
+    strike = -90.0 - strike
+    dip = 90.0 - dip
+    strike = strike * DEG2RAD
+    dip = dip * DEG2RAD
+    rake = rake * DEG2RAD
+    x = x - x0 - length / 2.0 * math.sin(strike) + width / 2.0 * math.sin(dip) * math.cos(strike)
+    y = y - y0 - length / 2.0 * math.cos(strike) - width / 2.0 * math.sin(dip) * math.sin(strike)
+    z = z + width / 2.0 * math.cos(dip)
+    alpha = rot * DEG2RAD
+    xx, yy = x, y
+    x = +xx * math.cos(alpha) + yy * math.sin(alpha)
+    y = -xx * math.sin(alpha) + yy * math.cos(alpha)
+    strike = strike + rot * DEG2RAD
+    return slip, x, y, z, strike, dip, rake
+
+
+def fix(number: float) -> int:
+    """fix, src/elastic3d.f90:69-80 (round half down)."""
+    f, c = math.floor(number), math.ceil(number)
+    return int(c if (number - f) > 0.5 else f)
+
+
+@dataclass
+class Fault:
+    """One shear dislocation in input-file convention (src/input.f90:1299-1303)."""
+    slip: float
+    x: float
+    y: float
+    z: float
+    length: float
+    width: float
+    strike: float
+    dip: float
+    rake: float
+    beta: Optional[float] = None
+
+
+@dataclass
+class Plane:
+    """One afterslip plane in input-file convention (src/input.f90:1059-1062)."""
+    x: float
+    y: float
+    z: float
+    length: float
+    width: float
+    strike: float
+    dip: float
+    rake: float
+
+
+@dataclass
+class Event:
+    time: float
+    faults: List[Fault] = field(default_factory=list)
+
+
+@dataclass
+class Simulation:
+    """An input deck restricted to what the relaxation loop reads."""
+    sx1: int
+    sx2: int
+    sx3: int
+    dx1: float
+    dx2: float
+    dx3: float
+    beta: float = 0.2
+    nyquist: float = 2.0
+    lambda_: float = 1.0
+    mu: float = 1.0
+    gam: float = 0.0
+    interval: float = 1.0
+    odt: float = -1.0          # 2nd entry of the time line; <0 selects skip mode
+    tscale: float = 1.0
+    x0: float = 0.0
+    y0: float = 0.0
+    rot: float = 0.0
+    # interface lists: (depth, gammadot0, power, cohesion) for viscous layers,
+    # (depth, V0, (a-b)sigma, friction, cohesion) for fault creep
+    linear: List[Tuple[float, ...]] = field(default_factory=list)
+    nonlinear: List[Tuple[float, ...]] = field(default_factory=list)
+    faultcreep: List[Tuple[float, ...]] = field(default_factory=list)
+    planes: List[Plane] = field(default_factory=list)
+    events: List[Event] = field(default_factory=list)
+    name: str = "relax"
+
+    @property
+    def sx3h(self) -> int:
+        return self.sx3 // 2
+
+    @property
+    def skip(self) -> int:
+        # src/input.f90:308-316: "T, -n, t_s" -> skip = ceiling(n), odt < 0
+        return int(math.ceil(-self.odt)) if self.odt < 0 else 0
+
+    @property
+    def npoints(self) -> int:
+        return self.sx1 * self.sx2 * self.sx3
+
+    # -------------------------------------------------------------- #
+    def layer_lists(self):
+        lin = [relax_layer(z=d, gammadot0=g, stressexponent=1.0,
+                           cohesion=(c[0] if c else 0.0), friction=0.0, Gk=0.0)
+               for (d, g, *c) in self.linear]
+        non = [relax_layer(z=d, gammadot0=g, stressexponent=n, cohesion=c, friction=0.0, Gk=0.0)
+               for (d, g, n, c) in self.nonlinear]
+        fc = [relax_layer(z=d, gammadot0=v0, stressexponent=ab, friction=f, cohesion=c, Gk=0.0)
+              for (d, v0, ab, f, c) in self.faultcreep]
+        return lin, non, fc
+
+    def to_c(self, structure_fn: Callable[[Sequence[relax_layer], float, int], C.Array]):
+        """Returns (relax_config, keepalive) for this deck."""
+        keep = []
+        nz = self.sx3h
+        cfg = relax_config()
+        cfg.sx1, cfg.sx2, cfg.sx3 = self.sx1, self.sx2, self.sx3
+        cfg.dx1, cfg.dx2, cfg.dx3 = self.dx1, self.dx2, self.dx3
+        cfg.beta, cfg.nyquist = self.beta, self.nyquist
+        cfg.lambda_, cfg.mu, cfg.gam = self.lambda_, self.mu, self.gam
+        cfg.interval, cfg.tscale = self.interval, self.tscale
+        cfg.odt = self.odt
+        cfg.skip = self.skip
+        lin, non, fc = self.layer_lists()
+        for name, lst in (("linearstruc", lin), ("nonlinearstruc", non),
+                          ("faultcreepstruc", fc)):
+            if lst:
+                arr = structure_fn(lst, self.dx3, nz)
+                keep.append(arr)
+                setattr(cfg, name, C.cast(arr, C.POINTER(relax_layer)))
+        # afterslip planes (src/input.f90:1059-1101)
+        if self.planes:
+            parr = (relax_plane * len(self.planes))()
+            for k, p in enumerate(self.planes):
+                rake = p.rake - 180.0 if p.rake >= 0.0 else p.rake + 180.0
+                _, x, y, z, strike, dip, rake = wang_convention(
+                    0.0, p.x, p.y, p.z, p.length, p.width, p.strike, p.dip, rake,
+                    self.x0, self.y0, self.rot)
+                parr[k] = relax_plane(x=x, y=y, z=z, width=p.width, length=p.length,
+                                      strike=strike, dip=dip, rake=rake,
+                                      px2=fix(p.length / self.dx2), px3=fix(p.width / self.dx3))
+            keep.append(parr)
+            cfg.np = len(self.planes)
+            cfg.planes = C.cast(parr, C.POINTER(relax_plane))
+        # events
+        earr = (relax_event * max(1, len(self.events)))()
+        for e, ev in enumerate(self.events):
+            earr[e].time = ev.time
+            if ev.faults:
+                sarr = (relax_source * len(ev.faults))()
+                for k, f in enumerate(ev.faults):
+                    slip, x, y, z, strike, dip, rake = wang_convention(
+                        f.slip, f.x, f.y, f.z, f.length, f.width, f.strike, f.dip, f.rake,
+                        self.x0, self.y0, self.rot)
+                    sarr[k] = relax_source(slip=slip, x=x, y=y, z=z, width=f.width,
+                                           length=f.length, strike=strike, dip=dip, rake=rake,
+                                           period=0.0, phase=0.0,
+                                           beta=self.beta if f.beta is None else f.beta,
+                                           opening=0.0)
+                keep.append(sarr)
+                earr[e].ns = len(ev.faults)
+                earr[e].s = C.cast(sarr, C.POINTER(relax_source))
+        keep.append(earr)
+        cfg.ne = len(self.events)
+        cfg.events = C.cast(earr, C.POINTER(relax_event))
+        return cfg, keep
+
+    # field sizes in the reference layout
+    def vec_shape(self, full: bool = False):
+        return (3, self.sx3 if full else self.sx3h, self.sx2, self.sx1 + 2)
+
+    def tensor_shape(self):
+        return (self.sx3h, self.sx2, self.sx1)
+
+
+# ---------------------------------------------------------------------- #
+# synthetic workloads (seeded; shapes and distributions of the named
+# benchmark configurations)
+# ---------------------------------------------------------------------- #
+
+def linear_maxwell(sx: int = 128, sz: int = 128, dx: float = 0.8, steps: int = 20) -> Simulation:
+    """Plain FP32 linear Maxwell (n=1): vertical strike-slip fault L=40 W=15
+    centred, slip 1, uniform gammadot0 = 1 below 30 km, Dt = 0.5 exactly
+    (tm = 1/gammadot0, Dt = tm/10 * tscale with tscale = 5).  The FFT box is
+    sx*sx*sz; its physical half-space holds sz/2 layers."""
+    return Simulation(
+        sx1=sx, sx2=sx, sx3=sz, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0,
+        lambda_=1.0, mu=1.0, gam=0.0, interval=0.5 * steps, odt=-1, tscale=5.0,
+        linear=[(30.0, 1.0)],
+        events=[Event(0.0, [Fault(1.0, -20.0, 0.0, 0.0, 40.0, 15.0, 0.0, 90.0, 0.0)])],
+        name=f"linear-maxwell-{sx}x{sx}x{sz}")
+
+
+def powerlaw_thrust(sx: int = 256, sz: int = 128, dx: float = 0.5, steps: int = 200,
+                    afterslip: bool = True) -> Simulation:
+    """Power-law n=3 under a 20-degree thrust: eta(z) = 10^(1.5 - z/20) below
+    20 km entered as one nonlinear interface per dx3 layer, thrust L=80 W=40
+    slip 2 (normalised units), one rate-strengthening afterslip plane
+    down-dip of it (50 km x 20 km, i.e. 40 patches of 5 km when binned),
+    a-b = 1e-3 at a normalised effective normal stress of 100, i.e.
+    (a-b)sigma = 0.1.  Adaptive dt (skip mode, tscale 1)."""
+    depth = dx * sz / 2
+    nl = []
+    z = 20.0
+    while z < depth + 1e-9:
+        nl.append((z, 10.0 ** (z / 20.0 - 1.5), 3.0, 0.0))
+        z += dx
+    top = 1.0
+    bottom = top + 40.0 * math.sin(math.radians(20.0))
+    planes = []
+    fc = []
+    if afterslip:
+        planes = [Plane(x=-25.0, y=40.0 * math.cos(math.radians(20.0)), z=bottom, length=50.0,
+                        width=20.0, strike=0.0, dip=20.0, rake=90.0)]
+        fc = [(0.0, 1.0, 0.1, 0.0, 0.0)]
+    return Simulation(
+        sx1=sx, sx2=sx, sx3=sz, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0,
+        lambda_=1.0, mu=1.0, gam=0.0, interval=1.0e6, odt=-1, tscale=1.0,
+        nonlinear=nl, faultcreep=fc, planes=planes,
+        events=[Event(0.0, [Fault(2.0, -40.0, 0.0, top, 80.0, 40.0, 0.0, 20.0, 90.0)])],
+        name=f"powerlaw-thrust-{sx}x{sx}x{sz}")
+
+
+def random_faults(seed: int, sx: int = 512, sz: int = 256, dx: float = 0.4, nfaults: int = 3,
+                  lid: float = 25.0, n: float = 3.5, gam: float = 8.3e-4) -> Simulation:
+    """Large instance with gravity: faults drawn from `seed` (lengths U[20,100],
+    dip U[30,90], slip lognormal median 1 sigma 0.5, width L/2), power-law
+    n below an elastic lid."""
+    rng = np.random.default_rng(seed)
+    half = 0.3 * sx * dx
+    faults = []
+    for _ in range(nfaults):
+        L = float(rng.uniform(20, 100))
+        dip = float(rng.uniform(30, 90))
+        slip = float(np.exp(rng.normal(0.0, 0.5)))
+        faults.append(Fault(slip, float(rng.uniform(-half, half - L)),
+                            float(rng.uniform(-half, half)), float(rng.uniform(0, 5)), L, L / 2,
+                            float(rng.uniform(0, 360)), dip, float(rng.uniform(-180, 180))))
+    return Simulation(
+        sx1=sx, sx2=sx, sx3=sz, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0, lambda_=1.0,
+        mu=1.0, gam=gam, interval=1.0e6, odt=-1, tscale=1.0,
+        nonlinear=[(lid, 1.0, n, 0.0)], events=[Event(0.0, faults)],
+        name=f"random-faults-{sx}x{sx}x{sz}-seed{seed}")
+
+
+def reference_output2() -> Simulation:
+    """The input echoed in examples/tutorials/output2.param:8-62 (power-law
+    n=3 relaxation after a strike-slip fault, 256^3)."""
+    return Simulation(
+        sx1=256, sx2=256, sx3=256, dx1=0.05, dx2=0.05, dx3=0.05, beta=0.2, nyquist=2.0,
+        lambda_=1.0, mu=1.0, gam=8.33e-4, interval=100.0, odt=-1, tscale=0.5,
+        nonlinear=[(2.0, 5e3, 3.0, 0.0), (8.0, 5e3, 3.0, 0.0)],
+        events=[Event(0.0, [Fault(1.0, -1.0, 0.0, 0.0, 2.0, 1.0, 0.0, 90.0, 0.0)])],
+        name="reference-output2")
+
+
+def reference_output3() -> Simulation:
+    """The input echoed in examples/tutorials/output3.param:8-69 (afterslip
+    on a vertical plane below a strike-slip fault, 256^3)."""
+    return Simulation(
+        sx1=256, sx2=256, sx3=256, dx1=0.05, dx2=0.05, dx3=0.05, beta=0.2, nyquist=1.0,
+        lambda_=1.0, mu=1.0, gam=8.33e-4, interval=0.5, odt=-1, tscale=1e-2,
+        faultcreep=[(1.0, 1e3, 1e3, 0.0, 0.0)],
+        planes=[Plane(-2.0, 0.0, 1.0, 4.0, 2.0, 0.0, 90.0, 0.0)],
+        events=[Event(0.0, [Fault(1.0, -0.5, 0.0, 0.0, 1.0, 1.0, 0.0, 90.0, 0.0)])],
+        name="reference-output3")
+
+
+WORKLOADS = {
+    "linear-maxwell": linear_maxwell,
+    "powerlaw-thrust": powerlaw_thrust,
+    "random-faults": random_faults,
+}
