@@ -1,0 +1,366 @@
+"""Benchmark of the RELAX relaxation step on B200.
+
+Workload: power-law (n = 3) relaxation under a 20-degree thrust with one
+rate-strengthening afterslip plane, FFT box 256 x 256 x 128 (dx = 0.5 km),
+adaptive time step -- synthetic, seeded input of the named configuration
+(relax_b200.config.powerlaw_thrust).  A "step" is one RK2
+predictor/corrector step of RELAX's time loop (src/relax.f90:555-890).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  value = grid points x steps / s over all ranks
+(replicas: every rank advances its own instance; no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt*RK2-steps/s"
+UNIT = "grid-pt*steps/s"
+
+
+def workload():
+    from relax_b200.config import powerlaw_thrust
+    return powerlaw_thrust(sx=256, sz=128, dx=0.5)
+
+
+def config_desc(sim):
+    return {
+        "workload": f"power-law n=3 thrust + afterslip plane, box {sim.sx1}x{sim.sx2}x{sim.sx3}, "
+                    f"dx={sim.dx1} km, adaptive dt",
+        "grid": [sim.sx1, sim.sx2, sim.sx3],
+        "grid_points": sim.npoints,
+        "afterslip_planes": len(sim.planes),
+        "l2": "inputs larger than L2: ~0.7 GB device working set per step (126 MB L2)",
+        "parallelism": "replicas",
+    }
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                except ValueError:
+                    continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, r in rows for k in range(4) if r[k].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(rows), "reasons": reasons}
+
+
+# --------------------------------------------------------------------------
+# algorithmic bytes per launch of each kernel (FP32 fields)
+# --------------------------------------------------------------------------
+def kernel_bytes(sim):
+    sx1, sx2, sx3 = sim.sx1, sim.sx2, sim.sx3
+    h = sx3 // 2
+    nh = sx1 * sx2 * h
+    K1 = sx1 // 2 + 1
+    spec_plane = 3 * sx2 * K1 * 8          # one x3-plane of the 3-component spectrum
+    sig = 24 if sim.planes else 0
+    return {
+        # tau, m, u in; tau, m (+ sig with afterslip planes) out
+        "k_stress<END>": nh * (24 + 24 + 12 + 24 + 24 + sig),
+        # m, tau, v, gamma in; m, gamma (+ sig) out
+        "k_stress<CORR>": nh * (24 + 24 + 12 + 4 + 24 + 4 + sig),
+        # moment in, spectrum (body planes + traction plane) out
+        "k_xfwd": nh * 24 + (h + 1) * spec_plane,
+        "k_ypass<fwd>": 2 * (h + 1) * spec_plane,
+        # body planes + traction plane in, body planes out
+        "k_zspec": (h + 1) * spec_plane + h * spec_plane,
+        "k_ypass<inv>": 2 * h * spec_plane,
+        # spectrum + base field in, field out
+        "k_xinv": h * spec_plane + nh * 12 + nh * 12,
+    }
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles():
+    """dram read+write bytes per launch of the dominant kernel, from the
+    committed ncu summary (scaled to the benchmark grid), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+# --------------------------------------------------------------------------
+# the CPU oracle (reported baseline, reference arm)
+# --------------------------------------------------------------------------
+def cpu_sample(sim, nsteps: int):
+    """Times RK2 steps 2..nsteps of the oracle (FP32 restatement of the
+    reference CPU path) on the host cores; returns (rate, cores, seconds)."""
+    import ctypes as C
+    from oracle.oracle import Oracle
+    from relax_b200.config import relax_step_log
+    o = Oracle(32)
+    cfg, keep = sim.to_c(o.structure_fn)
+    st = o.lib.orc_state_create(C.byref(cfg))
+    lg = relax_step_log()
+    try:
+        o.lib.orc_coseismic(st, C.byref(lg))
+        o.lib.orc_step(st, None, C.byref(lg))          # step 1 untimed
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            rc = o.lib.orc_step(st, None, C.byref(lg))
+            assert rc == 0
+        dt = time.perf_counter() - t0
+    finally:
+        o.lib.orc_state_free(st)
+    return sim.npoints * nsteps / dt, o.threads(), dt
+
+
+def run_reference(args, rank, world):
+    sim = workload()
+    if rank != 0:
+        return 0
+    # each reference step is one full oracle RK2 step of the workload; the
+    # run is bounded to a few minutes of host time
+    t0 = time.perf_counter()
+    rate1, cores, dt1 = cpu_sample(sim, 1)
+    per_step = dt1
+    budget = 150.0
+    k = max(1, min(args.steps, int(budget / max(per_step, 1e-3)) - 1))
+    rate, cores, dt = cpu_sample(sim, k)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+        "steps": k, "warmup": 1, "ms_per_step": 1e3 * dt / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_desc(sim),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{k} RK2 steps of the full {sim.sx1}x{sim.sx2}x{sim.sx3} "
+                                   "workload after the coseismic solve and one untimed step "
+                                   "(the reference cannot be compiled here; the oracle restates "
+                                   "its CPU path)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.perf_counter() - t0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# the B200 arm
+# --------------------------------------------------------------------------
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    from relax_b200.api import Relax
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    sim = workload()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    r = Relax(sim, device=local_rank)
+    r.coseismic()
+    for _ in range(args.warmup):
+        r.step()
+    sptr = r.lib.relax_get_stream
+    import ctypes as C
+    s = C.c_void_p()
+    sptr(r.h, C.byref(s))
+    stream = torch.cuda.ExternalStream(s.value)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
+    clk = ClockSampler(local_rank)
+    clk.start()
+    time.sleep(0.3)
+    barrier()
+    n0 = r.launch_count()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        lg = r.step()
+        if lg[0] == 0:
+            raise RuntimeError("simulation ended inside the timed region")
+    ev1.record(stream)
+    barrier()
+    launches = r.launch_count() - n0
+    ms = ev0.elapsed_time(ev1)
+    clocks = clk.stop()
+    ms = allmax(ms)
+    ms_step = ms / args.steps
+    value = world * sim.npoints * args.steps / (ms / 1e3)
+
+    # per-kernel durations (CUDA events around each launch, separate pass)
+    r.profile(True)
+    nprof = max(3, min(args.steps, 10))
+    for _ in range(nprof):
+        r.step()
+    prof = r.profile_read()
+    r.profile(False)
+    algo = kernel_bytes(sim)
+    kernels = {}
+    for name, (tot, n) in prof.items():
+        d = {"ms_total": tot, "launches": n, "ms_per_launch": tot / n}
+        if name in algo:
+            d["alg_bytes"] = algo[name]
+            d["gbs"] = algo[name] / (tot / n / 1e3) / 1e9
+        kernels[name] = d
+    step_ms_prof = sum(v[0] for v in prof.values()) / nprof
+    dom = max((k for k in kernels if k in algo), key=lambda k: kernels[k]["ms_total"])
+    peak, peak_kind = peaks()
+    ach = kernels[dom]["gbs"]
+    traffic = traffic_from_profiles().get(dom)
+    r.close()
+
+    # end to end through the public API with host buffers: create (H2D of the
+    # deck, structures and prestress), coseismic solve, K steps each reading
+    # back its log record, D2H of the displacement and stress fields
+    barrier()
+    t0 = time.perf_counter()
+    r2 = Relax(sim, device=local_rank)
+    r2.coseismic()
+    for _ in range(args.steps):
+        r2.step()
+    u = r2.field("u")
+    tau = r2.field("tau")
+    r2.close()
+    torch.cuda.synchronize()
+    e2e_s = allmax(time.perf_counter() - t0)
+    nz = sim.sx3h
+    h2d = (6 * 4 * sim.sx1 * sim.sx2 * nz + 64 * 6 * nz * 3) / args.steps
+    d2h = 120 + (u.nbytes + tau.nbytes) / args.steps
+    e2e = {"value": world * sim.npoints * args.steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+           "timing": "host wall clock around create + coseismic + K steps + field readback"}
+
+    if rank != 0:
+        return 0
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        rate, cores, dt = cpu_sample(sim, 2)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "2 RK2 steps of the same workload on the host cores (after the "
+                         "coseismic solve and one untimed step), FP32 oracle restating the "
+                         "reference CPU path"}
+    b_alg = 536.0 * sim.npoints
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_desc(sim),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak,
+                     "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                     "traffic": traffic},
+        "step_roofline": {"alg_bytes_per_step": b_alg,
+                          "achieved_gbs": b_alg / (ms_step / 1e3) / 1e9,
+                          "frac": b_alg / (ms_step / 1e3) / 1e9 / peak,
+                          "note": "536 B per grid point per RK2 step of the reference data flow; "
+                                  "the fused kernels move less than that"},
+        "kernels": kernels,
+        "kernel_ms_per_step": step_ms_prof,
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            rc = run_reference(args, rank, world)
+        else:
+            rc = run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

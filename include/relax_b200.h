@@ -41,7 +41,7 @@ extern "C" {
 #define RELAX_ERR_FRICTION     6   /* tau/((a-b)sigma) > 20, the abort of
                                       src/friction3d.f90:204-215         */
 #define RELAX_ERR_POWER        7   /* stress exponent < 0.999999, the abort
-                                      of src/viscoelastic3d.f90:271-276   */
+                                      of src/viscoelastic3d.f90:262-267   */
 
 /* ------------------------------------------------------------------ */
 /* data types (binary compatible with the reference)                   */
@@ -200,8 +200,18 @@ int relax_get_patches(relax_ctx *ctx, int k, relax_slippatch *host, size_t n);
 /* Current time, step counter, event index. */
 int relax_get_time(relax_ctx *ctx, double *t, int *i, int *e);
 
-/* Per-stage device timing of the last step (ms), for profiling. */
+/* Waits for the context's stream. */
 int relax_synchronize(relax_ctx *ctx);
+
+/* Per-stage device timing: while enabled, every kernel the context launches
+ * is bracketed by CUDA events on its stream; relax_profile_read sums the
+ * durations of one stage (name: the kernel).  Enabling clears the record.
+ * relax_launch_count counts this context's kernel launches (always on). */
+int relax_profile(relax_ctx *ctx, int enable);
+int relax_profile_stages(void);
+int relax_profile_read(relax_ctx *ctx, int stage, double *total_ms,
+                       int *launches, const char **name);
+int relax_launch_count(relax_ctx *ctx, long long *n);
 
 /* ------------------------------------------------------------------ */
 /* stateless operators on device buffers (reference layout)           */
@@ -290,7 +300,7 @@ void cuinit_(int sx1, int sx2, int sx3, double dx1, double dx2, double dx3,
 void cudeinit_(void);
 /* src/cuelastic.cu:1493 -- v = 0, t = 0 */
 void curesetvectors_(void);
-/* src/cuelastic.cu:1596 -- 1: tau, 2: moment, 3: sig <- 0 */
+/* src/cuelastic.cu:1596 -- E_TENSOR_TYPE 1: sig, 2: moment, 3: tau <- 0 */
 void cutensormemset_(int eType);
 /* src/cuelastic.cu:1572 -- dir 0: device->host, 1: host->device */
 void copytau_(ST_TENSOR_C *host, int sx1, int sx2, int sx3h, int dir);

@@ -323,7 +323,7 @@ static int optimalfilter(int sx1, int sx2, int sx3, double *k1, double *k2, doub
 int orc_stressupdate(const real *v1, const real *v2, const real *v3, double lambda, double mu,
                      double dx1, double dx2, double dx3, int sx1, int sx2, int sx3, otensor *sig)
 {
-    double ker1[16], ker2[16], ker3[16];
+    double ker1[16] = {0}, ker2[16] = {0}, ker3[16] = {0};
     int len1, len2, len3;
     if (optimalfilter(sx1, sx2, sx3, ker1, ker2, ker3, &len1, &len2, &len3)) return ORC_ERR_ARG;
     for (int l = 0; l < len1; l++) ker1[l] /= dx1;
@@ -392,7 +392,7 @@ int orc_equivalentbodyforce(const otensor *sig, double dx1, double dx2, double d
                             int sx2, int sx3, real *c1, real *c2, real *c3, real *t1, real *t2,
                             real *t3)
 {
-    double ker1[16], ker2[16], ker3[16];
+    double ker1[16] = {0}, ker2[16] = {0}, ker3[16] = {0};
     int len1, len2, len3;
     if (optimalfilter(sx1, sx2, sx3, ker1, ker2, ker3, &len1, &len2, &len3)) return ORC_ERR_ARG;
     for (int l = 0; l < len1; l++) ker1[l] /= dx1;

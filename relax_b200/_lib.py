@@ -1,0 +1,106 @@
+"""ctypes binding of librelax_b200.so (the C ABI of include/relax_b200.h).
+
+The library is built in-tree by ``relax_b200/csrc/Makefile`` (nvcc, sm_100a).
+There is no fallback: if the library is missing, ``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+
+from .config import (relax_config, relax_layer, relax_slippatch, relax_step_log, relax_tensor,
+                     relax_tensor_layer)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "librelax_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "relax_b200.h")
+
+_lib = None
+
+
+class RelaxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"relax error {code}: {msg}")
+        self.code = code
+
+
+def build(verbose: bool = False):
+    """Compiles the CUDA library for sm_100a (cross-compiles without a GPU)."""
+    out = subprocess.run(["make", "-s", "-C", os.path.join(HERE, "csrc")], capture_output=not verbose,
+                         text=True)
+    if out.returncode != 0:
+        raise RuntimeError("building librelax_b200.so failed:\n" + (out.stderr or "") + (out.stdout or ""))
+
+
+def header_functions():
+    """Names of the functions include/relax_b200.h declares."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z_0-9]*\s*\**\s*([A-Za-z_][A-Za-z_0-9]*)\s*\(",
+                       text, flags=re.M)
+    return sorted(set(n for n in names if n not in ("if", "while", "for")))
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise RuntimeError(f"{LIBPATH} is missing: build it with relax_b200._lib.build() "
+                           "(the CUDA path has no fallback)")
+    lib = C.CDLL(LIBPATH)
+    P, I, D, S = C.c_void_p, C.c_int, C.c_double, C.c_size_t
+    FP = C.POINTER(C.c_float)
+    sig = {
+        "relax_version": (C.c_char_p, []),
+        "relax_last_error": (C.c_char_p, []),
+        "relax_viscoelastic_structure": (I, [P, I, D, I, P]),
+        "relax_tensor_structure": (I, [P, I, D, I, P]),
+        "relax_create": (I, [C.POINTER(relax_config), I, C.POINTER(P)]),
+        "relax_destroy": (I, [P]),
+        "relax_get_stream": (I, [P, C.POINTER(P)]),
+        "relax_coseismic": (I, [P, I, C.POINTER(relax_step_log)]),
+        "relax_step": (I, [P, C.POINTER(D), C.POINTER(relax_step_log)]),
+        "relax_run": (I, [P, I, C.POINTER(D), C.POINTER(relax_step_log), C.POINTER(I)]),
+        "relax_get_field": (I, [P, I, P, S]),
+        "relax_set_field": (I, [P, I, P, S]),
+        "relax_get_patches": (I, [P, I, C.POINTER(relax_slippatch), S]),
+        "relax_get_time": (I, [P, C.POINTER(D), C.POINTER(I), C.POINTER(I)]),
+        "relax_synchronize": (I, [P]),
+        "relax_profile": (I, [P, I]),
+        "relax_profile_stages": (I, []),
+        "relax_profile_read": (I, [P, I, C.POINTER(D), C.POINTER(I), C.POINTER(C.c_char_p)]),
+        "relax_launch_count": (I, [P, C.POINTER(C.c_longlong)]),
+        "relax_op_stressupdate": (I, [P, P, P, D, D, D, D, D, I, I, I, P, P]),
+        "relax_op_bodyforce": (I, [P, D, D, D, I, I, I, P, P, P, P, P, P, P]),
+        "relax_op_viscouseigenstress": (I, [D, P, P, P, I, I, I, P, C.POINTER(D), P, P, P]),
+        "relax_op_frictioneigenstress": (I, [D, D, D, D, D, D, D, D, D, P, D, P, I, I, I, D, D, D, P,
+                                             C.POINTER(D), P]),
+        "relax_op_green": (I, [P, P, P, P, P, P, I, I, I, D, D, D, D, D, D, P]),
+        "relax_op_fft3": (I, [P, I, I, I, D, D, D, I, P]),
+        "relax_op_tensoramplitude": (I, [P, I, I, I, D, D, D, C.POINTER(D), P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int):
+    if rc != 0:
+        msg = load().relax_last_error().decode(errors="replace")
+        raise RelaxError(rc, msg)
+
+
+def structure_fn(layers, dx3: float, nz: int):
+    """viscoelasticstructure through the library (host-side helper)."""
+    lib = load()
+    arr_in = (relax_layer * len(layers))(*layers)
+    out = (relax_layer * nz)()
+    check(lib.relax_viscoelastic_structure(C.cast(arr_in, C.c_void_p), len(layers), dx3, nz,
+                                           C.cast(out, C.c_void_p)))
+    return out

@@ -1,0 +1,128 @@
+"""Python mirror of the context API: one RELAX instance on one GPU.
+
+    sim = relax_b200.config.powerlaw_thrust()
+    with Relax(sim) as r:
+        log0 = r.coseismic()
+        for _ in range(10):
+            log = r.step()
+        u = r.field("u")
+
+Every call goes through ``librelax_b200.so``; host arrays use RELAX's layout
+(padded vectors (3, sx3/2, sx2, sx1+2), TENSOR structs (sx3/2, sx2, sx1)).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .config import TENSOR_DTYPE, Simulation, relax_slippatch, relax_step_log
+
+FIELDS = {"u": 1, "sig": 2, "tau": 3, "moment": 4, "gamma": 5}
+
+
+class Relax:
+    def __init__(self, sim: Simulation, device: int = 0):
+        self.lib = _lib.load()
+        self.sim = sim
+        self.cfg, self._keep = sim.to_c(_lib.structure_fn)
+        h = C.c_void_p()
+        _lib.check(self.lib.relax_create(C.byref(self.cfg), device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.relax_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- time loop ---------------------------------------------------------
+    def coseismic(self, e: int = 0) -> tuple:
+        lg = relax_step_log()
+        _lib.check(self.lib.relax_coseismic(self.h, e, C.byref(lg)))
+        return lg.as_tuple()
+
+    def step(self, dt: Optional[float] = None) -> tuple:
+        lg = relax_step_log()
+        dtp = C.byref(C.c_double(dt)) if dt is not None else None
+        _lib.check(self.lib.relax_step(self.h, dtp, C.byref(lg)))
+        return lg.as_tuple()
+
+    def run(self, nsteps: int, dt_schedule: Optional[Sequence[float]] = None) -> List[tuple]:
+        logs = (relax_step_log * (nsteps + 1))()
+        n = C.c_int(0)
+        sched = None
+        if dt_schedule is not None:
+            arr = (C.c_double * nsteps)(*dt_schedule[:nsteps])
+            sched = C.cast(arr, C.POINTER(C.c_double))
+        _lib.check(self.lib.relax_run(self.h, nsteps, sched, logs, C.byref(n)))
+        return [logs[k].as_tuple() for k in range(n.value + 1)]
+
+    def synchronize(self):
+        _lib.check(self.lib.relax_synchronize(self.h))
+
+    # -- profiling -----------------------------------------------------------
+    def profile(self, enable: bool):
+        _lib.check(self.lib.relax_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        """{kernel name: (total ms, launches)} of the recorded stages."""
+        out = {}
+        for s in range(self.lib.relax_profile_stages()):
+            ms = C.c_double()
+            n = C.c_int()
+            name = C.c_char_p()
+            _lib.check(self.lib.relax_profile_read(self.h, s, C.byref(ms), C.byref(n), C.byref(name)))
+            if n.value:
+                out[name.value.decode()] = (ms.value, n.value)
+        return out
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        _lib.check(self.lib.relax_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    # -- fields --------------------------------------------------------------
+    def field(self, name: str) -> np.ndarray:
+        s = self.sim
+        if name == "u":
+            a = np.zeros(s.vec_shape(), np.float32)
+        elif name == "gamma":
+            a = np.zeros(s.vec_shape()[1:], np.float32)
+        else:
+            a = np.zeros(s.tensor_shape(), TENSOR_DTYPE)
+        _lib.check(self.lib.relax_get_field(self.h, FIELDS[name], a.ctypes.data_as(C.c_void_p),
+                                            a.nbytes))
+        return a
+
+    def set_field(self, name: str, a: np.ndarray):
+        a = np.ascontiguousarray(a)
+        _lib.check(self.lib.relax_set_field(self.h, FIELDS[name], a.ctypes.data_as(C.c_void_p),
+                                            a.nbytes))
+
+    def patches(self, k: int):
+        p = self.cfg.planes[k]
+        n = p.px2 * p.px3
+        arr = (relax_slippatch * n)()
+        _lib.check(self.lib.relax_get_patches(self.h, k, arr, n))
+        return arr
+
+    def time(self):
+        t = C.c_double()
+        i = C.c_int()
+        e = C.c_int()
+        _lib.check(self.lib.relax_get_time(self.h, C.byref(t), C.byref(i), C.byref(e)))
+        return t.value, i.value, e.value

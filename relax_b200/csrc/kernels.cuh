@@ -1,0 +1,1177 @@
+// kernels.cuh -- sm_100a kernels of RELAX's relaxation step.
+//
+// Field layout on the device: structure of arrays, i1 fastest, physical
+// half-space only (sx3h layers); a tensor field is 6 planes
+// {s11,s12,s13,s22,s23,s33} of nh floats, a vector field 3 planes.
+#pragma once
+
+#include "common.cuh"
+
+namespace relax {
+// kernels and their argument types have internal linkage: each translation
+// unit that launches them carries its own copy
+namespace {
+
+// ------------------------------------------------------------------------
+// small helpers
+// ------------------------------------------------------------------------
+__device__ __forceinline__ float warp_min(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide min / sum in a fixed order (deterministic).  All threads of
+// the block must call; the result is valid in thread 0.
+__device__ __forceinline__ float block_min(float v, float *sh)
+{
+    v = warp_min(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = l < nw ? sh[l] : 3.0e38f;
+        v = warp_min(v);
+    }
+    return v;
+}
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = l < nw ? sh[l] : 0.0;
+        v = warp_sum(v);
+    }
+    return v;
+}
+
+// tensornorm, src/elastic3d.f90:311-319
+__device__ __forceinline__ float tnorm6(float a, float b, float c, float d, float e, float f)
+{
+    return sqrtf((a * a + 2.f * b * b + 2.f * c * c + d * d + 2.f * e * e + f * f) * 0.5f);
+}
+
+__device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ float4 ldc4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ float geti(const float4 &v, int j) { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
+
+// ------------------------------------------------------------------------
+// Fused stress / eigenstress kernel.
+//
+//   MODE_OP   sig += C:E(w)                                (stressupdate)
+//   MODE_INIT sig = -tau + C:E(w);         m = eigen(sig)  (coseismic end)
+//   MODE_END  tau += Dt m; sig = -tau + C:E(w); m = eigen(sig)
+//             (corrector tail + stressupdate + next predictor eigenstress,
+//              src/relax.f90:836,888-890 then :569-600)
+//   MODE_CORR sig = -Dt/2 m - tau + C:E(w); m = eigen(sig); gamma += Dt gd
+//             (src/relax.f90:696-738)
+//   MODE_EIGEN m += eigen(sig), gamma = gd tauc/mu where active
+//             (viscouseigenstress as called, for the operator API)
+// C:E is Hooke's law on the FIR/finite-difference strain of
+// src/elastic3d.f90:956-1180 (central differences for sx >= 15, one-sided
+// at the top and bottom layers); eigen is viscouseigenstress,
+// src/viscoelastic3d.f90:217-314, for the linear and the power-law
+// mechanisms.  Per-block Maxwell-time minima and tensor-amplitude sums
+// (src/elastic3d.f90:446-466) go to partial arrays reduced in a fixed order.
+// Each thread handles 4 consecutive points along x1 (float4 I/O).
+// ------------------------------------------------------------------------
+enum { MODE_OP = 0, MODE_INIT = 1, MODE_END = 2, MODE_CORR = 3, MODE_EIGEN = 4 };
+
+struct StressArgs {
+    Grid g;
+    const float *w;          // strain source (3 x nh)
+    float *tau;              // 6 x nh
+    float *m;                // 6 x nh
+    float *sig;              // 6 x nh (MODE_OP: in/out)
+    float *gamma;            // nh (MODE_CORR)
+    const float *dg0[2];     // weak-zone fluidity perturbations or null
+    const DepthVisc *visc[2];// per-depth rheology (null = mechanism absent)
+    const float *spdev;      // 6 x sx3h deviatoric prestress (or null)
+    const StepState *st;
+    float k1, k2, k3, k3b;   // 0.5/dx1, 0.5/dx2, 0.5/dx3, 1/dx3
+    float lam, mu2, muinv;   // lambda, 2 mu, 1/mu
+    int store_sig;
+    float *tm_part;          // [2][gridDim.x]
+    double *amp_part;        // [2][gridDim.x] (power, cei)
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_stress(StressArgs a)
+{
+    __shared__ float shf[32];
+    __shared__ double shd[32];
+    const Grid &g = a.g;
+    const int q4 = g.sx1 >> 2;
+    const size_t nq = g.nh >> 2;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = q < nq;
+    float tmin[2] = {3.0e38f, 3.0e38f};
+    double amp_m = 0.0, amp_t = 0.0;
+
+    if (live) {
+        const int i1 = (int)(q % q4) * 4;
+        const size_t r = q / q4;
+        const int i2 = (int)(r % g.sx2), i3 = (int)(r / g.sx2);
+        const size_t nh = g.nh;
+        const size_t row = ((size_t)i3 * g.sx2 + i2) * g.sx1;
+        const size_t idx = row + i1;
+        const int i1m = (i1 + g.sx1 - 1) % g.sx1, i1p = (i1 + 4) % g.sx1;
+        const size_t rym = ((size_t)i3 * g.sx2 + (i2 + g.sx2 - 1) % g.sx2) * g.sx1 + i1;
+        const size_t ryp = ((size_t)i3 * g.sx2 + (i2 + 1) % g.sx2) * g.sx1 + i1;
+        size_t rzm, rzp;
+        float kz;
+        if (i3 == 0) { rzm = idx; rzp = idx + g.plane; kz = a.k3b; }
+        else if (i3 == g.sx3h - 1) { rzm = idx - g.plane; rzp = idx; kz = a.k3b; }
+        else { rzm = idx - g.plane; rzp = idx + g.plane; kz = a.k3; }
+
+        // strain derivatives d_x, d_y, d_z of w1, w2, w3 at 4 points
+        float dxw[3][4], dyw[3][4], dzw[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (MODE == MODE_EIGEN) break;
+            const float *wc = a.w + c * nh;
+            const float4 cv = ld4(wc + idx);
+            const float lft = __ldg(wc + row + i1m), rgt = __ldg(wc + row + i1p);
+            dxw[c][0] = (cv.y - lft) * a.k1;
+            dxw[c][1] = (cv.z - cv.x) * a.k1;
+            dxw[c][2] = (cv.w - cv.y) * a.k1;
+            dxw[c][3] = (rgt - cv.z) * a.k1;
+            const float4 ym = ld4(wc + rym), yp = ld4(wc + ryp);
+            dyw[c][0] = (yp.x - ym.x) * a.k2;
+            dyw[c][1] = (yp.y - ym.y) * a.k2;
+            dyw[c][2] = (yp.z - ym.z) * a.k2;
+            dyw[c][3] = (yp.w - ym.w) * a.k2;
+            const float4 zm = ld4(wc + rzm), zp = ld4(wc + rzp);
+            dzw[c][0] = (zp.x - zm.x) * kz;
+            dzw[c][1] = (zp.y - zm.y) * kz;
+            dzw[c][2] = (zp.z - zm.z) * kz;
+            dzw[c][3] = (zp.w - zm.w) * kz;
+        }
+
+        // base stress
+        float s[6][4];
+        if (MODE == MODE_OP || MODE == MODE_EIGEN) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const float4 v = ldc4(a.sig + c * nh + idx);
+                s[c][0] = v.x; s[c][1] = v.y; s[c][2] = v.z; s[c][3] = v.w;
+            }
+        } else if (MODE == MODE_INIT) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const float4 t = ldc4(a.tau + c * nh + idx);
+                s[c][0] = -t.x; s[c][1] = -t.y; s[c][2] = -t.z; s[c][3] = -t.w;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                amp_t += (double)tnorm6(-s[0][j], -s[1][j], -s[2][j], -s[3][j], -s[4][j], -s[5][j]);
+        } else if (MODE == MODE_END) {
+            const float dt = (float)a.st->Dt;
+            float tn[6][4], mm[6][4];
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const float4 t = ldc4(a.tau + c * nh + idx);
+                const float4 m = ldc4(a.m + c * nh + idx);
+                mm[c][0] = m.x; mm[c][1] = m.y; mm[c][2] = m.z; mm[c][3] = m.w;
+                tn[c][0] = t.x + dt * m.x; tn[c][1] = t.y + dt * m.y;
+                tn[c][2] = t.z + dt * m.z; tn[c][3] = t.w + dt * m.w;
+                st4(a.tau + c * nh + idx, make_float4(tn[c][0], tn[c][1], tn[c][2], tn[c][3]));
+#pragma unroll
+                for (int j = 0; j < 4; j++) s[c][j] = -tn[c][j];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                amp_m += (double)tnorm6(mm[0][j], mm[1][j], mm[2][j], mm[3][j], mm[4][j], mm[5][j]);
+                amp_t += (double)tnorm6(tn[0][j], tn[1][j], tn[2][j], tn[3][j], tn[4][j], tn[5][j]);
+            }
+        } else {  // MODE_CORR
+            const float c1 = -(float)(a.st->Dt / 2);
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const float4 t = ldc4(a.tau + c * nh + idx);
+                const float4 m = ldc4(a.m + c * nh + idx);
+                s[c][0] = c1 * m.x - t.x; s[c][1] = c1 * m.y - t.y;
+                s[c][2] = c1 * m.z - t.z; s[c][3] = c1 * m.w - t.w;
+            }
+        }
+
+        // Hooke's law on the strain, src/elastic3d.f90:129-142
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (MODE == MODE_EIGEN) break;
+            const float e11 = dxw[0][j];
+            const float e12 = (dxw[1][j] + dyw[0][j]) * 0.5f;
+            const float e13 = (dxw[2][j] + dzw[0][j]) * 0.5f;
+            const float e22 = dyw[1][j];
+            const float e23 = (dyw[2][j] + dzw[1][j]) * 0.5f;
+            const float e33 = dzw[2][j];
+            const float tr = e11 + e22 + e33;
+            s[0][j] += a.mu2 * e11 + a.lam * tr;
+            s[1][j] += a.mu2 * e12;
+            s[2][j] += a.mu2 * e13;
+            s[3][j] += a.mu2 * e22 + a.lam * tr;
+            s[4][j] += a.mu2 * e23;
+            s[5][j] += a.mu2 * e33 + a.lam * tr;
+        }
+        if (MODE == MODE_OP || (MODE != MODE_EIGEN && a.store_sig)) {
+#pragma unroll
+            for (int c = 0; c < 6; c++)
+                st4(a.sig + c * nh + idx, make_float4(s[c][0], s[c][1], s[c][2], s[c][3]));
+        }
+
+        if (MODE != MODE_OP) {
+            // viscouseigenstress for the linear and power-law mechanisms
+            float mo[6][4];
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (MODE == MODE_EIGEN) v = ldc4(a.m + c * nh + idx);
+                mo[c][0] = v.x; mo[c][1] = v.y; mo[c][2] = v.z; mo[c][3] = v.w;
+            }
+            float sp[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (a.spdev) {
+#pragma unroll
+                for (int c = 0; c < 6; c++) sp[c] = __ldg(a.spdev + c * g.sx3h + i3);
+            }
+            float gsum[4] = {0.f, 0.f, 0.f, 0.f};
+            const float dtf = MODE == MODE_CORR ? (float)a.st->Dt : 0.f;
+            float4 gold = make_float4(0.f, 0.f, 0.f, 0.f);
+            if ((MODE == MODE_CORR || MODE == MODE_EIGEN) && a.gamma) gold = ldc4(a.gamma + idx);
+            float gacc[4] = {gold.x, gold.y, gold.z, gold.w};
+#pragma unroll
+            for (int mech = 0; mech < 2; mech++) {
+                if (!a.visc[mech]) continue;
+                const DepthVisc dv = a.visc[mech][i3];
+                float g0v[4] = {dv.g0, dv.g0, dv.g0, dv.g0};
+                if (a.dg0[mech]) {
+                    const float4 d = ld4(a.dg0[mech] + idx);
+                    g0v[0] += d.x; g0v[1] += d.y; g0v[2] += d.z; g0v[3] += d.w;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    gsum[j] = 0.f;
+                    if (!(g0v[j] >= 1.0e-20f)) continue;
+                    const float tr3 = (s[0][j] + s[3][j] + s[5][j]) * (1.f / 3.f);
+                    const float d11 = s[0][j] - tr3, d22 = s[3][j] - tr3, d33 = s[5][j] - tr3;
+                    const float tau = tnorm6(d11 + sp[0], s[1][j] + sp[1], s[2][j] + sp[2],
+                                             d22 + sp[3], s[4][j] + sp[4], d33 + sp[5]);
+                    const float tauc = fmaxf(0.f, tau - dv.cohesion);
+                    if (!(tauc > 1.0e-20f)) continue;
+                    const float x = tauc * a.muinv;
+                    const float pe = dv.power - 1.f;
+                    float gd;
+                    if (pe == 0.f) gd = g0v[j];
+                    else if (pe == 1.f) gd = g0v[j] * x;
+                    else if (pe == 2.f) gd = g0v[j] * x * x;
+                    else gd = g0v[j] * powf(x, pe);
+                    const float gd2 = 2.f * gd, gp2 = 2.f * g0v[j] * dv.tpow;
+                    mo[0][j] += gd2 * d11 - gp2 * sp[0];
+                    mo[1][j] += gd2 * s[1][j] - gp2 * sp[1];
+                    mo[2][j] += gd2 * s[2][j] - gp2 * sp[2];
+                    mo[3][j] += gd2 * d22 - gp2 * sp[3];
+                    mo[4][j] += gd2 * s[4][j] - gp2 * sp[4];
+                    mo[5][j] += gd2 * d33 - gp2 * sp[5];
+                    tmin[mech] = fminf(tmin[mech], 1.f / gd);
+                    gsum[j] = gd * x;
+                    if (MODE == MODE_EIGEN) gacc[j] = gsum[j];
+                }
+                if (MODE == MODE_CORR) {
+#pragma unroll
+                    for (int j = 0; j < 4; j++) gacc[j] = gacc[j] + dtf * gsum[j];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 6; c++)
+                st4(a.m + c * nh + idx, make_float4(mo[c][0], mo[c][1], mo[c][2], mo[c][3]));
+            if ((MODE == MODE_CORR || MODE == MODE_EIGEN) && a.gamma)
+                st4(a.gamma + idx, make_float4(gacc[0], gacc[1], gacc[2], gacc[3]));
+        }
+    }
+
+    if (MODE == MODE_INIT || MODE == MODE_END || MODE == MODE_EIGEN) {
+        const float t0 = block_min(tmin[0], shf);
+        __syncthreads();
+        const float t1 = block_min(tmin[1], shf);
+        __syncthreads();
+        const double am = block_sum(amp_m, shd);
+        __syncthreads();
+        const double at = block_sum(amp_t, shd);
+        if (threadIdx.x == 0) {
+            a.tm_part[blockIdx.x] = t0;
+            a.tm_part[gridDim.x + blockIdx.x] = t1;
+            a.amp_part[blockIdx.x] = am;
+            a.amp_part[gridDim.x + blockIdx.x] = at;
+        }
+    }
+}
+
+// tau += Dt m with the amplitude of m (coseismic-event path of the step,
+// src/relax.f90:836 followed by :858-886)
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_tau_update(Grid g, float *tau, const float *m,
+                                                               const StepState *st, double *amp_part)
+{
+    __shared__ double shd[32];
+    const size_t nq = g.nh >> 2;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double am = 0.0;
+    if (q < nq) {
+        const float dt = (float)st->Dt;
+        float mm[6][4];
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            const float4 t = ldc4(tau + c * g.nh + 4 * q), v = ldc4(m + c * g.nh + 4 * q);
+            mm[c][0] = v.x; mm[c][1] = v.y; mm[c][2] = v.z; mm[c][3] = v.w;
+            st4(tau + c * g.nh + 4 * q, make_float4(t.x + dt * v.x, t.y + dt * v.y, t.z + dt * v.z, t.w + dt * v.w));
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) am += (double)tnorm6(mm[0][j], mm[1][j], mm[2][j], mm[3][j], mm[4][j], mm[5][j]);
+    }
+    am = block_sum(am, shd);
+    if (threadIdx.x == 0) amp_part[blockIdx.x] = am;
+}
+
+// ------------------------------------------------------------------------
+// frictioneigenstress, src/friction3d.f90:82-241, for one afterslip plane,
+// launched over the index box that bounds the plane's band.
+// ------------------------------------------------------------------------
+struct FrictionArgs {
+    Grid g;
+    double x, y, z, L, W, strike, dip, rake, beta, mu;
+    const double *fc;        // 4 x sx3h: V0, (a-b)sigma, friction, cohesion
+    const float *sig;        // 6 x nh
+    float *m;                // 6 x nh
+    int j1lo, n1, j2lo, n2, i3lo, n3;
+    int want_tm;
+    float *tm_part;          // one per block
+    int *err;
+};
+
+__device__ __forceinline__ double d_gauss(double x, double s)
+{
+    return exp(-0.5 * (x / s) * (x / s)) / sqrt(6.28318530717958623199592693708837032318) / s;
+}
+__device__ __forceinline__ double d_omega(double x, double beta)
+{
+    const double ax = fabs(x);
+    if (ax <= (1.0 - 2.0 * beta) / (1.0 - beta) / 2.0) return 1.0;
+    if (ax < 1.0 / (1.0 - beta) / 2.0) {
+        const double c = cos(3.141592653589793115997963468544185161 * ((1.0 - beta) * ax - 0.5 + beta) / 2.0 / beta);
+        return c * c;
+    }
+    return 0.0;
+}
+__device__ __forceinline__ double d_omegap(double x, double beta)
+{
+    const double ax = fabs(x);
+    if (ax > (1.0 - 2.0 * beta) / (1.0 - beta) / 2.0 && ax < 1.0 / (1.0 - beta) / 2.0)
+        return -copysign(1.0, x) * 3.141592653589793115997963468544185161 * (1.0 - beta) / 2.0 / beta *
+               sin(3.141592653589793115997963468544185161 * ((1.0 - beta) * ax - 0.5 + beta) / beta);
+    return 0.0;
+}
+__device__ __forceinline__ double d_gaussp(double x, double s)
+{
+    return -x * exp(-0.5 * (x / s) * (x / s)) / sqrt(6.28318530717958623199592693708837032318) / (s * s * s);
+}
+__device__ __forceinline__ double my_sinh(double x)
+{
+    return fabs(x) > 11.0 ? copysign(1.0, x) * sinh(11.0) : sinh(x);
+}
+
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_friction(FrictionArgs a)
+{
+    __shared__ float shf[32];
+    const Grid &g = a.g;
+    const size_t n = (size_t)a.n1 * a.n2 * a.n3;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float tm = 3.0e38f;
+    if (t < n) {
+        const int j1 = a.j1lo + (int)(t % a.n1);
+        const int j2 = a.j2lo + (int)((t / a.n1) % a.n2);
+        const int i3 = a.i3lo + (int)(t / ((size_t)a.n1 * a.n2));
+        const double dx1 = g.dx1, dx2 = g.dx2, dx3 = g.dx3;
+        const double x3 = (double)i3 * dx3;
+        const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+        const double mwp = Wp > Lp ? Wp : Lp;
+        // shifted coordinates: index j (may be negative) -> x = j dx
+        const double x1 = (double)j1 * dx1, x2 = (double)j2 * dx2;
+        bool ok = !(fabs(x3 - a.z) > Lp && fabs(x3 + a.z) > Lp);
+        ok = ok && !(fabs(x1 - a.x) > mwp || fabs(x2 - a.y) > mwp);
+        const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+        const double cr = cos(a.rake), sr = sin(a.rake);
+        const double x2r0 = cs * a.x - ss * a.y;
+        const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+        double x2r = cs * x1 - ss * x2;
+        const double x1s = cd * x2r - sd * x3, x1i = cd * x2r + sd * x3;
+        ok = ok && !(fabs(x1s - xr) > 7.01 * dx1 && fabs(x1i - xr) > 7.01 * dx1);
+        if (ok) {
+            const double x2s = ss * x1 + cs * x2;
+            const double x3s = sd * x2r + cd * x3, x3i = -sd * x2r + cd * x3;
+            double temp1 = d_gauss(x1s - xr, dx1), temp2 = d_omega((x2s - yr) / a.W, a.beta);
+            double temp3 = d_omega((x3s - zr) / a.L, a.beta);
+            const double sourc = temp1 * temp2 * temp3;
+            temp1 = d_gauss(x1i - xr, dx1);
+            temp3 = d_omega((x3i + zr) / a.L, a.beta);
+            const double impulse = sourc + temp1 * temp2 * temp3;
+            const int i1 = (j1 + g.sx1) % g.sx1, i2 = (j2 + g.sx2) % g.sx2;
+            const size_t o = ((size_t)i3 * g.sx2 + i2) * g.sx1 + i1;
+            double sv[6];
+#pragma unroll
+            for (int c = 0; c < 6; c++) sv[c] = (double)a.sig[c * g.nh + o];
+            const double n0 = cd * cs, n1 = -cd * ss, n2 = -sd;
+            const double r0 = ss * cr + cs * sd * sr, r1 = cs * cr - ss * sd * sr, r2 = cd * sr;
+            const double t0 = sv[0] * n0 + sv[1] * n1 + sv[2] * n2;
+            const double t1 = sv[1] * n0 + sv[3] * n1 + sv[4] * n2;
+            const double t2 = sv[2] * n0 + sv[4] * n1 + sv[5] * n2;
+            const double taun = t0 * n0 + t1 * n1 + t2 * n2;
+            double ts0 = t0 - taun * n0, ts1 = t1 - taun * n1, ts2 = t2 - taun * n2;
+            const double taus = sqrt(ts0 * ts0 + ts1 * ts1 + ts2 * ts2);
+            const double vo = a.fc[i3], tauc = a.fc[g.sx3h + i3];
+            const double fr = a.fc[2 * g.sx3h + i3], coh = a.fc[3 * g.sx3h + i3];
+            double tau = taus + fr * taun - coh;
+            if (tau < 0.0) tau = 0.0;
+            const bool back = (ts0 * r0 + ts1 * r1 + ts2 * r2) < 0.0 &&
+                              fabs(a.rake) < 6.28318530717958623199592693708837032318 * 1.5;
+            if (!back) {
+                if ((tau / tauc) > 20) atomicOr(a.err, 1 << RELAX_ERR_FRICTION);
+                ts0 /= taus; ts1 /= taus; ts2 /= taus;
+                const double gd = vo * 2.0 * my_sinh(tau / tauc);
+                if (a.want_tm) {
+                    const float cand = (float)(tau / a.mu / gd * ((a.L < a.W ? a.L : a.W) / sqrt(dx1 * dx3)));
+                    if (cand < tm) tm = cand;
+                }
+                const double b = 2.0 * a.mu * impulse * gd;
+                const double b0 = b * n0, b1 = b * n1, b2 = b * n2;
+                float *mp = a.m + o;
+                mp[0 * g.nh] += (float)(ts0 * b0);
+                mp[1 * g.nh] += (float)((ts0 * b1 + ts1 * b0) / 2.0);
+                mp[2 * g.nh] += (float)((ts0 * b2 + ts2 * b0) / 2.0);
+                mp[3 * g.nh] += (float)(ts1 * b1);
+                mp[4 * g.nh] += (float)((ts1 * b2 + ts2 * b1) / 2.0);
+                mp[5 * g.nh] += (float)(ts2 * b2);
+            }
+        }
+    }
+    if (a.want_tm) {
+        tm = block_min(tm, shf);
+        if (threadIdx.x == 0) a.tm_part[blockIdx.x] = tm;
+    }
+}
+
+// monitorfriction + frictionadd, src/friction3d.f90:263-453, one thread
+// per patch.  dt = 0 leaves the cumulative slip unchanged.
+struct MonitorArgs {
+    Grid g;
+    double x, y, z, strike, dip, rake;
+    const double *fc;
+    const float *sig;
+    relax_slippatch *patch;
+    int px2, px3;
+    const StepState *st;
+};
+
+__global__ void k_monitor(MonitorArgs a)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.px2 * a.px3) return;
+    const Grid &g = a.g;
+    const int j2 = t % a.px2 + 1, j3 = t / a.px2 + 1;
+    relax_slippatch *p = a.patch + t;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double cr = cos(a.rake), sr = sin(a.rake);
+    const double svv[3] = {ss, cs, 0.0}, dvv[3] = {-cs * sd, ss * sd, -cd};
+    const double n[3] = {cd * cs, -cd * ss, -sd};
+    const double r[3] = {ss * cr + cs * sd * sr, cs * cr - ss * sd * sr, cd * sr};
+    const double x2 = cs * a.x - ss * a.y;
+    const double xr = cd * x2 - sd * a.z;
+    double yr = ss * a.x + cs * a.y, zr = sd * x2 + cd * a.z;
+    yr = (double)((float)yr + (float)(((double)j2 - (double)a.px2 / 2.0 - 1.0) * g.dx2));
+    zr = (double)((float)zr + (float)(((double)j3 - (double)a.px3 / 2.0 - 1.0) * g.dx3));
+    const double x2p = cd * xr + sd * zr;
+    const double X1 = cs * x2p + ss * yr, X2 = -ss * x2p + cs * yr, X3 = -sd * xr + cd * zr;
+    p->x1 = X1; p->x2 = X2; p->x3 = X3; p->lx = yr; p->lz = zr;
+    bool ok = !(X1 > (double)(g.sx1 / 2 - 1) * g.dx1 || X1 < -(double)(g.sx1 / 2) * g.dx1 ||
+                X2 > (double)(g.sx2 / 2 - 1) * g.dx2 || X2 < -(double)(g.sx2 / 2) * g.dx2 ||
+                X3 > (double)(g.sx3h - 1) * g.dx3 || X3 < 0.0);
+    if (ok) {
+        auto fix = [](double v) { double f = floor(v), c = ceil(v); return (int)((v - f) > 0.5 ? c : f); };
+        const int i1 = ((g.sx1 + fix(X1 / g.dx1)) % g.sx1 + g.sx1) % g.sx1;
+        const int i2 = ((g.sx2 + fix(X2 / g.dx2)) % g.sx2 + g.sx2) % g.sx2;
+        const int i3 = fix(X3 / g.dx3);
+        if (i3 >= 0 && i3 < g.sx3h) {
+            const size_t o = ((size_t)i3 * g.sx2 + i2) * g.sx1 + i1;
+            float s6[6];
+            for (int c = 0; c < 6; c++) s6[c] = a.sig[c * g.nh + o];
+            p->sig.s11 = s6[0]; p->sig.s12 = s6[1]; p->sig.s13 = s6[2];
+            p->sig.s22 = s6[3]; p->sig.s23 = s6[4]; p->sig.s33 = s6[5];
+            const double t0 = s6[0] * n[0] + s6[1] * n[1] + s6[2] * n[2];
+            const double t1 = s6[1] * n[0] + s6[3] * n[1] + s6[4] * n[2];
+            const double t2 = s6[2] * n[0] + s6[4] * n[1] + s6[5] * n[2];
+            const double taun = t0 * n[0] + t1 * n[1] + t2 * n[2];
+            double ts[3] = {t0 - taun * n[0], t1 - taun * n[1], t2 - taun * n[2]};
+            const double taus = sqrt(ts[0] * ts[0] + ts[1] * ts[1] + ts[2] * ts[2]);
+            const double vo = a.fc[i3], tauc = a.fc[g.sx3h + i3];
+            const double fr = a.fc[2 * g.sx3h + i3], coh = a.fc[3 * g.sx3h + i3];
+            double tau = taus + fr * taun - coh;
+            if (tau < 0.0) tau = 0.0;
+            const bool back = (ts[0] * r[0] + ts[1] * r[1] + ts[2] * r[2]) < 0.0 &&
+                              fabs(a.rake) < 6.28318530717958623199592693708837032318 * 1.5;
+            if (!back) {
+                p->taus = taus;
+                p->v = vo * 2.0 * my_sinh(tau / tauc);
+                for (int k = 0; k < 3; k++) ts[k] /= taus;
+                p->vss = p->v * (ts[0] * svv[0] + ts[1] * svv[1] + ts[2] * svv[2]);
+                p->vds = p->v * (ts[0] * dvv[0] + ts[1] * dvv[1] + ts[2] * dvv[2]);
+            }
+        }
+    }
+    const double dt = a.st ? a.st->Dt : 0.0;
+    p->ss = p->ss + dt * p->vss;
+    p->ds = p->ds + dt * p->vds;
+    p->slip = sqrt(p->ds * p->ds + p->ss * p->ss);
+}
+
+// ------------------------------------------------------------------------
+// 3-D transform, pass 1: R2C along x1.
+//   MODE_DIV: the input is the equivalent body force -div(m) of the moment
+//             tensor (equivalentbodyforce, src/elastic3d.f90:1214-1506)
+//             computed on the fly, and the traction t_i = m_i3(x3=0).
+//   MODE_REAL: the input is read from real arrays (any pitches).
+// Output: spectrum planes [0, nin) and the traction plane sx3, scaled by
+// dx1 dx2 dx3 (dx1 dx2 for the traction), src/fourier.f90:195-199.
+// ------------------------------------------------------------------------
+enum { XIN_DIV = 0, XIN_REAL = 1 };
+
+struct XfArgs {
+    Grid g;
+    float2 *S;
+    FftPlan pm;              // complex length M = sx1/2
+    const float2 *tw1;       // exp(-2 pi i k / sx1)
+    int nin, rows;
+    int has_trac;            // blockIdx.y == nin is the traction plane
+    const float *m;          // XIN_DIV: 6 x nh moment
+    float k1, k2, k3, k3b;
+    const float *in[3];      // XIN_REAL
+    size_t rp, pp;           // row / plane pitch (elements)
+    const float *tin[3];
+    size_t trp;
+    const float *tload;      // optional surface load added to t3 (sx1 x sx2)
+    float scale3, scale2;
+};
+
+template <int XIN>
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_xfwd(XfArgs a)
+{
+    extern __shared__ float2 sm[];
+    const Grid &g = a.g;
+    const int M = g.M, ls = M + 1, rows = a.rows, L = 3 * rows;
+    float2 *A = sm, *B = sm + (size_t)L * ls;
+    const int i2base = blockIdx.x * rows;
+    const int pi = blockIdx.y;                 // [0, nin] ; nin = traction
+    const bool trac = a.has_trac && pi == a.nin;
+    const int i3 = pi;
+    const int nthr = blockDim.x;
+
+    for (int t = threadIdx.x; t < L * M; t += nthr) {
+        const int line = t / M, n = t % M;
+        const int c = line / rows, r = line % rows, i2 = i2base + r;
+        float v[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int i1 = 2 * n + h;
+            float x;
+            if (XIN == XIN_DIV) {
+                const size_t rowo = (size_t)i2 * g.sx1;
+                if (trac) {
+                    const int cz = c == 0 ? 2 : c == 1 ? 4 : 5;
+                    x = a.m[cz * g.nh + rowo + i1];
+                    if (c == 2 && a.tload) x += a.tload[rowo + i1];
+                    x *= a.scale2;
+                } else {
+                    const int cx = c == 0 ? 0 : c == 1 ? 1 : 2;
+                    const int cy = c == 0 ? 1 : c == 1 ? 3 : 4;
+                    const int cz = c == 0 ? 2 : c == 1 ? 4 : 5;
+                    const size_t pl = (size_t)i3 * g.plane;
+                    const float *mx = a.m + cx * g.nh + pl + rowo;
+                    const float fx = (__ldg(mx + (i1 + 1) % g.sx1) - __ldg(mx + (i1 + g.sx1 - 1) % g.sx1)) * a.k1;
+                    const float *my = a.m + cy * g.nh + pl + i1;
+                    const float fy = (__ldg(my + (size_t)((i2 + 1) % g.sx2) * g.sx1) -
+                                      __ldg(my + (size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1)) * a.k2;
+                    const float *mz = a.m + cz * g.nh + rowo + i1;
+                    float fz;
+                    if (i3 == 0) fz = (__ldg(mz + g.plane) - __ldg(mz)) * a.k3b;
+                    else if (i3 == g.sx3h - 1) fz = (__ldg(mz + pl) - __ldg(mz + pl - g.plane)) * a.k3b;
+                    else fz = (__ldg(mz + pl + g.plane) - __ldg(mz + pl - g.plane)) * a.k3;
+                    x = -(fx + fy + fz) * a.scale3;
+                }
+            } else {
+                if (trac) {
+                    x = a.tin[c][(size_t)i2 * a.trp + i1];
+                    if (c == 2 && a.tload) x += a.tload[(size_t)i2 * g.sx1 + i1];
+                    x *= a.scale2;
+                } else {
+                    x = a.in[c][(size_t)i3 * a.pp + (size_t)i2 * a.rp + i1] * a.scale3;
+                }
+            }
+            v[h] = x;
+        }
+        A[line * ls + n] = make_float2(v[0], v[1]);
+    }
+    __syncthreads();
+    float2 *R = fft_smem<-1>(A, B, a.pm, L, 1, ls);
+    // unpack: X[k] = (Z_k + conj Z_{M-k})/2 - i/2 W^k (Z_k - conj Z_{M-k})
+    const int p = trac ? g.sx3 : i3;
+    for (int t = threadIdx.x; t < L * (M + 1); t += nthr) {
+        const int line = t / (M + 1), k = t % (M + 1);
+        const int c = line / rows, r = line % rows;
+        const float2 zk = R[line * ls + (k == M ? 0 : k)];
+        const float2 zm = cconj(R[line * ls + (k == 0 ? 0 : M - k)]);
+        const float2 e = cscale(cadd(zk, zm), 0.5f);
+        const float2 d = csub(zk, zm);
+        const float2 w = __ldg(&a.tw1[k]);
+        const float2 wd = cmul(w, d);
+        const float2 X = make_float2(e.x + 0.5f * wd.y, e.y - 0.5f * wd.x);
+        a.S[sidx(g, c, p, i2base + r, k)] = X;
+    }
+}
+
+// pass 2 / 4: complex transform along x2 for a tile of x1 wavenumbers
+struct YArgs {
+    Grid g;
+    float2 *S;
+    FftPlan py;
+    int tw;            // tile width (k1 columns)
+    int nbody;         // body planes [0, nbody)
+    int traction;      // also the traction plane (index nbody of blockIdx.y)
+};
+
+template <int SIGN>
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_ypass(YArgs a)
+{
+    extern __shared__ float2 sm[];
+    const Grid &g = a.g;
+    const int TW = a.tw, n = g.sx2;
+    const int k1t = blockIdx.x * TW, ncol = min(TW, g.K1 - k1t);
+    const int p = (a.traction && (int)blockIdx.y == a.nbody) ? g.sx3 : (int)blockIdx.y;
+    const int c = blockIdx.z;
+    float2 *A = sm, *B = sm + (size_t)n * TW;
+    const size_t base = sidx(g, c, p, 0, k1t);
+    for (int t = threadIdx.x; t < n * TW; t += blockDim.x) {
+        const int i2 = t / TW, col = t % TW;
+        A[t] = col < ncol ? a.S[base + (size_t)i2 * g.K1 + col] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2 *R = fft_smem<SIGN>(A, B, a.py, TW, TW, 1);
+    for (int t = threadIdx.x; t < n * TW; t += blockDim.x) {
+        const int i2 = t / TW, col = t % TW;
+        if (col < ncol) a.S[base + (size_t)i2 * g.K1 + col] = R[t];
+    }
+}
+
+// ------------------------------------------------------------------------
+// pass 3: the Fourier-domain Green's function on whole x3 columns.
+// For a tile of x1 wavenumbers at one k2, all three components:
+//   forward transform along x3 (input planes [0, nin), zero below),
+//   elasticresponse (src/green.f90:51-101),
+//   surfacetractioncowling (src/green.f90:327-377; the k3 sum in FP64,
+//   fixed order), p = t - p (src/green.f90:1082-1084),
+//   cerrutimodified (src/green.f90:520-612; per-column coefficients FP64),
+//   inverse transform along x3, planes [0, nout) written back.
+// ------------------------------------------------------------------------
+struct ZArgs {
+    Grid g;
+    float2 *S;
+    FftPlan pz;
+    int tw, nin, nout;
+    float ratio1, ratio2;            // elastic response constants
+    double lambda, mu, gam;
+};
+
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_zspec(ZArgs a)
+{
+    extern __shared__ float2 sm[];
+    const Grid &g = a.g;
+    const int TW = a.tw, n = g.sx3, L = 3 * TW;
+    const int k1t = blockIdx.x * TW, ncol = min(TW, g.K1 - k1t);
+    const int k2i = blockIdx.y;
+    const int nthr = blockDim.x;
+    float2 *A = sm, *B = sm + (size_t)n * L;
+    double *red = reinterpret_cast<double *>(sm + 2 * (size_t)n * L);      // [P][TW][6]
+    const int P = nthr / TW;
+    float *colc = reinterpret_cast<float *>(red + (size_t)P * TW * 6);     // [TW][10]
+
+    for (int t = threadIdx.x; t < n * L; t += nthr) {
+        const int j = t / L, line = t % L, c = line / TW, col = line % TW;
+        A[t] = (j < a.nin && col < ncol) ? a.S[sidx(g, c, j, k2i, k1t + col)] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2 *R = fft_smem<-1>(A, B, a.pz, L, L, 1);
+    float2 *O = R == A ? B : A;
+
+    const double PI2 = 6.28318530717958623199592693708837032318;
+    const double k2v = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
+    // elastic response + surface-traction partial sums
+    {
+        const int col = threadIdx.x % TW, part = threadIdx.x / TW;
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        if (part < P) {
+            const double k1v = (double)(k1t + col) / (g.sx1 * g.dx1);
+            const float k1f = (float)k1v, k2f = (float)k2v;
+            const double modulus = a.lambda + 2.0 * a.mu;
+            const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
+            const double grav = 2.0 * a.mu * alpha * a.gam;
+            for (int j = part; j < n; j += P) {
+                const double k3v = (j < n / 2) ? (double)j / (n * g.dx3) : -(double)(n - j) / (n * g.dx3);
+                const float k3f = (float)k3v;
+                float2 *p0 = R + (size_t)j * L + col;
+                float2 c1 = p0[0], c2 = p0[TW], c3 = p0[2 * TW];
+                const float r2 = k1f * k1f + k2f * k2f + k3f * k3f;
+                float2 u1, u2, u3;
+                if (r2 > 0.f && col < ncol) {
+                    const float den = a.ratio1 / (r2 * r2);
+                    const float a1 = k2f * k2f + k3f * k3f + a.ratio2 * r2;
+                    const float a2 = k1f * k1f + k3f * k3f + a.ratio2 * r2;
+                    const float a3 = k1f * k1f + k2f * k2f + a.ratio2 * r2;
+                    u1.x = (a1 * c1.x - k1f * (k2f * c2.x + k3f * c3.x)) * den;
+                    u1.y = (a1 * c1.y - k1f * (k2f * c2.y + k3f * c3.y)) * den;
+                    u2.x = (a2 * c2.x - k2f * (k1f * c1.x + k3f * c3.x)) * den;
+                    u2.y = (a2 * c2.y - k2f * (k1f * c1.y + k3f * c3.y)) * den;
+                    u3.x = (a3 * c3.x - k3f * (k1f * c1.x + k2f * c2.x)) * den;
+                    u3.y = (a3 * c3.y - k3f * (k1f * c1.y + k2f * c2.y)) * den;
+                } else {
+                    u1 = u2 = u3 = make_float2(0.f, 0.f);
+                }
+                p0[0] = u1; p0[TW] = u2; p0[2 * TW] = u3;
+                // i 2 pi (...) terms, src/green.f90:363-366
+                const double a1r = a.mu * (k3v * u1.x + k1v * u3.x), a1i = a.mu * (k3v * u1.y + k1v * u3.y);
+                const double a2r = a.mu * (k3v * u2.x + k2v * u3.x), a2i = a.mu * (k3v * u2.y + k2v * u3.y);
+                const double a3r = modulus * k3v * u3.x + a.lambda * (k1v * u1.x + k2v * u2.x);
+                const double a3i = modulus * k3v * u3.y + a.lambda * (k1v * u1.y + k2v * u2.y);
+                acc[0] += -PI2 * a1i; acc[1] += PI2 * a1r;
+                acc[2] += -PI2 * a2i; acc[3] += PI2 * a2r;
+                acc[4] += -PI2 * a3i - grav * u3.x; acc[5] += PI2 * a3r - grav * u3.y;
+            }
+            for (int q = 0; q < 6; q++) red[((size_t)part * TW + col) * 6 + q] = acc[q];
+        }
+    }
+    __syncthreads();
+    // fixed-order reduction over the parts, then p = t - sum/(sx3 dx3) and
+    // the per-column Cerruti coefficients
+    if (threadIdx.x < TW) {
+        const int col = threadIdx.x;
+        double s[6] = {0, 0, 0, 0, 0, 0};
+        for (int pp = 0; pp < P; pp++)
+            for (int q = 0; q < 6; q++) s[q] += red[((size_t)pp * TW + col) * 6 + q];
+        float *cc = colc + col * 12;
+        for (int q = 0; q < 12; q++) cc[q] = 0.f;
+        const double k1v = (double)(k1t + col) / (g.sx1 * g.dx1);
+        if (col < ncol && !(k1v == 0.0 && k2v == 0.0)) {
+            const double d = (double)n * g.dx3;
+            double p[6];
+            for (int c = 0; c < 3; c++) {
+                const float2 tc = a.S[sidx(g, c, g.sx3, k2i, k1t + col)];
+                p[2 * c] = (double)tc.x - s[2 * c] / d;
+                p[2 * c + 1] = (double)tc.y - s[2 * c + 1] / d;
+            }
+            const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
+            const double beta = PI2 * sqrt(k1v * k1v + k2v * k2v);
+            const double h = a.gam / beta;
+            const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
+            // b1' = p1 c0, b2' = p2 c0 (b_i = fi b_i'), Q = b1' k1 + b2' k2
+            const double b1r = p[0] * c0, b1i = p[1] * c0, b2r = p[2] * c0, b2i = p[3] * c0;
+            const double qr = PI2 * k1v * p[0] + PI2 * k2v * p[2], qi = PI2 * k1v * p[1] + PI2 * k2v * p[3];
+            const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
+            const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
+            const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
+            cc[0] = (float)b1r; cc[1] = (float)b1i; cc[2] = (float)b2r; cc[3] = (float)b2i;
+            cc[4] = (float)b3r; cc[5] = (float)b3i;
+            cc[6] = (float)(b1r * k1v + b2r * k2v); cc[7] = (float)(b1i * k1v + b2i * k2v);
+            cc[8] = (float)beta; cc[9] = (float)k1v; cc[10] = (float)k2v; cc[11] = 1.f;
+        }
+    }
+    __syncthreads();
+    // cerrutimodified, applied to every k3
+    {
+        const float alpha = (float)((a.lambda + a.mu) / (a.lambda + 2.0 * a.mu));
+        const float pi2 = 6.28318530717958623f;
+        for (int t = threadIdx.x; t < n * TW; t += nthr) {
+            const int j = t / TW, col = t % TW;
+            const float *cc = colc + col * 12;
+            if (cc[11] == 0.f) continue;
+            const float beta = cc[8], k1f = cc[9], k2f = cc[10];
+            const float k3f = (float)((j < n / 2) ? (double)j / (n * g.dx3) : -(double)(n - j) / (n * g.dx3));
+            const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + beta * beta);
+            const float gg = pi2 * k3f * fi;
+            const float b3r = cc[4], b3i = cc[5];
+            // tmp = alpha i beta 2pi b3 (1 - 1/alpha - i g)
+            const float er = 1.f - 1.f / alpha, ei = -gg;
+            const float gr = b3r * er - b3i * ei, gi = b3r * ei + b3i * er;
+            const float ab = alpha * beta * pi2;
+            const float tmr = -ab * gi, tmi = ab * gr;
+            // v3 = -alpha beta^2 b3 (1/alpha - i g)
+            const float hr = 1.f / alpha, hi = -gg, ab2 = -alpha * beta * beta;
+            const float v3r = ab2 * (b3r * hr - b3i * hi), v3i = ab2 * (b3r * hi + b3i * hr);
+            // S = fi Q ; C = S (1 - i g)
+            const float sr = fi * cc[6], si = fi * cc[7];
+            const float cr = sr + si * gg, ci = si - sr * gg;
+            const float ap = alpha * pi2 * pi2, bb2 = 2.f * beta * beta * fi;
+            float2 *p0 = R + (size_t)j * L + col;
+            float2 u1 = p0[0], u2 = p0[TW], u3 = p0[2 * TW];
+            u1.x += tmr * k1f * fi - bb2 * cc[0] + ap * k1f * cr;
+            u1.y += tmi * k1f * fi - bb2 * cc[1] + ap * k1f * ci;
+            u2.x += tmr * k2f * fi - bb2 * cc[2] + ap * k2f * cr;
+            u2.y += tmi * k2f * fi - bb2 * cc[3] + ap * k2f * ci;
+            const float ak = alpha * beta * pi2 * pi2 * k3f * fi;
+            u3.x += v3r * fi + ak * sr;
+            u3.y += v3i * fi + ak * si;
+            p0[0] = u1; p0[TW] = u2; p0[2 * TW] = u3;
+        }
+    }
+    __syncthreads();
+    float2 *R2 = fft_smem<+1>(R, O, a.pz, L, L, 1);
+    for (int t = threadIdx.x; t < a.nout * L; t += nthr) {
+        const int j = t / L, line = t % L, c = line / TW, col = line % TW;
+        if (col < ncol) a.S[sidx(g, c, j, k2i, k1t + col)] = R2[t];
+    }
+}
+
+// pass 5: C2R along x1, scaled by 2/(sx1 dx1 sx2 dx2 sx3 dx3), with the
+// field update out = base + coef * w  (fieldadd, src/elastic3d.f90:3774-3812)
+struct XiArgs {
+    Grid g;
+    const float2 *S;
+    FftPlan pm;
+    const float2 *tw1;
+    int rows;
+    float *out[3];
+    const float *base[3];
+    size_t rp, pp;           // pitches of out/base
+    const StepState *st;     // coef = cmul * Dt (or cmul when st is null)
+    float cmul, scale;
+};
+
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
+{
+    extern __shared__ float2 sm[];
+    const Grid &g = a.g;
+    const int M = g.M, ls = M + 1, rows = a.rows, L = 3 * rows;
+    float2 *A = sm, *B = sm + (size_t)L * ls;
+    const int i2base = blockIdx.x * rows, i3 = blockIdx.y;
+    const int nthr = blockDim.x;
+    for (int t = threadIdx.x; t < L * M; t += nthr) {
+        const int line = t / M, k = t % M;
+        const int c = line / rows, r = line % rows;
+        const size_t base = sidx(g, c, i3, i2base + r, 0);
+        float2 xk = a.S[base + k], xm = a.S[base + (M - k)];
+        if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
+        const float2 e = cscale(cadd(xk, cconj(xm)), 0.5f);
+        const float2 d = cscale(csub(xk, cconj(xm)), 0.5f);
+        const float2 o = cmul(d, cconj(__ldg(&a.tw1[k])));
+        A[line * ls + k] = make_float2(e.x - o.y, e.y + o.x);   // E + i O
+    }
+    __syncthreads();
+    float2 *R = fft_smem<+1>(A, B, a.pm, L, 1, ls);
+    const float coef = a.st ? (float)(a.cmul * a.st->Dt) : a.cmul;
+    for (int t = threadIdx.x; t < L * M; t += nthr) {
+        const int line = t / M, nn = t % M;
+        const int c = line / rows, r = line % rows, i2 = i2base + r;
+        const float2 z = R[line * ls + nn];
+        const size_t o = (size_t)i3 * a.pp + (size_t)i2 * a.rp + 2 * nn;
+        float w0 = z.x * a.scale, w1 = z.y * a.scale;
+        if (a.base[c]) {
+            w0 = a.base[c][o] + coef * w0;
+            w1 = a.base[c][o + 1] + coef * w1;
+        }
+        *reinterpret_cast<float2 *>(a.out[c] + o) = make_float2(w0, w1);
+    }
+}
+
+// ------------------------------------------------------------------------
+// time step: reduction of the Maxwell-time minima and integrationstep
+// (src/relax.f90:650-677, :1420-1452), one block.
+// ------------------------------------------------------------------------
+__global__ void k_dt(StepState *st, DtPolicy pol, const float *tm_part, int ntm,
+                     const float *fr_part, int nfr)
+{
+    __shared__ float shf[32];
+    float m0 = 3.0e38f, m1 = 3.0e38f, m2 = 3.0e38f;
+    for (int i = threadIdx.x; i < ntm; i += blockDim.x) {
+        m0 = fminf(m0, tm_part[i]);
+        m1 = fminf(m1, tm_part[ntm + i]);
+    }
+    for (int i = threadIdx.x; i < nfr; i += blockDim.x) m2 = fminf(m2, fr_part[i]);
+    m0 = block_min(m0, shf);
+    __syncthreads();
+    m1 = block_min(m1, shf);
+    __syncthreads();
+    m2 = block_min(m2, shf);
+    if (threadIdx.x == 0) {
+        const double STEP_MAX = 1e7;
+        double mw[3];
+        const float mf[3] = {m0, m1, m2};
+        for (int k = 0; k < 3; k++) {
+            // tm = min(REAL(STEP_MAX), min over cells), src/viscoelastic3d.f90:242-245
+            const float v = fminf((float)STEP_MAX, mf[k]);
+            mw[k] = pol.mech[k] ? (double)v : STEP_MAX;
+            st->maxwell[k] = mw[k];
+        }
+        double tm = 1.0 / ((double)pol.mech[0] / mw[0] + (double)pol.mech[1] / mw[1] +
+                           (double)pol.mech[2] / mw[2]);
+        if (tm > STEP_MAX) tm = STEP_MAX;
+        if (pol.has_inter && tm == STEP_MAX) tm = pol.interval / 20.0;
+        st->tm = tm;
+        double Dt = tm / 10.0;
+        const double t = st->t;
+        if (0 == pol.skip) {
+            if ((t + Dt) >= ((double)st->oi * pol.odt) - Dt * 0.04) Dt = (double)st->oi * pol.odt - t;
+        } else {
+            Dt = Dt * pol.tscale;
+            if (pol.has_next_event)
+                if ((t + Dt - pol.next_event_time) >= 0.0) Dt = pol.next_event_time - t;
+        }
+        if (st->use_override) Dt = st->dt_override;
+        st->Dt = Dt;
+    }
+}
+
+// fixed-order sums of the amplitude partials -> power, C:E^i of the log
+__global__ void k_reduce_amp(StepState *st, const double *amp_part, int n, const double *amp_alt,
+                             double dv)
+{
+    __shared__ double shd[32];
+    double a0 = 0.0, a1 = 0.0;
+    const double *pp = amp_alt ? amp_alt : amp_part;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a0 += pp[i];
+        a1 += amp_part[n + i];
+    }
+    a0 = block_sum(a0, shd);
+    __syncthreads();
+    a1 = block_sum(a1, shd);
+    if (threadIdx.x == 0) {
+        st->power = a0 * dv;
+        st->cei = a1 * dv;
+    }
+}
+
+// ------------------------------------------------------------------------
+// coseismic sources (setup): source (src/elastic3d.f90:2064-2252, CPU
+// branch), momentdensityshear (:2661-2750).  L = width, W = length as the
+// call sites pass them (src/relax.f90:1148-1152, :1191-1196).
+// ------------------------------------------------------------------------
+struct SrcArgs {
+    Grid g;
+    double mu, s, x, y, z, L, W, strike, dip, rake, beta;
+    float *f[3];             // body force (3 x nh, physical layers)
+    float *t[3];             // traction (3 x plane)
+    float *tau;              // 6 x nh (momentdensityshear)
+};
+
+__global__ void k_source_force(SrcArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = i3 * g.dx3;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double cr = cos(a.rake), sr = sin(a.rake), scale = -a.mu * a.s;
+    const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+    const double mlw = Wp > Lp ? Wp : Lp;
+    const double x2r0 = cs * a.x - ss * a.y;
+    const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+    if (fabs(x3 - a.z) > Lp && fabs(x3 + a.z) > Lp) return;
+    if (fabs(x1 - a.x) > mlw || fabs(x2 - a.y) > mlw) return;
+    const double x2r = cs * x1 - ss * x2;
+    const double x1s = cd * x2r - sd * x3, x1i = cd * x2r + sd * x3;
+    if (fabs(x1s - xr) > 7.01 * g.dx1 && fabs(x1i - xr) > 7.01 * g.dx1) return;
+    const double x2s = ss * x1 + cs * x2;
+    const double x3s = sd * x2r + cd * x3, x3i = -sd * x2r + cd * x3;
+    double temp1 = d_gauss(x1s - xr, g.dx1), temp2 = d_omega((x2s - yr) / a.W, a.beta);
+    double temp3 = d_omega((x3s - zr) / a.L, a.beta);
+    const double sourc = scale * d_gaussp(x1s - xr, g.dx1) * temp2 * temp3;
+    const double dblcp = scale / a.W * temp1 * d_omegap((x2s - yr) / a.W, a.beta) * temp3;
+    const double dipcs = scale / a.L * temp1 * temp2 * d_omegap((x3s - zr) / a.L, a.beta);
+    temp1 = d_gauss(x1i - xr, g.dx1);
+    temp3 = d_omega((x3i + zr) / a.L, a.beta);
+    const double image = scale * d_gaussp(x1i - xr, g.dx1) * temp2 * temp3;
+    const double cplei = scale / a.W * temp1 * d_omegap((x2s - yr) / a.W, a.beta) * temp3;
+    float &f1 = a.f[0][q], &f2 = a.f[1][q], &f3 = a.f[2][q];
+    if (2.01 * 0.01745329251994329547437168059786927 > a.dip) {
+        f1 = (float)(f1 + cr * ss * (sourc + image) + cr * cd * cs * (dblcp + cplei));
+        f2 = (float)(f2 + cr * cs * (sourc + image) - cr * cd * ss * (dblcp + cplei));
+        f3 = (float)(f3 - cr * sd * (dblcp - cplei));
+    } else {
+        f1 = (float)(f1 + cr * ss * (sourc) + cr * cd * cs * (dblcp));
+        f2 = (float)(f2 + cr * cs * (sourc) - cr * cd * ss * (dblcp));
+        f3 = (float)(f3 - cr * sd * (dblcp));
+    }
+    f1 = (float)(f1 + cd * sr * cs * dipcs + sd * sr * cs * sourc);
+    f2 = (float)(f2 - cd * sr * ss * dipcs - sd * sr * ss * sourc);
+    f3 = (float)(f3 + cd * sr * sourc - sd * sr * dipcs);
+}
+
+__global__ void k_source_traction(SrcArgs a)
+{
+    const Grid &g = a.g;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (int)g.plane) return;
+    const int i1 = q % g.sx1, i2 = q / g.sx1;
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = 0.0;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double cr = cos(a.rake), sr = sin(a.rake);
+    const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+    const double mlw = Wp > Lp ? Wp : Lp;
+    const double x2r0 = cs * a.x - ss * a.y;
+    const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+    if (fabs(x1 - a.x) > mlw || fabs(x2 - a.y) > mlw) return;
+    const double x2r = cs * x1 - ss * x2;
+    const double x1s = cd * x2r - sd * x3, x1i = cd * x2r + sd * x3;
+    const double w701 = (double)7.01f;   // default-real literal of src/elastic3d.f90:2139
+    if (fabs(x1s - xr) > w701 * g.dx1 && fabs(x1i - xr) > w701 * g.dx1) return;
+    const double x2s = ss * x1 + cs * x2;
+    const double x3s = sd * x2r + cd * x3, x3i = -sd * x2r + cd * x3;
+    double temp1 = d_gauss(x1s - xr, g.dx1), temp2 = d_omega((x2s - yr) / a.W, a.beta);
+    double temp3 = d_omega((x3s - zr) / a.L, a.beta);
+    double sourc = temp1 * temp2 * temp3;
+    temp1 = d_gauss(x1i - xr, g.dx1);
+    temp3 = d_omega((x3i + zr) / a.L, a.beta);
+    sourc = sourc + temp1 * temp2 * temp3;
+    const double n[3] = {cd * cs * sourc, -cd * ss * sourc, -sd * sourc};
+    const double b[3] = {a.mu * a.s * (ss * cr + cs * sd * sr), a.mu * a.s * (cs * cr - ss * sd * sr),
+                         a.mu * a.s * (cd * sr)};
+    a.t[0][q] += (float)((n[0] * b[2] + n[2] * b[0]) / 2.0);
+    a.t[1][q] += (float)((n[1] * b[2] + n[2] * b[1]) / 2.0);
+    a.t[2][q] += (float)(n[2] * b[2]);
+}
+
+__global__ void k_moment_shear(SrcArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = i3 * g.dx3;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double cr = cos(a.rake), sr = sin(a.rake);
+    const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+    const double x2r0 = cs * a.x - ss * a.y;
+    const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+    if (fabs(x3 - a.z) > Lp) return;
+    if (fabs(x1 - a.x) > Wp || fabs(x2 - a.y) > Wp) return;
+    const double x2r = cs * x1 - ss * x2;
+    const double x1s = cd * x2r - sd * x3, x1i = cd * x2r + sd * x3;
+    const double w701 = (double)7.01f;   // default-real literal of src/elastic3d.f90:2712
+    if (fabs(x1s - xr) > w701 * g.dx1 && fabs(x1i - xr) > w701 * g.dx1) return;
+    const double x2s = ss * x1 + cs * x2;
+    const double x3s = sd * x2r + cd * x3, x3i = -sd * x2r + cd * x3;
+    double temp1 = d_gauss(x1s - xr, g.dx1), temp2 = d_omega((x2s - yr) / a.W, a.beta);
+    double temp3 = d_omega((x3s - zr) / a.L, a.beta);
+    double ap = temp1 * temp2 * temp3;
+    temp1 = d_gauss(x1i - xr, g.dx1);
+    temp3 = d_omega((x3i + zr) / a.L, a.beta);
+    ap = ap + temp1 * temp2 * temp3;
+    const double n[3] = {cd * cs * ap, -cd * ss * ap, -sd * ap};
+    const double s[3] = {a.s * (ss * cr + cs * sd * sr), a.s * (cs * cr - ss * sd * sr), a.s * (cd * sr)};
+    const float rmu = 2.0f * (float)a.mu;
+    const float e[6] = {(float)(n[0] * s[0]), (float)((n[0] * s[1] + n[1] * s[0]) / 2.0),
+                        (float)((n[0] * s[2] + n[2] * s[0]) / 2.0), (float)(n[1] * s[1]),
+                        (float)((n[1] * s[2] + n[2] * s[1]) / 2.0), (float)(n[2] * s[2])};
+    for (int c = 0; c < 6; c++) a.tau[c * g.nh + q] += rmu * e[c];
+}
+
+// ------------------------------------------------------------------------
+// layout conversion between RELAX's arrays and the device layout
+// ------------------------------------------------------------------------
+// AoS TENSOR (sx1, sx2, sx3h) <-> SoA
+__global__ void k_aos_to_soa(const relax_tensor *src, float *dst, size_t n)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const relax_tensor t = src[q];
+    dst[q] = t.s11; dst[n + q] = t.s12; dst[2 * n + q] = t.s13;
+    dst[3 * n + q] = t.s22; dst[4 * n + q] = t.s23; dst[5 * n + q] = t.s33;
+}
+__global__ void k_soa_to_aos(const float *src, relax_tensor *dst, size_t n)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    relax_tensor t;
+    t.s11 = src[q]; t.s12 = src[n + q]; t.s13 = src[2 * n + q];
+    t.s22 = src[3 * n + q]; t.s23 = src[4 * n + q]; t.s33 = src[5 * n + q];
+    dst[q] = t;
+}
+// padded (sx1+2) rows <-> compact rows, nrows rows of sx1
+__global__ void k_unpad(const float *src, float *dst, int sx1, size_t nrows)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nrows * sx1) return;
+    const size_t r = q / sx1, i = q % sx1;
+    dst[q] = src[r * (sx1 + 2) + i];
+}
+__global__ void k_pad(const float *src, float *dst, int sx1, size_t nrows)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nrows * (sx1 + 2)) return;
+    const size_t r = q / (sx1 + 2), i = q % (sx1 + 2);
+    dst[q] = i < (size_t)sx1 ? src[r * sx1 + i] : 0.f;
+}
+
+// compact rows back into the first sx1 entries of padded rows
+__global__ void k_repad(const float *src, float *dst, int sx1, size_t nrows)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nrows * sx1) return;
+    const size_t r = q / sx1, i = q % sx1;
+    dst[r * (sx1 + 2) + i] = src[q];
+}
+
+// standalone equivalentbodyforce (for the operator API): c_i -= div(sig),
+// t_i += sig_i3(x3=0) on padded arrays
+__global__ void k_bodyforce(Grid g, const float *m, float *c1, float *c2, float *c3, float *t1,
+                            float *t2, float *t3, float k1, float k2, float k3, float k3b)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    float *cc[3] = {c1, c2, c3}, *tt[3] = {t1, t2, t3};
+    const size_t rowo = (size_t)i2 * g.sx1, pl = (size_t)i3 * g.plane;
+    const size_t po = ((size_t)i3 * g.sx2 + i2) * (g.sx1 + 2) + i1;
+    for (int c = 0; c < 3; c++) {
+        const int cx = c == 0 ? 0 : c == 1 ? 1 : 2;
+        const int cy = c == 0 ? 1 : c == 1 ? 3 : 4;
+        const int cz = c == 0 ? 2 : c == 1 ? 4 : 5;
+        const float *mx = m + cx * g.nh + pl + rowo;
+        const float fx = (mx[(i1 + 1) % g.sx1] - mx[(i1 + g.sx1 - 1) % g.sx1]) * k1;
+        const float *my = m + cy * g.nh + pl + i1;
+        const float fy = (my[(size_t)((i2 + 1) % g.sx2) * g.sx1] - my[(size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1]) * k2;
+        const float *mz = m + cz * g.nh + rowo + i1;
+        float fz;
+        if (i3 == 0) fz = (mz[g.plane] - mz[0]) * k3b;
+        else if (i3 == g.sx3h - 1) fz = (mz[pl] - mz[pl - g.plane]) * k3b;
+        else fz = (mz[pl + g.plane] - mz[pl - g.plane]) * k3;
+        cc[c][po] = cc[c][po] - (fx + fy + fz);
+        if (i3 == 0) tt[c][(size_t)i2 * (g.sx1 + 2) + i1] += m[cz * g.nh + rowo + i1];
+    }
+}
+
+}  // namespace
+}  // namespace relax

@@ -1,0 +1,1548 @@
+// relax_b200.cu -- context API, RK2 driver and operator entry points of the
+// B200 relaxation-loop library (C ABI in include/relax_b200.h).
+//
+// The driver restates the reference's time loop (src/relax.f90:555-890,
+// GPU variant src/curelax.f90:447-927) over fused device kernels:
+//
+//   predictor  [m, Maxwell minima already computed by the previous step's
+//               tail kernel]  friction planes -> k_dt (integrationstep on
+//               device) -> Green(-div m) with v = u + Dt/2 w fused in the
+//               last pass
+//   corrector  k_stress<CORR>: sig = -Dt/2 m - tau + C:E(v), m = eigen(sig),
+//               gamma += Dt gd -> friction planes, patch monitor ->
+//               Green(-div m) with u += Dt w fused in the last pass
+//   tail       k_stress<END>: tau += Dt m, sig = -tau + C:E(u), next
+//               predictor m = eigen(sig), Maxwell minima, log amplitudes
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace relax;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(RELAX_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,       \
+                        cudaGetErrorString(e_));                                          \
+    } while (0)
+
+#define CKL()                                                                             \
+    do {                                                                                  \
+        cudaError_t e_ = cudaGetLastError();                                              \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(RELAX_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__,          \
+                        cudaGetErrorString(e_));                                          \
+    } while (0)
+
+#define TRY(call)                  \
+    do {                               \
+        int r_ = (call);               \
+        if (r_ != RELAX_OK) return r_; \
+    } while (0)
+
+static unsigned nblocks(size_t n, int t = RELAX_NTHREADS) { return (unsigned)((n + t - 1) / t); }
+
+// ---------------------------------------------------------------------------
+// FFT plans and twiddle tables
+// ---------------------------------------------------------------------------
+static bool factor(int n, int *r, int *nr)
+{
+    int k = 0;
+    while (n % 8 == 0 && n > 8) { r[k++] = 8; n /= 8; }
+    if (n == 8) { r[k++] = 8; n = 1; }
+    while (n % 4 == 0) { r[k++] = 4; n /= 4; }
+    while (n % 2 == 0) { r[k++] = 2; n /= 2; }
+    while (n % 3 == 0) { r[k++] = 3; n /= 3; }
+    *nr = k;
+    return n == 1 && k <= 12;
+}
+
+static bool fft_size_ok(int n)
+{
+    int r[16], k;
+    return n >= 2 && factor(n, r, &k);
+}
+
+// Per-stage device timing: CUDA events recorded around every launch of the
+// context's stream while enabled; launches are counted always.
+enum Stage {
+    ST_STRESS_END = 0, ST_STRESS_CORR, ST_STRESS_INIT, ST_XFWD, ST_YFWD, ST_ZSPEC, ST_YINV, ST_XINV,
+    ST_FRICTION, ST_MONITOR, ST_DT, ST_REDUCE, ST_SOURCE, ST_OTHER, ST_COUNT
+};
+static const char *kStageNames[ST_COUNT] = {
+    "k_stress<END>", "k_stress<CORR>", "k_stress<INIT>", "k_xfwd", "k_ypass<fwd>", "k_zspec",
+    "k_ypass<inv>", "k_xinv", "k_friction", "k_monitor", "k_dt", "k_reduce_amp", "k_source", "other"};
+
+struct Prof {
+    bool on = false;
+    long long launches = 0;
+    std::vector<cudaEvent_t> pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> recs;
+    size_t used = 0;
+    cudaEvent_t get()
+    {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+    void begin(int stage, cudaStream_t st, cudaEvent_t *e0)
+    {
+        launches++;
+        if (!on) return;
+        *e0 = get();
+        cudaEventRecord(*e0, st);
+        recs.push_back({stage, {*e0, nullptr}});
+    }
+    void end(cudaStream_t st)
+    {
+        if (!on) return;
+        cudaEvent_t e1 = get();
+        cudaEventRecord(e1, st);
+        recs.back().second.second = e1;
+    }
+    void reset()
+    {
+        recs.clear();
+        used = 0;
+    }
+    ~Prof()
+    {
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+#define TIMED(prof, stage, st, launch)                     \
+    do {                                                    \
+        cudaEvent_t e0_ = nullptr;                          \
+        if (prof) (prof)->begin((stage), (st), &e0_);       \
+        launch;                                             \
+        CKL();                                              \
+        if (prof) (prof)->end(st);                          \
+    } while (0)
+
+struct Spectral {
+    Prof *prof = nullptr;
+    Grid g{};
+    float2 *S = nullptr;
+    float2 *tw = nullptr;          // tables for M, sx1, sx2, sx3
+    FftPlan pm{}, py{}, pz{};
+    const float2 *tw1 = nullptr;
+    int rows = 1, twy = 16, twz = 16;
+    size_t smx = 0, smy = 0, smz = 0;
+
+    int init(const Grid &gg, cudaStream_t st)
+    {
+        g = gg;
+        int nr;
+        if (!factor(g.M, pm.r, &pm.nr) || !factor(g.sx2, py.r, &py.nr) || !factor(g.sx3, pz.r, &pz.nr))
+            return fail(RELAX_ERR_UNSUPPORTED, "FFT sizes must be products of 2 and 3 (sx1/2=%d sx2=%d sx3=%d)",
+                        g.M, g.sx2, g.sx3);
+        (void)nr;
+        pm.n = g.M; py.n = g.sx2; pz.n = g.sx3;
+        const int ns[4] = {g.M, g.sx1, g.sx2, g.sx3};
+        size_t tot = 0;
+        for (int i = 0; i < 4; i++) tot += ns[i];
+        std::vector<float2> h(tot);
+        size_t off[4], o = 0;
+        for (int i = 0; i < 4; i++) {
+            off[i] = o;
+            for (int j = 0; j < ns[i]; j++) {
+                const double a = -2.0 * M_PI * (double)j / (double)ns[i];
+                h[o + j] = make_float2((float)cos(a), (float)sin(a));
+            }
+            o += ns[i];
+        }
+        CK(cudaMalloc(&tw, tot * sizeof(float2)));
+        CK(cudaMemcpyAsync(tw, h.data(), tot * sizeof(float2), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        pm.tw = tw + off[0];
+        tw1 = tw + off[1];
+        py.tw = tw + off[2];
+        pz.tw = tw + off[3];
+        CK(cudaMalloc(&S, 3 * (size_t)(g.sx3 + 1) * g.sx2 * g.K1 * sizeof(float2)));
+        // tile choices
+        rows = 1;
+        while (rows * 2 <= std::max(1, 1024 / g.M) && g.sx2 % (rows * 2) == 0) rows *= 2;
+        twy = 16;
+        while (twy > 1 && 2 * (size_t)g.sx2 * twy * 8 > 96 * 1024) twy /= 2;
+        twz = 16;
+        while (twz > 1 && 2 * (size_t)g.sx3 * 3 * twz * 8 > 100 * 1024) twz /= 2;
+        smx = 2 * (size_t)3 * rows * (g.M + 1) * sizeof(float2);
+        smy = 2 * (size_t)g.sx2 * twy * sizeof(float2);
+        const int P = RELAX_NTHREADS / twz;
+        smz = 2 * (size_t)g.sx3 * 3 * twz * sizeof(float2) + (size_t)P * twz * 6 * sizeof(double) +
+              (size_t)twz * 12 * sizeof(float);
+        CK(cudaFuncSetAttribute(k_xfwd<XIN_DIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+        CK(cudaFuncSetAttribute(k_xfwd<XIN_REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+        CK(cudaFuncSetAttribute(k_xinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+        CK(cudaFuncSetAttribute(k_ypass<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+        CK(cudaFuncSetAttribute(k_ypass<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
+        CK(cudaFuncSetAttribute(k_zspec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+        return RELAX_OK;
+    }
+
+    void release()
+    {
+        if (S) cudaFree(S);
+        if (tw) cudaFree(tw);
+        S = nullptr;
+        tw = nullptr;
+    }
+
+    // Green's function: forward (x pass from `xa`), y, z spectral, y inverse,
+    // x inverse with the epilogue in `xi`.
+    int green(XfArgs xa, bool div, int nin, int nout, XiArgs xi, double lambda, double mu, double gam,
+              cudaStream_t st)
+    {
+        xa.g = g; xa.S = S; xa.pm = pm; xa.tw1 = tw1; xa.nin = nin; xa.rows = rows; xa.has_trac = 1;
+        xa.scale3 = (float)(g.dx1 * g.dx2 * g.dx3);
+        xa.scale2 = (float)(g.dx1 * g.dx2);
+        dim3 gx(g.sx2 / rows, nin + 1);
+        if (div) TIMED(prof, ST_XFWD, st, (k_xfwd<XIN_DIV><<<gx, RELAX_NTHREADS, smx, st>>>(xa)));
+        else TIMED(prof, ST_XFWD, st, (k_xfwd<XIN_REAL><<<gx, RELAX_NTHREADS, smx, st>>>(xa)));
+        YArgs ya{g, S, py, twy, nin, 1};
+        TIMED(prof, ST_YFWD, st,
+              (k_ypass<-1><<<dim3((g.K1 + twy - 1) / twy, nin + 1, 3), RELAX_NTHREADS, smy, st>>>(ya)));
+        ZArgs za;
+        za.g = g; za.S = S; za.pz = pz; za.tw = twz; za.nin = nin; za.nout = nout;
+        za.ratio1 = (float)((lambda + mu) / (lambda + 2.0 * mu) / mu / (4.0 * M_PI * M_PI));
+        za.ratio2 = (float)(mu / (lambda + mu));
+        za.lambda = lambda; za.mu = mu; za.gam = gam;
+        TIMED(prof, ST_ZSPEC, st, (k_zspec<<<dim3((g.K1 + twz - 1) / twz, g.sx2), RELAX_NTHREADS, smz, st>>>(za)));
+        YArgs yb{g, S, py, twy, nout, 0};
+        TIMED(prof, ST_YINV, st,
+              (k_ypass<+1><<<dim3((g.K1 + twy - 1) / twy, nout, 3), RELAX_NTHREADS, smy, st>>>(yb)));
+        xi.g = g; xi.S = S; xi.pm = pm; xi.tw1 = tw1; xi.rows = rows;
+        xi.scale = (float)(2.0 / ((double)g.sx1 * g.dx1 * g.sx2 * g.dx2 * g.sx3 * g.dx3));
+        TIMED(prof, ST_XINV, st, (k_xinv<<<dim3(g.sx2 / rows, nout), RELAX_NTHREADS, smx, st>>>(xi)));
+        return RELAX_OK;
+    }
+};
+
+static int make_grid(Grid &g, int sx1, int sx2, int sx3, double dx1, double dx2, double dx3)
+{
+    if (sx1 < 16 || sx2 < 2 || sx3 < 4 || (sx1 % 4) || (sx3 % 2))
+        return fail(RELAX_ERR_UNSUPPORTED, "grid %dx%dx%d: need sx1 >= 16 and a multiple of 4, even sx3",
+                    sx1, sx2, sx3);
+    if ((sx2 >= 5 && sx2 <= 14) || sx3 / 2 < 15)
+        return fail(RELAX_ERR_UNSUPPORTED,
+                    "grid %dx%dx%d: the 7-point FIR differentiator (5 <= sx <= 14) is not implemented; "
+                    "sx2 must be <= 4 or >= 15 and sx3/2 >= 15", sx1, sx2, sx3);
+    if (!fft_size_ok(sx1 / 2) || !fft_size_ok(sx2) || !fft_size_ok(sx3))
+        return fail(RELAX_ERR_UNSUPPORTED, "grid %dx%dx%d: FFT lengths must be products of 2 and 3", sx1, sx2, sx3);
+    if (!(dx1 > 0 && dx2 > 0 && dx3 > 0)) return fail(RELAX_ERR_ARG, "non-positive sampling");
+    g.sx1 = sx1; g.sx2 = sx2; g.sx3 = sx3; g.sx3h = sx3 / 2;
+    g.M = sx1 / 2; g.K1 = sx1 / 2 + 1;
+    g.dx1 = dx1; g.dx2 = dx2; g.dx3 = dx3;
+    g.plane = (size_t)sx1 * sx2;
+    g.nh = g.plane * g.sx3h;
+    return RELAX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host helpers: depth structures (src/elastic3d.f90:630-829)
+// ---------------------------------------------------------------------------
+static int fixr(double v)
+{
+    double f = floor(v), c = ceil(v);
+    return (int)((v - f) > 0.5 ? c : f);
+}
+
+extern "C" int relax_viscoelastic_structure(const relax_layer *layers, int nv, double dx3, int sx3,
+                                            relax_layer *vs)
+{
+    if (nv <= 0 || !layers || !vs || sx3 <= 0) return fail(RELAX_ERR_ARG, "invalid structure arguments");
+    for (int k = 0; k < sx3; k++) {
+        vs[k].z = 0; vs[k].gammadot0 = 0; vs[k].friction = 0.6; vs[k].cohesion = 0;
+        vs[k].stressexponent = layers[0].stressexponent; vs[k].Gk = 0;
+    }
+    double z0 = fixr(layers[0].z / dx3) * dx3, z1 = z0;
+    double g0 = 0, p0 = 0, f0 = 0, c0 = 0, k0 = 0, g1 = 0, p1 = 0, f1 = 0, c1 = 0, k1 = 0;
+    int i3e = 1;
+    for (int k = 0; k < nv; k++) {
+        z1 = fixr(layers[k].z / dx3) * dx3;
+        if (z1 < z0) return fail(RELAX_ERR_ARG, "invalid mechanical structure: depths must be increasing");
+        g1 = layers[k].gammadot0; p1 = layers[k].stressexponent; f1 = layers[k].friction;
+        c1 = layers[k].cohesion; k1 = layers[k].Gk;
+        if (z1 == z0) {
+            i3e = fixr(z1 / dx3 + 1);
+        } else {
+            const int i3s = fixr(z0 / dx3) + 1;
+            i3e = std::min(fixr(z1 / dx3 + 1), sx3);
+            for (int i3 = std::max(i3s, 1); i3 <= i3e; i3++) {
+                const double z = (i3 - 1.0) * dx3;
+                vs[i3 - 1].gammadot0 = ((z - z0) * g1 + (z1 - z) * g0) / (z1 - z0);
+                vs[i3 - 1].stressexponent = ((z - z0) * p1 + (z1 - z) * p0) / (z1 - z0);
+                vs[i3 - 1].friction = ((z - z0) * f1 + (z1 - z) * f0) / (z1 - z0);
+                vs[i3 - 1].cohesion = ((z - z0) * c1 + (z1 - z) * c0) / (z1 - z0);
+                vs[i3 - 1].Gk = ((z - z0) * k1 + (z1 - z) * k0) / (z1 - z0);
+            }
+        }
+        z0 = z1; g0 = g1; p0 = p1; f0 = f1; c0 = c1; k0 = k1;
+    }
+    if (fixr(z1 / dx3) < sx3 - 1)
+        for (int i3 = std::max(i3e, 1); i3 <= sx3; i3++) {
+            vs[i3 - 1].gammadot0 = (float)g1;   // REAL(...), src/elastic3d.f90:821-825
+            vs[i3 - 1].stressexponent = (float)p1;
+            vs[i3 - 1].friction = (float)f1;
+            vs[i3 - 1].cohesion = (float)c1;
+            vs[i3 - 1].Gk = (float)k1;
+        }
+    return RELAX_OK;
+}
+
+extern "C" int relax_tensor_structure(const relax_tensor_layer *layers, int nv, double dx3, int sx3,
+                                      relax_tensor_layer *vs)
+{
+    if (nv <= 0 || !layers || !vs || sx3 <= 0) return fail(RELAX_ERR_ARG, "invalid tensor structure");
+    memset(vs, 0, sizeof(relax_tensor_layer) * (size_t)sx3);
+    double z0 = fixr(layers[0].z / dx3) * dx3, z1 = z0;
+    relax_tensor t0{}, t1{};
+    int i3e = 1;
+    for (int k = 0; k < nv; k++) {
+        z1 = fixr(layers[k].z / dx3) * dx3;
+        if (z1 < z0) return fail(RELAX_ERR_ARG, "invalid tensor structure: depths must be increasing");
+        t1 = layers[k].t;
+        if (z1 == z0) {
+            i3e = fixr(z1 / dx3 + 1);
+        } else {
+            const int i3s = fixr(z0 / dx3) + 1;
+            i3e = std::min(fixr(z1 / dx3 + 1), sx3);
+            for (int i3 = std::max(i3s, 1); i3 <= i3e; i3++) {
+                const double z = (i3 - 1.0) * dx3;
+                const float a = (float)(z - z0), b = (float)(z1 - z), s = (float)(1.0 / (z1 - z0));
+                relax_tensor t;
+                t.s11 = s * (a * t1.s11 + b * t0.s11); t.s12 = s * (a * t1.s12 + b * t0.s12);
+                t.s13 = s * (a * t1.s13 + b * t0.s13); t.s22 = s * (a * t1.s22 + b * t0.s22);
+                t.s23 = s * (a * t1.s23 + b * t0.s23); t.s33 = s * (a * t1.s33 + b * t0.s33);
+                vs[i3 - 1].t = t;
+            }
+        }
+        z0 = z1; t0 = t1;
+    }
+    if (fixr(z1 / dx3) < sx3 - 1)
+        for (int i3 = std::max(i3e, 1); i3 <= sx3; i3++) vs[i3 - 1].t = t1;
+    return RELAX_OK;
+}
+
+extern "C" void relax_wang_convention(double *slip, double *x, double *y, double *z, double length,
+                                      double width, double *strike, double *dip, double *rake, double x0,
+                                      double y0, double rot)
+{
+    const double D2R = 0.01745329251994329547437168059786927;
+    *slip = -*slip;
+    *strike = -90.0 - *strike;
+    *dip = 90.0 - *dip;
+    *strike *= D2R; *dip *= D2R; *rake *= D2R;
+    *x = *x - x0 - length / 2.0 * sin(*strike) + width / 2.0 * sin(*dip) * cos(*strike);
+    *y = *y - y0 - length / 2.0 * cos(*strike) - width / 2.0 * sin(*dip) * sin(*strike);
+    *z = *z + width / 2.0 * cos(*dip);
+    const double a = rot * D2R, xx = *x, yy = *y;
+    *x = +xx * cos(a) + yy * sin(a);
+    *y = -xx * sin(a) + yy * cos(a);
+    *strike += rot * D2R;
+}
+
+// deviatoric prestress and (taup/mu)^(n-1) per depth, as
+// src/viscoelastic3d.f90:254-258 computes them (REAL*4 deviatoric part)
+static void prestress_terms(const relax_tensor_layer *pre, int nz, double mu, const relax_layer *vs,
+                            std::vector<float> *spdev, std::vector<DepthVisc> *dv)
+{
+    if (spdev) spdev->assign(6 * (size_t)nz, 0.f);
+    dv->resize(nz);
+    for (int i3 = 0; i3 < nz; i3++) {
+        float s[6] = {0, 0, 0, 0, 0, 0};
+        if (pre) {
+            const relax_tensor &t = pre[i3].t;
+            const float diag = (float)((double)(t.s11 + t.s22 + t.s33) / 3.0);
+            s[0] = t.s11 - diag; s[1] = t.s12; s[2] = t.s13;
+            s[3] = t.s22 - diag; s[4] = t.s23; s[5] = t.s33 - diag;
+        }
+        if (spdev)
+            for (int c = 0; c < 6; c++) (*spdev)[(size_t)c * nz + i3] = s[c];
+        const double taup = sqrt(((double)(s[0] * s[0]) + 2.0 * (double)(s[1] * s[1]) + 2.0 * (double)(s[2] * s[2]) +
+                                  (double)(s[3] * s[3]) + 2.0 * (double)(s[4] * s[4]) + (double)(s[5] * s[5])) / 2.0);
+        DepthVisc d;
+        d.g0 = (float)vs[i3].gammadot0;
+        d.power = (float)vs[i3].stressexponent;
+        d.cohesion = (float)vs[i3].cohesion;
+        d.tpow = (float)pow(taup / mu, vs[i3].stressexponent - 1);
+        (*dv)[i3] = d;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct EventCopy {
+    double time;
+    std::vector<relax_source> s, ts, m, l;
+};
+
+struct relax_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    Grid g{};
+    Spectral sp;
+    relax_config cfg{};
+    std::vector<relax_layer> lin, non, fc;
+    std::vector<relax_tensor_layer> pre;
+    std::vector<relax_plane> planes;
+    std::vector<EventCopy> events;
+    EventCopy inter;
+    std::vector<float> hdg0[2];
+
+    // device fields
+    float *tau = nullptr, *m = nullptr, *sig = nullptr, *u = nullptr, *vp = nullptr, *gamma = nullptr;
+    float *work = nullptr, *twork = nullptr, *tload = nullptr;
+    DepthVisc *visc[2] = {nullptr, nullptr};
+    float *spdev = nullptr, *dg0[2] = {nullptr, nullptr};
+    double *fcd = nullptr;
+    relax_slippatch *patch = nullptr;
+    std::vector<int> patch_off;
+    StepState *dst = nullptr, *hst = nullptr;   // device state, pinned host mirror
+    float *tm_part = nullptr, *fr_part = nullptr;
+    double *amp_part = nullptr, *amp_alt = nullptr;
+    int *err = nullptr;
+    int nblk = 0, nfr = 0;
+
+    // host time-loop state
+    double t = 0.0;
+    int i = 0, e = 0, oi = 1;
+    bool cos_done = false, m_valid = false, sig_valid = false;
+    bool store_sig = false;
+    relax_step_log pending{};
+    Prof prof;
+};
+
+static void free_ctx(relax_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    float *fs[] = {c->tau, c->m, c->sig, c->u, c->vp, c->gamma, c->work, c->twork, c->tload, c->spdev,
+                   c->dg0[0], c->dg0[1], c->tm_part, c->fr_part};
+    for (float *p : fs)
+        if (p) cudaFree(p);
+    if (c->visc[0]) cudaFree(c->visc[0]);
+    if (c->visc[1]) cudaFree(c->visc[1]);
+    if (c->fcd) cudaFree(c->fcd);
+    if (c->patch) cudaFree(c->patch);
+    if (c->dst) cudaFree(c->dst);
+    if (c->hst) cudaFreeHost(c->hst);
+    if (c->amp_part) cudaFree(c->amp_part);
+    if (c->amp_alt) cudaFree(c->amp_alt);
+    if (c->err) cudaFree(c->err);
+    c->sp.release();
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+extern "C" const char *relax_version(void) { return "relax_b200 1.0 (sm_100a)"; }
+extern "C" const char *relax_last_error(void) { return g_err.c_str(); }
+
+template <typename T>
+static int dalloc(T **p, size_t n)
+{
+    cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return fail(RELAX_ERR_NOMEM, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
+    return RELAX_OK;
+}
+
+static int create(const relax_config *cfg, int device, relax_ctx *c)
+{
+    c->device = device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    TRY(make_grid(c->g, cfg->sx1, cfg->sx2, cfg->sx3, cfg->dx1, cfg->dx2, cfg->dx3));
+    const Grid &g = c->g;
+    const int nz = g.sx3h;
+    c->cfg = *cfg;
+    if (cfg->ne <= 0 || !cfg->events) return fail(RELAX_ERR_ARG, "at least one event is required");
+    if (cfg->np > 0 && (!cfg->planes || !cfg->faultcreepstruc))
+        return fail(RELAX_ERR_ARG, "afterslip planes need a fault-creep structure");
+    auto copyv = [&](const relax_layer *p, std::vector<relax_layer> &v) {
+        if (p) v.assign(p, p + nz);
+    };
+    copyv(cfg->linearstruc, c->lin);
+    copyv(cfg->nonlinearstruc, c->non);
+    copyv(cfg->faultcreepstruc, c->fc);
+    if (cfg->stressstruc) c->pre.assign(cfg->stressstruc, cfg->stressstruc + nz);
+    if (cfg->np > 0) c->planes.assign(cfg->planes, cfg->planes + cfg->np);
+    auto copye = [](const relax_event &e, EventCopy &o) {
+        o.time = e.time;
+        if (e.ns > 0 && e.s) o.s.assign(e.s, e.s + e.ns);
+        if (e.nt > 0 && e.ts) o.ts.assign(e.ts, e.ts + e.nt);
+        if (e.nm > 0 && e.m) o.m.assign(e.m, e.m + e.nm);
+        if (e.nl > 0 && e.l) o.l.assign(e.l, e.l + e.nl);
+    };
+    c->events.resize(cfg->ne);
+    for (int k = 0; k < cfg->ne; k++) {
+        copye(cfg->events[k], c->events[k]);
+        if (!c->events[k].ts.empty() || !c->events[k].m.empty())
+            return fail(RELAX_ERR_UNSUPPORTED, "tensile and dilatation sources are not supported");
+    }
+    copye(cfg->inter, c->inter);
+    for (const auto *v : {&c->lin, &c->non})
+        for (const auto &l : *v)
+            if (l.stressexponent < 0.999999)
+                return fail(RELAX_ERR_POWER, "invalid power exponent %g", l.stressexponent);
+    c->cfg.stressstruc = nullptr; c->cfg.linearstruc = nullptr; c->cfg.nonlinearstruc = nullptr;
+    c->cfg.faultcreepstruc = nullptr; c->cfg.planes = nullptr; c->cfg.events = nullptr;
+    c->cfg.lineardgammadot0 = nullptr; c->cfg.nonlineardgammadot0 = nullptr;
+
+    const size_t nh = g.nh;
+    TRY(dalloc(&c->tau, 6 * nh));
+    TRY(dalloc(&c->m, 6 * nh));
+    TRY(dalloc(&c->sig, 6 * nh));
+    TRY(dalloc(&c->u, 3 * nh));
+    TRY(dalloc(&c->vp, 3 * nh));
+    TRY(dalloc(&c->gamma, nh));
+    TRY(dalloc(&c->work, 3 * nh));
+    TRY(dalloc(&c->twork, 3 * g.plane));
+    TRY(dalloc(&c->tload, g.plane));
+    CK(cudaMemsetAsync(c->m, 0, 6 * nh * sizeof(float), c->st));
+    CK(cudaMemsetAsync(c->sig, 0, 6 * nh * sizeof(float), c->st));
+    CK(cudaMemsetAsync(c->u, 0, 3 * nh * sizeof(float), c->st));
+    CK(cudaMemsetAsync(c->vp, 0, 3 * nh * sizeof(float), c->st));
+    CK(cudaMemsetAsync(c->gamma, 0, nh * sizeof(float), c->st));
+    TRY(c->sp.init(g, c->st));
+    c->sp.prof = &c->prof;
+
+    // tau = -prestress (src/relax.f90:287-297)
+    {
+        std::vector<float> h(6 * nh, 0.f);
+        if (!c->pre.empty())
+            for (int i3 = 0; i3 < nz; i3++) {
+                const relax_tensor &t = c->pre[i3].t;
+                const float v[6] = {-t.s11, -t.s12, -t.s13, -t.s22, -t.s23, -t.s33};
+                for (int cc = 0; cc < 6; cc++)
+                    std::fill(h.begin() + cc * nh + (size_t)i3 * g.plane, h.begin() + cc * nh + (size_t)(i3 + 1) * g.plane, v[cc]);
+            }
+        CK(cudaMemcpy(c->tau, h.data(), 6 * nh * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    // rheology tables
+    std::vector<float> spdev;
+    const relax_tensor_layer *pre = c->pre.empty() ? nullptr : c->pre.data();
+    const std::vector<relax_layer> *vs[2] = {&c->lin, &c->non};
+    const float *dgs[2] = {cfg->lineardgammadot0, cfg->nonlineardgammadot0};
+    for (int k = 0; k < 2; k++) {
+        if (vs[k]->empty()) continue;
+        std::vector<DepthVisc> dv;
+        prestress_terms(pre, nz, cfg->mu, vs[k]->data(), &spdev, &dv);
+        TRY(dalloc(&c->visc[k], nz));
+        CK(cudaMemcpy(c->visc[k], dv.data(), nz * sizeof(DepthVisc), cudaMemcpyHostToDevice));
+        if (dgs[k]) {
+            TRY(dalloc(&c->dg0[k], nh));
+            CK(cudaMemcpy(c->dg0[k], dgs[k], nh * sizeof(float), cudaMemcpyHostToDevice));
+        }
+    }
+    if (pre) {
+        if (spdev.empty()) {
+            std::vector<DepthVisc> dv;
+            std::vector<relax_layer> dummy(nz);
+            for (auto &l : dummy) l.stressexponent = 1.0;
+            prestress_terms(pre, nz, cfg->mu, dummy.data(), &spdev, &dv);
+        }
+        TRY(dalloc(&c->spdev, 6 * (size_t)nz));
+        CK(cudaMemcpy(c->spdev, spdev.data(), 6 * nz * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    if (!c->fc.empty()) {
+        std::vector<double> h(4 * (size_t)nz);
+        for (int i3 = 0; i3 < nz; i3++) {
+            h[i3] = c->fc[i3].gammadot0;
+            h[nz + i3] = c->fc[i3].stressexponent;
+            h[2 * nz + i3] = c->fc[i3].friction;
+            h[3 * nz + i3] = c->fc[i3].cohesion;
+        }
+        TRY(dalloc(&c->fcd, 4 * (size_t)nz));
+        CK(cudaMemcpy(c->fcd, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // afterslip patches
+    int np_tot = 0;
+    for (auto &p : c->planes) {
+        c->patch_off.push_back(np_tot);
+        np_tot += std::max(0, p.px2) * std::max(0, p.px3);
+    }
+    if (np_tot > 0) {
+        TRY(dalloc(&c->patch, np_tot));
+        CK(cudaMemset(c->patch, 0, np_tot * sizeof(relax_slippatch)));
+    }
+    // reductions
+    c->nblk = (int)nblocks(nh / 4);
+    TRY(dalloc(&c->tm_part, 2 * (size_t)c->nblk));
+    TRY(dalloc(&c->amp_part, 2 * (size_t)c->nblk));
+    TRY(dalloc(&c->amp_alt, 2 * (size_t)c->nblk));
+    c->nfr = 1;
+    TRY(dalloc(&c->fr_part, 1));
+    TRY(dalloc(&c->dst, 1));
+    CK(cudaMemset(c->dst, 0, sizeof(StepState)));
+    CK(cudaMallocHost(&c->hst, sizeof(StepState)));
+    memset(c->hst, 0, sizeof(StepState));
+    TRY(dalloc(&c->err, 1));
+    CK(cudaMemset(c->err, 0, sizeof(int)));
+    c->store_sig = !c->planes.empty();
+    CK(cudaStreamSynchronize(c->st));
+    return RELAX_OK;
+}
+
+extern "C" int relax_create(const relax_config *cfg, int device, relax_ctx **out)
+{
+    if (!cfg || !out) return fail(RELAX_ERR_ARG, "null argument");
+    *out = nullptr;
+    relax_ctx *c = new relax_ctx();
+    int rc = create(cfg, device, c);
+    if (rc != RELAX_OK) {
+        free_ctx(c);
+        return rc;
+    }
+    *out = c;
+    return RELAX_OK;
+}
+
+extern "C" int relax_destroy(relax_ctx *c)
+{
+    free_ctx(c);
+    return RELAX_OK;
+}
+
+extern "C" int relax_get_stream(relax_ctx *c, void **s)
+{
+    if (!c || !s) return fail(RELAX_ERR_ARG, "null argument");
+    *s = (void *)c->st;
+    return RELAX_OK;
+}
+
+extern "C" int relax_synchronize(relax_ctx *c)
+{
+    if (!c) return fail(RELAX_ERR_ARG, "null context");
+    CK(cudaStreamSynchronize(c->st));
+    return RELAX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// step pieces
+// ---------------------------------------------------------------------------
+static StressArgs stress_args(relax_ctx *c, const float *w)
+{
+    const Grid &g = c->g;
+    StressArgs a{};
+    a.g = g;
+    a.w = w;
+    a.tau = c->tau; a.m = c->m; a.sig = c->sig; a.gamma = c->gamma;
+    a.dg0[0] = c->dg0[0]; a.dg0[1] = c->dg0[1];
+    a.visc[0] = c->visc[0]; a.visc[1] = c->visc[1];
+    a.spdev = c->spdev;
+    a.st = c->dst;
+    a.k1 = (float)(0.5 / g.dx1); a.k2 = (float)(0.5 / g.dx2);
+    a.k3 = (float)(0.5 / g.dx3); a.k3b = (float)(1.0 / g.dx3);
+    a.lam = (float)c->cfg.lambda; a.mu2 = (float)(2.0 * c->cfg.mu); a.muinv = (float)(1.0 / c->cfg.mu);
+    a.store_sig = c->store_sig;
+    a.tm_part = c->tm_part;
+    a.amp_part = c->amp_part;
+    return a;
+}
+
+template <int MODE>
+static int launch_stress(relax_ctx *c, StressArgs a)
+{
+    const int stage = MODE == MODE_END ? ST_STRESS_END : MODE == MODE_CORR ? ST_STRESS_CORR
+                      : MODE == MODE_INIT ? ST_STRESS_INIT : ST_OTHER;
+    TIMED(&c->prof, stage, c->st, (k_stress<MODE><<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(a)));
+    return RELAX_OK;
+}
+
+static XfArgs xf_div(relax_ctx *c)
+{
+    XfArgs x{};
+    const Grid &g = c->g;
+    x.m = c->m;
+    x.k1 = (float)(0.5 / g.dx1); x.k2 = (float)(0.5 / g.dx2);
+    x.k3 = (float)(0.5 / g.dx3); x.k3b = (float)(1.0 / g.dx3);
+    x.tload = nullptr;
+    return x;
+}
+
+static XiArgs xi_update(relax_ctx *c, float *out, const float *base, float cmul, bool use_dt)
+{
+    XiArgs x{};
+    const Grid &g = c->g;
+    for (int k = 0; k < 3; k++) {
+        x.out[k] = out + k * g.nh;
+        x.base[k] = base ? base + k * g.nh : nullptr;
+    }
+    x.rp = g.sx1; x.pp = g.plane;
+    x.st = use_dt ? c->dst : nullptr;
+    x.cmul = cmul;
+    return x;
+}
+
+// surface loads (traction, src/elastic3d.f90:2517-2590) into tload
+static int upload_loads(relax_ctx *c, const EventCopy &ev, double t, double Dt, bool rate, bool *any)
+{
+    *any = false;
+    if (ev.l.empty()) return RELAX_OK;
+    const Grid &g = c->g;
+    std::vector<float> h(g.plane, 0.f);
+    for (const auto &l : ev.l) {
+        const double L = l.length, W = l.width, beta = l.beta;
+        const double Lp = L * (1.0 + 2.0 * beta) / 2.0, Wp = W * (1.0 + 2.0 * beta) / 2.0;
+        if (Lp == 0 || Wp == 0) continue;
+        const double mm = std::max(Lp, Wp);
+        for (int i2 = 0; i2 < g.sx2; i2++)
+            for (int i1 = 0; i1 < g.sx1; i1++) {
+                const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+                const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+                if (fabs(x1 - l.x) > mm || fabs(x2 - l.y) > mm) continue;
+                auto om = [beta](double x) {
+                    const double ax = fabs(x);
+                    if (ax <= (1.0 - 2.0 * beta) / (1.0 - beta) / 2.0) return 1.0;
+                    if (ax < 1.0 / (1.0 - beta) / 2.0) {
+                        const double cc = cos(M_PI * ((1.0 - beta) * ax - 0.5 + beta) / 2.0 / beta);
+                        return cc * cc;
+                    }
+                    return 0.0;
+                };
+                const double amp = om((x1 - l.x) / L) * om((x2 - l.y) / W) * l.slip;
+                float &v = h[(size_t)i2 * g.sx1 + i1];
+                if (rate) {
+                    if (l.period != 0)
+                        v = (float)(v - amp * (sin(2 * M_PI * (t + Dt) / l.period + l.phase) -
+                                               sin(2 * M_PI * t / l.period + l.phase)) / Dt);
+                } else {
+                    v = (float)(l.period == 0 ? v - amp : v - amp * sin(2 * M_PI * t / l.period + l.phase));
+                }
+            }
+    }
+    CK(cudaMemcpyAsync(c->tload, h.data(), g.plane * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    *any = true;
+    return RELAX_OK;
+}
+
+// shear sources of one event: body force + traction into work/twork, and
+// the relaxed moment density into tau (dislocations, src/relax.f90:1116-1289)
+static int event_sources(relax_ctx *c, const EventCopy &ev, bool *any)
+{
+    const Grid &g = c->g;
+    CK(cudaMemsetAsync(c->work, 0, 3 * g.nh * sizeof(float), c->st));
+    CK(cudaMemsetAsync(c->twork, 0, 3 * g.plane * sizeof(float), c->st));
+    const double mind = std::min(std::min(g.dx1, g.dx2), g.dx3);
+    for (const auto &s : ev.s) {
+        SrcArgs a{};
+        a.g = g; a.mu = c->cfg.mu; a.s = s.slip; a.x = s.x; a.y = s.y; a.z = s.z;
+        a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.rake = s.rake; a.beta = s.beta;
+        for (int k = 0; k < 3; k++) { a.f[k] = c->work + k * g.nh; a.t[k] = c->twork + k * g.plane; }
+        a.tau = c->tau;
+        if (c->cfg.nyquist * mind < s.length || c->cfg.nyquist * mind < s.width) {
+            k_source_traction<<<nblocks(g.plane), RELAX_NTHREADS, 0, c->st>>>(a);
+            CKL();
+            k_source_force<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+            CKL();
+        }
+    }
+    for (const auto &s : ev.s) {
+        SrcArgs a{};
+        a.g = g; a.mu = c->cfg.mu; a.s = s.slip; a.x = s.x; a.y = s.y; a.z = s.z;
+        a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.rake = s.rake; a.beta = s.beta;
+        a.tau = c->tau;
+        k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
+    }
+    *any = !ev.s.empty() || !ev.l.empty();
+    return RELAX_OK;
+}
+
+// coseismic Green's function of work/twork; u += result
+static int event_green(relax_ctx *c, bool loads)
+{
+    const Grid &g = c->g;
+    XfArgs xa{};
+    for (int k = 0; k < 3; k++) {
+        xa.in[k] = c->work + k * g.nh;
+        xa.tin[k] = c->twork + k * g.plane;
+    }
+    xa.rp = g.sx1; xa.pp = g.plane; xa.trp = g.sx1;
+    xa.tload = loads ? c->tload : nullptr;
+    XiArgs xi = xi_update(c, c->u, c->u, 1.0f, false);
+    return c->sp.green(xa, false, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st);
+}
+
+static int friction_planes(relax_ctx *c, bool want_tm, int *nblk_out)
+{
+    const Grid &g = c->g;
+    int blk_total = 0;
+    *nblk_out = 0;
+    for (size_t k = 0; k < c->planes.size(); k++) {
+        const relax_plane &p = c->planes[k];
+        FrictionArgs a{};
+        a.g = g;
+        a.x = p.x; a.y = p.y; a.z = p.z; a.L = p.width; a.W = p.length;
+        a.strike = p.strike; a.dip = p.dip; a.rake = p.rake; a.beta = c->cfg.beta; a.mu = c->cfg.mu;
+        a.fc = c->fcd; a.sig = c->sig; a.m = c->m; a.err = c->err; a.want_tm = want_tm;
+        const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+        const double mw = std::max(Wp, Lp);
+        // x1 index box (shifted coordinates j*dx1, j in [-sx1/2, sx1/2-1])
+        int j1lo = (int)ceil((p.x - mw) / g.dx1) - 1, j1hi = (int)floor((p.x + mw) / g.dx1) + 1;
+        j1lo = std::max(j1lo, -g.sx1 / 2); j1hi = std::min(j1hi, g.sx1 / 2 - 1);
+        int j2lo = (int)ceil((p.y - mw) / g.dx2) - 1, j2hi = (int)floor((p.y + mw) / g.dx2) + 1;
+        j2lo = std::max(j2lo, -g.sx2 / 2); j2hi = std::min(j2hi, g.sx2 / 2 - 1);
+        const double zlo = std::min(p.z, -p.z) - Lp, zhi = std::max(p.z, -p.z) + Lp;
+        int i3lo = std::max(0, (int)floor(zlo / g.dx3) - 1), i3hi = std::min(g.sx3h - 1, (int)ceil(zhi / g.dx3) + 1);
+        if (j1hi < j1lo || j2hi < j2lo || i3hi < i3lo) continue;
+        a.j1lo = j1lo; a.n1 = j1hi - j1lo + 1; a.j2lo = j2lo; a.n2 = j2hi - j2lo + 1;
+        a.i3lo = i3lo; a.n3 = i3hi - i3lo + 1;
+        const size_t n = (size_t)a.n1 * a.n2 * a.n3;
+        const int nb = (int)nblocks(n);
+        if (want_tm) {
+            if (blk_total + nb > c->nfr) {
+                // grow the partial array (stream-ordered free/alloc)
+                CK(cudaStreamSynchronize(c->st));
+                float *np = nullptr;
+                TRY(dalloc(&np, (size_t)(blk_total + nb) * 2));
+                if (c->fr_part) {
+                    CK(cudaMemcpy(np, c->fr_part, c->nfr * sizeof(float), cudaMemcpyDeviceToDevice));
+                    cudaFree(c->fr_part);
+                }
+                c->fr_part = np;
+                c->nfr = (blk_total + nb) * 2;
+            }
+            a.tm_part = c->fr_part + blk_total;
+        }
+        TIMED(&c->prof, ST_FRICTION, c->st, (k_friction<<<nb, RELAX_NTHREADS, 0, c->st>>>(a)));
+        blk_total += nb;
+    }
+    *nblk_out = blk_total;
+    return RELAX_OK;
+}
+
+static int monitor_planes(relax_ctx *c, bool with_dt)
+{
+    for (size_t k = 0; k < c->planes.size(); k++) {
+        const relax_plane &p = c->planes[k];
+        const int n = std::max(0, p.px2) * std::max(0, p.px3);
+        if (n == 0) continue;
+        MonitorArgs a{};
+        a.g = c->g;
+        a.x = p.x; a.y = p.y; a.z = p.z; a.strike = p.strike; a.dip = p.dip; a.rake = p.rake;
+        a.fc = c->fcd; a.sig = c->sig; a.patch = c->patch + c->patch_off[k];
+        a.px2 = p.px2; a.px3 = p.px3;
+        a.st = with_dt ? c->dst : nullptr;
+        TIMED(&c->prof, ST_MONITOR, c->st, (k_monitor<<<nblocks(n, 128), 128, 0, c->st>>>(a)));
+    }
+    return RELAX_OK;
+}
+
+static int check_err(relax_ctx *c)
+{
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (h & (1 << RELAX_ERR_FRICTION))
+        return fail(RELAX_ERR_FRICTION, "wrong value of (a-b)sigma: tau/((a-b)sigma) > 20");
+    return RELAX_OK;
+}
+
+// sig = -tau + C:E(u), next predictor moment, log amplitude of tau
+static int tail_init(relax_ctx *c)
+{
+    TRY(launch_stress<MODE_INIT>(c, stress_args(c, c->u)));
+    k_reduce_amp<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->amp_part, c->nblk, nullptr,
+                                                    c->g.dx1 * c->g.dx2 * c->g.dx3);
+    CKL();
+    c->m_valid = true;
+    c->sig_valid = c->store_sig;
+    return RELAX_OK;
+}
+
+extern "C" int relax_coseismic(relax_ctx *c, int e, relax_step_log *log0)
+{
+    if (!c) return fail(RELAX_ERR_ARG, "null context");
+    if (e < 0 || e >= (int)c->events.size()) return fail(RELAX_ERR_ARG, "event %d out of range", e);
+    CK(cudaSetDevice(c->device));
+    bool any = false, loads = false;
+    TRY(event_sources(c, c->events[e], &any));
+    TRY(upload_loads(c, c->events[e], c->t, 0.0, false, &loads));
+    if (any) TRY(event_green(c, loads));
+    TRY(tail_init(c));
+    CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (e == 0) { c->t = 0.0; c->i = 0; c->oi = 1; }
+    c->e = e;
+    c->cos_done = true;
+    if (log0) {
+        memset(log0, 0, sizeof *log0);
+        log0->i = 0;
+        log0->cei = c->hst->cei;
+    }
+    return RELAX_OK;
+}
+
+static DtPolicy policy(relax_ctx *c)
+{
+    DtPolicy p{};
+    p.interval = c->cfg.interval; p.odt = c->cfg.odt; p.tscale = c->cfg.tscale; p.skip = c->cfg.skip;
+    p.has_next_event = c->e < (int)c->events.size() - 1;
+    p.next_event_time = p.has_next_event ? c->events[c->e + 1].time : 0.0;
+    p.has_inter = !c->inter.s.empty() || !c->inter.ts.empty();
+    p.mech[0] = !c->lin.empty();
+    p.mech[1] = !c->non.empty();
+    p.mech[2] = !c->fc.empty();
+    return p;
+}
+
+static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
+{
+    const Grid &g = c->g;
+    const double STEP_MAX = 1e7;
+    (void)STEP_MAX;
+    if (!c->cos_done) TRY(relax_coseismic(c, 0, nullptr));
+    if (!c->m_valid) TRY(tail_init(c));
+    memset(log, 0, sizeof *log);
+    if (c->t >= c->cfg.interval) return RELAX_OK;
+
+    // ---- predictor -------------------------------------------------------
+    int nfr = 0;
+    if (!c->fc.empty()) TRY(friction_planes(c, true, &nfr));
+    c->hst->use_override = dt_override ? 1 : 0;
+    c->hst->dt_override = dt_override ? *dt_override : 0.0;
+    c->hst->t = c->t;
+    c->hst->oi = c->oi;
+    CK(cudaMemcpyAsync(c->dst, c->hst, sizeof(StepState), cudaMemcpyHostToDevice, c->st));
+    TIMED(&c->prof, ST_DT, c->st,
+          (k_dt<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, policy(c), c->tm_part, c->nblk, c->fr_part, nfr)));
+    CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double Dt = c->hst->Dt;
+    double mw[3] = {c->hst->maxwell[0], c->hst->maxwell[1], c->hst->maxwell[2]};
+    if (!(Dt > 0.0) || !std::isfinite(Dt)) return fail(RELAX_ERR_ARG, "invalid time step %g", Dt);
+
+    const EventCopy &ev = c->events[c->e];
+    bool loads = false;
+    // note: the reference passes Dt/2.d8 here (src/relax.f90:685)
+    TRY(upload_loads(c, ev, c->t, Dt / 2.0e8, true, &loads));
+    {
+        XfArgs xa = xf_div(c);
+        xa.tload = loads ? c->tload : nullptr;
+        XiArgs xi = xi_update(c, c->vp, c->u, 0.5f, true);
+        TRY(c->sp.green(xa, true, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st));
+    }
+    // ---- corrector -------------------------------------------------------
+    TRY(launch_stress<MODE_CORR>(c, stress_args(c, c->vp)));
+    if (!c->fc.empty()) {
+        int unused = 0;
+        TRY(friction_planes(c, false, &unused));
+        TRY(monitor_planes(c, true));
+    }
+    if (!c->inter.s.empty()) {
+        for (const auto &s : c->inter.s) {
+            SrcArgs a{};
+            a.g = g; a.mu = c->cfg.mu; a.s = s.slip; a.x = s.x; a.y = s.y; a.z = s.z;
+            a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.rake = s.rake; a.beta = s.beta;
+            a.tau = c->m;
+            k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+            CKL();
+            a.tau = c->tau;   // src/relax.f90:1228-1235 also adds it to tau
+            k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+            CKL();
+        }
+    }
+    TRY(upload_loads(c, ev, c->t, Dt, true, &loads));
+    {
+        XfArgs xa = xf_div(c);
+        xa.tload = loads ? c->tload : nullptr;
+        XiArgs xi = xi_update(c, c->u, c->u, 1.0f, true);
+        TRY(c->sp.green(xa, true, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st));
+    }
+    c->t = c->t + Dt;
+    c->i++;
+    int fired = 0;
+    if (c->e < (int)c->events.size() - 1 && fabs(c->t - c->events[c->e + 1].time) < 1e-6) {
+        // tau += Dt m, then the coseismic event, then the stress
+        k_tau_update<<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(g, c->tau, c->m, c->dst, c->amp_alt);
+        CKL();
+        c->e++;
+        fired = 1;
+        bool any = false, ld = false;
+        TRY(event_sources(c, c->events[c->e], &any));
+        TRY(upload_loads(c, c->events[c->e], c->t, 0.0, false, &ld));
+        TRY(event_green(c, ld));
+        TRY(launch_stress<MODE_INIT>(c, stress_args(c, c->u)));
+        k_reduce_amp<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->amp_part, c->nblk, c->amp_alt,
+                                                        g.dx1 * g.dx2 * g.dx3);
+        CKL();
+    } else {
+        TRY(launch_stress<MODE_END>(c, stress_args(c, c->u)));
+        TIMED(&c->prof, ST_REDUCE, c->st,
+              (k_reduce_amp<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->amp_part, c->nblk, nullptr,
+                                                             g.dx1 * g.dx2 * g.dx3)));
+    }
+    c->m_valid = true;
+    c->sig_valid = c->store_sig;
+    // isoutput, src/relax.f90:1364-1376
+    {
+        const double odt = c->cfg.odt, etime = c->events[c->e].time;
+        if ((0 == c->cfg.skip && fabs(c->t - c->oi * odt) < 1e-6 * odt) ||
+            (0 < c->cfg.skip && ((c->i - 1) % c->cfg.skip) == 0) || fabs(c->t - etime) < 1e-6)
+            c->oi++;
+    }
+    if (!c->fc.empty()) TRY(check_err(c));
+    CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    log->i = c->i;
+    log->event = fired;
+    log->dt = Dt;
+    log->tm_ve = mw[0]; log->tm_pl = mw[1]; log->tm_as = mw[2];
+    log->t = c->t;
+    log->power = c->hst->power;
+    log->cei = c->hst->cei;
+    return RELAX_OK;
+}
+
+extern "C" int relax_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
+{
+    if (!c || !log) return fail(RELAX_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->device));
+    return do_step(c, dt_override, log);
+}
+
+extern "C" int relax_run(relax_ctx *c, int max_steps, const double *dt_schedule, relax_step_log *logs,
+                         int *nsteps_done)
+{
+    if (!c || !logs) return fail(RELAX_ERR_ARG, "null argument");
+    if (c->cos_done) return fail(RELAX_ERR_STATE, "relax_run needs a context that has not been stepped");
+    CK(cudaSetDevice(c->device));
+    if (nsteps_done) *nsteps_done = 0;
+    TRY(relax_coseismic(c, 0, &logs[0]));
+    for (int k = 0; k < max_steps; k++) {
+        relax_step_log lg;
+        TRY(do_step(c, dt_schedule ? &dt_schedule[k] : nullptr, &lg));
+        if (lg.i == 0) break;
+        logs[k + 1] = lg;
+        if (nsteps_done) *nsteps_done = k + 1;
+    }
+    return RELAX_OK;
+}
+
+extern "C" int relax_get_time(relax_ctx *c, double *t, int *i, int *e)
+{
+    if (!c) return fail(RELAX_ERR_ARG, "null context");
+    if (t) *t = c->t;
+    if (i) *i = c->i;
+    if (e) *e = c->e;
+    return RELAX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// field access in the reference layout
+// ---------------------------------------------------------------------------
+__global__ void k_scale(float *p, size_t n, float s)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) p[q] *= s;
+}
+
+static int field_sig(relax_ctx *c)
+{
+    const Grid &g = c->g;
+    if (c->sig_valid) return RELAX_OK;
+    CK(cudaMemcpyAsync(c->sig, c->tau, 6 * g.nh * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+    k_scale<<<nblocks(6 * g.nh), RELAX_NTHREADS, 0, c->st>>>(c->sig, 6 * g.nh, -1.f);
+    CKL();
+    StressArgs a = stress_args(c, c->u);
+    TRY(launch_stress<MODE_OP>(c, a));
+    c->sig_valid = true;
+    return RELAX_OK;
+}
+
+extern "C" int relax_get_field(relax_ctx *c, int which, void *host, size_t bytes)
+{
+    if (!c || !host) return fail(RELAX_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->device));
+    const Grid &g = c->g;
+    const size_t nvec = (size_t)(g.sx1 + 2) * g.sx2 * g.sx3h;
+    float *tmp = nullptr;
+    switch (which) {
+    case RELAX_FIELD_U:
+    case RELAX_FIELD_GAMMA: {
+        const int nc = which == RELAX_FIELD_U ? 3 : 1;
+        if (bytes != nc * nvec * sizeof(float)) return fail(RELAX_ERR_ARG, "field size %zu != %zu", bytes, nc * nvec * sizeof(float));
+        TRY(dalloc(&tmp, nc * nvec));
+        const float *src = which == RELAX_FIELD_U ? c->u : c->gamma;
+        for (int k = 0; k < nc; k++) {
+            k_pad<<<nblocks(nvec), RELAX_NTHREADS, 0, c->st>>>(src + k * g.nh, tmp + k * nvec, g.sx1,
+                                                                  (size_t)g.sx2 * g.sx3h);
+        }
+        break;
+    }
+    case RELAX_FIELD_SIG:
+    case RELAX_FIELD_TAU:
+    case RELAX_FIELD_MOMENT: {
+        if (bytes != g.nh * sizeof(relax_tensor)) return fail(RELAX_ERR_ARG, "field size %zu != %zu", bytes, g.nh * sizeof(relax_tensor));
+        if (which == RELAX_FIELD_SIG) TRY(field_sig(c));
+        const float *src = which == RELAX_FIELD_SIG ? c->sig : which == RELAX_FIELD_TAU ? c->tau : c->m;
+        TRY(dalloc(&tmp, 6 * g.nh));
+        k_soa_to_aos<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(src, (relax_tensor *)tmp, g.nh);
+        break;
+    }
+    default:
+        return fail(RELAX_ERR_ARG, "unknown field %d", which);
+    }
+    CKL();
+    CK(cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    cudaFree(tmp);
+    return RELAX_OK;
+}
+
+extern "C" int relax_set_field(relax_ctx *c, int which, const void *host, size_t bytes)
+{
+    if (!c || !host) return fail(RELAX_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->device));
+    const Grid &g = c->g;
+    const size_t nvec = (size_t)(g.sx1 + 2) * g.sx2 * g.sx3h;
+    float *tmp = nullptr;
+    switch (which) {
+    case RELAX_FIELD_U:
+    case RELAX_FIELD_GAMMA: {
+        const int nc = which == RELAX_FIELD_U ? 3 : 1;
+        if (bytes != nc * nvec * sizeof(float)) return fail(RELAX_ERR_ARG, "field size mismatch");
+        TRY(dalloc(&tmp, nc * nvec));
+        CK(cudaMemcpyAsync(tmp, host, bytes, cudaMemcpyHostToDevice, c->st));
+        float *dst = which == RELAX_FIELD_U ? c->u : c->gamma;
+        for (int k = 0; k < nc; k++)
+            k_unpad<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(tmp + k * nvec, dst + k * g.nh, g.sx1,
+                                                                 (size_t)g.sx2 * g.sx3h);
+        break;
+    }
+    case RELAX_FIELD_SIG:
+    case RELAX_FIELD_TAU:
+    case RELAX_FIELD_MOMENT: {
+        if (bytes != g.nh * sizeof(relax_tensor)) return fail(RELAX_ERR_ARG, "field size mismatch");
+        TRY(dalloc(&tmp, 6 * g.nh));
+        CK(cudaMemcpyAsync(tmp, host, bytes, cudaMemcpyHostToDevice, c->st));
+        float *dst = which == RELAX_FIELD_SIG ? c->sig : which == RELAX_FIELD_TAU ? c->tau : c->m;
+        k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>((const relax_tensor *)tmp, dst, g.nh);
+        break;
+    }
+    default:
+        return fail(RELAX_ERR_ARG, "unknown field %d", which);
+    }
+    CKL();
+    CK(cudaStreamSynchronize(c->st));
+    cudaFree(tmp);
+    if (which == RELAX_FIELD_SIG) c->sig_valid = true;
+    else c->m_valid = false, c->sig_valid = false;
+    if (which == RELAX_FIELD_MOMENT) c->m_valid = true;
+    return RELAX_OK;
+}
+
+extern "C" int relax_get_patches(relax_ctx *c, int k, relax_slippatch *host, size_t n)
+{
+    if (!c || !host) return fail(RELAX_ERR_ARG, "null argument");
+    if (k < 0 || k >= (int)c->planes.size()) return fail(RELAX_ERR_ARG, "plane %d out of range", k);
+    const size_t np = (size_t)std::max(0, c->planes[k].px2) * std::max(0, c->planes[k].px3);
+    if (n != np) return fail(RELAX_ERR_ARG, "plane %d has %zu patches", k, np);
+    CK(cudaMemcpyAsync(host, c->patch + c->patch_off[k], np * sizeof(relax_slippatch), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return RELAX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stateless operators on device buffers in the reference layout
+// ---------------------------------------------------------------------------
+struct Scratch {
+    std::vector<void *> p;
+    cudaStream_t st;
+    explicit Scratch(cudaStream_t s) : st(s) {}
+    template <typename T>
+    int get(T **out, size_t n)
+    {
+        void *q = nullptr;
+        cudaError_t e = cudaMallocAsync(&q, std::max<size_t>(n, 1) * sizeof(T), st);
+        if (e != cudaSuccess) return fail(RELAX_ERR_NOMEM, "cudaMallocAsync: %s", cudaGetErrorString(e));
+        p.push_back(q);
+        *out = (T *)q;
+        return RELAX_OK;
+    }
+    ~Scratch()
+    {
+        for (void *q : p) cudaFreeAsync(q, st);
+    }
+};
+
+static StressArgs op_args(const Grid &g, double lambda, double mu)
+{
+    StressArgs a{};
+    a.g = g;
+    a.k1 = (float)(0.5 / g.dx1); a.k2 = (float)(0.5 / g.dx2);
+    a.k3 = (float)(0.5 / g.dx3); a.k3b = (float)(1.0 / g.dx3);
+    a.lam = (float)lambda; a.mu2 = (float)(2.0 * mu); a.muinv = (float)(1.0 / mu);
+    return a;
+}
+
+extern "C" int relax_op_stressupdate(const float *u1, const float *u2, const float *u3, double lambda,
+                                     double mu, double dx1, double dx2, double dx3, int sx1, int sx2,
+                                     int sx3h, relax_tensor *sig, void *stream)
+{
+    Grid g;
+    TRY(make_grid(g, sx1, sx2, 2 * sx3h, dx1, dx2, dx3));
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc(st);
+    float *w, *s;
+    TRY(sc.get(&w, 3 * g.nh));
+    TRY(sc.get(&s, 6 * g.nh));
+    const float *us[3] = {u1, u2, u3};
+    for (int k = 0; k < 3; k++)
+        k_unpad<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(us[k], w + k * g.nh, sx1, (size_t)sx2 * sx3h);
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(sig, s, g.nh);
+    StressArgs a = op_args(g, lambda, mu);
+    a.w = w;
+    a.sig = s;
+    k_stress<MODE_OP><<<nblocks(g.nh / 4), RELAX_NTHREADS, 0, st>>>(a);
+    k_soa_to_aos<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(s, sig, g.nh);
+    CKL();
+    return RELAX_OK;
+}
+
+extern "C" int relax_op_bodyforce(const relax_tensor *sig, double dx1, double dx2, double dx3, int sx1,
+                                  int sx2, int sx3h, float *c1, float *c2, float *c3, float *t1, float *t2,
+                                  float *t3, void *stream)
+{
+    Grid g;
+    TRY(make_grid(g, sx1, sx2, 2 * sx3h, dx1, dx2, dx3));
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc(st);
+    float *s;
+    TRY(sc.get(&s, 6 * g.nh));
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(sig, s, g.nh);
+    k_bodyforce<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(g, s, c1, c2, c3, t1, t2, t3, (float)(0.5 / dx1),
+                                                          (float)(0.5 / dx2), (float)(0.5 / dx3), (float)(1.0 / dx3));
+    CKL();
+    return RELAX_OK;
+}
+
+extern "C" int relax_op_viscouseigenstress(double mu, const relax_layer *structure,
+                                           const relax_tensor_layer *prestress, const relax_tensor *sig,
+                                           int sx1, int sx2, int sx3h, relax_tensor *moment,
+                                           double *maxwelltime, float *gamma, const float *dgammadot0,
+                                           void *stream)
+{
+    Grid g;
+    TRY(make_grid(g, sx1, sx2, 2 * sx3h, 1.0, 1.0, 1.0));
+    if (!structure) return fail(RELAX_ERR_ARG, "null structure");
+    for (int i = 0; i < sx3h; i++)
+        if (structure[i].stressexponent < 0.999999) return fail(RELAX_ERR_POWER, "invalid power exponent");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc(st);
+    std::vector<float> spdev;
+    std::vector<DepthVisc> dv;
+    prestress_terms(prestress, sx3h, mu, structure, &spdev, &dv);
+    float *s, *mo, *gm = nullptr, *spd = nullptr, *tmp;
+    DepthVisc *dvd;
+    double *amp;
+    const int nb = (int)nblocks(g.nh / 4);
+    TRY(sc.get(&s, 6 * g.nh));
+    TRY(sc.get(&mo, 6 * g.nh));
+    TRY(sc.get(&dvd, sx3h));
+    TRY(sc.get(&tmp, 2 * (size_t)nb));
+    TRY(sc.get(&amp, 2 * (size_t)nb));
+    CK(cudaMemcpyAsync(dvd, dv.data(), sx3h * sizeof(DepthVisc), cudaMemcpyHostToDevice, st));
+    if (prestress) {
+        TRY(sc.get(&spd, 6 * (size_t)sx3h));
+        CK(cudaMemcpyAsync(spd, spdev.data(), 6 * sx3h * sizeof(float), cudaMemcpyHostToDevice, st));
+    }
+    if (gamma) {
+        TRY(sc.get(&gm, g.nh));
+        k_unpad<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(gamma, gm, sx1, (size_t)sx2 * sx3h);
+    }
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(sig, s, g.nh);
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(moment, mo, g.nh);
+    StressArgs a = op_args(g, 1.0, mu);
+    a.sig = s; a.m = mo; a.gamma = gm; a.visc[0] = dvd; a.spdev = spd;
+    a.dg0[0] = dgammadot0;
+    a.tm_part = tmp; a.amp_part = amp;
+    k_stress<MODE_EIGEN><<<nb, RELAX_NTHREADS, 0, st>>>(a);
+    k_soa_to_aos<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(mo, moment, g.nh);
+    if (gamma)   // back into the first sx1 entries of each padded row
+        k_repad<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(gm, gamma, sx1, (size_t)sx2 * sx3h);
+    CKL();
+    if (maxwelltime) {
+        std::vector<float> h(nb);
+        CK(cudaMemcpyAsync(h.data(), tmp, nb * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        float tm = (float)*maxwelltime;
+        for (float v : h) tm = std::min(tm, v);
+        *maxwelltime = std::min((double)tm, *maxwelltime);
+    }
+    return RELAX_OK;
+}
+
+extern "C" int relax_op_frictioneigenstress(double x, double y, double z, double L, double W, double strike,
+                                            double dip, double rake, double beta, const relax_tensor *sig,
+                                            double mu, const relax_layer *structure, int sx1, int sx2,
+                                            int sx3h, double dx1, double dx2, double dx3,
+                                            relax_tensor *moment, double *maxwelltime, void *stream)
+{
+    // a private context-free run of the plane kernel
+    Grid g;
+    TRY(make_grid(g, sx1, sx2, 2 * sx3h, dx1, dx2, dx3));
+    if (!structure) return fail(RELAX_ERR_ARG, "null structure");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc(st);
+    float *s, *mo;
+    double *fcd;
+    int *err;
+    TRY(sc.get(&s, 6 * g.nh));
+    TRY(sc.get(&mo, 6 * g.nh));
+    TRY(sc.get(&fcd, 4 * (size_t)sx3h));
+    TRY(sc.get(&err, 1));
+    std::vector<double> h(4 * (size_t)sx3h);
+    for (int i3 = 0; i3 < sx3h; i3++) {
+        h[i3] = structure[i3].gammadot0; h[sx3h + i3] = structure[i3].stressexponent;
+        h[2 * sx3h + i3] = structure[i3].friction; h[3 * sx3h + i3] = structure[i3].cohesion;
+    }
+    CK(cudaMemcpyAsync(fcd, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(sig, s, g.nh);
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(moment, mo, g.nh);
+    FrictionArgs a{};
+    a.g = g; a.x = x; a.y = y; a.z = z; a.L = L; a.W = W; a.strike = strike; a.dip = dip; a.rake = rake;
+    a.beta = beta; a.mu = mu; a.fc = fcd; a.sig = s; a.m = mo; a.err = err; a.want_tm = maxwelltime != nullptr;
+    a.j1lo = -sx1 / 2; a.n1 = sx1; a.j2lo = -sx2 / 2; a.n2 = sx2; a.i3lo = 0; a.n3 = sx3h;
+    const int nb = (int)nblocks(g.nh);
+    float *tmp;
+    TRY(sc.get(&tmp, nb));
+    a.tm_part = tmp;
+    k_friction<<<nb, RELAX_NTHREADS, 0, st>>>(a);
+    k_soa_to_aos<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(mo, moment, g.nh);
+    CKL();
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    std::vector<float> ht(nb);
+    if (maxwelltime) CK(cudaMemcpyAsync(ht.data(), tmp, nb * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (maxwelltime) {
+        float tm = (float)*maxwelltime;
+        for (float v : ht) tm = std::min(tm, v);
+        *maxwelltime = std::min((double)tm, *maxwelltime);
+    }
+    if (herr) return fail(RELAX_ERR_FRICTION, "wrong value of (a-b)sigma: tau/((a-b)sigma) > 20");
+    return RELAX_OK;
+}
+
+extern "C" int relax_op_green(float *c1, float *c2, float *c3, float *t1, float *t2, float *t3, int sx1,
+                              int sx2, int sx3, double dx1, double dx2, double dx3, double lambda, double mu,
+                              double gam, void *stream)
+{
+    Grid g;
+    TRY(make_grid(g, sx1, sx2, sx3, dx1, dx2, dx3));
+    cudaStream_t st = (cudaStream_t)stream;
+    Spectral sp;
+    int rc = sp.init(g, st);
+    if (rc != RELAX_OK) {
+        sp.release();
+        return rc;
+    }
+    XfArgs xa{};
+    float *cs[3] = {c1, c2, c3}, *ts[3] = {t1, t2, t3};
+    for (int k = 0; k < 3; k++) { xa.in[k] = cs[k]; xa.tin[k] = ts[k]; }
+    xa.rp = sx1 + 2; xa.pp = (size_t)(sx1 + 2) * sx2; xa.trp = sx1 + 2;
+    XiArgs xi{};
+    for (int k = 0; k < 3; k++) { xi.out[k] = cs[k]; xi.base[k] = nullptr; }
+    xi.rp = sx1 + 2; xi.pp = (size_t)(sx1 + 2) * sx2; xi.st = nullptr; xi.cmul = 1.f;
+    rc = sp.green(xa, false, sx3, sx3, xi, lambda, mu, gam, st);
+    cudaStreamSynchronize(st);
+    sp.release();
+    return rc;
+}
+
+__global__ void k_amp_aos(const relax_tensor *t, size_t n, double *part)
+{
+    __shared__ double shd[32];
+    double a = 0.0;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const relax_tensor v = t[q];
+        a += (double)tnorm6(v.s11, v.s12, v.s13, v.s22, v.s23, v.s33);
+    }
+    a = block_sum(a, shd);
+    if (threadIdx.x == 0) part[blockIdx.x] = a;
+}
+
+extern "C" int relax_op_tensoramplitude(const relax_tensor *t, int sx1, int sx2, int sx3h, double dx1,
+                                        double dx2, double dx3, double *amp, void *stream)
+{
+    if (!t || !amp || sx1 <= 0 || sx2 <= 0 || sx3h <= 0) return fail(RELAX_ERR_ARG, "invalid arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc(st);
+    const int nb = 296;
+    double *part;
+    TRY(sc.get(&part, nb));
+    k_amp_aos<<<nb, RELAX_NTHREADS, 0, st>>>(t, (size_t)sx1 * sx2 * sx3h, part);
+    CKL();
+    std::vector<double> h(nb);
+    CK(cudaMemcpyAsync(h.data(), part, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double s = 0;
+    for (double v : h) s += v;
+    *amp = s * (dx1 * dx2 * dx3);
+    return RELAX_OK;
+}
+
+// fft3 (src/fourier.f90:177-201) on a padded (sx1+2, sx2, sx3) array
+__global__ void k_zfft_plain(Grid g, float2 *S, FftPlan pz, int tw, int sign)
+{
+    extern __shared__ float2 sm[];
+    const int n = g.sx3;
+    const int k1t = blockIdx.x * tw, ncol = min(tw, g.K1 - k1t), k2 = blockIdx.y;
+    float2 *A = sm, *B = sm + (size_t)n * tw;
+    for (int t = threadIdx.x; t < n * tw; t += blockDim.x) {
+        const int j = t / tw, col = t % tw;
+        A[t] = col < ncol ? S[sidx(g, 0, j, k2, k1t + col)] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2 *R = sign < 0 ? fft_smem<-1>(A, B, pz, tw, tw, 1) : fft_smem<+1>(A, B, pz, tw, tw, 1);
+    for (int t = threadIdx.x; t < n * tw; t += blockDim.x) {
+        const int j = t / tw, col = t % tw;
+        if (col < ncol) S[sidx(g, 0, j, k2, k1t + col)] = R[t];
+    }
+}
+
+__global__ void k_spec_copy(Grid g, float2 *S, float *data, int to_data)
+{
+    const size_t n = (size_t)g.K1 * g.sx2 * g.sx3;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int k1 = (int)(q % g.K1), i2 = (int)((q / g.K1) % g.sx2), i3 = (int)(q / ((size_t)g.K1 * g.sx2));
+    float2 *d = reinterpret_cast<float2 *>(data + ((size_t)i3 * g.sx2 + i2) * (g.sx1 + 2)) + k1;
+    if (to_data) *d = S[sidx(g, 0, i3, i2, k1)];
+    else S[sidx(g, 0, i3, i2, k1)] = *d;
+}
+
+extern "C" int relax_op_fft3(float *data, int sx1, int sx2, int sx3, double dx1, double dx2, double dx3,
+                             int direction, void *stream)
+{
+    Grid g;
+    if (!data) return fail(RELAX_ERR_ARG, "null data");
+    if (sx1 < 4 || sx1 % 4 || !fft_size_ok(sx1 / 2) || !fft_size_ok(sx2) || !fft_size_ok(sx3))
+        return fail(RELAX_ERR_UNSUPPORTED, "FFT sizes %dx%dx%d", sx1, sx2, sx3);
+    g.sx1 = sx1; g.sx2 = sx2; g.sx3 = sx3; g.sx3h = sx3 / 2; g.M = sx1 / 2; g.K1 = sx1 / 2 + 1;
+    g.dx1 = dx1; g.dx2 = dx2; g.dx3 = dx3; g.plane = (size_t)sx1 * sx2; g.nh = g.plane * g.sx3h;
+    cudaStream_t st = (cudaStream_t)stream;
+    Spectral sp;
+    int rc = sp.init(g, st);
+    if (rc != RELAX_OK) {
+        sp.release();
+        return rc;
+    }
+    const int twz = std::max(1, std::min(16, (int)(96 * 1024 / (2 * (size_t)sx3 * 8))));
+    int tw = 1;
+    while (tw * 2 <= twz) tw *= 2;
+    const size_t smz = 2 * (size_t)sx3 * tw * sizeof(float2);
+    cudaFuncSetAttribute(k_zfft_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+    if (direction < 0) {
+        XfArgs xa{};
+        xa.g = g; xa.S = sp.S; xa.pm = sp.pm; xa.tw1 = sp.tw1; xa.nin = sx3; xa.rows = sp.rows; xa.has_trac = 0;
+        xa.in[0] = data; xa.rp = sx1 + 2; xa.pp = (size_t)(sx1 + 2) * sx2;
+        xa.scale3 = (float)(dx1 * dx2 * dx3);
+        // only component 0 is meaningful: point the others at the same data
+        xa.in[1] = data; xa.in[2] = data;
+        k_xfwd<XIN_REAL><<<dim3(sx2 / sp.rows, sx3), RELAX_NTHREADS, sp.smx, st>>>(xa);
+        YArgs ya{g, sp.S, sp.py, sp.twy, sx3, 0};
+        k_ypass<-1><<<dim3((g.K1 + sp.twy - 1) / sp.twy, sx3, 1), RELAX_NTHREADS, sp.smy, st>>>(ya);
+        k_zfft_plain<<<dim3((g.K1 + tw - 1) / tw, sx2), RELAX_NTHREADS, smz, st>>>(g, sp.S, sp.pz, tw, -1);
+        k_spec_copy<<<nblocks((size_t)g.K1 * sx2 * sx3), RELAX_NTHREADS, 0, st>>>(g, sp.S, data, 1);
+    } else {
+        k_spec_copy<<<nblocks((size_t)g.K1 * sx2 * sx3), RELAX_NTHREADS, 0, st>>>(g, sp.S, data, 0);
+        k_zfft_plain<<<dim3((g.K1 + tw - 1) / tw, sx2), RELAX_NTHREADS, smz, st>>>(g, sp.S, sp.pz, tw, +1);
+        YArgs yb{g, sp.S, sp.py, sp.twy, sx3, 0};
+        k_ypass<+1><<<dim3((g.K1 + sp.twy - 1) / sp.twy, sx3, 1), RELAX_NTHREADS, sp.smy, st>>>(yb);
+        // component 0 only: k_xinv handles 3 components; use a 1-row-per-line
+        // variant through the same kernel with out/base of components 1,2
+        // pointed at a scratch buffer
+        Scratch sc(st);
+        float *junk;
+        rc = sc.get(&junk, (size_t)(sx1 + 2) * sx2 * sx3);
+        if (rc == RELAX_OK) {
+            XiArgs xi{};
+            xi.g = g; xi.S = sp.S; xi.pm = sp.pm; xi.tw1 = sp.tw1; xi.rows = sp.rows;
+            xi.out[0] = data; xi.out[1] = junk; xi.out[2] = junk;
+            xi.base[0] = xi.base[1] = xi.base[2] = nullptr;
+            xi.rp = sx1 + 2; xi.pp = (size_t)(sx1 + 2) * sx2; xi.st = nullptr; xi.cmul = 1.f;
+            xi.scale = (float)(2.0 / ((double)sx1 * dx1 * sx2 * dx2 * sx3 * dx3));
+            k_xinv<<<dim3(sx2 / sp.rows, sx3), RELAX_NTHREADS, sp.smx, st>>>(xi);
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaStreamSynchronize(st);
+    sp.release();
+    if (rc != RELAX_OK) return rc;
+    if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "relax_op_fft3: %s", cudaGetErrorString(e));
+    return RELAX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-stage device timing
+// ---------------------------------------------------------------------------
+extern "C" int relax_profile(relax_ctx *c, int enable)
+{
+    if (!c) return fail(RELAX_ERR_ARG, "null context");
+    CK(cudaStreamSynchronize(c->st));
+    c->prof.reset();
+    c->prof.on = enable != 0;
+    return RELAX_OK;
+}
+
+extern "C" int relax_profile_stages(void) { return ST_COUNT; }
+
+extern "C" int relax_profile_read(relax_ctx *c, int stage, double *total_ms, int *launches, const char **name)
+{
+    if (!c || stage < 0 || stage >= ST_COUNT) return fail(RELAX_ERR_ARG, "invalid stage");
+    CK(cudaStreamSynchronize(c->st));
+    double tot = 0.0;
+    int n = 0;
+    for (auto &rec : c->prof.recs) {
+        if (rec.first != stage || !rec.second.second) continue;
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, rec.second.first, rec.second.second));
+        tot += ms;
+        n++;
+    }
+    if (total_ms) *total_ms = tot;
+    if (launches) *launches = n;
+    if (name) *name = kStageNames[stage];
+    return RELAX_OK;
+}
+
+extern "C" int relax_launch_count(relax_ctx *c, long long *n)
+{
+    if (!c || !n) return fail(RELAX_ERR_ARG, "null argument");
+    *n = c->prof.launches;
+    return RELAX_OK;
+}

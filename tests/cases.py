@@ -1,0 +1,62 @@
+"""Small seeded decks for the parity tests (shapes of the benchmark
+workloads, sizes the CPU oracle finishes in seconds)."""
+import math
+
+import numpy as np
+
+from relax_b200.config import Event, Fault, Plane, Simulation
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def tensor_array(t):
+    """structured TENSOR array -> (..., 6) float64"""
+    return np.stack([t[n].astype(np.float64) for n in t.dtype.names], axis=-1)
+
+
+def linear_small(sx=64, sz=32, dx=1.0, steps=5):
+    """Linear Maxwell (n=1) below 6 km, vertical strike-slip fault, Dt = 0.5."""
+    return Simulation(
+        sx1=sx, sx2=sx, sx3=sz, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0, lambda_=1.0, mu=1.0,
+        gam=0.0, interval=0.5 * steps, odt=-1, tscale=5.0, linear=[(6.0, 1.0)],
+        events=[Event(0.0, [Fault(1.0, -10.0, 0.0, 0.0, 20.0, 6.0, 0.0, 90.0, 0.0)])],
+        name="linear-small")
+
+
+def powerlaw_small(sx=64, sz=32, dx=1.0, gam=8.3e-4, afterslip=True):
+    """Power-law n=3 with depth-dependent prefactor, 20-degree thrust, one
+    afterslip plane down-dip, gravity."""
+    depth = dx * sz / 2
+    nl = []
+    z = 8.0
+    while z < depth + 1e-9:
+        nl.append((z, 10.0 ** (z / 8.0 - 1.0), 3.0, 0.0))
+        z += dx
+    top = 1.0
+    bottom = top + 16.0 * math.sin(math.radians(20.0))
+    planes, fc = [], []
+    if afterslip:
+        planes = [Plane(x=-10.0, y=16.0 * math.cos(math.radians(20.0)), z=bottom, length=20.0,
+                        width=8.0, strike=0.0, dip=20.0, rake=90.0)]
+        fc = [(0.0, 1.0, 0.1, 0.0, 0.0)]
+    return Simulation(
+        sx1=sx, sx2=sx, sx3=sz, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0, lambda_=1.0,
+        mu=1.0, gam=gam, interval=1.0e6, odt=-1, tscale=1.0, nonlinear=nl, faultcreep=fc,
+        planes=planes,
+        events=[Event(0.0, [Fault(2.0, -16.0, 0.0, top, 32.0, 16.0, 0.0, 20.0, 90.0)])],
+        name="powerlaw-small")
+
+
+def two_events(sx=64, sz=32, dx=1.0):
+    """Linear Maxwell with a second coseismic event at t = 1.0 (the step
+    before it is shortened to land on the event time)."""
+    s = linear_small(sx, sz, dx, steps=8)
+    s.tscale = 3.0   # Dt = 0.3 -> steps land on 0.3, 0.6, 0.9, then 1.0
+    s.events.append(Event(1.0, [Fault(0.5, -5.0, 8.0, 0.0, 10.0, 5.0, 30.0, 60.0, 45.0)]))
+    s.name = "two-events"
+    return s

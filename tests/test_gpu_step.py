@@ -1,0 +1,124 @@
+"""Full relaxation runs on the GPU against the CPU oracle.
+
+The GPU run is adaptive; the oracle replays the GPU's Dt sequence (a fixed
+dt schedule, so that a last-bit difference in a Maxwell-time minimum cannot
+change the step size).  Tolerances (relative L2 of each field against the
+FP32 oracle): <= 1e-5 after one step, <= 1e-4 after the run; the errors
+against the FP64 oracle are asserted at the same bounds.
+"""
+import numpy as np
+import pytest
+
+from relax_b200.api import Relax
+from relax_b200.config import linear_maxwell
+
+from cases import linear_small, powerlaw_small, rel_l2, tensor_array, two_events
+
+pytestmark = pytest.mark.gpu
+
+
+def compare(gpu, ref, tol):
+    errs = {}
+    errs["u"] = rel_l2(gpu["u"][..., :-2], ref["u"][..., :-2])
+    for k in ("sig", "tau"):
+        errs[k] = rel_l2(tensor_array(gpu[k]), tensor_array(ref[k]))
+    if np.abs(ref["gamma"]).max() > 0:
+        errs["gamma"] = rel_l2(gpu["gamma"][..., :-2], ref["gamma"][..., :-2])
+    for k, v in errs.items():
+        assert v <= tol, (k, v, errs)
+    return errs
+
+
+def gpu_run(sim, nsteps):
+    with Relax(sim) as r:
+        logs = [r.coseismic()]
+        for _ in range(nsteps):
+            lg = r.step()
+            if lg[0] == 0:
+                break
+            logs.append(lg)
+        fields = {k: r.field(k) for k in ("u", "sig", "tau", "gamma")}
+        patches = [r.patches(k) for k in range(len(sim.planes))]
+    return logs, fields, patches
+
+
+def check_logs(glogs, rlogs, tol):
+    assert len(glogs) == len(rlogs)
+    for g, o in zip(glogs, rlogs):
+        assert g[0] == o[0]
+        for c in (1, 5, 6, 7):       # Dt, t, power, C:E^i
+            assert abs(g[c] - o[c]) <= tol * max(abs(o[c]), 1e-30), (g, o, c)
+        for c in (2, 3, 4):          # Maxwell times (minima over the grid)
+            assert abs(g[c] - o[c]) <= 1e-5 * abs(o[c]), (g, o, c)
+
+
+@pytest.mark.parametrize("builder,nsteps", [(linear_small, 1), (linear_small, 5),
+                                            (powerlaw_small, 1), (powerlaw_small, 6)])
+def test_run_matches_fp32_oracle(oracle32, oracle64, builder, nsteps):
+    sim = builder()
+    glogs, gf, gp = gpu_run(sim, nsteps)
+    assert len(glogs) == nsteps + 1
+    dts = [l[1] for l in glogs[1:]]
+    rlogs, rf = oracle32.run(sim, nsteps, dt_schedule=dts)
+    tol = 1e-5 if nsteps == 1 else 1e-4
+    check_logs(glogs, rlogs, 10 * tol)
+    compare(gf, rf, tol)
+    # adaptive Dt of the oracle itself agrees with the GPU's
+    alogs, _ = oracle32.run(sim, 1, fields=False)
+    assert abs(alogs[1][1] - glogs[1][1]) <= 1e-5 * alogs[1][1]
+    # error against the FP64 oracle of the same method
+    dlogs, df = oracle64.run(sim, nsteps, dt_schedule=dts)
+    compare(gf, df, tol)
+    # afterslip patches
+    for k, patches in enumerate(gp):
+        rp = rf["patches"][k]
+        v = np.array([p.v for p in patches]); vr = np.array([p.v for p in rp])
+        s = np.array([p.slip for p in patches]); sr = np.array([p.slip for p in rp])
+        assert rel_l2(v, vr) <= 10 * tol and rel_l2(s, sr) <= 10 * tol
+
+
+def test_second_event_fires_and_matches(oracle32):
+    sim = two_events()
+    glogs, gf, _ = gpu_run(sim, 5)
+    times = [l[5] for l in glogs]
+    assert any(abs(t - 1.0) < 1e-9 for t in times), times
+    dts = [l[1] for l in glogs[1:]]
+    rlogs, rf = oracle32.run(sim, len(dts), dt_schedule=dts)
+    check_logs(glogs, rlogs, 1e-4)
+    compare(gf, rf, 1e-4)
+
+
+def test_linear_maxwell_time_step_is_exact():
+    """n = 1, gammadot0 = 1: tm = 1 exactly, Dt = tm/10 * tscale = 0.5."""
+    sim = linear_small()
+    glogs, _, _ = gpu_run(sim, 3)
+    for l in glogs[1:]:
+        assert l[2] == 1.0 and l[1] == 0.5
+
+
+def test_runs_are_deterministic():
+    """No atomics on the data path: two runs are bitwise identical."""
+    sim = powerlaw_small()
+    a = gpu_run(sim, 3)
+    b = gpu_run(sim, 3)
+    assert a[0] == b[0]
+    for k in a[1]:
+        assert np.array_equal(a[1][k].view(np.uint8), b[1][k].view(np.uint8)), k
+
+
+def test_linear_maxwell_benchmark_size_matches_oracle(oracle32):
+    """The linear-Maxwell workload at its full size (128^2 x 128 box), 3 steps."""
+    sim = linear_maxwell(sx=128, sz=128, dx=0.8, steps=3)
+    glogs, gf, _ = gpu_run(sim, 3)
+    dts = [l[1] for l in glogs[1:]]
+    rlogs, rf = oracle32.run(sim, 3, dt_schedule=dts)
+    check_logs(glogs, rlogs, 1e-4)
+    compare(gf, rf, 1e-4)
+
+
+def test_state_errors():
+    sim = linear_small()
+    with Relax(sim) as r:
+        r.coseismic()
+        with pytest.raises(Exception):
+            r.run(2)   # relax_run needs a fresh context
