@@ -106,7 +106,8 @@ def test_bodyforce_matches_oracle(oracle32, sx1, sx2, sx3):
     oracle32.bodyforce(sig, dx, sx1, sx2, sx3h, cr, tr)
     dc = [dev(c[k]) for k in range(3)]
     dt = [dev(t[k]) for k in range(3)]
-    _lib.check(lib.relax_op_bodyforce(ptr(dev(sig.view(np.float32))), *dx, sx1, sx2, sx3h,
+    dsig = dev(sig.view(np.float32))   # held: a temporary's block may be reused
+    _lib.check(lib.relax_op_bodyforce(ptr(dsig), *dx, sx1, sx2, sx3h,
                                       *[ptr(x) for x in dc], *[ptr(x) for x in dt], None))
     torch.cuda.synchronize()
     gc = np.stack([x.cpu().numpy() for x in dc])
@@ -141,10 +142,11 @@ def test_viscous_eigenstress_matches_oracle(oracle32, power, prestress):
     assert rc == 0
     dm = dev(mom.view(np.float32))
     dg = dev(gamma)
+    dsig = dev(sig.view(np.float32))
     tm = C.c_double(1e7)
     _lib.check(lib.relax_op_viscouseigenstress(
         1.0, C.cast(st, C.c_void_p), None if pre is None else C.cast(pre, C.c_void_p),
-        ptr(dev(sig.view(np.float32))), sx1, sx2, sx3h, ptr(dm), C.byref(tm), ptr(dg), None, None))
+        ptr(dsig), sx1, sx2, sx3h, ptr(dm), C.byref(tm), ptr(dg), None, None))
     torch.cuda.synchronize()
     gm = dm.cpu().numpy().view(TENSOR_DTYPE).reshape(mom.shape)
     assert rel_l2(tensor_array(gm), tensor_array(mref)) < 1e-5
@@ -170,10 +172,11 @@ def test_friction_eigenstress_matches_oracle(oracle32):
                                             maxwell=1e7)
     assert rc == 0
     dm = dev(mom.view(np.float32))
+    dsig = dev(sig.view(np.float32))
     tm = C.c_double(1e7)
     _lib.check(lib.relax_op_frictioneigenstress(
         plane.x, plane.y, plane.z, plane.width, plane.length, plane.strike, plane.dip, plane.rake, 0.2,
-        ptr(dev(sig.view(np.float32))), 1.0, C.cast(st, C.c_void_p), sx1, sx2, sx3h, *dx, ptr(dm),
+        ptr(dsig), 1.0, C.cast(st, C.c_void_p), sx1, sx2, sx3h, *dx, ptr(dm),
         C.byref(tm), None))
     torch.cuda.synchronize()
     gm = dm.cpu().numpy().view(TENSOR_DTYPE).reshape(mom.shape)
@@ -198,10 +201,11 @@ def test_friction_abort_is_reported(oracle32):
     mom = np.zeros((sx3h, sx2, sx1), TENSOR_DTYPE)
     rc, _ = oracle32.frictioneigenstress(plane, 0.2, sig, 1.0, st, sx1, sx2, sx3h, (1, 1, 1), mom.copy())
     assert rc == 6
+    dsig = dev(sig.view(np.float32))
+    dmom = dev(mom.view(np.float32))
     rc = lib.relax_op_frictioneigenstress(
         plane.x, plane.y, plane.z, plane.width, plane.length, plane.strike, plane.dip, plane.rake, 0.2,
-        ptr(dev(sig.view(np.float32))), 1.0, C.cast(st, C.c_void_p), sx1, sx2, sx3h, 1.0, 1.0, 1.0,
-        ptr(dev(mom.view(np.float32))), None, None)
+        ptr(dsig), 1.0, C.cast(st, C.c_void_p), sx1, sx2, sx3h, 1.0, 1.0, 1.0, ptr(dmom), None, None)
     assert rc == 6
 
 
@@ -251,8 +255,8 @@ def test_tensoramplitude_matches_oracle(oracle32):
     t = tensors_random(rng, (16, 32, 64))
     ref = oracle32.tensoramplitude(t, (0.5, 0.5, 0.5))
     amp = C.c_double()
-    _lib.check(lib.relax_op_tensoramplitude(ptr(dev(t.view(np.float32))), 64, 32, 16, 0.5, 0.5, 0.5,
-                                            C.byref(amp), None))
+    dt_ = dev(t.view(np.float32))
+    _lib.check(lib.relax_op_tensoramplitude(ptr(dt_), 64, 32, 16, 0.5, 0.5, 0.5, C.byref(amp), None))
     assert abs(amp.value - ref) <= 1e-6 * ref
 
 
