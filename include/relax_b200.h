@@ -271,6 +271,22 @@ int relax_op_green(float *c1, float *c2, float *c3, float *t1, float *t2,
                    double dx2, double dx3, double lambda, double mu,
                    double gam, void *stream);
 
+/* greenfunctioncowling like relax_op_green, for callers that cannot
+ * allocate device memory (a host whose pool allocator owns the device, or
+ * code where cudaMalloc/cudaFree are not allowed): no allocation at all.
+ * It has no counterpart in the reference.  Its scratch is one fixed 16 MiB
+ * device array per device (held while the library is loaded), so grids
+ * whose spectrum and twiddle tables exceed 16 MiB (3*(sx3+1)*sx2*(sx1/2+1)*8
+ * + (sx1/2 + sx1 + sx2 + sx3)*8 bytes, e.g. above 128 x 128 x 64) return
+ * RELAX_ERR_ARG.  The first call on each device looks the array up
+ * (cudaGetSymbolAddress) and sets kernel attributes: make that first call
+ * before any stream capture.  All calls share the array; calls that overlap
+ * on the GPU race on it, so order them on one stream. */
+int relax_op_green_noalloc(float *c1, float *c2, float *c3, float *t1,
+                           float *t2, float *t3, int sx1, int sx2, int sx3,
+                           double dx1, double dx2, double dx3, double lambda,
+                           double mu, double gam, void *stream);
+
 /* 3-D real<->complex FFT in place on a (sx1+2, sx2, sx3) array with
  * RELAX's normalisation (src/fourier.f90:177-201): direction -1 forward
  * (x dx1 dx2 dx3), +1 inverse (/ (sx1 dx1 sx2 dx2 sx3 dx3)). */

@@ -79,6 +79,7 @@ def load() -> C.CDLL:
         "relax_op_frictioneigenstress": (I, [D, D, D, D, D, D, D, D, D, P, D, P, I, I, I, D, D, D, P,
                                              C.POINTER(D), P]),
         "relax_op_green": (I, [P, P, P, P, P, P, I, I, I, D, D, D, D, D, D, P]),
+        "relax_op_green_noalloc": (I, [P, P, P, P, P, P, I, I, I, D, D, D, D, D, D, P]),
         "relax_op_fft3": (I, [P, I, I, I, D, D, D, I, P]),
         "relax_op_tensoramplitude": (I, [P, I, I, I, D, D, D, C.POINTER(D), P]),
     }

@@ -41,6 +41,13 @@ static int fail(int code, const char *fmt, ...)
     return code;
 }
 
+// error reporting for the allocation-free operator of noalloc.cu (not exported)
+extern "C" __attribute__((visibility("hidden"))) int relax_noalloc_fail(int code, const char *msg)
+{
+    g_err = msg;
+    return code;
+}
+
 #define CK(call)                                                                          \
     do {                                                                                  \
         cudaError_t e_ = (call);                                                          \
