@@ -6,6 +6,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "rfft.cuh"
 
 namespace relax {
 // kernels and their argument types have internal linkage: each translation
@@ -647,6 +648,123 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xfwd(XfArgs a)
     }
 }
 
+
+// pass 1, register-resident: -div(m) (or the traction m_i3, or real input
+// rows) -> packed real FFT along x1 for rows of M = N1*N2 complex values; RW
+// rows of one plane per block, N2 threads per row, components in turn.
+template <int XIN, int N1, int N2, int RW>
+__global__ void __launch_bounds__(RW *N2) k_xfwd_reg(XfArgs a)
+{
+    constexpr int M = N1 * N2, Q = N1 / N2, N2P = N2 + 1;
+    constexpr int RS0 = (N1 * N2P > M + 1 ? N1 * N2P : M + 1);
+    constexpr int RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
+    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    extern __shared__ float2 smx[];
+    const Grid &g = a.g;
+    const int t = threadIdx.x % N2, r = threadIdx.x / N2;
+    const int i2 = blockIdx.x * RW + r, pi = blockIdx.y;
+    const bool trac = a.has_trac && pi == a.nin;
+    const int i3 = pi;
+    float2 *T = smx + r * RS;
+    const size_t rowo = (size_t)i2 * g.sx1;
+#pragma unroll 1
+    for (int c = 0; c < 3; c++) {
+        float2 z[N1];
+        if (XIN == XIN_DIV) {
+            const int cx = c == 0 ? 0 : c == 1 ? 1 : 2;
+            const int cy = c == 0 ? 1 : c == 1 ? 3 : 4;
+            const int cz = c == 0 ? 2 : c == 1 ? 4 : 5;
+            if (trac) {
+                const float *mt = a.m + cz * g.nh + rowo;
+#pragma unroll
+                for (int j1 = 0; j1 < N1; j1++) {
+                    const int i1 = 2 * (N2 * j1 + t);
+                    float2 v = *reinterpret_cast<const float2 *>(mt + i1);
+                    if (c == 2 && a.tload) {
+                        const float2 l = *reinterpret_cast<const float2 *>(a.tload + rowo + i1);
+                        v.x += l.x; v.y += l.y;
+                    }
+                    z[j1] = make_float2(v.x * a.scale2, v.y * a.scale2);
+                }
+            } else {
+                const size_t pl = (size_t)i3 * g.plane;
+                const float *mx = a.m + cx * g.nh + pl + rowo;
+                const float *myp = a.m + cy * g.nh + pl + (size_t)((i2 + 1) % g.sx2) * g.sx1;
+                const float *mym = a.m + cy * g.nh + pl + (size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1;
+                const float *mz = a.m + cz * g.nh + rowo;
+                size_t zp, zm;
+                float kz;
+                if (i3 == 0) { zp = g.plane; zm = 0; kz = a.k3b; }
+                else if (i3 == g.sx3h - 1) { zp = pl; zm = pl - g.plane; kz = a.k3b; }
+                else { zp = pl + g.plane; zm = pl - g.plane; kz = a.k3; }
+#pragma unroll
+                for (int j1 = 0; j1 < N1; j1++) {
+                    const int i1 = 2 * (N2 * j1 + t);
+                    const float2 xc = __ldg(reinterpret_cast<const float2 *>(mx + i1));
+                    const float xl = __ldg(mx + (i1 + g.sx1 - 1) % g.sx1);
+                    const float xr = __ldg(mx + (i1 + 2) % g.sx1);
+                    const float2 yp = __ldg(reinterpret_cast<const float2 *>(myp + i1));
+                    const float2 ym = __ldg(reinterpret_cast<const float2 *>(mym + i1));
+                    const float2 zpv = __ldg(reinterpret_cast<const float2 *>(mz + zp + i1));
+                    const float2 zmv = __ldg(reinterpret_cast<const float2 *>(mz + zm + i1));
+                    const float f0 = (xc.y - xl) * a.k1 + (yp.x - ym.x) * a.k2 + (zpv.x - zmv.x) * kz;
+                    const float f1 = (xr - xc.x) * a.k1 + (yp.y - ym.y) * a.k2 + (zpv.y - zmv.y) * kz;
+                    z[j1] = make_float2(-f0 * a.scale3, -f1 * a.scale3);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j1 = 0; j1 < N1; j1++) {
+                const int i1 = 2 * (N2 * j1 + t);
+                float2 v;
+                if (trac) {
+                    v = make_float2(a.tin[c][(size_t)i2 * a.trp + i1], a.tin[c][(size_t)i2 * a.trp + i1 + 1]);
+                    if (c == 2 && a.tload) { v.x += a.tload[rowo + i1]; v.y += a.tload[rowo + i1 + 1]; }
+                    v.x *= a.scale2; v.y *= a.scale2;
+                } else {
+                    const float *src = a.in[c] + (size_t)i3 * a.pp + (size_t)i2 * a.rp + i1;
+                    v = make_float2(src[0] * a.scale3, src[1] * a.scale3);
+                }
+                z[j1] = v;
+            }
+        }
+        // complex FFT of length M of the packed row
+        RDft<N1, -1>::run(z);
+#pragma unroll
+        for (int k1 = 1; k1 < N1; k1++)
+            if (t) z[k1] = cmul(z[k1], twn<-1>(a.pm.tw, t * k1));
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) T[k1 * N2P + t] = z[k1];
+        __syncthreads();
+        float2 y[Q][N2];
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+#pragma unroll
+            for (int jj = 0; jj < N2; jj++) y[q][jj] = T[(t + N2 * q) * N2P + jj];
+            RDft<N2, -1>::run(y[q]);
+        }
+        __syncthreads();
+        // natural order Z[k1 + N1 k2] into the row buffer for the unpacking
+#pragma unroll
+        for (int q = 0; q < Q; q++)
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) T[(t + N2 * q) + N1 * k2] = y[q][k2];
+        __syncthreads();
+        const int p = trac ? g.sx3 : i3;
+        float2 *dst = a.S + sidx(g, c, p, i2, 0);
+        for (int k = t; k <= M; k += N2) {
+            const float2 zk = T[k == M ? 0 : k];
+            const float2 zm = cconj(T[k == 0 ? 0 : M - k]);
+            const float2 e = cscale(cadd(zk, zm), 0.5f);
+            const float2 d = csub(zk, zm);
+            const float2 w = __ldg(&a.tw1[k]);
+            const float2 wd = cmul(w, d);
+            dst[k] = make_float2(e.x + 0.5f * wd.y, e.y - 0.5f * wd.x);
+        }
+        __syncthreads();
+    }
+}
+
 // pass 2 / 4: complex transform along x2 for a tile of x1 wavenumbers
 struct YArgs {
     Grid g;
@@ -847,6 +965,450 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_zspec(ZArgs a)
     }
 }
 
+
+// ------------------------------------------------------------------------
+// Register-resident variants of passes 2-4 (see rfft.cuh): columns of
+// length n = N1*N2, CW columns per block, N2 threads per column.
+// ------------------------------------------------------------------------
+
+// pass 2 / 4 along x2
+template <int N1, int N2, int CW, int SIGN>
+__global__ void __launch_bounds__(CW *N2) k_ypass_reg(YArgs a)
+{
+    constexpr int n = N1 * N2, Q = N1 / N2;
+    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    extern __shared__ float2 smy[];
+    const Grid &g = a.g;
+    const int c = threadIdx.x % CW, t = threadIdx.x / CW;
+    const int k1t = blockIdx.x * CW;
+    const bool ok = k1t + c < g.K1;
+    const int p = (a.traction && (int)blockIdx.y == a.nbody) ? g.sx3 : (int)blockIdx.y;
+    const size_t base = sidx(g, blockIdx.z, p, 0, k1t + c);
+    float2 x[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++)
+        x[j1] = ok ? a.S[base + (size_t)(N2 * j1 + t) * g.K1] : make_float2(0.f, 0.f);
+    RDft<N1, SIGN>::run(x);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; k1++)
+        if (t) x[k1] = cmul(x[k1], twn<SIGN>(a.py.tw, t * k1));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) smy[(k1 * N2 + t) * CW + c] = x[k1];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        float2 y[N2];
+        const int k1 = t + N2 * q;
+#pragma unroll
+        for (int jj = 0; jj < N2; jj++) y[jj] = smy[(k1 * N2 + jj) * CW + c];
+        RDft<N2, SIGN>::run(y);
+        if (ok) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) a.S[base + (size_t)(k1 + N1 * k2) * g.K1] = y[k2];
+        }
+    }
+    (void)n;
+}
+
+// pass 3: the spectral Green's function on whole x3 columns (as k_zspec)
+template <int N1, int N2, int CW>
+__global__ void __launch_bounds__(CW *N2) k_zspec_reg(ZArgs a)
+{
+    constexpr int n = N1 * N2, Q = N1 / N2;
+    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    extern __shared__ float2 smz[];
+    double *red = reinterpret_cast<double *>(smz + n * CW);          // [N2][CW][6]
+    float *colc = reinterpret_cast<float *>(red + N2 * CW * 6);       // [CW][12]
+    const Grid &g = a.g;
+    const int c = threadIdx.x % CW, t = threadIdx.x / CW;
+    const int k1t = blockIdx.x * CW, k2i = blockIdx.y;
+    const bool ok = k1t + c < g.K1;
+    const double PI2 = 6.28318530717958623199592693708837032318;
+
+    // load and stage A (forward), three components
+    float2 x[3][N1];
+#pragma unroll
+    for (int cp = 0; cp < 3; cp++) {
+#pragma unroll
+        for (int j1 = 0; j1 < N1; j1++) {
+            const int i3 = N2 * j1 + t;
+            x[cp][j1] = (ok && i3 < a.nin) ? a.S[sidx(g, cp, i3, k2i, k1t + c)] : make_float2(0.f, 0.f);
+        }
+    }
+#pragma unroll
+    for (int cp = 0; cp < 3; cp++) {
+        RDft<N1, -1>::run(x[cp]);
+#pragma unroll
+        for (int k1 = 1; k1 < N1; k1++)
+            if (t) x[cp][k1] = cmul(x[cp][k1], twn<-1>(a.pz.tw, t * k1));
+    }
+    // transpose, stage B: y[cp][q][k2] = X[(t + N2 q) + N1 k2]
+    float2 y[3][Q][N2];
+#pragma unroll
+    for (int cp = 0; cp < 3; cp++) {
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) smz[(k1 * N2 + t) * CW + c] = x[cp][k1];
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < Q; q++)
+#pragma unroll
+            for (int jj = 0; jj < N2; jj++) y[cp][q][jj] = smz[((t + N2 * q) * N2 + jj) * CW + c];
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < Q; q++) RDft<N2, -1>::run(y[cp][q]);
+    }
+
+    // elastic response and the surface-traction partial sums
+    const double k1v = (double)(k1t + c) / (g.sx1 * g.dx1);
+    const double k2v = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
+    const float k1f = (float)k1v, k2f = (float)k2v;
+    const double modulus = a.lambda + 2.0 * a.mu;
+    const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
+    const double grav = 2.0 * a.mu * alpha * a.gam;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) {
+            const int j = (t + N2 * q) + N1 * k2;
+            const double k3v = (j < n / 2) ? (double)j / (n * g.dx3) : -(double)(n - j) / (n * g.dx3);
+            const float k3f = (float)k3v;
+            const float2 c1 = y[0][q][k2], c2 = y[1][q][k2], c3 = y[2][q][k2];
+            const float r2 = k1f * k1f + k2f * k2f + k3f * k3f;
+            float2 u1, u2, u3;
+            if (r2 > 0.f) {
+                const float den = a.ratio1 / (r2 * r2);
+                const float a1 = k2f * k2f + k3f * k3f + a.ratio2 * r2;
+                const float a2 = k1f * k1f + k3f * k3f + a.ratio2 * r2;
+                const float a3 = k1f * k1f + k2f * k2f + a.ratio2 * r2;
+                u1.x = (a1 * c1.x - k1f * (k2f * c2.x + k3f * c3.x)) * den;
+                u1.y = (a1 * c1.y - k1f * (k2f * c2.y + k3f * c3.y)) * den;
+                u2.x = (a2 * c2.x - k2f * (k1f * c1.x + k3f * c3.x)) * den;
+                u2.y = (a2 * c2.y - k2f * (k1f * c1.y + k3f * c3.y)) * den;
+                u3.x = (a3 * c3.x - k3f * (k1f * c1.x + k2f * c2.x)) * den;
+                u3.y = (a3 * c3.y - k3f * (k1f * c1.y + k2f * c2.y)) * den;
+            } else {
+                u1 = u2 = u3 = make_float2(0.f, 0.f);
+            }
+            y[0][q][k2] = u1; y[1][q][k2] = u2; y[2][q][k2] = u3;
+            const double a1r = a.mu * (k3v * u1.x + k1v * u3.x), a1i = a.mu * (k3v * u1.y + k1v * u3.y);
+            const double a2r = a.mu * (k3v * u2.x + k2v * u3.x), a2i = a.mu * (k3v * u2.y + k2v * u3.y);
+            const double a3r = modulus * k3v * u3.x + a.lambda * (k1v * u1.x + k2v * u2.x);
+            const double a3i = modulus * k3v * u3.y + a.lambda * (k1v * u1.y + k2v * u2.y);
+            acc[0] += -PI2 * a1i; acc[1] += PI2 * a1r;
+            acc[2] += -PI2 * a2i; acc[3] += PI2 * a2r;
+            acc[4] += -PI2 * a3i - grav * u3.x; acc[5] += PI2 * a3r - grav * u3.y;
+        }
+    }
+#pragma unroll
+    for (int qq = 0; qq < 6; qq++) red[(t * CW + c) * 6 + qq] = acc[qq];
+    __syncthreads();
+    // fixed-order reduction over the column's threads, then the Cerruti
+    // coefficients of the column (FP64)
+    if (t == 0) {
+        double s[6] = {0, 0, 0, 0, 0, 0};
+        for (int tt = 0; tt < N2; tt++)
+            for (int qq = 0; qq < 6; qq++) s[qq] += red[(tt * CW + c) * 6 + qq];
+        float *cc = colc + c * 12;
+        for (int qq = 0; qq < 12; qq++) cc[qq] = 0.f;
+        if (ok && !(k1v == 0.0 && k2v == 0.0)) {
+            const double d = (double)n * g.dx3;
+            double p[6];
+            for (int cp = 0; cp < 3; cp++) {
+                const float2 tc = a.S[sidx(g, cp, g.sx3, k2i, k1t + c)];
+                p[2 * cp] = (double)tc.x - s[2 * cp] / d;
+                p[2 * cp + 1] = (double)tc.y - s[2 * cp + 1] / d;
+            }
+            const double beta = PI2 * sqrt(k1v * k1v + k2v * k2v);
+            const double h = a.gam / beta;
+            const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
+            const double b1r = p[0] * c0, b1i = p[1] * c0, b2r = p[2] * c0, b2i = p[3] * c0;
+            const double qr = PI2 * k1v * p[0] + PI2 * k2v * p[2], qi = PI2 * k1v * p[1] + PI2 * k2v * p[3];
+            const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
+            const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
+            const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
+            cc[0] = (float)b1r; cc[1] = (float)b1i; cc[2] = (float)b2r; cc[3] = (float)b2i;
+            cc[4] = (float)b3r; cc[5] = (float)b3i;
+            cc[6] = (float)(b1r * k1v + b2r * k2v); cc[7] = (float)(b1i * k1v + b2i * k2v);
+            cc[8] = (float)beta; cc[9] = (float)k1v; cc[10] = (float)k2v; cc[11] = 1.f;
+        }
+    }
+    __syncthreads();
+    {
+        const float *cc = colc + c * 12;
+        if (cc[11] != 0.f) {
+            const float alphaf = (float)alpha;
+            const float pi2 = 6.28318530717958623f;
+            const float beta = cc[8];
+            const float b3r = cc[4], b3i = cc[5];
+            const float er = 1.f - 1.f / alphaf, hr = 1.f / alphaf;
+            const float ab = alphaf * beta * pi2, ab2 = -alphaf * beta * beta;
+            const float ap = alphaf * pi2 * pi2;
+#pragma unroll
+            for (int q = 0; q < Q; q++) {
+#pragma unroll
+                for (int k2 = 0; k2 < N2; k2++) {
+                    const int j = (t + N2 * q) + N1 * k2;
+                    const float k3f = (float)((j < n / 2) ? (double)j / (n * g.dx3) : -(double)(n - j) / (n * g.dx3));
+                    const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + beta * beta);
+                    const float gg = pi2 * k3f * fi;
+                    const float ei = -gg;
+                    const float gr = b3r * er - b3i * ei, gi = b3r * ei + b3i * er;
+                    const float tmr = -ab * gi, tmi = ab * gr;
+                    const float hi = -gg;
+                    const float v3r = ab2 * (b3r * hr - b3i * hi), v3i = ab2 * (b3r * hi + b3i * hr);
+                    const float sr = fi * cc[6], si = fi * cc[7];
+                    const float cr = sr + si * gg, ci = si - sr * gg;
+                    const float bb2 = 2.f * beta * beta * fi;
+                    float2 &u1 = y[0][q][k2], &u2 = y[1][q][k2], &u3 = y[2][q][k2];
+                    u1.x += tmr * k1f * fi - bb2 * cc[0] + ap * k1f * cr;
+                    u1.y += tmi * k1f * fi - bb2 * cc[1] + ap * k1f * ci;
+                    u2.x += tmr * k2f * fi - bb2 * cc[2] + ap * k2f * cr;
+                    u2.y += tmi * k2f * fi - bb2 * cc[3] + ap * k2f * ci;
+                    const float ak = alphaf * beta * pi2 * pi2 * k3f * fi;
+                    u3.x += v3r * fi + ak * sr;
+                    u3.y += v3i * fi + ak * si;
+                }
+            }
+        }
+    }
+    // inverse: stage B^-1, twiddle, transpose, stage A^-1, store
+#pragma unroll
+    for (int cp = 0; cp < 3; cp++) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            RDft<N2, +1>::run(y[cp][q]);
+            const int k1 = t + N2 * q;
+#pragma unroll
+            for (int jj = 0; jj < N2; jj++) {
+                float2 v = y[cp][q][jj];
+                if (k1 && jj) v = cmul(v, twn<+1>(a.pz.tw, jj * k1));
+                smz[(k1 * N2 + jj) * CW + c] = v;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) x[cp][k1] = smz[(k1 * N2 + t) * CW + c];
+        __syncthreads();
+        RDft<N1, +1>::run(x[cp]);
+        if (ok) {
+#pragma unroll
+            for (int j1 = 0; j1 < N1; j1++) {
+                const int i3 = N2 * j1 + t;
+                if (i3 < a.nout) a.S[sidx(g, cp, i3, k2i, k1t + c)] = x[cp][j1];
+            }
+        }
+    }
+}
+
+
+// pass 3, register/shared-memory version.  The three components of CW
+// columns stay in shared memory (U[cp][k1][j2][c]) between the phases, so a
+// thread holds one N1 or 3 x N2 group at a time.  PRUNED: input planes
+// [n/2, n) are zero and only output planes [0, n/2) are wanted (the step's
+// Green's functions); otherwise nin/nout are honoured.
+template <int N1, int N2, int CW, bool PRUNED>
+__global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(ZArgs a)
+{
+    constexpr int n = N1 * N2, Q = N1 / N2;
+    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    extern __shared__ float2 smz[];
+    float2 *U = smz;                                                   // [3][N1][N2][CW]
+    double *red = reinterpret_cast<double *>(smz + 3 * n * CW);        // [N2][CW][6]
+    float *colc = reinterpret_cast<float *>(red + N2 * CW * 6);        // [CW][12]
+    const Grid &g = a.g;
+    const int c = threadIdx.x % CW, t = threadIdx.x / CW;
+    const int k1t = blockIdx.x * CW, k2i = blockIdx.y;
+    const bool ok = k1t + c < g.K1;
+    const double PI2 = 6.28318530717958623199592693708837032318;
+    const double inv_l3 = 1.0 / (n * g.dx3);
+    auto uidx = [&](int cp, int k1, int j) { return ((cp * N1 + k1) * N2 + j) * CW + c; };
+
+    // forward stage A: all loads first, then the three transforms
+    constexpr int NL = PRUNED ? N1 / 2 : N1;
+    float2 x[3][NL];
+#pragma unroll
+    for (int cp = 0; cp < 3; cp++)
+#pragma unroll
+        for (int j1 = 0; j1 < NL; j1++) {
+            const int i3 = N2 * j1 + t;
+            const bool ld = ok && (PRUNED || i3 < a.nin);
+            x[cp][j1] = ld ? a.S[sidx(g, cp, i3, k2i, k1t + c)] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+    for (int cp = 0; cp < 3; cp++) {
+        float2 z[N1];
+#pragma unroll
+        for (int j1 = 0; j1 < N1; j1++) z[j1] = j1 < NL ? x[cp][j1] : make_float2(0.f, 0.f);
+        RDft<N1, -1>::run(z);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) {
+            float2 v = z[k1];
+            if (k1 && t) v = cmul(v, twn<-1>(a.pz.tw, t * k1));
+            U[uidx(cp, k1, t)] = v;
+        }
+    }
+    __syncthreads();
+
+    // stage B, elastic response, surface-traction partial sums
+    const double k1v = (double)(k1t + c) / (g.sx1 * g.dx1);
+    const double k2v = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
+    const float k1f = (float)k1v, k2f = (float)k2v;
+    const double modulus = a.lambda + 2.0 * a.mu;
+    const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
+    const double grav = 2.0 * a.mu * alpha * a.gam;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        const int k1 = t + N2 * q;
+        float2 y[3][N2];
+#pragma unroll
+        for (int cp = 0; cp < 3; cp++) {
+#pragma unroll
+            for (int jj = 0; jj < N2; jj++) y[cp][jj] = U[uidx(cp, k1, jj)];
+            RDft<N2, -1>::run(y[cp]);
+        }
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) {
+            const int j = k1 + N1 * k2;
+            const double k3v = (double)(j < n / 2 ? j : j - n) * inv_l3;
+            const float k3f = (float)k3v;
+            const float2 c1 = y[0][k2], c2 = y[1][k2], c3 = y[2][k2];
+            const float r2 = k1f * k1f + k2f * k2f + k3f * k3f;
+            float2 u1, u2, u3;
+            if (r2 > 0.f) {
+                const float den = a.ratio1 / (r2 * r2);
+                const float a1 = k2f * k2f + k3f * k3f + a.ratio2 * r2;
+                const float a2 = k1f * k1f + k3f * k3f + a.ratio2 * r2;
+                const float a3 = k1f * k1f + k2f * k2f + a.ratio2 * r2;
+                u1.x = (a1 * c1.x - k1f * (k2f * c2.x + k3f * c3.x)) * den;
+                u1.y = (a1 * c1.y - k1f * (k2f * c2.y + k3f * c3.y)) * den;
+                u2.x = (a2 * c2.x - k2f * (k1f * c1.x + k3f * c3.x)) * den;
+                u2.y = (a2 * c2.y - k2f * (k1f * c1.y + k3f * c3.y)) * den;
+                u3.x = (a3 * c3.x - k3f * (k1f * c1.x + k2f * c2.x)) * den;
+                u3.y = (a3 * c3.y - k3f * (k1f * c1.y + k2f * c2.y)) * den;
+            } else {
+                u1 = u2 = u3 = make_float2(0.f, 0.f);
+            }
+            U[uidx(0, k1, k2)] = u1;
+            U[uidx(1, k1, k2)] = u2;
+            U[uidx(2, k1, k2)] = u3;
+            const double a1r = a.mu * (k3v * u1.x + k1v * u3.x), a1i = a.mu * (k3v * u1.y + k1v * u3.y);
+            const double a2r = a.mu * (k3v * u2.x + k2v * u3.x), a2i = a.mu * (k3v * u2.y + k2v * u3.y);
+            const double a3r = modulus * k3v * u3.x + a.lambda * (k1v * u1.x + k2v * u2.x);
+            const double a3i = modulus * k3v * u3.y + a.lambda * (k1v * u1.y + k2v * u2.y);
+            acc[0] += -PI2 * a1i; acc[1] += PI2 * a1r;
+            acc[2] += -PI2 * a2i; acc[3] += PI2 * a2r;
+            acc[4] += -PI2 * a3i - grav * u3.x; acc[5] += PI2 * a3r - grav * u3.y;
+        }
+    }
+#pragma unroll
+    for (int qq = 0; qq < 6; qq++) red[(t * CW + c) * 6 + qq] = acc[qq];
+    __syncthreads();
+    if (t == 0) {
+        double s[6] = {0, 0, 0, 0, 0, 0};
+        for (int tt = 0; tt < N2; tt++)
+            for (int qq = 0; qq < 6; qq++) s[qq] += red[(tt * CW + c) * 6 + qq];
+        float *cc = colc + c * 12;
+        for (int qq = 0; qq < 12; qq++) cc[qq] = 0.f;
+        if (ok && !(k1v == 0.0 && k2v == 0.0)) {
+            const double d = (double)n * g.dx3;
+            double p[6];
+            for (int cp = 0; cp < 3; cp++) {
+                const float2 tc = a.S[sidx(g, cp, g.sx3, k2i, k1t + c)];
+                p[2 * cp] = (double)tc.x - s[2 * cp] / d;
+                p[2 * cp + 1] = (double)tc.y - s[2 * cp + 1] / d;
+            }
+            const double beta = PI2 * sqrt(k1v * k1v + k2v * k2v);
+            const double h = a.gam / beta;
+            const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
+            const double b1r = p[0] * c0, b1i = p[1] * c0, b2r = p[2] * c0, b2i = p[3] * c0;
+            const double qr = PI2 * k1v * p[0] + PI2 * k2v * p[2], qi = PI2 * k1v * p[1] + PI2 * k2v * p[3];
+            const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
+            const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
+            const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
+            cc[0] = (float)b1r; cc[1] = (float)b1i; cc[2] = (float)b2r; cc[3] = (float)b2i;
+            cc[4] = (float)b3r; cc[5] = (float)b3i;
+            cc[6] = (float)(b1r * k1v + b2r * k2v); cc[7] = (float)(b1i * k1v + b2i * k2v);
+            cc[8] = (float)beta; cc[9] = (float)k1v; cc[10] = (float)k2v; cc[11] = 1.f;
+        }
+    }
+    __syncthreads();
+
+    // Cerruti correction, inverse stage B, twiddle (in place in U)
+    {
+        const float *cc = colc + c * 12;
+        const bool cerr = cc[11] != 0.f;
+        const float alphaf = (float)alpha;
+        const float pi2 = 6.28318530717958623f;
+        const float beta = cc[8];
+        const float b3r = cc[4], b3i = cc[5];
+        const float er = 1.f - 1.f / alphaf, hr = 1.f / alphaf;
+        const float ab = alphaf * beta * pi2, ab2 = -alphaf * beta * beta;
+        const float ap = alphaf * pi2 * pi2;
+        const float il3 = (float)inv_l3;
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const int k1 = t + N2 * q;
+            float2 y[3][N2];
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) {
+                float2 u1 = U[uidx(0, k1, k2)], u2 = U[uidx(1, k1, k2)], u3 = U[uidx(2, k1, k2)];
+                if (cerr) {
+                    const int j = k1 + N1 * k2;
+                    const float k3f = (float)(j < n / 2 ? j : j - n) * il3;
+                    const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + beta * beta);
+                    const float gg = pi2 * k3f * fi;
+                    const float ei = -gg;
+                    const float gr = b3r * er - b3i * ei, gi = b3r * ei + b3i * er;
+                    const float tmr = -ab * gi, tmi = ab * gr;
+                    const float hi = -gg;
+                    const float v3r = ab2 * (b3r * hr - b3i * hi), v3i = ab2 * (b3r * hi + b3i * hr);
+                    const float sr = fi * cc[6], si = fi * cc[7];
+                    const float cr = sr + si * gg, ci = si - sr * gg;
+                    const float bb2 = 2.f * beta * beta * fi;
+                    u1.x += tmr * k1f * fi - bb2 * cc[0] + ap * k1f * cr;
+                    u1.y += tmi * k1f * fi - bb2 * cc[1] + ap * k1f * ci;
+                    u2.x += tmr * k2f * fi - bb2 * cc[2] + ap * k2f * cr;
+                    u2.y += tmi * k2f * fi - bb2 * cc[3] + ap * k2f * ci;
+                    const float ak = alphaf * beta * pi2 * pi2 * k3f * fi;
+                    u3.x += v3r * fi + ak * sr;
+                    u3.y += v3i * fi + ak * si;
+                }
+                y[0][k2] = u1; y[1][k2] = u2; y[2][k2] = u3;
+            }
+#pragma unroll
+            for (int cp = 0; cp < 3; cp++) {
+                RDft<N2, +1>::run(y[cp]);
+#pragma unroll
+                for (int jj = 0; jj < N2; jj++) {
+                    float2 v = y[cp][jj];
+                    if (k1 && jj) v = cmul(v, twn<+1>(a.pz.tw, jj * k1));
+                    U[uidx(cp, k1, jj)] = v;
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // inverse stage A and store
+#pragma unroll
+    for (int cp = 0; cp < 3; cp++) {
+        float2 z[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) z[k1] = U[uidx(cp, k1, t)];
+        RDft<N1, +1>::run(z);
+        if (ok) {
+#pragma unroll
+            for (int j1 = 0; j1 < N1; j1++) {
+                const int i3 = N2 * j1 + t;
+                if (PRUNED ? j1 < N1 / 2 : i3 < a.nout) a.S[sidx(g, cp, i3, k2i, k1t + c)] = z[j1];
+            }
+        }
+    }
+    (void)x;
+}
+
 // pass 5: C2R along x1, scaled by 2/(sx1 dx1 sx2 dx2 sx3 dx3), with the
 // field update out = base + coef * w  (fieldadd, src/elastic3d.f90:3774-3812)
 struct XiArgs {
@@ -896,6 +1458,69 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
         }
         *reinterpret_cast<float2 *>(a.out[c] + o) = make_float2(w0, w1);
     }
+}
+
+
+// pass 5, register-resident: C2R along x1 for rows of M = N1*N2 complex
+// values, RW rows of one plane and one component per block, N2 threads per
+// row, with the field update out = base + coef * w.  Shared-memory rows are
+// padded (N2+1 per k1 group, row stride = 8 mod 16 float2) so both transpose
+// access patterns are free of bank conflicts.
+template <int N1, int N2, int RW>
+__global__ void __launch_bounds__(RW *N2) k_xinv_reg(XiArgs a)
+{
+    constexpr int M = N1 * N2, Q = N1 / N2, N2P = N2 + 1;
+    constexpr int RS0 = N1 * N2P, RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
+    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    extern __shared__ float2 smx[];
+    const Grid &g = a.g;
+    const int t = threadIdx.x % N2, r = threadIdx.x / N2;
+    const int i2 = blockIdx.x * RW + r, i3 = blockIdx.y, c = blockIdx.z;
+    const size_t base = sidx(g, c, i3, i2, 0);
+    float2 x[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) {
+        const int k = N2 * j1 + t;
+        float2 xk = a.S[base + k], xm = a.S[base + (M - k)];
+        if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
+        const float2 e = cscale(cadd(xk, cconj(xm)), 0.5f);
+        const float2 d = cscale(csub(xk, cconj(xm)), 0.5f);
+        const float2 o = cmul(d, cconj(__ldg(&a.tw1[k])));
+        x[j1] = make_float2(e.x - o.y, e.y + o.x);   // E + i O
+    }
+    RDft<N1, +1>::run(x);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; k1++)
+        if (t) x[k1] = cmul(x[k1], twn<+1>(a.pm.tw, t * k1));
+    float2 *T = smx + r * RS;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) T[k1 * N2P + t] = x[k1];
+    __syncthreads();
+    const float coef = a.st ? (float)(a.cmul * a.st->Dt) : a.cmul;
+    float *out = a.out[c];
+    const float *bs = a.base[c];
+    const size_t ro = (size_t)i3 * a.pp + (size_t)i2 * a.rp;
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        const int k1 = t + N2 * q;
+        float2 y[N2];
+#pragma unroll
+        for (int jj = 0; jj < N2; jj++) y[jj] = T[k1 * N2P + jj];
+        RDft<N2, +1>::run(y);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) {
+            const int nn = k1 + N1 * k2;
+            const size_t o = ro + 2 * (size_t)nn;
+            float w0 = y[k2].x * a.scale, w1 = y[k2].y * a.scale;
+            if (bs) {
+                const float2 b = *reinterpret_cast<const float2 *>(bs + o);
+                w0 = b.x + coef * w0;
+                w1 = b.y + coef * w1;
+            }
+            *reinterpret_cast<float2 *>(out + o) = make_float2(w0, w1);
+        }
+    }
+    (void)M;
 }
 
 // ------------------------------------------------------------------------

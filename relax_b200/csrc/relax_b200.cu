@@ -153,8 +153,113 @@ struct Prof {
         if (prof) (prof)->end(st);                          \
     } while (0)
 
+// register-resident column passes for the lengths they are instantiated for
+constexpr int kCW = 16;
+
+template <int N1, int N2>
+static cudaError_t launch_ypass_reg(const YArgs &ya, int sign, dim3 grid, cudaStream_t st)
+{
+    const size_t sm = (size_t)N1 * N2 * kCW * sizeof(float2);
+    if (sign < 0) {
+        cudaFuncSetAttribute(k_ypass_reg<N1, N2, kCW, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_ypass_reg<N1, N2, kCW, -1><<<grid, kCW * N2, sm, st>>>(ya);
+    } else {
+        cudaFuncSetAttribute(k_ypass_reg<N1, N2, kCW, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_ypass_reg<N1, N2, kCW, +1><<<grid, kCW * N2, sm, st>>>(ya);
+    }
+    return cudaGetLastError();
+}
+
+static bool ypass_reg(const YArgs &ya, int sign, dim3 grid, cudaStream_t st, cudaError_t *e)
+{
+    switch (ya.g.sx2) {
+    case 64: *e = launch_ypass_reg<8, 8>(ya, sign, grid, st); return true;
+    case 128: *e = launch_ypass_reg<16, 8>(ya, sign, grid, st); return true;
+    case 256: *e = launch_ypass_reg<16, 16>(ya, sign, grid, st); return true;
+    case 512: *e = launch_ypass_reg<32, 16>(ya, sign, grid, st); return true;
+    default: return false;
+    }
+}
+
+template <int N1, int N2>
+static cudaError_t launch_zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st)
+{
+    const size_t sm = 3 * (size_t)N1 * N2 * kCW * sizeof(float2) + (size_t)N2 * kCW * 6 * sizeof(double) +
+                      (size_t)kCW * 12 * sizeof(float);
+    const bool pruned = 2 * za.nin == za.g.sx3 && 2 * za.nout == za.g.sx3;
+    if (pruned) {
+        cudaFuncSetAttribute(k_zspec_sm<N1, N2, kCW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_zspec_sm<N1, N2, kCW, true><<<grid, kCW * N2, sm, st>>>(za);
+    } else {
+        cudaFuncSetAttribute(k_zspec_sm<N1, N2, kCW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_zspec_sm<N1, N2, kCW, false><<<grid, kCW * N2, sm, st>>>(za);
+    }
+    return cudaGetLastError();
+}
+
+static bool zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st, cudaError_t *e)
+{
+    switch (za.g.sx3) {
+    case 64: *e = launch_zspec_reg<8, 8>(za, grid, st); return true;
+    case 128: *e = launch_zspec_reg<16, 8>(za, grid, st); return true;
+    case 256: *e = launch_zspec_reg<16, 16>(za, grid, st); return true;
+    default: return false;
+    }
+}
+
+template <int N1, int N2>
+static cudaError_t launch_xinv_reg(const XiArgs &xi, int nout, cudaStream_t st)
+{
+    constexpr int RW = 16, N2P = N2 + 1, RS0 = N1 * N2P, RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
+    const size_t sm = (size_t)RW * RS * sizeof(float2);
+    cudaFuncSetAttribute(k_xinv_reg<N1, N2, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_xinv_reg<N1, N2, RW><<<dim3(xi.g.sx2 / RW, nout, 3), RW * N2, sm, st>>>(xi);
+    return cudaGetLastError();
+}
+
+static bool xinv_reg(const XiArgs &xi, int nout, cudaStream_t st, cudaError_t *e)
+{
+    if (xi.g.sx2 % 16) return false;
+    switch (xi.g.M) {
+    case 64: *e = launch_xinv_reg<8, 8>(xi, nout, st); return true;
+    case 128: *e = launch_xinv_reg<16, 8>(xi, nout, st); return true;
+    case 256: *e = launch_xinv_reg<16, 16>(xi, nout, st); return true;
+    default: return false;
+    }
+}
+
+template <int N1, int N2>
+static cudaError_t launch_xfwd_reg(const XfArgs &xa, bool div, dim3 grid, cudaStream_t st)
+{
+    constexpr int RW = 16, N2P = N2 + 1, M = N1 * N2;
+    constexpr int RS0 = (N1 * N2P > M + 1 ? N1 * N2P : M + 1), RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
+    const size_t sm = (size_t)RW * RS * sizeof(float2);
+    if (div) {
+        cudaFuncSetAttribute(k_xfwd_reg<XIN_DIV, N1, N2, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_xfwd_reg<XIN_DIV, N1, N2, RW><<<grid, RW * N2, sm, st>>>(xa);
+    } else {
+        cudaFuncSetAttribute(k_xfwd_reg<XIN_REAL, N1, N2, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_xfwd_reg<XIN_REAL, N1, N2, RW><<<grid, RW * N2, sm, st>>>(xa);
+    }
+    return cudaGetLastError();
+}
+
+static bool xfwd_reg(const XfArgs &xa, bool div, int nplanes, cudaStream_t st, cudaError_t *e)
+{
+    if (xa.g.sx2 % 16) return false;
+    const dim3 grid(xa.g.sx2 / 16, nplanes);
+    switch (xa.g.M) {
+    case 64: *e = launch_xfwd_reg<8, 8>(xa, div, grid, st); return true;
+    case 128: *e = launch_xfwd_reg<16, 8>(xa, div, grid, st); return true;
+    case 256: *e = launch_xfwd_reg<16, 16>(xa, div, grid, st); return true;
+    default: return false;
+    }
+}
+
 struct Spectral {
     Prof *prof = nullptr;
+    bool use_reg = true;   // register-resident y/z passes where instantiated
+    bool yreg = false;
     Grid g{};
     float2 *S = nullptr;
     float2 *tw = nullptr;          // tables for M, sx1, sx2, sx3
@@ -231,23 +336,61 @@ struct Spectral {
         xa.scale3 = (float)(g.dx1 * g.dx2 * g.dx3);
         xa.scale2 = (float)(g.dx1 * g.dx2);
         dim3 gx(g.sx2 / rows, nin + 1);
-        if (div) TIMED(prof, ST_XFWD, st, (k_xfwd<XIN_DIV><<<gx, RELAX_NTHREADS, smx, st>>>(xa)));
-        else TIMED(prof, ST_XFWD, st, (k_xfwd<XIN_REAL><<<gx, RELAX_NTHREADS, smx, st>>>(xa)));
+        bool xr0 = false;
+        cudaError_t re0 = cudaSuccess;
+        if (use_reg) {
+            TIMED(prof, ST_XFWD, st, (xr0 = xfwd_reg(xa, div, nin + 1, st, &re0)));
+            if (re0 != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_xfwd_reg: %s", cudaGetErrorString(re0));
+        }
+        if (!xr0) {
+            if (div) TIMED(prof, ST_XFWD, st, (k_xfwd<XIN_DIV><<<gx, RELAX_NTHREADS, smx, st>>>(xa)));
+            else TIMED(prof, ST_XFWD, st, (k_xfwd<XIN_REAL><<<gx, RELAX_NTHREADS, smx, st>>>(xa)));
+        }
         YArgs ya{g, S, py, twy, nin, 1};
-        TIMED(prof, ST_YFWD, st,
-              (k_ypass<-1><<<dim3((g.K1 + twy - 1) / twy, nin + 1, 3), RELAX_NTHREADS, smy, st>>>(ya)));
+        cudaError_t re = cudaSuccess;
+        if (use_reg) {
+            TIMED(prof, ST_YFWD, st, (ya.tw = kCW, yreg = ypass_reg(ya, -1, dim3((g.K1 + kCW - 1) / kCW, nin + 1, 3), st, &re)));
+            if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_ypass_reg: %s", cudaGetErrorString(re));
+        }
+        if (!use_reg || !yreg) {
+            ya.tw = twy;
+            TIMED(prof, ST_YFWD, st,
+                  (k_ypass<-1><<<dim3((g.K1 + twy - 1) / twy, nin + 1, 3), RELAX_NTHREADS, smy, st>>>(ya)));
+        }
         ZArgs za;
         za.g = g; za.S = S; za.pz = pz; za.tw = twz; za.nin = nin; za.nout = nout;
         za.ratio1 = (float)((lambda + mu) / (lambda + 2.0 * mu) / mu / (4.0 * M_PI * M_PI));
         za.ratio2 = (float)(mu / (lambda + mu));
         za.lambda = lambda; za.mu = mu; za.gam = gam;
-        TIMED(prof, ST_ZSPEC, st, (k_zspec<<<dim3((g.K1 + twz - 1) / twz, g.sx2), RELAX_NTHREADS, smz, st>>>(za)));
+        bool zr = false;
+        if (use_reg) {
+            TIMED(prof, ST_ZSPEC, st, (zr = zspec_reg(za, dim3((g.K1 + kCW - 1) / kCW, g.sx2), st, &re)));
+            if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_zspec_reg: %s", cudaGetErrorString(re));
+        }
+        if (!zr) {
+            za.tw = twz;
+            TIMED(prof, ST_ZSPEC, st, (k_zspec<<<dim3((g.K1 + twz - 1) / twz, g.sx2), RELAX_NTHREADS, smz, st>>>(za)));
+        }
         YArgs yb{g, S, py, twy, nout, 0};
-        TIMED(prof, ST_YINV, st,
-              (k_ypass<+1><<<dim3((g.K1 + twy - 1) / twy, nout, 3), RELAX_NTHREADS, smy, st>>>(yb)));
+        bool yr2 = false;
+        if (use_reg) {
+            yb.tw = kCW;
+            TIMED(prof, ST_YINV, st, (yr2 = ypass_reg(yb, +1, dim3((g.K1 + kCW - 1) / kCW, nout, 3), st, &re)));
+            if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_ypass_reg: %s", cudaGetErrorString(re));
+        }
+        if (!yr2) {
+            yb.tw = twy;
+            TIMED(prof, ST_YINV, st,
+                  (k_ypass<+1><<<dim3((g.K1 + twy - 1) / twy, nout, 3), RELAX_NTHREADS, smy, st>>>(yb)));
+        }
         xi.g = g; xi.S = S; xi.pm = pm; xi.tw1 = tw1; xi.rows = rows;
         xi.scale = (float)(2.0 / ((double)g.sx1 * g.dx1 * g.sx2 * g.dx2 * g.sx3 * g.dx3));
-        TIMED(prof, ST_XINV, st, (k_xinv<<<dim3(g.sx2 / rows, nout), RELAX_NTHREADS, smx, st>>>(xi)));
+        bool xr = false;
+        if (use_reg) {
+            TIMED(prof, ST_XINV, st, (xr = xinv_reg(xi, nout, st, &re)));
+            if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_xinv_reg: %s", cudaGetErrorString(re));
+        }
+        if (!xr) TIMED(prof, ST_XINV, st, (k_xinv<<<dim3(g.sx2 / rows, nout), RELAX_NTHREADS, smx, st>>>(xi)));
         return RELAX_OK;
     }
 };

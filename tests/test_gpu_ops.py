@@ -209,7 +209,12 @@ def test_friction_abort_is_reported(oracle32):
     assert rc == 6
 
 
-@pytest.mark.parametrize("sx1,sx2,sx3", GRIDS)
+# x2/x3 lengths 64..512 take the register-resident column kernels, the others
+# the shared-memory Stockham kernels
+GREEN_GRIDS = GRIDS + [(64, 64, 64), (64, 256, 128), (32, 512, 256), (128, 128, 128)]
+
+
+@pytest.mark.parametrize("sx1,sx2,sx3", GREEN_GRIDS)
 @pytest.mark.parametrize("gam", [0.0, 8.3e-4])
 def test_green_function_matches_oracle(oracle32, sx1, sx2, sx3, gam):
     lib = _lib.load()
