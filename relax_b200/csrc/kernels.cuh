@@ -351,6 +351,8 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_tau_update(Grid g, float *ta
 struct FrictionArgs {
     Grid g;
     double x, y, z, L, W, strike, dip, rake, beta, mu;
+    // plane geometry, precomputed on the host (src/friction3d.f90:128-152)
+    double cs, ss, cd, sd, cr, sr, xr, yr, zr, Wp, Lp;
     const double *fc;        // 4 x sx3h: V0, (a-b)sigma, friction, cohesion
     const float *sig;        // 6 x nh
     float *m;                // 6 x nh
@@ -404,16 +406,14 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_friction(FrictionArgs a)
         const int i3 = a.i3lo + (int)(t / ((size_t)a.n1 * a.n2));
         const double dx1 = g.dx1, dx2 = g.dx2, dx3 = g.dx3;
         const double x3 = (double)i3 * dx3;
-        const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+        const double Wp = a.Wp, Lp = a.Lp;
         const double mwp = Wp > Lp ? Wp : Lp;
         // shifted coordinates: index j (may be negative) -> x = j dx
         const double x1 = (double)j1 * dx1, x2 = (double)j2 * dx2;
         bool ok = !(fabs(x3 - a.z) > Lp && fabs(x3 + a.z) > Lp);
         ok = ok && !(fabs(x1 - a.x) > mwp || fabs(x2 - a.y) > mwp);
-        const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
-        const double cr = cos(a.rake), sr = sin(a.rake);
-        const double x2r0 = cs * a.x - ss * a.y;
-        const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+        const double cs = a.cs, ss = a.ss, cd = a.cd, sd = a.sd, cr = a.cr, sr = a.sr;
+        const double xr = a.xr, yr = a.yr, zr = a.zr;
         double x2r = cs * x1 - ss * x2;
         const double x1s = cd * x2r - sd * x3, x1i = cd * x2r + sd * x3;
         ok = ok && !(fabs(x1s - xr) > 7.01 * dx1 && fabs(x1i - xr) > 7.01 * dx1);
@@ -463,6 +463,110 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_friction(FrictionArgs a)
                 mp[4 * g.nh] += (float)((ts1 * b2 + ts2 * b1) / 2.0);
                 mp[5 * g.nh] += (float)(ts2 * b2);
             }
+        }
+    }
+    if (a.want_tm) {
+        tm = block_min(tm, shf);
+        if (threadIdx.x == 0) a.tm_part[blockIdx.x] = tm;
+    }
+}
+
+
+// The band of an afterslip plane and the geometric impulse of each band
+// point (src/friction3d.f90:143-183) do not change during a run: k_friction_mark
+// evaluates them once over the plane's index box (impulse, or -1 outside the
+// band); the host compacts the box into a point list for k_friction_pts.
+__global__ void k_friction_mark(FrictionArgs a, double *imp)
+{
+    const Grid &g = a.g;
+    const size_t n = (size_t)a.n1 * a.n2 * a.n3;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int j1 = a.j1lo + (int)(t % a.n1);
+    const int j2 = a.j2lo + (int)((t / a.n1) % a.n2);
+    const int i3 = a.i3lo + (int)(t / ((size_t)a.n1 * a.n2));
+    const double dx1 = g.dx1, dx2 = g.dx2, dx3 = g.dx3;
+    const double x3 = (double)i3 * dx3, x1 = (double)j1 * dx1, x2 = (double)j2 * dx2;
+    const double mwp = a.Wp > a.Lp ? a.Wp : a.Lp;
+    double out = -1.0;
+    bool ok = !(fabs(x3 - a.z) > a.Lp && fabs(x3 + a.z) > a.Lp);
+    ok = ok && !(fabs(x1 - a.x) > mwp || fabs(x2 - a.y) > mwp);
+    const double x2r = a.cs * x1 - a.ss * x2;
+    const double x1s = a.cd * x2r - a.sd * x3, x1i = a.cd * x2r + a.sd * x3;
+    ok = ok && !(fabs(x1s - a.xr) > 7.01 * dx1 && fabs(x1i - a.xr) > 7.01 * dx1);
+    if (ok) {
+        const double x2s = a.ss * x1 + a.cs * x2;
+        const double x3s = a.sd * x2r + a.cd * x3, x3i = -a.sd * x2r + a.cd * x3;
+        double temp1 = d_gauss(x1s - a.xr, dx1), temp2 = d_omega((x2s - a.yr) / a.W, a.beta);
+        double temp3 = d_omega((x3s - a.zr) / a.L, a.beta);
+        const double sourc = temp1 * temp2 * temp3;
+        temp1 = d_gauss(x1i - a.xr, dx1);
+        temp3 = d_omega((x3i + a.zr) / a.L, a.beta);
+        out = sourc + temp1 * temp2 * temp3;
+    }
+    imp[t] = out;
+}
+
+struct FrictionPtsArgs {
+    Grid g;
+    double mu, rake, L, W;
+    double n0, n1, n2, r0, r1, r2;     // plane normal and rake vectors
+    const double *fc;
+    const float *sig;
+    float *m;
+    const unsigned *idx;               // band points (flat physical index)
+    const double *imp;                 // their impulse
+    int npts;
+    int want_tm;
+    float *tm_part;
+    int *err;
+};
+
+// frictioneigenstress on the band points of one plane (the per-step part of
+// src/friction3d.f90:185-235)
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_friction_pts(FrictionPtsArgs a)
+{
+    __shared__ float shf[32];
+    const Grid &g = a.g;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    float tm = 3.0e38f;
+    if (t < a.npts) {
+        const size_t o = a.idx[t];
+        const int i3 = (int)(o / g.plane);
+        const double impulse = a.imp[t];
+        double sv[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) sv[c] = (double)a.sig[c * g.nh + o];
+        const double n0 = a.n0, n1 = a.n1, n2 = a.n2;
+        const double t0 = sv[0] * n0 + sv[1] * n1 + sv[2] * n2;
+        const double t1 = sv[1] * n0 + sv[3] * n1 + sv[4] * n2;
+        const double t2 = sv[2] * n0 + sv[4] * n1 + sv[5] * n2;
+        const double taun = t0 * n0 + t1 * n1 + t2 * n2;
+        double ts0 = t0 - taun * n0, ts1 = t1 - taun * n1, ts2 = t2 - taun * n2;
+        const double taus = sqrt(ts0 * ts0 + ts1 * ts1 + ts2 * ts2);
+        const double vo = a.fc[i3], tauc = a.fc[g.sx3h + i3];
+        const double fr = a.fc[2 * g.sx3h + i3], coh = a.fc[3 * g.sx3h + i3];
+        double tau = taus + fr * taun - coh;
+        if (tau < 0.0) tau = 0.0;
+        const bool back = (ts0 * a.r0 + ts1 * a.r1 + ts2 * a.r2) < 0.0 &&
+                          fabs(a.rake) < 6.28318530717958623199592693708837032318 * 1.5;
+        if (!back) {
+            if ((tau / tauc) > 20) atomicOr(a.err, 1 << RELAX_ERR_FRICTION);
+            ts0 /= taus; ts1 /= taus; ts2 /= taus;
+            const double gd = vo * 2.0 * my_sinh(tau / tauc);
+            if (a.want_tm) {
+                const float cand = (float)(tau / a.mu / gd * ((a.L < a.W ? a.L : a.W) / sqrt(g.dx1 * g.dx3)));
+                if (cand < tm) tm = cand;
+            }
+            const double b = 2.0 * a.mu * impulse * gd;
+            const double b0 = b * n0, b1 = b * n1, b2 = b * n2;
+            float *mp = a.m + o;
+            mp[0 * g.nh] += (float)(ts0 * b0);
+            mp[1 * g.nh] += (float)((ts0 * b1 + ts1 * b0) / 2.0);
+            mp[2 * g.nh] += (float)((ts0 * b2 + ts2 * b0) / 2.0);
+            mp[3 * g.nh] += (float)(ts1 * b1);
+            mp[4 * g.nh] += (float)((ts1 * b2 + ts2 * b1) / 2.0);
+            mp[5 * g.nh] += (float)(ts2 * b2);
         }
     }
     if (a.want_tm) {
@@ -764,6 +868,7 @@ __global__ void __launch_bounds__(RW *N2) k_xfwd_reg(XfArgs a)
         __syncthreads();
     }
 }
+
 
 // pass 2 / 4: complex transform along x2 for a tile of x1 wavenumbers
 struct YArgs {
@@ -1214,8 +1319,8 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
     extern __shared__ float2 smz[];
     float2 *U = smz;                                                   // [3][N1][N2][CW]
-    double *red = reinterpret_cast<double *>(smz + 3 * n * CW);        // [N2][CW][6]
-    float *colc = reinterpret_cast<float *>(red + N2 * CW * 6);        // [CW][12]
+    double *red = reinterpret_cast<double *>(smz + 3 * n * CW);        // [N2][CW][12]
+    float *colc = reinterpret_cast<float *>(red + N2 * CW * 12);       // [CW][16]
     const Grid &g = a.g;
     const int c = threadIdx.x % CW, t = threadIdx.x / CW;
     const int k1t = blockIdx.x * CW, k2i = blockIdx.y;
@@ -1235,29 +1340,32 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
             const bool ld = ok && (PRUNED || i3 < a.nin);
             x[cp][j1] = ld ? a.S[sidx(g, cp, i3, k2i, k1t + c)] : make_float2(0.f, 0.f);
         }
+    {
+        float2 tw[N1];   // W_n^(t k1), shared by the three components
 #pragma unroll
-    for (int cp = 0; cp < 3; cp++) {
-        float2 z[N1];
+        for (int k1 = 0; k1 < N1; k1++) tw[k1] = twn<-1>(a.pz.tw, t * k1);
 #pragma unroll
-        for (int j1 = 0; j1 < N1; j1++) z[j1] = j1 < NL ? x[cp][j1] : make_float2(0.f, 0.f);
-        RDft<N1, -1>::run(z);
+        for (int cp = 0; cp < 3; cp++) {
+            float2 z[N1];
 #pragma unroll
-        for (int k1 = 0; k1 < N1; k1++) {
-            float2 v = z[k1];
-            if (k1 && t) v = cmul(v, twn<-1>(a.pz.tw, t * k1));
-            U[uidx(cp, k1, t)] = v;
+            for (int j1 = 0; j1 < N1; j1++) z[j1] = j1 < NL ? x[cp][j1] : make_float2(0.f, 0.f);
+            RDft<N1, -1>::run(z);
+#pragma unroll
+            for (int k1 = 0; k1 < N1; k1++) U[uidx(cp, k1, t)] = k1 ? cmul(z[k1], tw[k1]) : z[k1];
         }
     }
     __syncthreads();
 
-    // stage B, elastic response, surface-traction partial sums
+    // stage B, elastic response, surface-traction moments
     const double k1v = (double)(k1t + c) / (g.sx1 * g.dx1);
     const double k2v = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
     const float k1f = (float)k1v, k2f = (float)k2v;
-    const double modulus = a.lambda + 2.0 * a.mu;
     const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
-    const double grav = 2.0 * a.mu * alpha * a.gam;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    // elasticresponse as u = A c - B k (k.c) with A = ratio1 (1 + ratio2) / r2,
+    // B = ratio1 / r2^2 (src/green.f90:78-90 rearranged); surface traction
+    // from the FP64 sums Sk_i = sum k3 u_i and S_i = sum u_i over k3
+    const float ra = a.ratio1 * (1.f + a.ratio2);
+    double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int q = 0; q < Q; q++) {
         const int k1 = t + N2 * q;
@@ -1271,54 +1379,60 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
 #pragma unroll
         for (int k2 = 0; k2 < N2; k2++) {
             const int j = k1 + N1 * k2;
-            const double k3v = (double)(j < n / 2 ? j : j - n) * inv_l3;
+            const int jw = j < n / 2 ? j : j - n;
+            const double k3v = (double)jw * inv_l3;
             const float k3f = (float)k3v;
             const float2 c1 = y[0][k2], c2 = y[1][k2], c3 = y[2][k2];
             const float r2 = k1f * k1f + k2f * k2f + k3f * k3f;
             float2 u1, u2, u3;
             if (r2 > 0.f) {
-                const float den = a.ratio1 / (r2 * r2);
-                const float a1 = k2f * k2f + k3f * k3f + a.ratio2 * r2;
-                const float a2 = k1f * k1f + k3f * k3f + a.ratio2 * r2;
-                const float a3 = k1f * k1f + k2f * k2f + a.ratio2 * r2;
-                u1.x = (a1 * c1.x - k1f * (k2f * c2.x + k3f * c3.x)) * den;
-                u1.y = (a1 * c1.y - k1f * (k2f * c2.y + k3f * c3.y)) * den;
-                u2.x = (a2 * c2.x - k2f * (k1f * c1.x + k3f * c3.x)) * den;
-                u2.y = (a2 * c2.y - k2f * (k1f * c1.y + k3f * c3.y)) * den;
-                u3.x = (a3 * c3.x - k3f * (k1f * c1.x + k2f * c2.x)) * den;
-                u3.y = (a3 * c3.y - k3f * (k1f * c1.y + k2f * c2.y)) * den;
+                const float ir2 = 1.f / r2;
+                const float A = ra * ir2, B = a.ratio1 * ir2 * ir2;
+                const float kcr = k1f * c1.x + k2f * c2.x + k3f * c3.x;
+                const float kci = k1f * c1.y + k2f * c2.y + k3f * c3.y;
+                u1 = make_float2(A * c1.x - B * k1f * kcr, A * c1.y - B * k1f * kci);
+                u2 = make_float2(A * c2.x - B * k2f * kcr, A * c2.y - B * k2f * kci);
+                u3 = make_float2(A * c3.x - B * k3f * kcr, A * c3.y - B * k3f * kci);
             } else {
                 u1 = u2 = u3 = make_float2(0.f, 0.f);
             }
             U[uidx(0, k1, k2)] = u1;
             U[uidx(1, k1, k2)] = u2;
             U[uidx(2, k1, k2)] = u3;
-            const double a1r = a.mu * (k3v * u1.x + k1v * u3.x), a1i = a.mu * (k3v * u1.y + k1v * u3.y);
-            const double a2r = a.mu * (k3v * u2.x + k2v * u3.x), a2i = a.mu * (k3v * u2.y + k2v * u3.y);
-            const double a3r = modulus * k3v * u3.x + a.lambda * (k1v * u1.x + k2v * u2.x);
-            const double a3i = modulus * k3v * u3.y + a.lambda * (k1v * u1.y + k2v * u2.y);
-            acc[0] += -PI2 * a1i; acc[1] += PI2 * a1r;
-            acc[2] += -PI2 * a2i; acc[3] += PI2 * a2r;
-            acc[4] += -PI2 * a3i - grav * u3.x; acc[5] += PI2 * a3r - grav * u3.y;
+            acc[0] = fma(k3v, (double)u1.x, acc[0]); acc[1] = fma(k3v, (double)u1.y, acc[1]);
+            acc[2] = fma(k3v, (double)u2.x, acc[2]); acc[3] = fma(k3v, (double)u2.y, acc[3]);
+            acc[4] = fma(k3v, (double)u3.x, acc[4]); acc[5] = fma(k3v, (double)u3.y, acc[5]);
+            acc[6] += u1.x; acc[7] += u1.y; acc[8] += u2.x; acc[9] += u2.y; acc[10] += u3.x; acc[11] += u3.y;
         }
     }
 #pragma unroll
-    for (int qq = 0; qq < 6; qq++) red[(t * CW + c) * 6 + qq] = acc[qq];
+    for (int qq = 0; qq < 12; qq++) red[(t * CW + c) * 12 + qq] = acc[qq];
     __syncthreads();
     if (t == 0) {
-        double s[6] = {0, 0, 0, 0, 0, 0};
+        double s[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int tt = 0; tt < N2; tt++)
-            for (int qq = 0; qq < 6; qq++) s[qq] += red[(tt * CW + c) * 6 + qq];
-        float *cc = colc + c * 12;
-        for (int qq = 0; qq < 12; qq++) cc[qq] = 0.f;
+            for (int qq = 0; qq < 12; qq++) s[qq] += red[(tt * CW + c) * 12 + qq];
+        float *cc = colc + c * 16;
+        for (int qq = 0; qq < 16; qq++) cc[qq] = 0.f;
         if (ok && !(k1v == 0.0 && k2v == 0.0)) {
+            // surfacetractioncowling (src/green.f90:356-366): i 2pi (...) - grav u3
+            const double modulus = a.lambda + 2.0 * a.mu;
+            const double grav = 2.0 * a.mu * alpha * a.gam;
+            const double a1r = a.mu * (s[0] + k1v * s[10]), a1i = a.mu * (s[1] + k1v * s[11]);
+            const double a2r = a.mu * (s[2] + k2v * s[10]), a2i = a.mu * (s[3] + k2v * s[11]);
+            const double a3r = modulus * s[4] + a.lambda * (k1v * s[6] + k2v * s[8]);
+            const double a3i = modulus * s[5] + a.lambda * (k1v * s[7] + k2v * s[9]);
+            const double sum[6] = {-PI2 * a1i, PI2 * a1r, -PI2 * a2i, PI2 * a2r,
+                                   -PI2 * a3i - grav * s[10], PI2 * a3r - grav * s[11]};
             const double d = (double)n * g.dx3;
             double p[6];
             for (int cp = 0; cp < 3; cp++) {
                 const float2 tc = a.S[sidx(g, cp, g.sx3, k2i, k1t + c)];
-                p[2 * cp] = (double)tc.x - s[2 * cp] / d;
-                p[2 * cp + 1] = (double)tc.y - s[2 * cp + 1] / d;
+                p[2 * cp] = (double)tc.x - sum[2 * cp] / d;
+                p[2 * cp + 1] = (double)tc.y - sum[2 * cp + 1] / d;
             }
+            // cerrutisolmodified (src/green.f90:578-609) written as
+            // u_i += fi (P_i + g R_i), g = 2 pi k3 fi, with per-column P_i, R_i
             const double beta = PI2 * sqrt(k1v * k1v + k2v * k2v);
             const double h = a.gam / beta;
             const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
@@ -1327,25 +1441,35 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
             const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
             const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
             const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
-            cc[0] = (float)b1r; cc[1] = (float)b1i; cc[2] = (float)b2r; cc[3] = (float)b2i;
-            cc[4] = (float)b3r; cc[5] = (float)b3i;
-            cc[6] = (float)(b1r * k1v + b2r * k2v); cc[7] = (float)(b1i * k1v + b2i * k2v);
-            cc[8] = (float)beta; cc[9] = (float)k1v; cc[10] = (float)k2v; cc[11] = 1.f;
+            const double Qr = b1r * k1v + b2r * k2v, Qi = b1i * k1v + b2i * k2v;
+            const double ab = alpha * beta * PI2, er = 1.0 - 1.0 / alpha, ab2 = -alpha * beta * beta;
+            const double ap = alpha * PI2 * PI2, bb = 2.0 * beta * beta;
+            // P_1 = i k1 ab er b3 - 2 beta^2 b1' + ap k1 Q ; R_1 = k1 ab b3 - i ap k1 Q
+            cc[0] = (float)(-k1v * ab * er * b3i - bb * b1r + ap * k1v * Qr);
+            cc[1] = (float)(k1v * ab * er * b3r - bb * b1i + ap * k1v * Qi);
+            cc[2] = (float)(k1v * ab * b3r + ap * k1v * Qi);
+            cc[3] = (float)(k1v * ab * b3i - ap * k1v * Qr);
+            cc[4] = (float)(-k2v * ab * er * b3i - bb * b2r + ap * k2v * Qr);
+            cc[5] = (float)(k2v * ab * er * b3r - bb * b2i + ap * k2v * Qi);
+            cc[6] = (float)(k2v * ab * b3r + ap * k2v * Qi);
+            cc[7] = (float)(k2v * ab * b3i - ap * k2v * Qr);
+            // P_3 = ab2 b3 / alpha ; R_3 = -i ab2 b3 + alpha beta 2pi Q
+            cc[8] = (float)(ab2 * b3r / alpha);
+            cc[9] = (float)(ab2 * b3i / alpha);
+            cc[10] = (float)(ab2 * b3i + alpha * beta * PI2 * Qr);
+            cc[11] = (float)(-ab2 * b3r + alpha * beta * PI2 * Qi);
+            cc[12] = (float)beta;
+            cc[13] = 1.f;
         }
     }
     __syncthreads();
 
     // Cerruti correction, inverse stage B, twiddle (in place in U)
     {
-        const float *cc = colc + c * 12;
-        const bool cerr = cc[11] != 0.f;
-        const float alphaf = (float)alpha;
+        const float *cc = colc + c * 16;
+        const bool cerr = cc[13] != 0.f;
         const float pi2 = 6.28318530717958623f;
-        const float beta = cc[8];
-        const float b3r = cc[4], b3i = cc[5];
-        const float er = 1.f - 1.f / alphaf, hr = 1.f / alphaf;
-        const float ab = alphaf * beta * pi2, ab2 = -alphaf * beta * beta;
-        const float ap = alphaf * pi2 * pi2;
+        const float beta = cc[12], b2 = beta * beta;
         const float il3 = (float)inv_l3;
 #pragma unroll
         for (int q = 0; q < Q; q++) {
@@ -1357,35 +1481,22 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
                 if (cerr) {
                     const int j = k1 + N1 * k2;
                     const float k3f = (float)(j < n / 2 ? j : j - n) * il3;
-                    const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + beta * beta);
+                    const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + b2);
                     const float gg = pi2 * k3f * fi;
-                    const float ei = -gg;
-                    const float gr = b3r * er - b3i * ei, gi = b3r * ei + b3i * er;
-                    const float tmr = -ab * gi, tmi = ab * gr;
-                    const float hi = -gg;
-                    const float v3r = ab2 * (b3r * hr - b3i * hi), v3i = ab2 * (b3r * hi + b3i * hr);
-                    const float sr = fi * cc[6], si = fi * cc[7];
-                    const float cr = sr + si * gg, ci = si - sr * gg;
-                    const float bb2 = 2.f * beta * beta * fi;
-                    u1.x += tmr * k1f * fi - bb2 * cc[0] + ap * k1f * cr;
-                    u1.y += tmi * k1f * fi - bb2 * cc[1] + ap * k1f * ci;
-                    u2.x += tmr * k2f * fi - bb2 * cc[2] + ap * k2f * cr;
-                    u2.y += tmi * k2f * fi - bb2 * cc[3] + ap * k2f * ci;
-                    const float ak = alphaf * beta * pi2 * pi2 * k3f * fi;
-                    u3.x += v3r * fi + ak * sr;
-                    u3.y += v3i * fi + ak * si;
+                    u1.x += fi * (cc[0] + gg * cc[2]); u1.y += fi * (cc[1] + gg * cc[3]);
+                    u2.x += fi * (cc[4] + gg * cc[6]); u2.y += fi * (cc[5] + gg * cc[7]);
+                    u3.x += fi * (cc[8] + gg * cc[10]); u3.y += fi * (cc[9] + gg * cc[11]);
                 }
                 y[0][k2] = u1; y[1][k2] = u2; y[2][k2] = u3;
             }
+            float2 tw[N2];   // W_n^(-jj k1), shared by the three components
+#pragma unroll
+            for (int jj = 0; jj < N2; jj++) tw[jj] = twn<+1>(a.pz.tw, jj * k1);
 #pragma unroll
             for (int cp = 0; cp < 3; cp++) {
                 RDft<N2, +1>::run(y[cp]);
 #pragma unroll
-                for (int jj = 0; jj < N2; jj++) {
-                    float2 v = y[cp][jj];
-                    if (k1 && jj) v = cmul(v, twn<+1>(a.pz.tw, jj * k1));
-                    U[uidx(cp, k1, jj)] = v;
-                }
+                for (int jj = 0; jj < N2; jj++) U[uidx(cp, k1, jj)] = jj ? cmul(y[cp][jj], tw[jj]) : y[cp][jj];
             }
         }
     }

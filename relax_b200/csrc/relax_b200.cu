@@ -184,8 +184,8 @@ static bool ypass_reg(const YArgs &ya, int sign, dim3 grid, cudaStream_t st, cud
 template <int N1, int N2>
 static cudaError_t launch_zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st)
 {
-    const size_t sm = 3 * (size_t)N1 * N2 * kCW * sizeof(float2) + (size_t)N2 * kCW * 6 * sizeof(double) +
-                      (size_t)kCW * 12 * sizeof(float);
+    const size_t sm = 3 * (size_t)N1 * N2 * kCW * sizeof(float2) + (size_t)N2 * kCW * 12 * sizeof(double) +
+                      (size_t)kCW * 16 * sizeof(float);
     const bool pruned = 2 * za.nin == za.g.sx3 && 2 * za.nout == za.g.sx3;
     if (pruned) {
         cudaFuncSetAttribute(k_zspec_sm<N1, N2, kCW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -210,7 +210,7 @@ static bool zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st, cudaError_t *
 template <int N1, int N2>
 static cudaError_t launch_xinv_reg(const XiArgs &xi, int nout, cudaStream_t st)
 {
-    constexpr int RW = 16, N2P = N2 + 1, RS0 = N1 * N2P, RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
+    constexpr int RW = 32, N2P = N2 + 1, RS0 = N1 * N2P, RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
     const size_t sm = (size_t)RW * RS * sizeof(float2);
     cudaFuncSetAttribute(k_xinv_reg<N1, N2, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_xinv_reg<N1, N2, RW><<<dim3(xi.g.sx2 / RW, nout, 3), RW * N2, sm, st>>>(xi);
@@ -219,7 +219,7 @@ static cudaError_t launch_xinv_reg(const XiArgs &xi, int nout, cudaStream_t st)
 
 static bool xinv_reg(const XiArgs &xi, int nout, cudaStream_t st, cudaError_t *e)
 {
-    if (xi.g.sx2 % 16) return false;
+    if (xi.g.sx2 % 32) return false;
     switch (xi.g.M) {
     case 64: *e = launch_xinv_reg<8, 8>(xi, nout, st); return true;
     case 128: *e = launch_xinv_reg<16, 8>(xi, nout, st); return true;
@@ -576,6 +576,10 @@ struct relax_ctx {
     double *fcd = nullptr;
     relax_slippatch *patch = nullptr;
     std::vector<int> patch_off;
+    // per afterslip plane: band points and their impulse (fixed geometry)
+    std::vector<unsigned *> band_idx;
+    std::vector<double *> band_imp;
+    std::vector<int> band_n;
     StepState *dst = nullptr, *hst = nullptr;   // device state, pinned host mirror
     float *tm_part = nullptr, *fr_part = nullptr;
     double *amp_part = nullptr, *amp_alt = nullptr;
@@ -604,6 +608,8 @@ static void free_ctx(relax_ctx *c)
     if (c->visc[1]) cudaFree(c->visc[1]);
     if (c->fcd) cudaFree(c->fcd);
     if (c->patch) cudaFree(c->patch);
+    for (auto p : c->band_idx) if (p) cudaFree(p);
+    for (auto p : c->band_imp) if (p) cudaFree(p);
     if (c->dst) cudaFree(c->dst);
     if (c->hst) cudaFreeHost(c->hst);
     if (c->amp_part) cudaFree(c->amp_part);
@@ -624,6 +630,8 @@ static int dalloc(T **p, size_t n)
     if (e != cudaSuccess) return fail(RELAX_ERR_NOMEM, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
     return RELAX_OK;
 }
+
+static int build_bands(relax_ctx *c);
 
 static int create(const relax_config *cfg, int device, relax_ctx *c)
 {
@@ -758,6 +766,7 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     TRY(dalloc(&c->err, 1));
     CK(cudaMemset(c->err, 0, sizeof(int)));
     c->store_sig = !c->planes.empty();
+    TRY(build_bands(c));
     CK(cudaStreamSynchronize(c->st));
     return RELAX_OK;
 }
@@ -944,35 +953,108 @@ static int event_green(relax_ctx *c, bool loads)
     return c->sp.green(xa, false, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st);
 }
 
+// strike/dip/rake trigonometry and the rotated plane centre of
+// src/friction3d.f90:128-152, once per plane on the host
+static void set_plane_geometry(FrictionArgs &a)
+{
+    a.cs = cos(a.strike); a.ss = sin(a.strike); a.cd = cos(a.dip); a.sd = sin(a.dip);
+    a.cr = cos(a.rake); a.sr = sin(a.rake);
+    const double x2r0 = a.cs * a.x - a.ss * a.y;
+    a.xr = a.cd * x2r0 - a.sd * a.z;
+    a.yr = a.ss * a.x + a.cs * a.y;
+    a.zr = a.sd * x2r0 + a.cd * a.z;
+    a.Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0;
+    a.Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+}
+
+// index box of a plane's band: x1, x2 as shifted-coordinate indices in
+// [-sx/2, sx/2-1], x3 in the physical layers
+static bool plane_box(const Grid &g, const FrictionArgs &a, int *j1lo, int *n1, int *j2lo, int *n2, int *i3lo, int *n3)
+{
+    const double mw = std::max(a.Wp, a.Lp);
+    int a1 = (int)ceil((a.x - mw) / g.dx1) - 1, b1 = (int)floor((a.x + mw) / g.dx1) + 1;
+    a1 = std::max(a1, -g.sx1 / 2); b1 = std::min(b1, g.sx1 / 2 - 1);
+    int a2 = (int)ceil((a.y - mw) / g.dx2) - 1, b2 = (int)floor((a.y + mw) / g.dx2) + 1;
+    a2 = std::max(a2, -g.sx2 / 2); b2 = std::min(b2, g.sx2 / 2 - 1);
+    const double zlo = std::min(a.z, -a.z) - a.Lp, zhi = std::max(a.z, -a.z) + a.Lp;
+    const int a3 = std::max(0, (int)floor(zlo / g.dx3) - 1), b3 = std::min(g.sx3h - 1, (int)ceil(zhi / g.dx3) + 1);
+    if (b1 < a1 || b2 < a2 || b3 < a3) return false;
+    *j1lo = a1; *n1 = b1 - a1 + 1; *j2lo = a2; *n2 = b2 - a2 + 1; *i3lo = a3; *n3 = b3 - a3 + 1;
+    return true;
+}
+
+static FrictionArgs plane_args(relax_ctx *c, const relax_plane &p)
+{
+    FrictionArgs a{};
+    a.g = c->g;
+    a.x = p.x; a.y = p.y; a.z = p.z; a.L = p.width; a.W = p.length;
+    a.strike = p.strike; a.dip = p.dip; a.rake = p.rake; a.beta = c->cfg.beta; a.mu = c->cfg.mu;
+    a.fc = c->fcd; a.sig = c->sig; a.m = c->m; a.err = c->err;
+    set_plane_geometry(a);
+    return a;
+}
+
+// band point lists of every plane, once per context
+static int build_bands(relax_ctx *c)
+{
+    const Grid &g = c->g;
+    for (size_t k = 0; k < c->planes.size(); k++) {
+        FrictionArgs a = plane_args(c, c->planes[k]);
+        c->band_idx.push_back(nullptr);
+        c->band_imp.push_back(nullptr);
+        c->band_n.push_back(0);
+        if (!plane_box(g, a, &a.j1lo, &a.n1, &a.j2lo, &a.n2, &a.i3lo, &a.n3)) continue;
+        const size_t n = (size_t)a.n1 * a.n2 * a.n3;
+        double *dimp = nullptr;
+        TRY(dalloc(&dimp, n));
+        k_friction_mark<<<nblocks(n), RELAX_NTHREADS, 0, c->st>>>(a, dimp);
+        std::vector<double> h(n);
+        cudaError_t e = cudaMemcpyAsync(h.data(), dimp, n * sizeof(double), cudaMemcpyDeviceToHost, c->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+        cudaFree(dimp);
+        if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "band of plane %zu: %s", k, cudaGetErrorString(e));
+        std::vector<unsigned> idx;
+        std::vector<double> imp;
+        for (size_t t = 0; t < n; t++) {
+            if (!(h[t] >= 0.0)) continue;
+            const int j1 = a.j1lo + (int)(t % a.n1);
+            const int j2 = a.j2lo + (int)((t / a.n1) % a.n2);
+            const int i3 = a.i3lo + (int)(t / ((size_t)a.n1 * a.n2));
+            const int i1 = (j1 + g.sx1) % g.sx1, i2 = (j2 + g.sx2) % g.sx2;
+            idx.push_back((unsigned)(((size_t)i3 * g.sx2 + i2) * g.sx1 + i1));
+            imp.push_back(h[t]);
+        }
+        c->band_n[k] = (int)idx.size();
+        if (idx.empty()) continue;
+        TRY(dalloc(&c->band_idx[k], idx.size()));
+        TRY(dalloc(&c->band_imp[k], imp.size()));
+        CK(cudaMemcpy(c->band_idx[k], idx.data(), idx.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->band_imp[k], imp.data(), imp.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return RELAX_OK;
+}
+
 static int friction_planes(relax_ctx *c, bool want_tm, int *nblk_out)
 {
     const Grid &g = c->g;
     int blk_total = 0;
     *nblk_out = 0;
     for (size_t k = 0; k < c->planes.size(); k++) {
+        if (c->band_n[k] == 0) continue;
         const relax_plane &p = c->planes[k];
-        FrictionArgs a{};
-        a.g = g;
-        a.x = p.x; a.y = p.y; a.z = p.z; a.L = p.width; a.W = p.length;
-        a.strike = p.strike; a.dip = p.dip; a.rake = p.rake; a.beta = c->cfg.beta; a.mu = c->cfg.mu;
-        a.fc = c->fcd; a.sig = c->sig; a.m = c->m; a.err = c->err; a.want_tm = want_tm;
-        const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
-        const double mw = std::max(Wp, Lp);
-        // x1 index box (shifted coordinates j*dx1, j in [-sx1/2, sx1/2-1])
-        int j1lo = (int)ceil((p.x - mw) / g.dx1) - 1, j1hi = (int)floor((p.x + mw) / g.dx1) + 1;
-        j1lo = std::max(j1lo, -g.sx1 / 2); j1hi = std::min(j1hi, g.sx1 / 2 - 1);
-        int j2lo = (int)ceil((p.y - mw) / g.dx2) - 1, j2hi = (int)floor((p.y + mw) / g.dx2) + 1;
-        j2lo = std::max(j2lo, -g.sx2 / 2); j2hi = std::min(j2hi, g.sx2 / 2 - 1);
-        const double zlo = std::min(p.z, -p.z) - Lp, zhi = std::max(p.z, -p.z) + Lp;
-        int i3lo = std::max(0, (int)floor(zlo / g.dx3) - 1), i3hi = std::min(g.sx3h - 1, (int)ceil(zhi / g.dx3) + 1);
-        if (j1hi < j1lo || j2hi < j2lo || i3hi < i3lo) continue;
-        a.j1lo = j1lo; a.n1 = j1hi - j1lo + 1; a.j2lo = j2lo; a.n2 = j2hi - j2lo + 1;
-        a.i3lo = i3lo; a.n3 = i3hi - i3lo + 1;
-        const size_t n = (size_t)a.n1 * a.n2 * a.n3;
-        const int nb = (int)nblocks(n);
+        FrictionArgs fa = plane_args(c, p);
+        FrictionPtsArgs a{};
+        a.g = g; a.mu = c->cfg.mu; a.rake = p.rake; a.L = p.width; a.W = p.length;
+        a.n0 = fa.cd * fa.cs; a.n1 = -fa.cd * fa.ss; a.n2 = -fa.sd;
+        a.r0 = fa.ss * fa.cr + fa.cs * fa.sd * fa.sr;
+        a.r1 = fa.cs * fa.cr - fa.ss * fa.sd * fa.sr;
+        a.r2 = fa.cd * fa.sr;
+        a.fc = c->fcd; a.sig = c->sig; a.m = c->m; a.err = c->err;
+        a.idx = c->band_idx[k]; a.imp = c->band_imp[k]; a.npts = c->band_n[k];
+        a.want_tm = want_tm;
+        const int nb = (int)nblocks(a.npts);
         if (want_tm) {
             if (blk_total + nb > c->nfr) {
-                // grow the partial array (stream-ordered free/alloc)
                 CK(cudaStreamSynchronize(c->st));
                 float *np = nullptr;
                 TRY(dalloc(&np, (size_t)(blk_total + nb) * 2));
@@ -985,7 +1067,7 @@ static int friction_planes(relax_ctx *c, bool want_tm, int *nblk_out)
             }
             a.tm_part = c->fr_part + blk_total;
         }
-        TIMED(&c->prof, ST_FRICTION, c->st, (k_friction<<<nb, RELAX_NTHREADS, 0, c->st>>>(a)));
+        TIMED(&c->prof, ST_FRICTION, c->st, (k_friction_pts<<<nb, RELAX_NTHREADS, 0, c->st>>>(a)));
         blk_total += nb;
     }
     *nblk_out = blk_total;
@@ -1086,7 +1168,7 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
     c->hst->oi = c->oi;
     CK(cudaMemcpyAsync(c->dst, c->hst, sizeof(StepState), cudaMemcpyHostToDevice, c->st));
     TIMED(&c->prof, ST_DT, c->st,
-          (k_dt<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, policy(c), c->tm_part, c->nblk, c->fr_part, nfr)));
+          (k_dt<<<1, 1024, 0, c->st>>>(c->dst, policy(c), c->tm_part, c->nblk, c->fr_part, nfr)));
     CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     const double Dt = c->hst->Dt;
@@ -1150,8 +1232,8 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
     } else {
         TRY(launch_stress<MODE_END>(c, stress_args(c, c->u)));
         TIMED(&c->prof, ST_REDUCE, c->st,
-              (k_reduce_amp<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->amp_part, c->nblk, nullptr,
-                                                             g.dx1 * g.dx2 * g.dx3)));
+              (k_reduce_amp<<<1, 1024, 0, c->st>>>(c->dst, c->amp_part, c->nblk, nullptr,
+                                                   g.dx1 * g.dx2 * g.dx3)));
     }
     c->m_valid = true;
     c->sig_valid = c->store_sig;
@@ -1485,6 +1567,7 @@ extern "C" int relax_op_frictioneigenstress(double x, double y, double z, double
     FrictionArgs a{};
     a.g = g; a.x = x; a.y = y; a.z = z; a.L = L; a.W = W; a.strike = strike; a.dip = dip; a.rake = rake;
     a.beta = beta; a.mu = mu; a.fc = fcd; a.sig = s; a.m = mo; a.err = err; a.want_tm = maxwelltime != nullptr;
+    set_plane_geometry(a);
     a.j1lo = -sx1 / 2; a.n1 = sx1; a.j2lo = -sx2 / 2; a.n2 = sx2; a.i3lo = 0; a.n3 = sx3h;
     const int nb = (int)nblocks(g.nh);
     float *tmp;
