@@ -40,6 +40,9 @@ struct StepState {
     double t, Dt, tm;          // time, current step, combined Maxwell time
     double maxwell[3];         // tm(ve), tm(pl), tm(as)
     double power, cei;         // log amplitudes of the last step
+    float tmin[2];             // Maxwell-time minima of the last stress pass
+    double dt_raw;             // the step chosen by k_dt before validation
+    int fire;                  // t + Dt reaches the next event
     double dt_override;        // used when use_override != 0
     int use_override;
     int i, e, oi;

@@ -105,15 +105,20 @@ struct StressArgs {
     float k1, k2, k3, k3b;   // 0.5/dx1, 0.5/dx2, 0.5/dx3, 1/dx3
     float lam, mu2, muinv;   // lambda, 2 mu, 1/mu
     int store_sig;
+    const unsigned char *sig_mask;   // store_sig: only groups of 4 points flagged here (null = all)
     float *tm_part;          // [2][gridDim.x]
     double *amp_part;        // [2][gridDim.x] (power, cei)
+    unsigned *ticket;        // INIT/END: blocks done (zero between launches), or null
+    StepState *fin;          // with ticket: receives tmin, power, cei
+    double dv;               // cell volume dx1 dx2 dx3 (amplitude scale)
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(RELAX_NTHREADS) k_stress(StressArgs a)
+__global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(StressArgs a)
 {
     __shared__ float shf[32];
     __shared__ double shd[32];
+    if (MODE == MODE_END && a.st->fire) return;   // the event branch of the step runs instead
     const Grid &g = a.g;
     const int q4 = g.sx1 >> 2;
     const size_t nq = g.nh >> 2;
@@ -138,65 +143,100 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_stress(StressArgs a)
         else if (i3 == g.sx3h - 1) { rzm = idx - g.plane; rzp = idx; kz = a.k3b; }
         else { rzm = idx - g.plane; rzp = idx + g.plane; kz = a.k3; }
 
-        // strain derivatives d_x, d_y, d_z of w1, w2, w3 at 4 points
-        float dxw[3][4], dyw[3][4], dzw[3][4];
+        // Hooke's law (src/elastic3d.f90:129-142) on the strain of w at 4
+        // points; h = C:E is added to the base stress below
+        float h[6][4];
+        if (MODE != MODE_EIGEN) {
+            float dxw[3][4], dyw[3][4], dzw[3][4];
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            if (MODE == MODE_EIGEN) break;
-            const float *wc = a.w + c * nh;
-            const float4 cv = ld4(wc + idx);
-            const float lft = __ldg(wc + row + i1m), rgt = __ldg(wc + row + i1p);
-            dxw[c][0] = (cv.y - lft) * a.k1;
-            dxw[c][1] = (cv.z - cv.x) * a.k1;
-            dxw[c][2] = (cv.w - cv.y) * a.k1;
-            dxw[c][3] = (rgt - cv.z) * a.k1;
-            const float4 ym = ld4(wc + rym), yp = ld4(wc + ryp);
-            dyw[c][0] = (yp.x - ym.x) * a.k2;
-            dyw[c][1] = (yp.y - ym.y) * a.k2;
-            dyw[c][2] = (yp.z - ym.z) * a.k2;
-            dyw[c][3] = (yp.w - ym.w) * a.k2;
-            const float4 zm = ld4(wc + rzm), zp = ld4(wc + rzp);
-            dzw[c][0] = (zp.x - zm.x) * kz;
-            dzw[c][1] = (zp.y - zm.y) * kz;
-            dzw[c][2] = (zp.z - zm.z) * kz;
-            dzw[c][3] = (zp.w - zm.w) * kz;
+            for (int c = 0; c < 3; c++) {
+                const float *wc = a.w + c * nh;
+                const float4 cv = ld4(wc + idx);
+                const float lft = __ldg(wc + row + i1m), rgt = __ldg(wc + row + i1p);
+                dxw[c][0] = (cv.y - lft) * a.k1;
+                dxw[c][1] = (cv.z - cv.x) * a.k1;
+                dxw[c][2] = (cv.w - cv.y) * a.k1;
+                dxw[c][3] = (rgt - cv.z) * a.k1;
+                const float4 ym = ld4(wc + rym), yp = ld4(wc + ryp);
+                dyw[c][0] = (yp.x - ym.x) * a.k2;
+                dyw[c][1] = (yp.y - ym.y) * a.k2;
+                dyw[c][2] = (yp.z - ym.z) * a.k2;
+                dyw[c][3] = (yp.w - ym.w) * a.k2;
+                const float4 zm = ld4(wc + rzm), zp = ld4(wc + rzp);
+                dzw[c][0] = (zp.x - zm.x) * kz;
+                dzw[c][1] = (zp.y - zm.y) * kz;
+                dzw[c][2] = (zp.z - zm.z) * kz;
+                dzw[c][3] = (zp.w - zm.w) * kz;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float e11 = dxw[0][j];
+                const float e12 = (dxw[1][j] + dyw[0][j]) * 0.5f;
+                const float e13 = (dxw[2][j] + dzw[0][j]) * 0.5f;
+                const float e22 = dyw[1][j];
+                const float e23 = (dyw[2][j] + dzw[1][j]) * 0.5f;
+                const float e33 = dzw[2][j];
+                const float tr = e11 + e22 + e33;
+                h[0][j] = a.mu2 * e11 + a.lam * tr;
+                h[1][j] = a.mu2 * e12;
+                h[2][j] = a.mu2 * e13;
+                h[3][j] = a.mu2 * e22 + a.lam * tr;
+                h[4][j] = a.mu2 * e23;
+                h[5][j] = a.mu2 * e33 + a.lam * tr;
+            }
         }
 
-        // base stress
+        // base stress + h.  Tensor amplitudes (tensornorm, weights 1 2 2 1 2 1
+        // over the components) accumulate one component at a time.
         float s[6][4];
-        if (MODE == MODE_OP || MODE == MODE_EIGEN) {
+        constexpr float wnorm[6] = {1.f, 2.f, 2.f, 1.f, 2.f, 1.f};
+        if (MODE == MODE_OP) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const float4 v = ldc4(a.sig + c * nh + idx);
+                s[c][0] = v.x + h[c][0]; s[c][1] = v.y + h[c][1]; s[c][2] = v.z + h[c][2]; s[c][3] = v.w + h[c][3];
+            }
+        } else if (MODE == MODE_EIGEN) {
 #pragma unroll
             for (int c = 0; c < 6; c++) {
                 const float4 v = ldc4(a.sig + c * nh + idx);
                 s[c][0] = v.x; s[c][1] = v.y; s[c][2] = v.z; s[c][3] = v.w;
             }
         } else if (MODE == MODE_INIT) {
+            float qt[4];
 #pragma unroll
             for (int c = 0; c < 6; c++) {
                 const float4 t = ldc4(a.tau + c * nh + idx);
-                s[c][0] = -t.x; s[c][1] = -t.y; s[c][2] = -t.z; s[c][3] = -t.w;
+                const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    qt[j] = c == 0 ? tv[j] * tv[j] : qt[j] + wnorm[c] * tv[j] * tv[j];
+                    s[c][j] = -tv[j] + h[c][j];
+                }
             }
 #pragma unroll
-            for (int j = 0; j < 4; j++)
-                amp_t += (double)tnorm6(-s[0][j], -s[1][j], -s[2][j], -s[3][j], -s[4][j], -s[5][j]);
+            for (int j = 0; j < 4; j++) amp_t += (double)sqrtf(qt[j] * 0.5f);
         } else if (MODE == MODE_END) {
             const float dt = (float)a.st->Dt;
-            float tn[6][4], mm[6][4];
+            float qm[4], qt[4];
 #pragma unroll
             for (int c = 0; c < 6; c++) {
                 const float4 t = ldc4(a.tau + c * nh + idx);
                 const float4 m = ldc4(a.m + c * nh + idx);
-                mm[c][0] = m.x; mm[c][1] = m.y; mm[c][2] = m.z; mm[c][3] = m.w;
-                tn[c][0] = t.x + dt * m.x; tn[c][1] = t.y + dt * m.y;
-                tn[c][2] = t.z + dt * m.z; tn[c][3] = t.w + dt * m.w;
-                st4(a.tau + c * nh + idx, make_float4(tn[c][0], tn[c][1], tn[c][2], tn[c][3]));
+                const float mv[4] = {m.x, m.y, m.z, m.w};
+                const float tn[4] = {t.x + dt * m.x, t.y + dt * m.y, t.z + dt * m.z, t.w + dt * m.w};
+                st4(a.tau + c * nh + idx, make_float4(tn[0], tn[1], tn[2], tn[3]));
 #pragma unroll
-                for (int j = 0; j < 4; j++) s[c][j] = -tn[c][j];
+                for (int j = 0; j < 4; j++) {
+                    qm[j] = c == 0 ? mv[j] * mv[j] : qm[j] + wnorm[c] * mv[j] * mv[j];
+                    qt[j] = c == 0 ? tn[j] * tn[j] : qt[j] + wnorm[c] * tn[j] * tn[j];
+                    s[c][j] = -tn[j] + h[c][j];
+                }
             }
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                amp_m += (double)tnorm6(mm[0][j], mm[1][j], mm[2][j], mm[3][j], mm[4][j], mm[5][j]);
-                amp_t += (double)tnorm6(tn[0][j], tn[1][j], tn[2][j], tn[3][j], tn[4][j], tn[5][j]);
+                amp_m += (double)sqrtf(qm[j] * 0.5f);
+                amp_t += (double)sqrtf(qt[j] * 0.5f);
             }
         } else {  // MODE_CORR
             const float c1 = -(float)(a.st->Dt / 2);
@@ -204,30 +244,11 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_stress(StressArgs a)
             for (int c = 0; c < 6; c++) {
                 const float4 t = ldc4(a.tau + c * nh + idx);
                 const float4 m = ldc4(a.m + c * nh + idx);
-                s[c][0] = c1 * m.x - t.x; s[c][1] = c1 * m.y - t.y;
-                s[c][2] = c1 * m.z - t.z; s[c][3] = c1 * m.w - t.w;
+                s[c][0] = (c1 * m.x - t.x) + h[c][0]; s[c][1] = (c1 * m.y - t.y) + h[c][1];
+                s[c][2] = (c1 * m.z - t.z) + h[c][2]; s[c][3] = (c1 * m.w - t.w) + h[c][3];
             }
         }
-
-        // Hooke's law on the strain, src/elastic3d.f90:129-142
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if (MODE == MODE_EIGEN) break;
-            const float e11 = dxw[0][j];
-            const float e12 = (dxw[1][j] + dyw[0][j]) * 0.5f;
-            const float e13 = (dxw[2][j] + dzw[0][j]) * 0.5f;
-            const float e22 = dyw[1][j];
-            const float e23 = (dyw[2][j] + dzw[1][j]) * 0.5f;
-            const float e33 = dzw[2][j];
-            const float tr = e11 + e22 + e33;
-            s[0][j] += a.mu2 * e11 + a.lam * tr;
-            s[1][j] += a.mu2 * e12;
-            s[2][j] += a.mu2 * e13;
-            s[3][j] += a.mu2 * e22 + a.lam * tr;
-            s[4][j] += a.mu2 * e23;
-            s[5][j] += a.mu2 * e33 + a.lam * tr;
-        }
-        if (MODE == MODE_OP || (MODE != MODE_EIGEN && a.store_sig)) {
+        if (MODE == MODE_OP || (MODE != MODE_EIGEN && a.store_sig && (!a.sig_mask || a.sig_mask[q]))) {
 #pragma unroll
             for (int c = 0; c < 6; c++)
                 st4(a.sig + c * nh + idx, make_float4(s[c][0], s[c][1], s[c][2], s[c][3]));
@@ -310,11 +331,61 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_stress(StressArgs a)
         const double am = block_sum(amp_m, shd);
         __syncthreads();
         const double at = block_sum(amp_t, shd);
+        __shared__ unsigned last;
         if (threadIdx.x == 0) {
             a.tm_part[blockIdx.x] = t0;
             a.tm_part[gridDim.x + blockIdx.x] = t1;
             a.amp_part[blockIdx.x] = am;
             a.amp_part[gridDim.x + blockIdx.x] = at;
+            if (a.ticket) {
+                __threadfence();
+                last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+            }
+        }
+        if (MODE != MODE_EIGEN && a.ticket) {
+            // the last block to finish reduces the partials of all blocks in
+            // a fixed order: Maxwell-time minima and the log amplitudes
+            __syncthreads();
+            if (last) {
+                __threadfence();
+                const int n = gridDim.x, nt = blockDim.x;
+                float m0 = 3.0e38f, m1 = 3.0e38f;
+                double s0 = 0.0, s1 = 0.0;
+                for (int b = 0; b < n; b += 8 * nt) {
+                    float v0[8], v1[8];
+                    double w0[8], w1[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const int i = b + u * nt + threadIdx.x;
+                        const bool in = i < n;
+                        v0[u] = in ? __ldcg(a.tm_part + i) : 3.0e38f;
+                        v1[u] = in ? __ldcg(a.tm_part + n + i) : 3.0e38f;
+                        w0[u] = in ? __ldcg(a.amp_part + i) : 0.0;
+                        w1[u] = in ? __ldcg(a.amp_part + n + i) : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        m0 = fminf(m0, v0[u]);
+                        m1 = fminf(m1, v1[u]);
+                        s0 += w0[u];
+                        s1 += w1[u];
+                    }
+                }
+                m0 = block_min(m0, shf);
+                __syncthreads();
+                m1 = block_min(m1, shf);
+                __syncthreads();
+                s0 = block_sum(s0, shd);
+                __syncthreads();
+                s1 = block_sum(s1, shd);
+                if (threadIdx.x == 0) {
+                    a.fin->tmin[0] = m0;
+                    a.fin->tmin[1] = m1;
+                    a.fin->power = s0 * a.dv;
+                    a.fin->cei = s1 * a.dv;
+                    *a.ticket = 0u;
+                }
+            }
         }
     }
 }
@@ -587,36 +658,72 @@ struct MonitorArgs {
     const StepState *st;
 };
 
-__global__ void k_monitor(MonitorArgs a)
+// Position of patch t of a plane and the grid cell it samples (the nearest
+// point, src/friction3d.f90:311-335); false when it falls outside the box.
+__device__ __forceinline__ bool monitor_cell(const MonitorArgs &a, int t, double X[3], double *yr_out,
+                                             double *zr_out, size_t *o, int *i3_out)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.px2 * a.px3) return;
     const Grid &g = a.g;
     const int j2 = t % a.px2 + 1, j3 = t / a.px2 + 1;
-    relax_slippatch *p = a.patch + t;
     const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
-    const double cr = cos(a.rake), sr = sin(a.rake);
-    const double svv[3] = {ss, cs, 0.0}, dvv[3] = {-cs * sd, ss * sd, -cd};
-    const double n[3] = {cd * cs, -cd * ss, -sd};
-    const double r[3] = {ss * cr + cs * sd * sr, cs * cr - ss * sd * sr, cd * sr};
     const double x2 = cs * a.x - ss * a.y;
     const double xr = cd * x2 - sd * a.z;
     double yr = ss * a.x + cs * a.y, zr = sd * x2 + cd * a.z;
     yr = (double)((float)yr + (float)(((double)j2 - (double)a.px2 / 2.0 - 1.0) * g.dx2));
     zr = (double)((float)zr + (float)(((double)j3 - (double)a.px3 / 2.0 - 1.0) * g.dx3));
     const double x2p = cd * xr + sd * zr;
-    const double X1 = cs * x2p + ss * yr, X2 = -ss * x2p + cs * yr, X3 = -sd * xr + cd * zr;
-    p->x1 = X1; p->x2 = X2; p->x3 = X3; p->lx = yr; p->lz = zr;
-    bool ok = !(X1 > (double)(g.sx1 / 2 - 1) * g.dx1 || X1 < -(double)(g.sx1 / 2) * g.dx1 ||
-                X2 > (double)(g.sx2 / 2 - 1) * g.dx2 || X2 < -(double)(g.sx2 / 2) * g.dx2 ||
-                X3 > (double)(g.sx3h - 1) * g.dx3 || X3 < 0.0);
-    if (ok) {
-        auto fix = [](double v) { double f = floor(v), c = ceil(v); return (int)((v - f) > 0.5 ? c : f); };
-        const int i1 = ((g.sx1 + fix(X1 / g.dx1)) % g.sx1 + g.sx1) % g.sx1;
-        const int i2 = ((g.sx2 + fix(X2 / g.dx2)) % g.sx2 + g.sx2) % g.sx2;
-        const int i3 = fix(X3 / g.dx3);
-        if (i3 >= 0 && i3 < g.sx3h) {
-            const size_t o = ((size_t)i3 * g.sx2 + i2) * g.sx1 + i1;
+    X[0] = cs * x2p + ss * yr; X[1] = -ss * x2p + cs * yr; X[2] = -sd * xr + cd * zr;
+    *yr_out = yr; *zr_out = zr;
+    const bool ok = !(X[0] > (double)(g.sx1 / 2 - 1) * g.dx1 || X[0] < -(double)(g.sx1 / 2) * g.dx1 ||
+                      X[1] > (double)(g.sx2 / 2 - 1) * g.dx2 || X[1] < -(double)(g.sx2 / 2) * g.dx2 ||
+                      X[2] > (double)(g.sx3h - 1) * g.dx3 || X[2] < 0.0);
+    if (!ok) return false;
+    auto fix = [](double v) { double f = floor(v), c = ceil(v); return (int)((v - f) > 0.5 ? c : f); };
+    const int i1 = ((g.sx1 + fix(X[0] / g.dx1)) % g.sx1 + g.sx1) % g.sx1;
+    const int i2 = ((g.sx2 + fix(X[1] / g.dx2)) % g.sx2 + g.sx2) % g.sx2;
+    const int i3 = fix(X[2] / g.dx3);
+    if (i3 < 0 || i3 >= g.sx3h) return false;
+    *o = ((size_t)i3 * g.sx2 + i2) * g.sx1 + i1;
+    *i3_out = i3;
+    return true;
+}
+
+// cells whose stress the friction and monitor kernels read: one flag per
+// group of 4 points along x1 (the stress kernels' float4 groups)
+__global__ void k_mark_points(const unsigned *idx, int n, unsigned char *mask)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) mask[idx[t] >> 2] = 1;
+}
+
+__global__ void k_mark_monitor(MonitorArgs a, unsigned char *mask)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.px2 * a.px3) return;
+    double X[3], yr, zr;
+    size_t o;
+    int i3;
+    if (monitor_cell(a, t, X, &yr, &zr, &o, &i3)) mask[o >> 2] = 1;
+}
+
+__global__ void k_monitor(MonitorArgs a)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.px2 * a.px3) return;
+    const Grid &g = a.g;
+    relax_slippatch *p = a.patch + t;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double cr = cos(a.rake), sr = sin(a.rake);
+    const double svv[3] = {ss, cs, 0.0}, dvv[3] = {-cs * sd, ss * sd, -cd};
+    const double n[3] = {cd * cs, -cd * ss, -sd};
+    const double r[3] = {ss * cr + cs * sd * sr, cs * cr - ss * sd * sr, cd * sr};
+    double X[3], yr, zr;
+    size_t o;
+    int i3;
+    const bool in = monitor_cell(a, t, X, &yr, &zr, &o, &i3);
+    p->x1 = X[0]; p->x2 = X[1]; p->x3 = X[2]; p->lx = yr; p->lz = zr;
+    if (in) {
+        {
             float s6[6];
             for (int c = 0; c < 6; c++) s6[c] = a.sig[c * g.nh + o];
             p->sig.s11 = s6[0]; p->sig.s12 = s6[1]; p->sig.s13 = s6[2];
@@ -756,16 +863,22 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xfwd(XfArgs a)
 // pass 1, register-resident: -div(m) (or the traction m_i3, or real input
 // rows) -> packed real FFT along x1 for rows of M = N1*N2 complex values; RW
 // rows of one plane per block, N2 threads per row, components in turn.
+// The body force of the block's rows is first built in the row buffers with
+// float4 loads (x neighbours by warp shuffle, one wrap-around load per warp
+// edge), then each row thread picks its stride-N2 elements from there.
 template <int XIN, int N1, int N2, int RW>
-__global__ void __launch_bounds__(RW *N2) k_xfwd_reg(XfArgs a)
+__global__ void __launch_bounds__(RW *N2, (RW * N2 <= 128) ? 8 : 4) k_xfwd_reg(XfArgs a)
 {
-    constexpr int M = N1 * N2, Q = N1 / N2, N2P = N2 + 1;
+    constexpr int M = N1 * N2, Q = N1 / N2, N2P = N2 + 1, NT = RW * N2;
     constexpr int RS0 = (N1 * N2P > M + 1 ? N1 * N2P : M + 1);
     constexpr int RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
+    constexpr int SX1 = 2 * M, R4 = SX1 / 4, ITS = RW * R4 / NT;
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    static_assert(R4 % 32 == 0 && NT % 32 == 0 && (RW * R4) % NT == 0, "a warp stages part of one row");
+    static_assert(RS % 2 == 0, "row buffers start on 16 bytes");
     extern __shared__ float2 smx[];
     const Grid &g = a.g;
-    const int t = threadIdx.x % N2, r = threadIdx.x / N2;
+    const int t = threadIdx.x % N2, r = threadIdx.x / N2, lane = threadIdx.x & 31;
     const int i2 = blockIdx.x * RW + r, pi = blockIdx.y;
     const bool trac = a.has_trac && pi == a.nin;
     const int i3 = pi;
@@ -774,11 +887,47 @@ __global__ void __launch_bounds__(RW *N2) k_xfwd_reg(XfArgs a)
 #pragma unroll 1
     for (int c = 0; c < 3; c++) {
         float2 z[N1];
-        if (XIN == XIN_DIV) {
+        if (XIN == XIN_DIV && !trac) {
             const int cx = c == 0 ? 0 : c == 1 ? 1 : 2;
             const int cy = c == 0 ? 1 : c == 1 ? 3 : 4;
             const int cz = c == 0 ? 2 : c == 1 ? 4 : 5;
-            if (trac) {
+            const size_t pl = (size_t)i3 * g.plane;
+            size_t zp, zm;
+            float kz;
+            if (i3 == 0) { zp = g.plane; zm = 0; kz = a.k3b; }
+            else if (i3 == g.sx3h - 1) { zp = pl; zm = pl - g.plane; kz = a.k3b; }
+            else { zp = pl + g.plane; zm = pl - g.plane; kz = a.k3; }
+#pragma unroll 2
+            for (int it = 0; it < ITS; it++) {
+                const int q = threadIdx.x + NT * it, rr = q / R4, x = 4 * (q % R4);
+                const int row = blockIdx.x * RW + rr;
+                const float *mx = a.m + cx * g.nh + pl + (size_t)row * SX1;
+                const float4 xc = __ldg(reinterpret_cast<const float4 *>(mx + x));
+                float xl = __shfl_up_sync(0xffffffffu, xc.w, 1);
+                float xr = __shfl_down_sync(0xffffffffu, xc.x, 1);
+                if (lane == 0) xl = __ldg(mx + (x + SX1 - 1) % SX1);
+                if (lane == 31) xr = __ldg(mx + (x + 4) % SX1);
+                const float *my = a.m + cy * g.nh + pl + x;
+                const float4 yp = __ldg(reinterpret_cast<const float4 *>(my + (size_t)((row + 1) % g.sx2) * SX1));
+                const float4 ym =
+                    __ldg(reinterpret_cast<const float4 *>(my + (size_t)((row + g.sx2 - 1) % g.sx2) * SX1));
+                const float *mz = a.m + cz * g.nh + (size_t)row * SX1 + x;
+                const float4 zpv = __ldg(reinterpret_cast<const float4 *>(mz + zp));
+                const float4 zmv = __ldg(reinterpret_cast<const float4 *>(mz + zm));
+                float4 f;
+                f.x = -((xc.y - xl) * a.k1 + (yp.x - ym.x) * a.k2 + (zpv.x - zmv.x) * kz) * a.scale3;
+                f.y = -((xc.z - xc.x) * a.k1 + (yp.y - ym.y) * a.k2 + (zpv.y - zmv.y) * kz) * a.scale3;
+                f.z = -((xc.w - xc.y) * a.k1 + (yp.z - ym.z) * a.k2 + (zpv.z - zmv.z) * kz) * a.scale3;
+                f.w = -((xr - xc.z) * a.k1 + (yp.w - ym.w) * a.k2 + (zpv.w - zmv.w) * kz) * a.scale3;
+                *reinterpret_cast<float4 *>(reinterpret_cast<float *>(smx + rr * RS) + x) = f;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j1 = 0; j1 < N1; j1++) z[j1] = T[N2 * j1 + t];
+            __syncthreads();
+        } else if (XIN == XIN_DIV) {
+            const int cz = c == 0 ? 2 : c == 1 ? 4 : 5;
+            {
                 const float *mt = a.m + cz * g.nh + rowo;
 #pragma unroll
                 for (int j1 = 0; j1 < N1; j1++) {
@@ -789,31 +938,6 @@ __global__ void __launch_bounds__(RW *N2) k_xfwd_reg(XfArgs a)
                         v.x += l.x; v.y += l.y;
                     }
                     z[j1] = make_float2(v.x * a.scale2, v.y * a.scale2);
-                }
-            } else {
-                const size_t pl = (size_t)i3 * g.plane;
-                const float *mx = a.m + cx * g.nh + pl + rowo;
-                const float *myp = a.m + cy * g.nh + pl + (size_t)((i2 + 1) % g.sx2) * g.sx1;
-                const float *mym = a.m + cy * g.nh + pl + (size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1;
-                const float *mz = a.m + cz * g.nh + rowo;
-                size_t zp, zm;
-                float kz;
-                if (i3 == 0) { zp = g.plane; zm = 0; kz = a.k3b; }
-                else if (i3 == g.sx3h - 1) { zp = pl; zm = pl - g.plane; kz = a.k3b; }
-                else { zp = pl + g.plane; zm = pl - g.plane; kz = a.k3; }
-#pragma unroll
-                for (int j1 = 0; j1 < N1; j1++) {
-                    const int i1 = 2 * (N2 * j1 + t);
-                    const float2 xc = __ldg(reinterpret_cast<const float2 *>(mx + i1));
-                    const float xl = __ldg(mx + (i1 + g.sx1 - 1) % g.sx1);
-                    const float xr = __ldg(mx + (i1 + 2) % g.sx1);
-                    const float2 yp = __ldg(reinterpret_cast<const float2 *>(myp + i1));
-                    const float2 ym = __ldg(reinterpret_cast<const float2 *>(mym + i1));
-                    const float2 zpv = __ldg(reinterpret_cast<const float2 *>(mz + zp + i1));
-                    const float2 zmv = __ldg(reinterpret_cast<const float2 *>(mz + zm + i1));
-                    const float f0 = (xc.y - xl) * a.k1 + (yp.x - ym.x) * a.k2 + (zpv.x - zmv.x) * kz;
-                    const float f1 = (xr - xc.x) * a.k1 + (yp.y - ym.y) * a.k2 + (zpv.y - zmv.y) * kz;
-                    z[j1] = make_float2(-f0 * a.scale3, -f1 * a.scale3);
                 }
             }
         } else {
@@ -1319,12 +1443,14 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
     extern __shared__ float2 smz[];
     float2 *U = smz;                                                   // [3][N1][N2][CW]
-    double *red = reinterpret_cast<double *>(smz + 3 * n * CW);        // [N2][CW][12]
-    float *colc = reinterpret_cast<float *>(red + N2 * CW * 12);       // [CW][16]
+    double *red = reinterpret_cast<double *>(smz + 3 * n * CW);        // [N2][CW][13]
+    float *colc = reinterpret_cast<float *>(red + N2 * CW * 13);       // [CW][17]
     const Grid &g = a.g;
     const int c = threadIdx.x % CW, t = threadIdx.x / CW;
-    const int k1t = blockIdx.x * CW, k2i = blockIdx.y;
-    const bool ok = k1t + c < g.K1;
+    // columns (k1, k2) flattened over the plane: col = k2 K1 + k1
+    const int col = blockIdx.x * CW + c;
+    const bool ok = col < g.sx2 * g.K1;
+    const int k2i = ok ? col / g.K1 : 0, k1c = ok ? col % g.K1 : 0;
     const double PI2 = 6.28318530717958623199592693708837032318;
     const double inv_l3 = 1.0 / (n * g.dx3);
     auto uidx = [&](int cp, int k1, int j) { return ((cp * N1 + k1) * N2 + j) * CW + c; };
@@ -1338,7 +1464,7 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
         for (int j1 = 0; j1 < NL; j1++) {
             const int i3 = N2 * j1 + t;
             const bool ld = ok && (PRUNED || i3 < a.nin);
-            x[cp][j1] = ld ? a.S[sidx(g, cp, i3, k2i, k1t + c)] : make_float2(0.f, 0.f);
+            x[cp][j1] = ld ? a.S[sidx(g, cp, i3, k2i, k1c)] : make_float2(0.f, 0.f);
         }
     {
         float2 tw[N1];   // W_n^(t k1), shared by the three components
@@ -1357,7 +1483,7 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
     __syncthreads();
 
     // stage B, elastic response, surface-traction moments
-    const double k1v = (double)(k1t + c) / (g.sx1 * g.dx1);
+    const double k1v = (double)k1c / (g.sx1 * g.dx1);
     const double k2v = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
     const float k1f = (float)k1v, k2f = (float)k2v;
     const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
@@ -1406,13 +1532,13 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
         }
     }
 #pragma unroll
-    for (int qq = 0; qq < 12; qq++) red[(t * CW + c) * 12 + qq] = acc[qq];
+    for (int qq = 0; qq < 12; qq++) red[(t * CW + c) * 13 + qq] = acc[qq];
     __syncthreads();
     if (t == 0) {
         double s[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int tt = 0; tt < N2; tt++)
-            for (int qq = 0; qq < 12; qq++) s[qq] += red[(tt * CW + c) * 12 + qq];
-        float *cc = colc + c * 16;
+            for (int qq = 0; qq < 12; qq++) s[qq] += red[(tt * CW + c) * 13 + qq];
+        float *cc = colc + c * 17;
         for (int qq = 0; qq < 16; qq++) cc[qq] = 0.f;
         if (ok && !(k1v == 0.0 && k2v == 0.0)) {
             // surfacetractioncowling (src/green.f90:356-366): i 2pi (...) - grav u3
@@ -1427,7 +1553,7 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
             const double d = (double)n * g.dx3;
             double p[6];
             for (int cp = 0; cp < 3; cp++) {
-                const float2 tc = a.S[sidx(g, cp, g.sx3, k2i, k1t + c)];
+                const float2 tc = a.S[sidx(g, cp, g.sx3, k2i, k1c)];
                 p[2 * cp] = (double)tc.x - sum[2 * cp] / d;
                 p[2 * cp + 1] = (double)tc.y - sum[2 * cp + 1] / d;
             }
@@ -1466,7 +1592,9 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
 
     // Cerruti correction, inverse stage B, twiddle (in place in U)
     {
-        const float *cc = colc + c * 16;
+        float cc[14];
+#pragma unroll
+        for (int qq = 0; qq < 14; qq++) cc[qq] = colc[c * 17 + qq];
         const bool cerr = cc[13] != 0.f;
         const float pi2 = 6.28318530717958623f;
         const float beta = cc[12], b2 = beta * beta;
@@ -1513,7 +1641,7 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
 #pragma unroll
             for (int j1 = 0; j1 < N1; j1++) {
                 const int i3 = N2 * j1 + t;
-                if (PRUNED ? j1 < N1 / 2 : i3 < a.nout) a.S[sidx(g, cp, i3, k2i, k1t + c)] = z[j1];
+                if (PRUNED ? j1 < N1 / 2 : i3 < a.nout) a.S[sidx(g, cp, i3, k2i, k1c)] = z[j1];
             }
         }
     }
@@ -1638,11 +1766,22 @@ __global__ void __launch_bounds__(RW *N2) k_xinv_reg(XiArgs a)
 // time step: reduction of the Maxwell-time minima and integrationstep
 // (src/relax.f90:650-677, :1420-1452), one block.
 // ------------------------------------------------------------------------
-__global__ void k_dt(StepState *st, DtPolicy pol, const float *tm_part, int ntm,
+// host-side inputs of one step's time-step choice
+struct DtIn {
+    double t, dt_override;
+    int oi, use_override;
+};
+
+__global__ void k_dt(StepState *st, DtPolicy pol, DtIn in, const float *tm_part, int ntm,
                      const float *fr_part, int nfr)
 {
     __shared__ float shf[32];
     float m0 = 3.0e38f, m1 = 3.0e38f, m2 = 3.0e38f;
+    if (ntm == 0 && threadIdx.x == 0) {
+        // minima already reduced by the stress kernel's last block
+        m0 = st->tmin[0];
+        m1 = st->tmin[1];
+    }
     for (int i = threadIdx.x; i < ntm; i += blockDim.x) {
         m0 = fminf(m0, tm_part[i]);
         m1 = fminf(m1, tm_part[ntm + i]);
@@ -1669,16 +1808,25 @@ __global__ void k_dt(StepState *st, DtPolicy pol, const float *tm_part, int ntm,
         if (pol.has_inter && tm == STEP_MAX) tm = pol.interval / 20.0;
         st->tm = tm;
         double Dt = tm / 10.0;
-        const double t = st->t;
+        const double t = in.t;
+        st->t = in.t;
+        st->oi = in.oi;
         if (0 == pol.skip) {
-            if ((t + Dt) >= ((double)st->oi * pol.odt) - Dt * 0.04) Dt = (double)st->oi * pol.odt - t;
+            if ((t + Dt) >= ((double)in.oi * pol.odt) - Dt * 0.04) Dt = (double)in.oi * pol.odt - t;
         } else {
             Dt = Dt * pol.tscale;
             if (pol.has_next_event)
                 if ((t + Dt - pol.next_event_time) >= 0.0) Dt = pol.next_event_time - t;
         }
-        if (st->use_override) Dt = st->dt_override;
-        st->Dt = Dt;
+        if (in.use_override) Dt = in.dt_override;
+        // an invalid step is reported by the host; Dt = 0 leaves the state
+        // unchanged meanwhile
+        const bool ok = Dt > 0.0 && isfinite(Dt);
+        st->dt_raw = Dt;
+        st->Dt = ok ? Dt : 0.0;
+        // t + Dt on the next event: the step ends with the event branch
+        // (src/relax.f90:859) instead of the END stress pass
+        st->fire = ok && pol.has_next_event && fabs((t + Dt) - pol.next_event_time) < 1e-6;
     }
 }
 

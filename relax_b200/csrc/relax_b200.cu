@@ -184,8 +184,8 @@ static bool ypass_reg(const YArgs &ya, int sign, dim3 grid, cudaStream_t st, cud
 template <int N1, int N2>
 static cudaError_t launch_zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st)
 {
-    const size_t sm = 3 * (size_t)N1 * N2 * kCW * sizeof(float2) + (size_t)N2 * kCW * 12 * sizeof(double) +
-                      (size_t)kCW * 16 * sizeof(float);
+    const size_t sm = 3 * (size_t)N1 * N2 * kCW * sizeof(float2) + (size_t)N2 * kCW * 13 * sizeof(double) +
+                      (size_t)kCW * 17 * sizeof(float);
     const bool pruned = 2 * za.nin == za.g.sx3 && 2 * za.nout == za.g.sx3;
     if (pruned) {
         cudaFuncSetAttribute(k_zspec_sm<N1, N2, kCW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -364,7 +364,7 @@ struct Spectral {
         za.lambda = lambda; za.mu = mu; za.gam = gam;
         bool zr = false;
         if (use_reg) {
-            TIMED(prof, ST_ZSPEC, st, (zr = zspec_reg(za, dim3((g.K1 + kCW - 1) / kCW, g.sx2), st, &re)));
+            TIMED(prof, ST_ZSPEC, st, (zr = zspec_reg(za, dim3((g.sx2 * g.K1 + kCW - 1) / kCW), st, &re)));
             if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_zspec_reg: %s", cudaGetErrorString(re));
         }
         if (!zr) {
@@ -580,6 +580,10 @@ struct relax_ctx {
     std::vector<unsigned *> band_idx;
     std::vector<double *> band_imp;
     std::vector<int> band_n;
+    // groups of 4 points whose stress friction or monitoring reads; the
+    // stress kernels store sig only there
+    unsigned char *sig_mask = nullptr;
+    unsigned *ticket = nullptr;                 // last-block counter of the stress kernels
     StepState *dst = nullptr, *hst = nullptr;   // device state, pinned host mirror
     float *tm_part = nullptr, *fr_part = nullptr;
     double *amp_part = nullptr, *amp_alt = nullptr;
@@ -610,11 +614,12 @@ static void free_ctx(relax_ctx *c)
     if (c->patch) cudaFree(c->patch);
     for (auto p : c->band_idx) if (p) cudaFree(p);
     for (auto p : c->band_imp) if (p) cudaFree(p);
+    if (c->sig_mask) cudaFree(c->sig_mask);
+    if (c->ticket) cudaFree(c->ticket);
     if (c->dst) cudaFree(c->dst);
     if (c->hst) cudaFreeHost(c->hst);
     if (c->amp_part) cudaFree(c->amp_part);
     if (c->amp_alt) cudaFree(c->amp_alt);
-    if (c->err) cudaFree(c->err);
     c->sp.release();
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -763,8 +768,9 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     CK(cudaMemset(c->dst, 0, sizeof(StepState)));
     CK(cudaMallocHost(&c->hst, sizeof(StepState)));
     memset(c->hst, 0, sizeof(StepState));
-    TRY(dalloc(&c->err, 1));
-    CK(cudaMemset(c->err, 0, sizeof(int)));
+    c->err = &c->dst->error;   // read back with the step state
+    TRY(dalloc(&c->ticket, 1));
+    CK(cudaMemset(c->ticket, 0, sizeof(unsigned)));
     c->store_sig = !c->planes.empty();
     TRY(build_bands(c));
     CK(cudaStreamSynchronize(c->st));
@@ -823,6 +829,10 @@ static StressArgs stress_args(relax_ctx *c, const float *w)
     a.k3 = (float)(0.5 / g.dx3); a.k3b = (float)(1.0 / g.dx3);
     a.lam = (float)c->cfg.lambda; a.mu2 = (float)(2.0 * c->cfg.mu); a.muinv = (float)(1.0 / c->cfg.mu);
     a.store_sig = c->store_sig;
+    a.sig_mask = c->sig_mask;
+    a.ticket = c->ticket;
+    a.fin = c->dst;
+    a.dv = g.dx1 * g.dx2 * g.dx3;
     a.tm_part = c->tm_part;
     a.amp_part = c->amp_part;
     return a;
@@ -1031,6 +1041,25 @@ static int build_bands(relax_ctx *c)
         CK(cudaMemcpy(c->band_idx[k], idx.data(), idx.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(c->band_imp[k], imp.data(), imp.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
+    if (c->planes.empty()) return RELAX_OK;
+    TRY(dalloc(&c->sig_mask, g.nh / 4));
+    CK(cudaMemsetAsync(c->sig_mask, 0, g.nh / 4, c->st));
+    for (size_t k = 0; k < c->planes.size(); k++) {
+        if (c->band_n[k] > 0) {
+            k_mark_points<<<nblocks(c->band_n[k]), RELAX_NTHREADS, 0, c->st>>>(c->band_idx[k], c->band_n[k],
+                                                                               c->sig_mask);
+            CKL();
+        }
+        const relax_plane &p = c->planes[k];
+        const int n = std::max(0, p.px2) * std::max(0, p.px3);
+        if (n == 0) continue;
+        MonitorArgs a{};
+        a.g = g;
+        a.x = p.x; a.y = p.y; a.z = p.z; a.strike = p.strike; a.dip = p.dip; a.rake = p.rake;
+        a.px2 = p.px2; a.px3 = p.px3;
+        k_mark_monitor<<<nblocks(n, 128), 128, 0, c->st>>>(a, c->sig_mask);
+        CKL();
+    }
     return RELAX_OK;
 }
 
@@ -1091,13 +1120,18 @@ static int monitor_planes(relax_ctx *c, bool with_dt)
     return RELAX_OK;
 }
 
+// device error flags, from the step state last copied to the host
 static int check_err(relax_ctx *c)
 {
-    int h = 0;
-    CK(cudaMemcpyAsync(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    if (h & (1 << RELAX_ERR_FRICTION))
+    if (c->hst->error & (1 << RELAX_ERR_FRICTION))
         return fail(RELAX_ERR_FRICTION, "wrong value of (a-b)sigma: tau/((a-b)sigma) > 20");
+    return RELAX_OK;
+}
+
+static int pull_state(relax_ctx *c)
+{
+    CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
     return RELAX_OK;
 }
 
@@ -1109,7 +1143,7 @@ static int tail_init(relax_ctx *c)
                                                     c->g.dx1 * c->g.dx2 * c->g.dx3);
     CKL();
     c->m_valid = true;
-    c->sig_valid = c->store_sig;
+    c->sig_valid = c->store_sig && !c->sig_mask;
     return RELAX_OK;
 }
 
@@ -1162,20 +1196,27 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
     // ---- predictor -------------------------------------------------------
     int nfr = 0;
     if (!c->fc.empty()) TRY(friction_planes(c, true, &nfr));
-    c->hst->use_override = dt_override ? 1 : 0;
-    c->hst->dt_override = dt_override ? *dt_override : 0.0;
-    c->hst->t = c->t;
-    c->hst->oi = c->oi;
-    CK(cudaMemcpyAsync(c->dst, c->hst, sizeof(StepState), cudaMemcpyHostToDevice, c->st));
+    DtIn din{};
+    din.t = c->t;
+    din.dt_override = dt_override ? *dt_override : 0.0;
+    din.oi = c->oi;
+    din.use_override = dt_override ? 1 : 0;
+    // the Maxwell-time minima come reduced from the last INIT/END stress pass
     TIMED(&c->prof, ST_DT, c->st,
-          (k_dt<<<1, 1024, 0, c->st>>>(c->dst, policy(c), c->tm_part, c->nblk, c->fr_part, nfr)));
-    CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    const double Dt = c->hst->Dt;
-    double mw[3] = {c->hst->maxwell[0], c->hst->maxwell[1], c->hst->maxwell[2]};
-    if (!(Dt > 0.0) || !std::isfinite(Dt)) return fail(RELAX_ERR_ARG, "invalid time step %g", Dt);
-
+          (k_dt<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, policy(c), din, nullptr, 0, c->fr_part, nfr)));
+    // The kernels take Dt from the device state.  The host needs it before
+    // the end of the step only for surface loads (evaluated on the host at
+    // t + Dt); otherwise the step runs with one synchronisation, at its end.
+    // An invalid Dt is replaced by 0 on the device, so that the step leaves
+    // the state unchanged, and reported here.
     const EventCopy &ev = c->events[c->e];
+    double Dt = 0.0;
+    if (!ev.l.empty()) {
+        TRY(pull_state(c));
+        Dt = c->hst->Dt;
+        if (!(c->hst->dt_raw > 0.0) || !std::isfinite(c->hst->dt_raw))
+            return fail(RELAX_ERR_ARG, "invalid time step %g", c->hst->dt_raw);
+    }
     bool loads = false;
     // note: the reference passes Dt/2.d8 here (src/relax.f90:685)
     TRY(upload_loads(c, ev, c->t, Dt / 2.0e8, true, &loads));
@@ -1212,15 +1253,24 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
         XiArgs xi = xi_update(c, c->u, c->u, 1.0f, true);
         TRY(c->sp.green(xa, true, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st));
     }
+    // tau += Dt m, sig, next predictor moment; tmin, power and cei reduced by
+    // the kernel's last block.  When t + Dt reaches the next event (the test
+    // of src/relax.f90:859, made by k_dt) the kernel does nothing and the
+    // event branch below runs instead.
+    TRY(launch_stress<MODE_END>(c, stress_args(c, c->u)));
+    TRY(pull_state(c));
+    if (!(c->hst->dt_raw > 0.0) || !std::isfinite(c->hst->dt_raw))
+        return fail(RELAX_ERR_ARG, "invalid time step %g", c->hst->dt_raw);
+    Dt = c->hst->Dt;
+    const double mw[3] = {c->hst->maxwell[0], c->hst->maxwell[1], c->hst->maxwell[2]};
     c->t = c->t + Dt;
     c->i++;
-    int fired = 0;
-    if (c->e < (int)c->events.size() - 1 && fabs(c->t - c->events[c->e + 1].time) < 1e-6) {
+    const int fired = c->hst->fire;
+    if (fired) {
         // tau += Dt m, then the coseismic event, then the stress
         k_tau_update<<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(g, c->tau, c->m, c->dst, c->amp_alt);
         CKL();
         c->e++;
-        fired = 1;
         bool any = false, ld = false;
         TRY(event_sources(c, c->events[c->e], &any));
         TRY(upload_loads(c, c->events[c->e], c->t, 0.0, false, &ld));
@@ -1229,14 +1279,10 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
         k_reduce_amp<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->amp_part, c->nblk, c->amp_alt,
                                                         g.dx1 * g.dx2 * g.dx3);
         CKL();
-    } else {
-        TRY(launch_stress<MODE_END>(c, stress_args(c, c->u)));
-        TIMED(&c->prof, ST_REDUCE, c->st,
-              (k_reduce_amp<<<1, 1024, 0, c->st>>>(c->dst, c->amp_part, c->nblk, nullptr,
-                                                   g.dx1 * g.dx2 * g.dx3)));
+        TRY(pull_state(c));
     }
     c->m_valid = true;
-    c->sig_valid = c->store_sig;
+    c->sig_valid = c->store_sig && !c->sig_mask;
     // isoutput, src/relax.f90:1364-1376
     {
         const double odt = c->cfg.odt, etime = c->events[c->e].time;
@@ -1245,8 +1291,6 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
             c->oi++;
     }
     if (!c->fc.empty()) TRY(check_err(c));
-    CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
     log->i = c->i;
     log->event = fired;
     log->dt = Dt;
