@@ -1239,198 +1239,6 @@ __global__ void __launch_bounds__(CW *N2) k_ypass_reg(YArgs a)
     (void)n;
 }
 
-// pass 3: the spectral Green's function on whole x3 columns (as k_zspec)
-template <int N1, int N2, int CW>
-__global__ void __launch_bounds__(CW *N2) k_zspec_reg(ZArgs a)
-{
-    constexpr int n = N1 * N2, Q = N1 / N2;
-    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
-    extern __shared__ float2 smz[];
-    double *red = reinterpret_cast<double *>(smz + n * CW);          // [N2][CW][6]
-    float *colc = reinterpret_cast<float *>(red + N2 * CW * 6);       // [CW][12]
-    const Grid &g = a.g;
-    const int c = threadIdx.x % CW, t = threadIdx.x / CW;
-    const int k1t = blockIdx.x * CW, k2i = blockIdx.y;
-    const bool ok = k1t + c < g.K1;
-    const double PI2 = 6.28318530717958623199592693708837032318;
-
-    // load and stage A (forward), three components
-    float2 x[3][N1];
-#pragma unroll
-    for (int cp = 0; cp < 3; cp++) {
-#pragma unroll
-        for (int j1 = 0; j1 < N1; j1++) {
-            const int i3 = N2 * j1 + t;
-            x[cp][j1] = (ok && i3 < a.nin) ? a.S[sidx(g, cp, i3, k2i, k1t + c)] : make_float2(0.f, 0.f);
-        }
-    }
-#pragma unroll
-    for (int cp = 0; cp < 3; cp++) {
-        RDft<N1, -1>::run(x[cp]);
-#pragma unroll
-        for (int k1 = 1; k1 < N1; k1++)
-            if (t) x[cp][k1] = cmul(x[cp][k1], twn<-1>(a.pz.tw, t * k1));
-    }
-    // transpose, stage B: y[cp][q][k2] = X[(t + N2 q) + N1 k2]
-    float2 y[3][Q][N2];
-#pragma unroll
-    for (int cp = 0; cp < 3; cp++) {
-#pragma unroll
-        for (int k1 = 0; k1 < N1; k1++) smz[(k1 * N2 + t) * CW + c] = x[cp][k1];
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < Q; q++)
-#pragma unroll
-            for (int jj = 0; jj < N2; jj++) y[cp][q][jj] = smz[((t + N2 * q) * N2 + jj) * CW + c];
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < Q; q++) RDft<N2, -1>::run(y[cp][q]);
-    }
-
-    // elastic response and the surface-traction partial sums
-    const double k1v = (double)(k1t + c) / (g.sx1 * g.dx1);
-    const double k2v = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
-    const float k1f = (float)k1v, k2f = (float)k2v;
-    const double modulus = a.lambda + 2.0 * a.mu;
-    const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
-    const double grav = 2.0 * a.mu * alpha * a.gam;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-#pragma unroll
-        for (int k2 = 0; k2 < N2; k2++) {
-            const int j = (t + N2 * q) + N1 * k2;
-            const double k3v = (j < n / 2) ? (double)j / (n * g.dx3) : -(double)(n - j) / (n * g.dx3);
-            const float k3f = (float)k3v;
-            const float2 c1 = y[0][q][k2], c2 = y[1][q][k2], c3 = y[2][q][k2];
-            const float r2 = k1f * k1f + k2f * k2f + k3f * k3f;
-            float2 u1, u2, u3;
-            if (r2 > 0.f) {
-                const float den = a.ratio1 / (r2 * r2);
-                const float a1 = k2f * k2f + k3f * k3f + a.ratio2 * r2;
-                const float a2 = k1f * k1f + k3f * k3f + a.ratio2 * r2;
-                const float a3 = k1f * k1f + k2f * k2f + a.ratio2 * r2;
-                u1.x = (a1 * c1.x - k1f * (k2f * c2.x + k3f * c3.x)) * den;
-                u1.y = (a1 * c1.y - k1f * (k2f * c2.y + k3f * c3.y)) * den;
-                u2.x = (a2 * c2.x - k2f * (k1f * c1.x + k3f * c3.x)) * den;
-                u2.y = (a2 * c2.y - k2f * (k1f * c1.y + k3f * c3.y)) * den;
-                u3.x = (a3 * c3.x - k3f * (k1f * c1.x + k2f * c2.x)) * den;
-                u3.y = (a3 * c3.y - k3f * (k1f * c1.y + k2f * c2.y)) * den;
-            } else {
-                u1 = u2 = u3 = make_float2(0.f, 0.f);
-            }
-            y[0][q][k2] = u1; y[1][q][k2] = u2; y[2][q][k2] = u3;
-            const double a1r = a.mu * (k3v * u1.x + k1v * u3.x), a1i = a.mu * (k3v * u1.y + k1v * u3.y);
-            const double a2r = a.mu * (k3v * u2.x + k2v * u3.x), a2i = a.mu * (k3v * u2.y + k2v * u3.y);
-            const double a3r = modulus * k3v * u3.x + a.lambda * (k1v * u1.x + k2v * u2.x);
-            const double a3i = modulus * k3v * u3.y + a.lambda * (k1v * u1.y + k2v * u2.y);
-            acc[0] += -PI2 * a1i; acc[1] += PI2 * a1r;
-            acc[2] += -PI2 * a2i; acc[3] += PI2 * a2r;
-            acc[4] += -PI2 * a3i - grav * u3.x; acc[5] += PI2 * a3r - grav * u3.y;
-        }
-    }
-#pragma unroll
-    for (int qq = 0; qq < 6; qq++) red[(t * CW + c) * 6 + qq] = acc[qq];
-    __syncthreads();
-    // fixed-order reduction over the column's threads, then the Cerruti
-    // coefficients of the column (FP64)
-    if (t == 0) {
-        double s[6] = {0, 0, 0, 0, 0, 0};
-        for (int tt = 0; tt < N2; tt++)
-            for (int qq = 0; qq < 6; qq++) s[qq] += red[(tt * CW + c) * 6 + qq];
-        float *cc = colc + c * 12;
-        for (int qq = 0; qq < 12; qq++) cc[qq] = 0.f;
-        if (ok && !(k1v == 0.0 && k2v == 0.0)) {
-            const double d = (double)n * g.dx3;
-            double p[6];
-            for (int cp = 0; cp < 3; cp++) {
-                const float2 tc = a.S[sidx(g, cp, g.sx3, k2i, k1t + c)];
-                p[2 * cp] = (double)tc.x - s[2 * cp] / d;
-                p[2 * cp + 1] = (double)tc.y - s[2 * cp + 1] / d;
-            }
-            const double beta = PI2 * sqrt(k1v * k1v + k2v * k2v);
-            const double h = a.gam / beta;
-            const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
-            const double b1r = p[0] * c0, b1i = p[1] * c0, b2r = p[2] * c0, b2i = p[3] * c0;
-            const double qr = PI2 * k1v * p[0] + PI2 * k2v * p[2], qi = PI2 * k1v * p[1] + PI2 * k2v * p[3];
-            const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
-            const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
-            const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
-            cc[0] = (float)b1r; cc[1] = (float)b1i; cc[2] = (float)b2r; cc[3] = (float)b2i;
-            cc[4] = (float)b3r; cc[5] = (float)b3i;
-            cc[6] = (float)(b1r * k1v + b2r * k2v); cc[7] = (float)(b1i * k1v + b2i * k2v);
-            cc[8] = (float)beta; cc[9] = (float)k1v; cc[10] = (float)k2v; cc[11] = 1.f;
-        }
-    }
-    __syncthreads();
-    {
-        const float *cc = colc + c * 12;
-        if (cc[11] != 0.f) {
-            const float alphaf = (float)alpha;
-            const float pi2 = 6.28318530717958623f;
-            const float beta = cc[8];
-            const float b3r = cc[4], b3i = cc[5];
-            const float er = 1.f - 1.f / alphaf, hr = 1.f / alphaf;
-            const float ab = alphaf * beta * pi2, ab2 = -alphaf * beta * beta;
-            const float ap = alphaf * pi2 * pi2;
-#pragma unroll
-            for (int q = 0; q < Q; q++) {
-#pragma unroll
-                for (int k2 = 0; k2 < N2; k2++) {
-                    const int j = (t + N2 * q) + N1 * k2;
-                    const float k3f = (float)((j < n / 2) ? (double)j / (n * g.dx3) : -(double)(n - j) / (n * g.dx3));
-                    const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + beta * beta);
-                    const float gg = pi2 * k3f * fi;
-                    const float ei = -gg;
-                    const float gr = b3r * er - b3i * ei, gi = b3r * ei + b3i * er;
-                    const float tmr = -ab * gi, tmi = ab * gr;
-                    const float hi = -gg;
-                    const float v3r = ab2 * (b3r * hr - b3i * hi), v3i = ab2 * (b3r * hi + b3i * hr);
-                    const float sr = fi * cc[6], si = fi * cc[7];
-                    const float cr = sr + si * gg, ci = si - sr * gg;
-                    const float bb2 = 2.f * beta * beta * fi;
-                    float2 &u1 = y[0][q][k2], &u2 = y[1][q][k2], &u3 = y[2][q][k2];
-                    u1.x += tmr * k1f * fi - bb2 * cc[0] + ap * k1f * cr;
-                    u1.y += tmi * k1f * fi - bb2 * cc[1] + ap * k1f * ci;
-                    u2.x += tmr * k2f * fi - bb2 * cc[2] + ap * k2f * cr;
-                    u2.y += tmi * k2f * fi - bb2 * cc[3] + ap * k2f * ci;
-                    const float ak = alphaf * beta * pi2 * pi2 * k3f * fi;
-                    u3.x += v3r * fi + ak * sr;
-                    u3.y += v3i * fi + ak * si;
-                }
-            }
-        }
-    }
-    // inverse: stage B^-1, twiddle, transpose, stage A^-1, store
-#pragma unroll
-    for (int cp = 0; cp < 3; cp++) {
-#pragma unroll
-        for (int q = 0; q < Q; q++) {
-            RDft<N2, +1>::run(y[cp][q]);
-            const int k1 = t + N2 * q;
-#pragma unroll
-            for (int jj = 0; jj < N2; jj++) {
-                float2 v = y[cp][q][jj];
-                if (k1 && jj) v = cmul(v, twn<+1>(a.pz.tw, jj * k1));
-                smz[(k1 * N2 + jj) * CW + c] = v;
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k1 = 0; k1 < N1; k1++) x[cp][k1] = smz[(k1 * N2 + t) * CW + c];
-        __syncthreads();
-        RDft<N1, +1>::run(x[cp]);
-        if (ok) {
-#pragma unroll
-            for (int j1 = 0; j1 < N1; j1++) {
-                const int i3 = N2 * j1 + t;
-                if (i3 < a.nout) a.S[sidx(g, cp, i3, k2i, k1t + c)] = x[cp][j1];
-            }
-        }
-    }
-}
-
-
 // pass 3, register/shared-memory version.  The three components of CW
 // columns stay in shared memory (U[cp][k1][j2][c]) between the phases, so a
 // thread holds one N1 or 3 x N2 group at a time.  PRUNED: input planes
@@ -1648,6 +1456,231 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
     (void)x;
 }
 
+// pass 3, phased version: 3 x CW x N2 threads per block of CW columns, each
+// phase with its own assignment of threads to work so that no thread holds
+// more than one component's N1 values:
+//   A   (component, column, t): forward stage A of one component
+//   B   (component, column, t): forward stage B, natural order k3
+//   E   (column, s): elastic response at points k3 = s, s + 3 N2, ...,
+//       with per-thread FP32 partial sums of k3 u_i and u_i
+//   R   (column, sum): FP64 sums of the partials; then one thread per column
+//       forms the surface traction and the Cerruti coefficients
+//   C   (component, column, t): Cerruti correction, inverse stage B
+//   D   (component, column, t): inverse stage A and store
+// PRUNED: input planes [n/2, n) are zero and only output planes [0, n/2)
+// are written (the step's Green's functions); otherwise nin/nout hold.
+template <int N1, int N2, int CW, bool PRUNED>
+__global__ void __launch_bounds__(3 * CW * N2, (3 * CW * N2 <= 384) ? 3 : 1) k_zspec_ph(ZArgs a)
+{
+    constexpr int n = N1 * N2, Q = N1 / N2, NT = 3 * CW * N2, NS = NT / CW;
+    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    extern __shared__ float2 smz[];
+    float2 *U = smz;                                                   // [3][N1][N2][CW]
+    float *red = reinterpret_cast<float *>(smz + 3 * n * CW);          // [NS][12][CW]
+    double *sums = reinterpret_cast<double *>(red + NS * 12 * CW);     // [12][CW]
+    float *colc = reinterpret_cast<float *>(sums + 12 * CW);           // [CW][17]
+    const Grid &g = a.g;
+    // transform phases: component cp, column c, thread t of the column
+    const int cp = threadIdx.x / (CW * N2), c = threadIdx.x % CW, t = (threadIdx.x / CW) % N2;
+    // columns (k1, k2) flattened over the plane: col = k2 K1 + k1
+    const int col = blockIdx.x * CW + c;
+    const bool ok = col < g.sx2 * g.K1;
+    const int k2i = ok ? col / g.K1 : 0, k1c = ok ? col % g.K1 : 0;
+    const double PI2 = 6.28318530717958623199592693708837032318;
+    const double inv_l3 = 1.0 / (n * g.dx3);
+    auto uidx = [&](int cc, int k1, int j) { return ((cc * N1 + k1) * N2 + j) * CW + c; };
+
+    // ---- A: forward stage A
+    {
+        constexpr int NL = PRUNED ? N1 / 2 : N1;
+        float2 z[N1];
+#pragma unroll
+        for (int j1 = 0; j1 < N1; j1++) {
+            const int i3 = N2 * j1 + t;
+            const bool ld = j1 < NL && ok && (PRUNED || i3 < a.nin);
+            z[j1] = ld ? a.S[sidx(g, cp, i3, k2i, k1c)] : make_float2(0.f, 0.f);
+        }
+        RDft<N1, -1>::run(z);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) U[uidx(cp, k1, t)] = k1 && t ? cmul(z[k1], twn<-1>(a.pz.tw, t * k1)) : z[k1];
+    }
+    __syncthreads();
+    // ---- B: forward stage B; k3 = k1 + N1 k2 lands in U[cp][k1][k2]
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        const int k1 = t + N2 * q;
+        float2 y[N2];
+#pragma unroll
+        for (int jj = 0; jj < N2; jj++) y[jj] = U[uidx(cp, k1, jj)];
+        RDft<N2, -1>::run(y);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) U[uidx(cp, k1, k2)] = y[k2];
+    }
+    __syncthreads();
+
+    // ---- E: elastic response u = A c - B k (k.c), A = ratio1 (1 + ratio2) / r2,
+    // B = ratio1 / r2^2 (elasticresponse, src/green.f90:78-90, rearranged)
+    const double k1v = (double)k1c / (g.sx1 * g.dx1);
+    const double k2v = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
+    {
+        const int s = threadIdx.x / CW;
+        const float k1f = (float)k1v, k2f = (float)k2v;
+        const float k12 = k1f * k1f + k2f * k2f;
+        const float ra = a.ratio1 * (1.f + a.ratio2);
+        const float il3 = (float)inv_l3;
+        // partial sums over k3 of jw u_i (k3 = jw / (n dx3)) and of u_i
+        float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < (n + NS - 1) / NS; i++) {
+            const int j = s + NS * i;
+            if (j < n) {
+                const int k1 = j % N1, k2 = j / N1;
+                const int jw = j < n / 2 ? j : j - n;
+                const float k3f = (float)((double)jw * inv_l3);
+                const float2 c1 = U[uidx(0, k1, k2)], c2 = U[uidx(1, k1, k2)], c3 = U[uidx(2, k1, k2)];
+                const float r2 = k12 + k3f * k3f;
+                float2 u1, u2, u3;
+                if (r2 > 0.f) {
+                    const float ir2 = 1.f / r2;
+                    const float A = ra * ir2, B = a.ratio1 * ir2 * ir2;
+                    const float kcr = k1f * c1.x + k2f * c2.x + k3f * c3.x;
+                    const float kci = k1f * c1.y + k2f * c2.y + k3f * c3.y;
+                    u1 = make_float2(A * c1.x - B * k1f * kcr, A * c1.y - B * k1f * kci);
+                    u2 = make_float2(A * c2.x - B * k2f * kcr, A * c2.y - B * k2f * kci);
+                    u3 = make_float2(A * c3.x - B * k3f * kcr, A * c3.y - B * k3f * kci);
+                } else {
+                    u1 = u2 = u3 = make_float2(0.f, 0.f);
+                }
+                U[uidx(0, k1, k2)] = u1;
+                U[uidx(1, k1, k2)] = u2;
+                U[uidx(2, k1, k2)] = u3;
+                const float w = (float)jw;
+                acc[0] += w * u1.x; acc[1] += w * u1.y; acc[2] += w * u2.x;
+                acc[3] += w * u2.y; acc[4] += w * u3.x; acc[5] += w * u3.y;
+                acc[6] += u1.x; acc[7] += u1.y; acc[8] += u2.x; acc[9] += u2.y; acc[10] += u3.x; acc[11] += u3.y;
+            }
+        }
+        (void)il3;
+#pragma unroll
+        for (int qq = 0; qq < 12; qq++) red[(s * 12 + qq) * CW + c] = acc[qq];
+    }
+    __syncthreads();
+    // ---- R: FP64 sums, one thread per (sum, column)
+    if (threadIdx.x < 12 * CW) {
+        const int qq = threadIdx.x / CW;
+        double v = 0.0;
+#pragma unroll 4
+        for (int s = 0; s < NS; s++) v += (double)red[(s * 12 + qq) * CW + c];
+        sums[qq * CW + c] = qq < 6 ? v * inv_l3 : v;
+    }
+    __syncthreads();
+    if (threadIdx.x < CW) {
+        double s[12];
+#pragma unroll
+        for (int qq = 0; qq < 12; qq++) s[qq] = sums[qq * CW + c];
+        float *cc = colc + c * 17;
+        for (int qq = 0; qq < 14; qq++) cc[qq] = 0.f;
+        const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
+        if (ok && !(k1v == 0.0 && k2v == 0.0)) {
+            // surfacetractioncowling (src/green.f90:356-366): i 2pi (...) - grav u3
+            const double modulus = a.lambda + 2.0 * a.mu;
+            const double grav = 2.0 * a.mu * alpha * a.gam;
+            const double a1r = a.mu * (s[0] + k1v * s[10]), a1i = a.mu * (s[1] + k1v * s[11]);
+            const double a2r = a.mu * (s[2] + k2v * s[10]), a2i = a.mu * (s[3] + k2v * s[11]);
+            const double a3r = modulus * s[4] + a.lambda * (k1v * s[6] + k2v * s[8]);
+            const double a3i = modulus * s[5] + a.lambda * (k1v * s[7] + k2v * s[9]);
+            const double sum[6] = {-PI2 * a1i, PI2 * a1r, -PI2 * a2i, PI2 * a2r,
+                                   -PI2 * a3i - grav * s[10], PI2 * a3r - grav * s[11]};
+            const double d = (double)n * g.dx3;
+            double p[6];
+            for (int k = 0; k < 3; k++) {
+                const float2 tc = a.S[sidx(g, k, g.sx3, k2i, k1c)];
+                p[2 * k] = (double)tc.x - sum[2 * k] / d;
+                p[2 * k + 1] = (double)tc.y - sum[2 * k + 1] / d;
+            }
+            // cerrutisolmodified (src/green.f90:578-609) written as
+            // u_i += fi (P_i + g R_i), g = 2 pi k3 fi, with per-column P_i, R_i
+            const double beta = PI2 * sqrt(k1v * k1v + k2v * k2v);
+            const double h = a.gam / beta;
+            const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
+            const double b1r = p[0] * c0, b1i = p[1] * c0, b2r = p[2] * c0, b2i = p[3] * c0;
+            const double qr = PI2 * k1v * p[0] + PI2 * k2v * p[2], qi = PI2 * k1v * p[1] + PI2 * k2v * p[3];
+            const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
+            const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
+            const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
+            const double Qr = b1r * k1v + b2r * k2v, Qi = b1i * k1v + b2i * k2v;
+            const double ab = alpha * beta * PI2, er = 1.0 - 1.0 / alpha, ab2 = -alpha * beta * beta;
+            const double ap = alpha * PI2 * PI2, bb = 2.0 * beta * beta;
+            // P_1 = i k1 ab er b3 - 2 beta^2 b1' + ap k1 Q ; R_1 = k1 ab b3 - i ap k1 Q
+            cc[0] = (float)(-k1v * ab * er * b3i - bb * b1r + ap * k1v * Qr);
+            cc[1] = (float)(k1v * ab * er * b3r - bb * b1i + ap * k1v * Qi);
+            cc[2] = (float)(k1v * ab * b3r + ap * k1v * Qi);
+            cc[3] = (float)(k1v * ab * b3i - ap * k1v * Qr);
+            cc[4] = (float)(-k2v * ab * er * b3i - bb * b2r + ap * k2v * Qr);
+            cc[5] = (float)(k2v * ab * er * b3r - bb * b2i + ap * k2v * Qi);
+            cc[6] = (float)(k2v * ab * b3r + ap * k2v * Qi);
+            cc[7] = (float)(k2v * ab * b3i - ap * k2v * Qr);
+            // P_3 = ab2 b3 / alpha ; R_3 = -i ab2 b3 + alpha beta 2pi Q
+            cc[8] = (float)(ab2 * b3r / alpha);
+            cc[9] = (float)(ab2 * b3i / alpha);
+            cc[10] = (float)(ab2 * b3i + alpha * beta * PI2 * Qr);
+            cc[11] = (float)(-ab2 * b3r + alpha * beta * PI2 * Qi);
+            cc[12] = (float)beta;
+            cc[13] = 1.f;
+        }
+    }
+    __syncthreads();
+
+    // ---- C: Cerruti correction of this component, inverse stage B, twiddle
+    {
+        const float *cq = colc + c * 17;
+        const float P0 = cq[4 * cp], P1 = cq[4 * cp + 1], R0 = cq[4 * cp + 2], R1 = cq[4 * cp + 3];
+        const float beta = cq[12];
+        const bool cerr = cq[13] != 0.f;
+        const float pi2 = 6.28318530717958623f;
+        const float b2 = beta * beta;
+        const float il3 = (float)inv_l3;
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const int k1 = t + N2 * q;
+            float2 y[N2];
+#pragma unroll
+            for (int k2 = 0; k2 < N2; k2++) {
+                float2 u = U[uidx(cp, k1, k2)];
+                if (cerr) {
+                    const int j = k1 + N1 * k2;
+                    const float k3f = (float)(j < n / 2 ? j : j - n) * il3;
+                    const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + b2);
+                    const float gg = pi2 * k3f * fi;
+                    u.x += fi * (P0 + gg * R0);
+                    u.y += fi * (P1 + gg * R1);
+                }
+                y[k2] = u;
+            }
+            RDft<N2, +1>::run(y);
+#pragma unroll
+            for (int jj = 0; jj < N2; jj++)
+                U[uidx(cp, k1, jj)] = jj && k1 ? cmul(y[jj], twn<+1>(a.pz.tw, jj * k1)) : y[jj];
+        }
+    }
+    __syncthreads();
+
+    // ---- D: inverse stage A and store
+    {
+        float2 z[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) z[k1] = U[uidx(cp, k1, t)];
+        RDft<N1, +1>::run(z);
+        if (ok) {
+#pragma unroll
+            for (int j1 = 0; j1 < N1; j1++) {
+                const int i3 = N2 * j1 + t;
+                if (PRUNED ? j1 < N1 / 2 : i3 < a.nout) a.S[sidx(g, cp, i3, k2i, k1c)] = z[j1];
+            }
+        }
+    }
+}
+
 // pass 5: C2R along x1, scaled by 2/(sx1 dx1 sx2 dx2 sx3 dx3), with the
 // field update out = base + coef * w  (fieldadd, src/elastic3d.f90:3774-3812)
 struct XiArgs {
@@ -1705,52 +1738,101 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
 // row, with the field update out = base + coef * w.  Shared-memory rows are
 // padded (N2+1 per k1 group, row stride = 8 mod 16 float2) so both transpose
 // access patterns are free of bank conflicts.
-template <int N1, int N2, int RW>
+template <int N1, int N2, int RW, int V>
 __global__ void __launch_bounds__(RW *N2) k_xinv_reg(XiArgs a)
 {
-    constexpr int M = N1 * N2, Q = N1 / N2, N2P = N2 + 1;
-    constexpr int RS0 = N1 * N2P, RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
+    // RW rows of one plane and component per block, N2 threads per row.
+    // (A) the block's spectrum rows, one contiguous run of RW*K1 values
+    //     in S, are staged in shared memory with 16-byte loads;
+    // (B) each row thread unpacks its stride-N2 inputs, transforms in
+    //     registers and leaves the real row in shared memory;
+    // (C) out = base + coef * scale * row with V-wide accesses (V = 4 for
+    //     16-byte aligned rows, else 2).
+    constexpr int M = N1 * N2, Q = N1 / N2, N2P = N2 + 1, K1 = M + 1, NT = RW * N2, SX1 = 2 * M;
+    constexpr int RS0 = (N1 * N2P > K1 ? N1 * N2P : K1), RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    static_assert(RS % 2 == 0 && (RW * K1) % 2 == 0, "float4 staging");
+    static_assert(V == 2 || V == 4, "V");
     extern __shared__ float2 smx[];
     const Grid &g = a.g;
     const int t = threadIdx.x % N2, r = threadIdx.x / N2;
-    const int i2 = blockIdx.x * RW + r, i3 = blockIdx.y, c = blockIdx.z;
-    const size_t base = sidx(g, c, i3, i2, 0);
+    const int i2b = blockIdx.x * RW, i3 = blockIdx.y, c = blockIdx.z;
+
+    // (A) rows i2b .. i2b+RW-1 are contiguous: sidx is linear in i2
+    {
+        const float4 *src = reinterpret_cast<const float4 *>(a.S + sidx(g, c, i3, i2b, 0));
+        constexpr int NF = RW * K1 / 2, ITS = (NF + NT - 1) / NT;
+#pragma unroll
+        for (int it = 0; it < ITS; it++) {
+            const int f = threadIdx.x + NT * it;
+            if (f < NF) {
+                const float4 v = __ldg(src + f);
+                const int e0 = 2 * f, e1 = 2 * f + 1;
+                smx[(e0 / K1) * RS + e0 % K1] = make_float2(v.x, v.y);
+                smx[(e1 / K1) * RS + e1 % K1] = make_float2(v.z, v.w);
+            }
+        }
+    }
+    __syncthreads();
+    float2 *T = smx + r * RS;
     float2 x[N1];
 #pragma unroll
     for (int j1 = 0; j1 < N1; j1++) {
         const int k = N2 * j1 + t;
-        float2 xk = a.S[base + k], xm = a.S[base + (M - k)];
+        float2 xk = T[k], xm = T[M - k];
         if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
         const float2 e = cscale(cadd(xk, cconj(xm)), 0.5f);
         const float2 d = cscale(csub(xk, cconj(xm)), 0.5f);
         const float2 o = cmul(d, cconj(__ldg(&a.tw1[k])));
         x[j1] = make_float2(e.x - o.y, e.y + o.x);   // E + i O
     }
+    __syncthreads();
     RDft<N1, +1>::run(x);
 #pragma unroll
     for (int k1 = 1; k1 < N1; k1++)
         if (t) x[k1] = cmul(x[k1], twn<+1>(a.pm.tw, t * k1));
-    float2 *T = smx + r * RS;
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) T[k1 * N2P + t] = x[k1];
     __syncthreads();
-    const float coef = a.st ? (float)(a.cmul * a.st->Dt) : a.cmul;
-    float *out = a.out[c];
-    const float *bs = a.base[c];
-    const size_t ro = (size_t)i3 * a.pp + (size_t)i2 * a.rp;
+    float2 y[Q][N2];
 #pragma unroll
     for (int q = 0; q < Q; q++) {
         const int k1 = t + N2 * q;
-        float2 y[N2];
 #pragma unroll
-        for (int jj = 0; jj < N2; jj++) y[jj] = T[k1 * N2P + jj];
-        RDft<N2, +1>::run(y);
+        for (int jj = 0; jj < N2; jj++) y[q][jj] = T[k1 * N2P + jj];
+        RDft<N2, +1>::run(y[q]);
+    }
+    __syncthreads();
+    // real row in natural order: float2 nn holds x1 = 2 nn, 2 nn + 1
 #pragma unroll
-        for (int k2 = 0; k2 < N2; k2++) {
-            const int nn = k1 + N1 * k2;
-            const size_t o = ro + 2 * (size_t)nn;
-            float w0 = y[k2].x * a.scale, w1 = y[k2].y * a.scale;
+    for (int q = 0; q < Q; q++)
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) T[(t + N2 * q) + N1 * k2] = y[q][k2];
+    __syncthreads();
+
+    // (C)
+    const float coef = a.st ? (float)(a.cmul * a.st->Dt) : a.cmul;
+    float *out = a.out[c];
+    const float *bs = a.base[c];
+    constexpr int RV = SX1 / V, ITC = RW * RV / NT;
+    static_assert((RW * RV) % NT == 0, "rows split evenly");
+#pragma unroll
+    for (int it = 0; it < ITC; it++) {
+        const int f = threadIdx.x + NT * it, rr = f / RV, x0 = V * (f % RV);
+        const size_t o = (size_t)i3 * a.pp + (size_t)(i2b + rr) * a.rp + x0;
+        const float *row = reinterpret_cast<const float *>(smx + rr * RS) + x0;
+        if (V == 4) {
+            const float4 w4 = *reinterpret_cast<const float4 *>(row);
+            float w[4] = {w4.x * a.scale, w4.y * a.scale, w4.z * a.scale, w4.w * a.scale};
+            if (bs) {
+                const float4 b = __ldg(reinterpret_cast<const float4 *>(bs + o));
+                w[0] = b.x + coef * w[0]; w[1] = b.y + coef * w[1];
+                w[2] = b.z + coef * w[2]; w[3] = b.w + coef * w[3];
+            }
+            *reinterpret_cast<float4 *>(out + o) = make_float4(w[0], w[1], w[2], w[3]);
+        } else {
+            const float2 w2 = *reinterpret_cast<const float2 *>(row);
+            float w0 = w2.x * a.scale, w1 = w2.y * a.scale;
             if (bs) {
                 const float2 b = *reinterpret_cast<const float2 *>(bs + o);
                 w0 = b.x + coef * w0;
@@ -1759,7 +1841,6 @@ __global__ void __launch_bounds__(RW *N2) k_xinv_reg(XiArgs a)
             *reinterpret_cast<float2 *>(out + o) = make_float2(w0, w1);
         }
     }
-    (void)M;
 }
 
 // ------------------------------------------------------------------------

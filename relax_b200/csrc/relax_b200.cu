@@ -210,16 +210,33 @@ static bool zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st, cudaError_t *
 template <int N1, int N2>
 static cudaError_t launch_xinv_reg(const XiArgs &xi, int nout, cudaStream_t st)
 {
-    constexpr int RW = 32, N2P = N2 + 1, RS0 = N1 * N2P, RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
+    constexpr int RW = 32, N2P = N2 + 1, K1 = N1 * N2 + 1;
+    constexpr int RS0 = (N1 * N2P > K1 ? N1 * N2P : K1), RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
     const size_t sm = (size_t)RW * RS * sizeof(float2);
-    cudaFuncSetAttribute(k_xinv_reg<N1, N2, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_xinv_reg<N1, N2, RW><<<dim3(xi.g.sx2 / RW, nout, 3), RW * N2, sm, st>>>(xi);
+    // 16-byte output rows: float4 epilogue
+    bool v4 = xi.rp % 4 == 0 && xi.pp % 4 == 0;
+    for (int k = 0; k < 3; k++) {
+        v4 = v4 && ((uintptr_t)xi.out[k] % 16 == 0);
+        if (xi.base[k]) v4 = v4 && ((uintptr_t)xi.base[k] % 16 == 0);
+    }
+    const dim3 grid(xi.g.sx2 / RW, nout, 3);
+    if (v4) {
+        cudaFuncSetAttribute(k_xinv_reg<N1, N2, RW, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_xinv_reg<N1, N2, RW, 4><<<grid, RW * N2, sm, st>>>(xi);
+    } else {
+        cudaFuncSetAttribute(k_xinv_reg<N1, N2, RW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_xinv_reg<N1, N2, RW, 2><<<grid, RW * N2, sm, st>>>(xi);
+    }
     return cudaGetLastError();
 }
 
 static bool xinv_reg(const XiArgs &xi, int nout, cudaStream_t st, cudaError_t *e)
 {
     if (xi.g.sx2 % 32) return false;
+    // the epilogue moves at least float2: even pitches, 8-byte aligned rows
+    if (xi.rp % 2 || xi.pp % 2) return false;
+    for (int k = 0; k < 3; k++)
+        if ((uintptr_t)xi.out[k] % 8 || (uintptr_t)xi.base[k] % 8) return false;
     switch (xi.g.M) {
     case 64: *e = launch_xinv_reg<8, 8>(xi, nout, st); return true;
     case 128: *e = launch_xinv_reg<16, 8>(xi, nout, st); return true;
