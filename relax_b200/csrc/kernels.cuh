@@ -324,13 +324,20 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(StressArgs a)
     }
 
     if (MODE == MODE_INIT || MODE == MODE_END || MODE == MODE_EIGEN) {
-        const float t0 = block_min(tmin[0], shf);
-        __syncthreads();
-        const float t1 = block_min(tmin[1], shf);
-        __syncthreads();
-        const double am = block_sum(amp_m, shd);
-        __syncthreads();
-        const double at = block_sum(amp_t, shd);
+        // the four block reductions in one pass (fixed order, one barrier)
+        float t0 = warp_min(tmin[0]), t1 = warp_min(tmin[1]);
+        double am = warp_sum(amp_m), at = warp_sum(amp_t);
+        {
+            const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+            if (l == 0) { shf[w] = t0; shf[16 + w] = t1; shd[w] = am; shd[16 + w] = at; }
+            __syncthreads();
+            if (w == 0) {
+                t0 = warp_min(l < nw ? shf[l] : 3.0e38f);
+                t1 = warp_min(l < nw ? shf[16 + l] : 3.0e38f);
+                am = warp_sum(l < nw ? shd[l] : 0.0);
+                at = warp_sum(l < nw ? shd[16 + l] : 0.0);
+            }
+        }
         __shared__ unsigned last;
         if (threadIdx.x == 0) {
             a.tm_part[blockIdx.x] = t0;
@@ -1209,10 +1216,14 @@ __global__ void __launch_bounds__(CW *N2) k_ypass_reg(YArgs a)
     extern __shared__ float2 smy[];
     const Grid &g = a.g;
     const int c = threadIdx.x % CW, t = threadIdx.x / CW;
-    const int k1t = blockIdx.x * CW;
-    const bool ok = k1t + c < g.K1;
-    const int p = (a.traction && (int)blockIdx.y == a.nbody) ? g.sx3 : (int)blockIdx.y;
-    const size_t base = sidx(g, blockIdx.z, p, 0, k1t + c);
+    // columns (component, plane, k1) flattened: f = (cp np + pi) K1 + k1
+    const int np = a.nbody + a.traction;
+    const int f = blockIdx.x * CW + c;
+    const bool ok = f < 3 * np * g.K1;
+    const int cp = ok ? f / (np * g.K1) : 0, rem = ok ? f % (np * g.K1) : 0;
+    const int pi = rem / g.K1, k1c = rem % g.K1;
+    const int p = (a.traction && pi == a.nbody) ? g.sx3 : pi;
+    const size_t base = sidx(g, cp, p, 0, k1c);
     float2 x[N1];
 #pragma unroll
     for (int j1 = 0; j1 < N1; j1++)
@@ -1245,14 +1256,14 @@ __global__ void __launch_bounds__(CW *N2) k_ypass_reg(YArgs a)
 // [n/2, n) are zero and only output planes [0, n/2) are wanted (the step's
 // Green's functions); otherwise nin/nout are honoured.
 template <int N1, int N2, int CW, bool PRUNED>
-__global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(ZArgs a)
+__global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(ZArgs a)
 {
     constexpr int n = N1 * N2, Q = N1 / N2;
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
     extern __shared__ float2 smz[];
     float2 *U = smz;                                                   // [3][N1][N2][CW]
-    double *red = reinterpret_cast<double *>(smz + 3 * n * CW);        // [N2][CW][13]
-    float *colc = reinterpret_cast<float *>(red + N2 * CW * 13);       // [CW][17]
+    float *red = reinterpret_cast<float *>(smz + 3 * n * CW);          // [N2][12][CW]
+    float *colc = red + N2 * 12 * CW;                                  // [CW][17]
     const Grid &g = a.g;
     const int c = threadIdx.x % CW, t = threadIdx.x / CW;
     // columns (k1, k2) flattened over the plane: col = k2 K1 + k1
@@ -1299,7 +1310,10 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
     // B = ratio1 / r2^2 (src/green.f90:78-90 rearranged); surface traction
     // from the FP64 sums Sk_i = sum k3 u_i and S_i = sum u_i over k3
     const float ra = a.ratio1 * (1.f + a.ratio2);
-    double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // FP32 partial sums of jw u_i (k3 = jw / (n dx3)) and of u_i over this
+    // thread's k3; the reference accumulates these in REAL*4 over all k3
+    // (src/green.f90:365-367)
+    float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int q = 0; q < Q; q++) {
         const int k1 = t + N2 * q;
@@ -1333,19 +1347,20 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
             U[uidx(0, k1, k2)] = u1;
             U[uidx(1, k1, k2)] = u2;
             U[uidx(2, k1, k2)] = u3;
-            acc[0] = fma(k3v, (double)u1.x, acc[0]); acc[1] = fma(k3v, (double)u1.y, acc[1]);
-            acc[2] = fma(k3v, (double)u2.x, acc[2]); acc[3] = fma(k3v, (double)u2.y, acc[3]);
-            acc[4] = fma(k3v, (double)u3.x, acc[4]); acc[5] = fma(k3v, (double)u3.y, acc[5]);
+            const float w = (float)jw;
+            acc[0] += w * u1.x; acc[1] += w * u1.y; acc[2] += w * u2.x;
+            acc[3] += w * u2.y; acc[4] += w * u3.x; acc[5] += w * u3.y;
             acc[6] += u1.x; acc[7] += u1.y; acc[8] += u2.x; acc[9] += u2.y; acc[10] += u3.x; acc[11] += u3.y;
         }
     }
 #pragma unroll
-    for (int qq = 0; qq < 12; qq++) red[(t * CW + c) * 13 + qq] = acc[qq];
+    for (int qq = 0; qq < 12; qq++) red[(t * 12 + qq) * CW + c] = acc[qq];
     __syncthreads();
     if (t == 0) {
         double s[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int tt = 0; tt < N2; tt++)
-            for (int qq = 0; qq < 12; qq++) s[qq] += red[(tt * CW + c) * 13 + qq];
+            for (int qq = 0; qq < 12; qq++) s[qq] += (double)red[(tt * 12 + qq) * CW + c];
+        for (int qq = 0; qq < 6; qq++) s[qq] *= inv_l3;
         float *cc = colc + c * 17;
         for (int qq = 0; qq < 16; qq++) cc[qq] = 0.f;
         if (ok && !(k1v == 0.0 && k2v == 0.0)) {
@@ -1454,231 +1469,6 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 3) k_zspec_sm(Z
         }
     }
     (void)x;
-}
-
-// pass 3, phased version: 3 x CW x N2 threads per block of CW columns, each
-// phase with its own assignment of threads to work so that no thread holds
-// more than one component's N1 values:
-//   A   (component, column, t): forward stage A of one component
-//   B   (component, column, t): forward stage B, natural order k3
-//   E   (column, s): elastic response at points k3 = s, s + 3 N2, ...,
-//       with per-thread FP32 partial sums of k3 u_i and u_i
-//   R   (column, sum): FP64 sums of the partials; then one thread per column
-//       forms the surface traction and the Cerruti coefficients
-//   C   (component, column, t): Cerruti correction, inverse stage B
-//   D   (component, column, t): inverse stage A and store
-// PRUNED: input planes [n/2, n) are zero and only output planes [0, n/2)
-// are written (the step's Green's functions); otherwise nin/nout hold.
-template <int N1, int N2, int CW, bool PRUNED>
-__global__ void __launch_bounds__(3 * CW * N2, (3 * CW * N2 <= 384) ? 3 : 1) k_zspec_ph(ZArgs a)
-{
-    constexpr int n = N1 * N2, Q = N1 / N2, NT = 3 * CW * N2, NS = NT / CW;
-    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
-    extern __shared__ float2 smz[];
-    float2 *U = smz;                                                   // [3][N1][N2][CW]
-    float *red = reinterpret_cast<float *>(smz + 3 * n * CW);          // [NS][12][CW]
-    double *sums = reinterpret_cast<double *>(red + NS * 12 * CW);     // [12][CW]
-    float *colc = reinterpret_cast<float *>(sums + 12 * CW);           // [CW][17]
-    const Grid &g = a.g;
-    // transform phases: component cp, column c, thread t of the column
-    const int cp = threadIdx.x / (CW * N2), c = threadIdx.x % CW, t = (threadIdx.x / CW) % N2;
-    // columns (k1, k2) flattened over the plane: col = k2 K1 + k1
-    const int col = blockIdx.x * CW + c;
-    const bool ok = col < g.sx2 * g.K1;
-    const int k2i = ok ? col / g.K1 : 0, k1c = ok ? col % g.K1 : 0;
-    const double PI2 = 6.28318530717958623199592693708837032318;
-    const double inv_l3 = 1.0 / (n * g.dx3);
-    auto uidx = [&](int cc, int k1, int j) { return ((cc * N1 + k1) * N2 + j) * CW + c; };
-
-    // ---- A: forward stage A
-    {
-        constexpr int NL = PRUNED ? N1 / 2 : N1;
-        float2 z[N1];
-#pragma unroll
-        for (int j1 = 0; j1 < N1; j1++) {
-            const int i3 = N2 * j1 + t;
-            const bool ld = j1 < NL && ok && (PRUNED || i3 < a.nin);
-            z[j1] = ld ? a.S[sidx(g, cp, i3, k2i, k1c)] : make_float2(0.f, 0.f);
-        }
-        RDft<N1, -1>::run(z);
-#pragma unroll
-        for (int k1 = 0; k1 < N1; k1++) U[uidx(cp, k1, t)] = k1 && t ? cmul(z[k1], twn<-1>(a.pz.tw, t * k1)) : z[k1];
-    }
-    __syncthreads();
-    // ---- B: forward stage B; k3 = k1 + N1 k2 lands in U[cp][k1][k2]
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-        const int k1 = t + N2 * q;
-        float2 y[N2];
-#pragma unroll
-        for (int jj = 0; jj < N2; jj++) y[jj] = U[uidx(cp, k1, jj)];
-        RDft<N2, -1>::run(y);
-#pragma unroll
-        for (int k2 = 0; k2 < N2; k2++) U[uidx(cp, k1, k2)] = y[k2];
-    }
-    __syncthreads();
-
-    // ---- E: elastic response u = A c - B k (k.c), A = ratio1 (1 + ratio2) / r2,
-    // B = ratio1 / r2^2 (elasticresponse, src/green.f90:78-90, rearranged)
-    const double k1v = (double)k1c / (g.sx1 * g.dx1);
-    const double k2v = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
-    {
-        const int s = threadIdx.x / CW;
-        const float k1f = (float)k1v, k2f = (float)k2v;
-        const float k12 = k1f * k1f + k2f * k2f;
-        const float ra = a.ratio1 * (1.f + a.ratio2);
-        const float il3 = (float)inv_l3;
-        // partial sums over k3 of jw u_i (k3 = jw / (n dx3)) and of u_i
-        float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int i = 0; i < (n + NS - 1) / NS; i++) {
-            const int j = s + NS * i;
-            if (j < n) {
-                const int k1 = j % N1, k2 = j / N1;
-                const int jw = j < n / 2 ? j : j - n;
-                const float k3f = (float)((double)jw * inv_l3);
-                const float2 c1 = U[uidx(0, k1, k2)], c2 = U[uidx(1, k1, k2)], c3 = U[uidx(2, k1, k2)];
-                const float r2 = k12 + k3f * k3f;
-                float2 u1, u2, u3;
-                if (r2 > 0.f) {
-                    const float ir2 = 1.f / r2;
-                    const float A = ra * ir2, B = a.ratio1 * ir2 * ir2;
-                    const float kcr = k1f * c1.x + k2f * c2.x + k3f * c3.x;
-                    const float kci = k1f * c1.y + k2f * c2.y + k3f * c3.y;
-                    u1 = make_float2(A * c1.x - B * k1f * kcr, A * c1.y - B * k1f * kci);
-                    u2 = make_float2(A * c2.x - B * k2f * kcr, A * c2.y - B * k2f * kci);
-                    u3 = make_float2(A * c3.x - B * k3f * kcr, A * c3.y - B * k3f * kci);
-                } else {
-                    u1 = u2 = u3 = make_float2(0.f, 0.f);
-                }
-                U[uidx(0, k1, k2)] = u1;
-                U[uidx(1, k1, k2)] = u2;
-                U[uidx(2, k1, k2)] = u3;
-                const float w = (float)jw;
-                acc[0] += w * u1.x; acc[1] += w * u1.y; acc[2] += w * u2.x;
-                acc[3] += w * u2.y; acc[4] += w * u3.x; acc[5] += w * u3.y;
-                acc[6] += u1.x; acc[7] += u1.y; acc[8] += u2.x; acc[9] += u2.y; acc[10] += u3.x; acc[11] += u3.y;
-            }
-        }
-        (void)il3;
-#pragma unroll
-        for (int qq = 0; qq < 12; qq++) red[(s * 12 + qq) * CW + c] = acc[qq];
-    }
-    __syncthreads();
-    // ---- R: FP64 sums, one thread per (sum, column)
-    if (threadIdx.x < 12 * CW) {
-        const int qq = threadIdx.x / CW;
-        double v = 0.0;
-#pragma unroll 4
-        for (int s = 0; s < NS; s++) v += (double)red[(s * 12 + qq) * CW + c];
-        sums[qq * CW + c] = qq < 6 ? v * inv_l3 : v;
-    }
-    __syncthreads();
-    if (threadIdx.x < CW) {
-        double s[12];
-#pragma unroll
-        for (int qq = 0; qq < 12; qq++) s[qq] = sums[qq * CW + c];
-        float *cc = colc + c * 17;
-        for (int qq = 0; qq < 14; qq++) cc[qq] = 0.f;
-        const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
-        if (ok && !(k1v == 0.0 && k2v == 0.0)) {
-            // surfacetractioncowling (src/green.f90:356-366): i 2pi (...) - grav u3
-            const double modulus = a.lambda + 2.0 * a.mu;
-            const double grav = 2.0 * a.mu * alpha * a.gam;
-            const double a1r = a.mu * (s[0] + k1v * s[10]), a1i = a.mu * (s[1] + k1v * s[11]);
-            const double a2r = a.mu * (s[2] + k2v * s[10]), a2i = a.mu * (s[3] + k2v * s[11]);
-            const double a3r = modulus * s[4] + a.lambda * (k1v * s[6] + k2v * s[8]);
-            const double a3i = modulus * s[5] + a.lambda * (k1v * s[7] + k2v * s[9]);
-            const double sum[6] = {-PI2 * a1i, PI2 * a1r, -PI2 * a2i, PI2 * a2r,
-                                   -PI2 * a3i - grav * s[10], PI2 * a3r - grav * s[11]};
-            const double d = (double)n * g.dx3;
-            double p[6];
-            for (int k = 0; k < 3; k++) {
-                const float2 tc = a.S[sidx(g, k, g.sx3, k2i, k1c)];
-                p[2 * k] = (double)tc.x - sum[2 * k] / d;
-                p[2 * k + 1] = (double)tc.y - sum[2 * k + 1] / d;
-            }
-            // cerrutisolmodified (src/green.f90:578-609) written as
-            // u_i += fi (P_i + g R_i), g = 2 pi k3 fi, with per-column P_i, R_i
-            const double beta = PI2 * sqrt(k1v * k1v + k2v * k2v);
-            const double h = a.gam / beta;
-            const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
-            const double b1r = p[0] * c0, b1i = p[1] * c0, b2r = p[2] * c0, b2i = p[3] * c0;
-            const double qr = PI2 * k1v * p[0] + PI2 * k2v * p[2], qi = PI2 * k1v * p[1] + PI2 * k2v * p[3];
-            const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
-            const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
-            const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
-            const double Qr = b1r * k1v + b2r * k2v, Qi = b1i * k1v + b2i * k2v;
-            const double ab = alpha * beta * PI2, er = 1.0 - 1.0 / alpha, ab2 = -alpha * beta * beta;
-            const double ap = alpha * PI2 * PI2, bb = 2.0 * beta * beta;
-            // P_1 = i k1 ab er b3 - 2 beta^2 b1' + ap k1 Q ; R_1 = k1 ab b3 - i ap k1 Q
-            cc[0] = (float)(-k1v * ab * er * b3i - bb * b1r + ap * k1v * Qr);
-            cc[1] = (float)(k1v * ab * er * b3r - bb * b1i + ap * k1v * Qi);
-            cc[2] = (float)(k1v * ab * b3r + ap * k1v * Qi);
-            cc[3] = (float)(k1v * ab * b3i - ap * k1v * Qr);
-            cc[4] = (float)(-k2v * ab * er * b3i - bb * b2r + ap * k2v * Qr);
-            cc[5] = (float)(k2v * ab * er * b3r - bb * b2i + ap * k2v * Qi);
-            cc[6] = (float)(k2v * ab * b3r + ap * k2v * Qi);
-            cc[7] = (float)(k2v * ab * b3i - ap * k2v * Qr);
-            // P_3 = ab2 b3 / alpha ; R_3 = -i ab2 b3 + alpha beta 2pi Q
-            cc[8] = (float)(ab2 * b3r / alpha);
-            cc[9] = (float)(ab2 * b3i / alpha);
-            cc[10] = (float)(ab2 * b3i + alpha * beta * PI2 * Qr);
-            cc[11] = (float)(-ab2 * b3r + alpha * beta * PI2 * Qi);
-            cc[12] = (float)beta;
-            cc[13] = 1.f;
-        }
-    }
-    __syncthreads();
-
-    // ---- C: Cerruti correction of this component, inverse stage B, twiddle
-    {
-        const float *cq = colc + c * 17;
-        const float P0 = cq[4 * cp], P1 = cq[4 * cp + 1], R0 = cq[4 * cp + 2], R1 = cq[4 * cp + 3];
-        const float beta = cq[12];
-        const bool cerr = cq[13] != 0.f;
-        const float pi2 = 6.28318530717958623f;
-        const float b2 = beta * beta;
-        const float il3 = (float)inv_l3;
-#pragma unroll
-        for (int q = 0; q < Q; q++) {
-            const int k1 = t + N2 * q;
-            float2 y[N2];
-#pragma unroll
-            for (int k2 = 0; k2 < N2; k2++) {
-                float2 u = U[uidx(cp, k1, k2)];
-                if (cerr) {
-                    const int j = k1 + N1 * k2;
-                    const float k3f = (float)(j < n / 2 ? j : j - n) * il3;
-                    const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + b2);
-                    const float gg = pi2 * k3f * fi;
-                    u.x += fi * (P0 + gg * R0);
-                    u.y += fi * (P1 + gg * R1);
-                }
-                y[k2] = u;
-            }
-            RDft<N2, +1>::run(y);
-#pragma unroll
-            for (int jj = 0; jj < N2; jj++)
-                U[uidx(cp, k1, jj)] = jj && k1 ? cmul(y[jj], twn<+1>(a.pz.tw, jj * k1)) : y[jj];
-        }
-    }
-    __syncthreads();
-
-    // ---- D: inverse stage A and store
-    {
-        float2 z[N1];
-#pragma unroll
-        for (int k1 = 0; k1 < N1; k1++) z[k1] = U[uidx(cp, k1, t)];
-        RDft<N1, +1>::run(z);
-        if (ok) {
-#pragma unroll
-            for (int j1 = 0; j1 < N1; j1++) {
-                const int i3 = N2 * j1 + t;
-                if (PRUNED ? j1 < N1 / 2 : i3 < a.nout) a.S[sidx(g, cp, i3, k2i, k1c)] = z[j1];
-            }
-        }
-    }
 }
 
 // pass 5: C2R along x1, scaled by 2/(sx1 dx1 sx2 dx2 sx3 dx3), with the

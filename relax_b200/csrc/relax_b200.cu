@@ -170,8 +170,11 @@ static cudaError_t launch_ypass_reg(const YArgs &ya, int sign, dim3 grid, cudaSt
     return cudaGetLastError();
 }
 
-static bool ypass_reg(const YArgs &ya, int sign, dim3 grid, cudaStream_t st, cudaError_t *e)
+static bool ypass_reg(const YArgs &ya, int sign, cudaStream_t st, cudaError_t *e)
 {
+    // CW columns per block over the flattened (component, plane, k1) columns
+    const size_t ncol = (size_t)3 * (ya.nbody + ya.traction) * ya.g.K1;
+    const dim3 grid((unsigned)((ncol + kCW - 1) / kCW));
     switch (ya.g.sx2) {
     case 64: *e = launch_ypass_reg<8, 8>(ya, sign, grid, st); return true;
     case 128: *e = launch_ypass_reg<16, 8>(ya, sign, grid, st); return true;
@@ -184,7 +187,7 @@ static bool ypass_reg(const YArgs &ya, int sign, dim3 grid, cudaStream_t st, cud
 template <int N1, int N2>
 static cudaError_t launch_zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st)
 {
-    const size_t sm = 3 * (size_t)N1 * N2 * kCW * sizeof(float2) + (size_t)N2 * kCW * 13 * sizeof(double) +
+    const size_t sm = 3 * (size_t)N1 * N2 * kCW * sizeof(float2) + (size_t)N2 * 12 * kCW * sizeof(float) +
                       (size_t)kCW * 17 * sizeof(float);
     const bool pruned = 2 * za.nin == za.g.sx3 && 2 * za.nout == za.g.sx3;
     if (pruned) {
@@ -366,7 +369,7 @@ struct Spectral {
         YArgs ya{g, S, py, twy, nin, 1};
         cudaError_t re = cudaSuccess;
         if (use_reg) {
-            TIMED(prof, ST_YFWD, st, (ya.tw = kCW, yreg = ypass_reg(ya, -1, dim3((g.K1 + kCW - 1) / kCW, nin + 1, 3), st, &re)));
+            TIMED(prof, ST_YFWD, st, (ya.tw = kCW, yreg = ypass_reg(ya, -1, st, &re)));
             if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_ypass_reg: %s", cudaGetErrorString(re));
         }
         if (!use_reg || !yreg) {
@@ -392,7 +395,7 @@ struct Spectral {
         bool yr2 = false;
         if (use_reg) {
             yb.tw = kCW;
-            TIMED(prof, ST_YINV, st, (yr2 = ypass_reg(yb, +1, dim3((g.K1 + kCW - 1) / kCW, nout, 3), st, &re)));
+            TIMED(prof, ST_YINV, st, (yr2 = ypass_reg(yb, +1, st, &re)));
             if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_ypass_reg: %s", cudaGetErrorString(re));
         }
         if (!yr2) {
