@@ -107,12 +107,11 @@ def kernel_bytes(sim):
     nh = sx1 * sx2 * h
     K1 = sx1 // 2 + 1
     spec_plane = 3 * sx2 * K1 * 8          # one x3-plane of the 3-component spectrum
-    sig = 24 if sim.planes else 0
     return {
-        # tau, m, u in; tau, m (+ sig with afterslip planes) out
-        "k_stress<END>": nh * (24 + 24 + 12 + 24 + 24 + sig),
-        # m, tau, v, gamma in; m, gamma (+ sig) out
-        "k_stress<CORR>": nh * (24 + 24 + 12 + 4 + 24 + 4 + sig),
+        # tau, m, u in; tau, m out (sig is stored only on the afterslip bands)
+        "k_stress<END>": nh * (24 + 24 + 12 + 24 + 24),
+        # m, tau, v, gamma in; m, gamma out
+        "k_stress<CORR>": nh * (24 + 24 + 12 + 4 + 24 + 4),
         # moment in, spectrum (body planes + traction plane) out
         "k_xfwd": nh * 24 + (h + 1) * spec_plane,
         "k_ypass<fwd>": 2 * (h + 1) * spec_plane,

@@ -111,11 +111,14 @@ struct StressArgs {
     unsigned *ticket;        // INIT/END: blocks done (zero between launches), or null
     StepState *fin;          // with ticket: receives tmin, power, cei
     double dv;               // cell volume dx1 dx2 dx3 (amplitude scale)
+    const struct StressArgs *tab;   // batched launch: one entry per member (blockIdx.y)
 };
 
-template <int MODE>
-__global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(StressArgs a)
+// BATCH: blockIdx.y selects a member of a batch, whose arguments are a0.tab[blockIdx.y]
+template <int MODE, bool BATCH = false>
+__global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(const __grid_constant__ StressArgs a0)
 {
+    const StressArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     __shared__ float shf[32];
     __shared__ double shd[32];
     if (MODE == MODE_END && a.st->fire) return;   // the event branch of the step runs instead
@@ -598,12 +601,15 @@ struct FrictionPtsArgs {
     int want_tm;
     float *tm_part;
     int *err;
+    const struct FrictionPtsArgs *tab;   // batched launch: one entry per member (blockIdx.y)
 };
 
 // frictioneigenstress on the band points of one plane (the per-step part of
 // src/friction3d.f90:185-235)
-__global__ void __launch_bounds__(RELAX_NTHREADS) k_friction_pts(FrictionPtsArgs a)
+template <bool BATCH = false>
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_friction_pts(const __grid_constant__ FrictionPtsArgs a0)
 {
+    const FrictionPtsArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     __shared__ float shf[32];
     const Grid &g = a.g;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -663,6 +669,7 @@ struct MonitorArgs {
     relax_slippatch *patch;
     int px2, px3;
     const StepState *st;
+    const struct MonitorArgs *tab;   // batched launch: one entry per member (blockIdx.y)
 };
 
 // Position of patch t of a plane and the grid cell it samples (the nearest
@@ -713,8 +720,10 @@ __global__ void k_mark_monitor(MonitorArgs a, unsigned char *mask)
     if (monitor_cell(a, t, X, &yr, &zr, &o, &i3)) mask[o >> 2] = 1;
 }
 
-__global__ void k_monitor(MonitorArgs a)
+template <bool BATCH = false>
+__global__ void k_monitor(const __grid_constant__ MonitorArgs a0)
 {
+    const MonitorArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.px2 * a.px3) return;
     const Grid &g = a.g;
@@ -788,6 +797,7 @@ struct XfArgs {
     size_t trp;
     const float *tload;      // optional surface load added to t3 (sx1 x sx2)
     float scale3, scale2;
+    const struct XfArgs *tab;   // batched launch: one entry per member (blockIdx.z)
 };
 
 template <int XIN>
@@ -873,9 +883,10 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xfwd(XfArgs a)
 // The body force of the block's rows is first built in the row buffers with
 // float4 loads (x neighbours by warp shuffle, one wrap-around load per warp
 // edge), then each row thread picks its stride-N2 elements from there.
-template <int XIN, int N1, int N2, int RW>
-__global__ void __launch_bounds__(RW *N2, (RW * N2 <= 128) ? 8 : 4) k_xfwd_reg(XfArgs a)
+template <int XIN, int N1, int N2, int RW, bool BATCH = false>
+__global__ void __launch_bounds__(RW *N2, (RW * N2 <= 128) ? 8 : 4) k_xfwd_reg(const __grid_constant__ XfArgs a0)
 {
+    const XfArgs &a = BATCH ? a0.tab[blockIdx.z] : a0;
     constexpr int M = N1 * N2, Q = N1 / N2, N2P = N2 + 1, NT = RW * N2;
     constexpr int RS0 = (N1 * N2P > M + 1 ? N1 * N2P : M + 1);
     constexpr int RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
@@ -1009,6 +1020,7 @@ struct YArgs {
     int tw;            // tile width (k1 columns)
     int nbody;         // body planes [0, nbody)
     int traction;      // also the traction plane (index nbody of blockIdx.y)
+    const struct YArgs *tab;   // batched launch: one entry per member (blockIdx.y)
 };
 
 template <int SIGN>
@@ -1051,6 +1063,7 @@ struct ZArgs {
     int tw, nin, nout;
     float ratio1, ratio2;            // elastic response constants
     double lambda, mu, gam;
+    const struct ZArgs *tab;         // batched launch: one entry per member (blockIdx.y)
 };
 
 __global__ void __launch_bounds__(RELAX_NTHREADS) k_zspec(ZArgs a)
@@ -1208,9 +1221,10 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_zspec(ZArgs a)
 // ------------------------------------------------------------------------
 
 // pass 2 / 4 along x2
-template <int N1, int N2, int CW, int SIGN>
-__global__ void __launch_bounds__(CW *N2) k_ypass_reg(YArgs a)
+template <int N1, int N2, int CW, int SIGN, bool BATCH = false>
+__global__ void __launch_bounds__(CW *N2) k_ypass_reg(const __grid_constant__ YArgs a0)
 {
+    const YArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     constexpr int n = N1 * N2, Q = N1 / N2;
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
     extern __shared__ float2 smy[];
@@ -1255,9 +1269,10 @@ __global__ void __launch_bounds__(CW *N2) k_ypass_reg(YArgs a)
 // thread holds one N1 or 3 x N2 group at a time.  PRUNED: input planes
 // [n/2, n) are zero and only output planes [0, n/2) are wanted (the step's
 // Green's functions); otherwise nin/nout are honoured.
-template <int N1, int N2, int CW, bool PRUNED>
-__global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(ZArgs a)
+template <int N1, int N2, int CW, bool PRUNED, bool BATCH = false>
+__global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(const __grid_constant__ ZArgs a0)
 {
+    const ZArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     constexpr int n = N1 * N2, Q = N1 / N2;
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
     extern __shared__ float2 smz[];
@@ -1484,6 +1499,7 @@ struct XiArgs {
     size_t rp, pp;           // pitches of out/base
     const StepState *st;     // coef = cmul * Dt (or cmul when st is null)
     float cmul, scale;
+    const struct XiArgs *tab;   // batched launch: one entry per member (blockIdx.z / 3)
 };
 
 __global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
@@ -1528,9 +1544,10 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
 // row, with the field update out = base + coef * w.  Shared-memory rows are
 // padded (N2+1 per k1 group, row stride = 8 mod 16 float2) so both transpose
 // access patterns are free of bank conflicts.
-template <int N1, int N2, int RW, int V>
-__global__ void __launch_bounds__(RW *N2) k_xinv_reg(XiArgs a)
+template <int N1, int N2, int RW, int V, bool BATCH = false>
+__global__ void __launch_bounds__(RW *N2) k_xinv_reg(const __grid_constant__ XiArgs a0)
 {
+    const XiArgs &a = BATCH ? a0.tab[blockIdx.z / 3] : a0;
     // RW rows of one plane and component per block, N2 threads per row.
     // (A) the block's spectrum rows, one contiguous run of RW*K1 values
     //     in S, are staged in shared memory with 16-byte loads;
@@ -1546,7 +1563,7 @@ __global__ void __launch_bounds__(RW *N2) k_xinv_reg(XiArgs a)
     extern __shared__ float2 smx[];
     const Grid &g = a.g;
     const int t = threadIdx.x % N2, r = threadIdx.x / N2;
-    const int i2b = blockIdx.x * RW, i3 = blockIdx.y, c = blockIdx.z;
+    const int i2b = blockIdx.x * RW, i3 = blockIdx.y, c = blockIdx.z % 3;
 
     // (A) rows i2b .. i2b+RW-1 are contiguous: sidx is linear in i2
     {
@@ -1643,8 +1660,8 @@ struct DtIn {
     int oi, use_override;
 };
 
-__global__ void k_dt(StepState *st, DtPolicy pol, DtIn in, const float *tm_part, int ntm,
-                     const float *fr_part, int nfr)
+__device__ __forceinline__ void dt_body(StepState *st, const DtPolicy &pol, const DtIn &in, const float *tm_part,
+                                        int ntm, const float *fr_part, int nfr)
 {
     __shared__ float shf[32];
     float m0 = 3.0e38f, m1 = 3.0e38f, m2 = 3.0e38f;
@@ -1699,6 +1716,27 @@ __global__ void k_dt(StepState *st, DtPolicy pol, DtIn in, const float *tm_part,
         // (src/relax.f90:859) instead of the END stress pass
         st->fire = ok && pol.has_next_event && fabs((t + Dt) - pol.next_event_time) < 1e-6;
     }
+}
+
+__global__ void k_dt(StepState *st, DtPolicy pol, DtIn in, const float *tm_part, int ntm,
+                     const float *fr_part, int nfr)
+{
+    dt_body(st, pol, in, tm_part, ntm, fr_part, nfr);
+}
+
+// one block per member of a batch
+struct DtArgs {
+    StepState *st;
+    DtPolicy pol;
+    DtIn in;
+    const float *fr_part;
+    int nfr;
+};
+
+__global__ void k_dt_batch(const DtArgs *tab)
+{
+    const DtArgs &a = tab[blockIdx.x];
+    dt_body(a.st, a.pol, a.in, nullptr, 0, a.fr_part, a.nfr);
 }
 
 // fixed-order sums of the amplitude partials -> power, C:E^i of the log
