@@ -214,6 +214,36 @@ int relax_profile_read(relax_ctx *ctx, int stage, double *total_ms,
 int relax_launch_count(relax_ctx *ctx, long long *n);
 
 /* ------------------------------------------------------------------ */
+/* batches (ensembles)                                                */
+/*                                                                    */
+/* No reference counterpart: RELAX runs one simulation per process.   */
+/* A batch holds members that share the grid (sx, dx), the elastic    */
+/* constants (lambda, mu, gam) and the number of afterslip planes;    */
+/* they differ in events, rheology, prestress, weak zones and plane   */
+/* geometry.  relax_batch_step advances every member by one RK2 step  */
+/* (each with its own adaptive Dt) with one launch per stage for all  */
+/* members and one host synchronisation; members whose time reached   */
+/* the interval stay put and report i = 0.  Grids without the         */
+/* register-resident passes (lengths other than 64/128/256 along x1    */
+/* and x3, 64..512 along x2) step the members in turn.  Events with   */
+/* surface loads are rejected (RELAX_ERR_UNSUPPORTED).  Each member is */
+/* a relax_ctx owned by the batch (relax_batch_member) for field and   */
+/* patch access; do not destroy or step it directly.                  */
+/* ------------------------------------------------------------------ */
+typedef struct relax_batch relax_batch;
+
+int relax_batch_create(const relax_config *members, int n, int device, relax_batch **batch);
+int relax_batch_destroy(relax_batch *batch);
+int relax_batch_size(relax_batch *batch, int *n);
+int relax_batch_member(relax_batch *batch, int k, relax_ctx **member);
+/* coseismic solve of event 0 of every member; logs: n entries or NULL */
+int relax_batch_coseismic(relax_batch *batch, relax_step_log *logs);
+/* logs: n entries */
+int relax_batch_step(relax_batch *batch, relax_step_log *logs);
+int relax_batch_launch_count(relax_batch *batch, long long *n);
+int relax_batch_get_stream(relax_batch *batch, void **stream);
+
+/* ------------------------------------------------------------------ */
 /* stateless operators on device buffers (reference layout)           */
 /*                                                                    */
 /* Each takes device pointers in RELAX's layout and a CUDA stream      */

@@ -73,6 +73,14 @@ def load() -> C.CDLL:
         "relax_profile_stages": (I, []),
         "relax_profile_read": (I, [P, I, C.POINTER(D), C.POINTER(I), C.POINTER(C.c_char_p)]),
         "relax_launch_count": (I, [P, C.POINTER(C.c_longlong)]),
+        "relax_batch_create": (I, [C.POINTER(relax_config), I, I, C.POINTER(P)]),
+        "relax_batch_destroy": (I, [P]),
+        "relax_batch_size": (I, [P, C.POINTER(I)]),
+        "relax_batch_member": (I, [P, I, C.POINTER(P)]),
+        "relax_batch_coseismic": (I, [P, C.POINTER(relax_step_log)]),
+        "relax_batch_step": (I, [P, C.POINTER(relax_step_log)]),
+        "relax_batch_launch_count": (I, [P, C.POINTER(C.c_longlong)]),
+        "relax_batch_get_stream": (I, [P, C.POINTER(P)]),
         "relax_op_stressupdate": (I, [P, P, P, D, D, D, D, D, I, I, I, P, P]),
         "relax_op_bodyforce": (I, [P, D, D, D, I, I, I, P, P, P, P, P, P, P]),
         "relax_op_viscouseigenstress": (I, [D, P, P, P, I, I, I, P, C.POINTER(D), P, P, P]),

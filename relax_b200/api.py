@@ -126,3 +126,84 @@ class Relax:
         e = C.c_int()
         _lib.check(self.lib.relax_get_time(self.h, C.byref(t), C.byref(i), C.byref(e)))
         return t.value, i.value, e.value
+
+
+class _Member(Relax):
+    """A batch member: field, patch and time access through the member's
+    context, which the batch owns."""
+
+    def __init__(self, lib, sim: Simulation, cfg, handle):
+        self.lib = lib
+        self.sim = sim
+        self.cfg = cfg
+        self.h = handle
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Members sharing grid and elastic constants, stepped together.
+
+        with Batch([sim_a, sim_b, ...]) as b:
+            b.coseismic()
+            for _ in range(100):
+                logs = b.step()          # one log tuple per member
+            u0 = b.member(0).field("u")
+    """
+
+    def __init__(self, sims: Sequence[Simulation], device: int = 0):
+        self.lib = _lib.load()
+        self.sims = list(sims)
+        cfgs, self._keep = [], []
+        for s in self.sims:
+            cfg, keep = s.to_c(_lib.structure_fn)
+            cfgs.append(cfg)
+            self._keep.append(keep)
+        self._cfgs = (type(cfgs[0]) * len(cfgs))(*cfgs)
+        h = C.c_void_p()
+        _lib.check(self.lib.relax_batch_create(self._cfgs, len(cfgs), device, C.byref(h)))
+        self.h = h
+        self.n = len(cfgs)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.relax_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def coseismic(self) -> List[tuple]:
+        logs = (relax_step_log * self.n)()
+        _lib.check(self.lib.relax_batch_coseismic(self.h, logs))
+        return [logs[k].as_tuple() for k in range(self.n)]
+
+    def step(self) -> List[tuple]:
+        logs = (relax_step_log * self.n)()
+        _lib.check(self.lib.relax_batch_step(self.h, logs))
+        return [logs[k].as_tuple() for k in range(self.n)]
+
+    def member(self, k: int) -> Relax:
+        h = C.c_void_p()
+        _lib.check(self.lib.relax_batch_member(self.h, k, C.byref(h)))
+        return _Member(self.lib, self.sims[k], self._cfgs[k], h)
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        _lib.check(self.lib.relax_batch_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _lib.check(self.lib.relax_batch_get_stream(self.h, C.byref(s)))
+        return s.value

@@ -892,7 +892,9 @@ __global__ void __launch_bounds__(RW *N2, (RW * N2 <= 128) ? 8 : 4) k_xfwd_reg(c
     constexpr int RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
     constexpr int SX1 = 2 * M, R4 = SX1 / 4, ITS = RW * R4 / NT;
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
-    static_assert(R4 % 32 == 0 && NT % 32 == 0 && (RW * R4) % NT == 0, "a warp stages part of one row");
+    static_assert(NT % 32 == 0 && (RW * R4) % NT == 0, "rows split evenly over the block");
+    // x neighbours by shuffle when every warp stages part of one row
+    constexpr bool SHFL = R4 % 32 == 0;
     static_assert(RS % 2 == 0, "row buffers start on 16 bytes");
     extern __shared__ float2 smx[];
     const Grid &g = a.g;
@@ -921,10 +923,16 @@ __global__ void __launch_bounds__(RW *N2, (RW * N2 <= 128) ? 8 : 4) k_xfwd_reg(c
                 const int row = blockIdx.x * RW + rr;
                 const float *mx = a.m + cx * g.nh + pl + (size_t)row * SX1;
                 const float4 xc = __ldg(reinterpret_cast<const float4 *>(mx + x));
-                float xl = __shfl_up_sync(0xffffffffu, xc.w, 1);
-                float xr = __shfl_down_sync(0xffffffffu, xc.x, 1);
-                if (lane == 0) xl = __ldg(mx + (x + SX1 - 1) % SX1);
-                if (lane == 31) xr = __ldg(mx + (x + 4) % SX1);
+                float xl, xr;
+                if (SHFL) {
+                    xl = __shfl_up_sync(0xffffffffu, xc.w, 1);
+                    xr = __shfl_down_sync(0xffffffffu, xc.x, 1);
+                    if (lane == 0) xl = __ldg(mx + (x + SX1 - 1) % SX1);
+                    if (lane == 31) xr = __ldg(mx + (x + 4) % SX1);
+                } else {
+                    xl = __ldg(mx + (x + SX1 - 1) % SX1);
+                    xr = __ldg(mx + (x + 4) % SX1);
+                }
                 const float *my = a.m + cy * g.nh + pl + x;
                 const float4 yp = __ldg(reinterpret_cast<const float4 *>(my + (size_t)((row + 1) % g.sx2) * SX1));
                 const float4 ym =

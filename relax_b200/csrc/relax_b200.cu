@@ -156,84 +156,119 @@ struct Prof {
 // register-resident column passes for the lengths they are instantiated for
 constexpr int kCW = 16;
 
+// Launch helpers of the register-resident passes.  `nm` members: with
+// nm > 1 the argument struct carries a device table (`tab`) with one entry
+// per member and the batched instantiation runs all members in one launch
+// (the member index is a spare grid dimension).
+template <typename K>
+static void set_smem(K kern, size_t sm)
+{
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+}
+
+template <int N1, int N2, int SIGN>
+static void launch_ypass_sign(const YArgs &ya, dim3 grid, size_t sm, int nm, cudaStream_t st)
+{
+    if (nm > 1) {
+        set_smem(k_ypass_reg<N1, N2, kCW, SIGN, true>, sm);
+        k_ypass_reg<N1, N2, kCW, SIGN, true><<<dim3(grid.x, nm), kCW * N2, sm, st>>>(ya);
+    } else {
+        set_smem(k_ypass_reg<N1, N2, kCW, SIGN>, sm);
+        k_ypass_reg<N1, N2, kCW, SIGN><<<grid, kCW * N2, sm, st>>>(ya);
+    }
+}
+
 template <int N1, int N2>
-static cudaError_t launch_ypass_reg(const YArgs &ya, int sign, dim3 grid, cudaStream_t st)
+static cudaError_t launch_ypass_reg(const YArgs &ya, int sign, dim3 grid, int nm, cudaStream_t st)
 {
     const size_t sm = (size_t)N1 * N2 * kCW * sizeof(float2);
-    if (sign < 0) {
-        cudaFuncSetAttribute(k_ypass_reg<N1, N2, kCW, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_ypass_reg<N1, N2, kCW, -1><<<grid, kCW * N2, sm, st>>>(ya);
-    } else {
-        cudaFuncSetAttribute(k_ypass_reg<N1, N2, kCW, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_ypass_reg<N1, N2, kCW, +1><<<grid, kCW * N2, sm, st>>>(ya);
-    }
+    if (sign < 0) launch_ypass_sign<N1, N2, -1>(ya, grid, sm, nm, st);
+    else launch_ypass_sign<N1, N2, +1>(ya, grid, sm, nm, st);
     return cudaGetLastError();
 }
 
-static bool ypass_reg(const YArgs &ya, int sign, cudaStream_t st, cudaError_t *e)
+static bool ypass_reg(const YArgs &ya, int sign, cudaStream_t st, cudaError_t *e, int nm = 1)
 {
     // CW columns per block over the flattened (component, plane, k1) columns
     const size_t ncol = (size_t)3 * (ya.nbody + ya.traction) * ya.g.K1;
     const dim3 grid((unsigned)((ncol + kCW - 1) / kCW));
     switch (ya.g.sx2) {
-    case 64: *e = launch_ypass_reg<8, 8>(ya, sign, grid, st); return true;
-    case 128: *e = launch_ypass_reg<16, 8>(ya, sign, grid, st); return true;
-    case 256: *e = launch_ypass_reg<16, 16>(ya, sign, grid, st); return true;
-    case 512: *e = launch_ypass_reg<32, 16>(ya, sign, grid, st); return true;
+    case 32: *e = launch_ypass_reg<8, 4>(ya, sign, grid, nm, st); return true;
+    case 96: *e = launch_ypass_reg<24, 4>(ya, sign, grid, nm, st); return true;
+    case 192: *e = launch_ypass_reg<24, 8>(ya, sign, grid, nm, st); return true;
+    case 64: *e = launch_ypass_reg<8, 8>(ya, sign, grid, nm, st); return true;
+    case 128: *e = launch_ypass_reg<16, 8>(ya, sign, grid, nm, st); return true;
+    case 256: *e = launch_ypass_reg<16, 16>(ya, sign, grid, nm, st); return true;
+    case 512: *e = launch_ypass_reg<32, 16>(ya, sign, grid, nm, st); return true;
     default: return false;
     }
 }
 
+template <int N1, int N2, bool PRUNED>
+static void launch_zspec_pr(const ZArgs &za, dim3 grid, size_t sm, int nm, cudaStream_t st)
+{
+    if (nm > 1) {
+        set_smem(k_zspec_sm<N1, N2, kCW, PRUNED, true>, sm);
+        k_zspec_sm<N1, N2, kCW, PRUNED, true><<<dim3(grid.x, nm), kCW * N2, sm, st>>>(za);
+    } else {
+        set_smem(k_zspec_sm<N1, N2, kCW, PRUNED>, sm);
+        k_zspec_sm<N1, N2, kCW, PRUNED><<<grid, kCW * N2, sm, st>>>(za);
+    }
+}
+
 template <int N1, int N2>
-static cudaError_t launch_zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st)
+static cudaError_t launch_zspec_reg(const ZArgs &za, dim3 grid, int nm, cudaStream_t st)
 {
     const size_t sm = 3 * (size_t)N1 * N2 * kCW * sizeof(float2) + (size_t)N2 * 12 * kCW * sizeof(float) +
                       (size_t)kCW * 17 * sizeof(float);
     const bool pruned = 2 * za.nin == za.g.sx3 && 2 * za.nout == za.g.sx3;
-    if (pruned) {
-        cudaFuncSetAttribute(k_zspec_sm<N1, N2, kCW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_zspec_sm<N1, N2, kCW, true><<<grid, kCW * N2, sm, st>>>(za);
-    } else {
-        cudaFuncSetAttribute(k_zspec_sm<N1, N2, kCW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_zspec_sm<N1, N2, kCW, false><<<grid, kCW * N2, sm, st>>>(za);
-    }
+    if (pruned) launch_zspec_pr<N1, N2, true>(za, grid, sm, nm, st);
+    else launch_zspec_pr<N1, N2, false>(za, grid, sm, nm, st);
     return cudaGetLastError();
 }
 
-static bool zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st, cudaError_t *e)
+static bool zspec_reg(const ZArgs &za, dim3 grid, cudaStream_t st, cudaError_t *e, int nm = 1)
 {
     switch (za.g.sx3) {
-    case 64: *e = launch_zspec_reg<8, 8>(za, grid, st); return true;
-    case 128: *e = launch_zspec_reg<16, 8>(za, grid, st); return true;
-    case 256: *e = launch_zspec_reg<16, 16>(za, grid, st); return true;
+    case 96: *e = launch_zspec_reg<24, 4>(za, grid, nm, st); return true;
+    case 64: *e = launch_zspec_reg<8, 8>(za, grid, nm, st); return true;
+    case 128: *e = launch_zspec_reg<16, 8>(za, grid, nm, st); return true;
+    case 256: *e = launch_zspec_reg<16, 16>(za, grid, nm, st); return true;
     default: return false;
     }
 }
 
+template <int N1, int N2, int V>
+static void launch_xinv_v(const XiArgs &xi, int nout, size_t sm, int nm, cudaStream_t st)
+{
+    constexpr int RW = 32;
+    if (nm > 1) {
+        set_smem(k_xinv_reg<N1, N2, RW, V, true>, sm);
+        k_xinv_reg<N1, N2, RW, V, true><<<dim3(xi.g.sx2 / RW, nout, 3 * nm), RW * N2, sm, st>>>(xi);
+    } else {
+        set_smem(k_xinv_reg<N1, N2, RW, V>, sm);
+        k_xinv_reg<N1, N2, RW, V><<<dim3(xi.g.sx2 / RW, nout, 3), RW * N2, sm, st>>>(xi);
+    }
+}
+
 template <int N1, int N2>
-static cudaError_t launch_xinv_reg(const XiArgs &xi, int nout, cudaStream_t st)
+static cudaError_t launch_xinv_reg(const XiArgs &xi, int nout, int nm, cudaStream_t st)
 {
     constexpr int RW = 32, N2P = N2 + 1, K1 = N1 * N2 + 1;
     constexpr int RS0 = (N1 * N2P > K1 ? N1 * N2P : K1), RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
     const size_t sm = (size_t)RW * RS * sizeof(float2);
-    // 16-byte output rows: float4 epilogue
+    // 16-byte output rows: float4 epilogue (the members of a batch share the layout)
     bool v4 = xi.rp % 4 == 0 && xi.pp % 4 == 0;
     for (int k = 0; k < 3; k++) {
         v4 = v4 && ((uintptr_t)xi.out[k] % 16 == 0);
         if (xi.base[k]) v4 = v4 && ((uintptr_t)xi.base[k] % 16 == 0);
     }
-    const dim3 grid(xi.g.sx2 / RW, nout, 3);
-    if (v4) {
-        cudaFuncSetAttribute(k_xinv_reg<N1, N2, RW, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xinv_reg<N1, N2, RW, 4><<<grid, RW * N2, sm, st>>>(xi);
-    } else {
-        cudaFuncSetAttribute(k_xinv_reg<N1, N2, RW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xinv_reg<N1, N2, RW, 2><<<grid, RW * N2, sm, st>>>(xi);
-    }
+    if (v4) launch_xinv_v<N1, N2, 4>(xi, nout, sm, nm, st);
+    else launch_xinv_v<N1, N2, 2>(xi, nout, sm, nm, st);
     return cudaGetLastError();
 }
 
-static bool xinv_reg(const XiArgs &xi, int nout, cudaStream_t st, cudaError_t *e)
+static bool xinv_reg(const XiArgs &xi, int nout, cudaStream_t st, cudaError_t *e, int nm = 1)
 {
     if (xi.g.sx2 % 32) return false;
     // the epilogue moves at least float2: even pitches, 8-byte aligned rows
@@ -241,39 +276,60 @@ static bool xinv_reg(const XiArgs &xi, int nout, cudaStream_t st, cudaError_t *e
     for (int k = 0; k < 3; k++)
         if ((uintptr_t)xi.out[k] % 8 || (uintptr_t)xi.base[k] % 8) return false;
     switch (xi.g.M) {
-    case 64: *e = launch_xinv_reg<8, 8>(xi, nout, st); return true;
-    case 128: *e = launch_xinv_reg<16, 8>(xi, nout, st); return true;
-    case 256: *e = launch_xinv_reg<16, 16>(xi, nout, st); return true;
+    case 32: *e = launch_xinv_reg<8, 4>(xi, nout, nm, st); return true;
+    case 96: *e = launch_xinv_reg<24, 4>(xi, nout, nm, st); return true;
+    case 64: *e = launch_xinv_reg<8, 8>(xi, nout, nm, st); return true;
+    case 128: *e = launch_xinv_reg<16, 8>(xi, nout, nm, st); return true;
+    case 256: *e = launch_xinv_reg<16, 16>(xi, nout, nm, st); return true;
     default: return false;
+    }
+}
+
+template <int XIN, int N1, int N2>
+static void launch_xfwd_in(const XfArgs &xa, dim3 grid, size_t sm, int nm, cudaStream_t st)
+{
+    constexpr int RW = 16;
+    if (nm > 1) {
+        set_smem(k_xfwd_reg<XIN, N1, N2, RW, true>, sm);
+        k_xfwd_reg<XIN, N1, N2, RW, true><<<dim3(grid.x, grid.y, nm), RW * N2, sm, st>>>(xa);
+    } else {
+        set_smem(k_xfwd_reg<XIN, N1, N2, RW>, sm);
+        k_xfwd_reg<XIN, N1, N2, RW><<<grid, RW * N2, sm, st>>>(xa);
     }
 }
 
 template <int N1, int N2>
-static cudaError_t launch_xfwd_reg(const XfArgs &xa, bool div, dim3 grid, cudaStream_t st)
+static cudaError_t launch_xfwd_reg(const XfArgs &xa, bool div, dim3 grid, int nm, cudaStream_t st)
 {
     constexpr int RW = 16, N2P = N2 + 1, M = N1 * N2;
     constexpr int RS0 = (N1 * N2P > M + 1 ? N1 * N2P : M + 1), RS = RS0 + ((8 - RS0 % 16) + 16) % 16;
     const size_t sm = (size_t)RW * RS * sizeof(float2);
-    if (div) {
-        cudaFuncSetAttribute(k_xfwd_reg<XIN_DIV, N1, N2, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xfwd_reg<XIN_DIV, N1, N2, RW><<<grid, RW * N2, sm, st>>>(xa);
-    } else {
-        cudaFuncSetAttribute(k_xfwd_reg<XIN_REAL, N1, N2, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xfwd_reg<XIN_REAL, N1, N2, RW><<<grid, RW * N2, sm, st>>>(xa);
-    }
+    if (div) launch_xfwd_in<XIN_DIV, N1, N2>(xa, grid, sm, nm, st);
+    else launch_xfwd_in<XIN_REAL, N1, N2>(xa, grid, sm, nm, st);
     return cudaGetLastError();
 }
 
-static bool xfwd_reg(const XfArgs &xa, bool div, int nplanes, cudaStream_t st, cudaError_t *e)
+static bool xfwd_reg(const XfArgs &xa, bool div, int nplanes, cudaStream_t st, cudaError_t *e, int nm = 1)
 {
     if (xa.g.sx2 % 16) return false;
     const dim3 grid(xa.g.sx2 / 16, nplanes);
     switch (xa.g.M) {
-    case 64: *e = launch_xfwd_reg<8, 8>(xa, div, grid, st); return true;
-    case 128: *e = launch_xfwd_reg<16, 8>(xa, div, grid, st); return true;
-    case 256: *e = launch_xfwd_reg<16, 16>(xa, div, grid, st); return true;
+    case 32: *e = launch_xfwd_reg<8, 4>(xa, div, grid, nm, st); return true;
+    case 96: *e = launch_xfwd_reg<24, 4>(xa, div, grid, nm, st); return true;
+    case 64: *e = launch_xfwd_reg<8, 8>(xa, div, grid, nm, st); return true;
+    case 128: *e = launch_xfwd_reg<16, 8>(xa, div, grid, nm, st); return true;
+    case 256: *e = launch_xfwd_reg<16, 16>(xa, div, grid, nm, st); return true;
     default: return false;
     }
+}
+
+// the lengths the register passes are instantiated for
+static bool reg_shape(const Grid &g)
+{
+    return (g.M == 32 || g.M == 64 || g.M == 96 || g.M == 128 || g.M == 256) && g.sx2 % 32 == 0 &&
+           (g.sx2 == 32 || g.sx2 == 64 || g.sx2 == 96 || g.sx2 == 128 || g.sx2 == 192 || g.sx2 == 256 ||
+            g.sx2 == 512) &&
+           (g.sx3 == 64 || g.sx3 == 96 || g.sx3 == 128 || g.sx3 == 256);
 }
 
 struct Spectral {
@@ -347,14 +403,38 @@ struct Spectral {
         tw = nullptr;
     }
 
+    // arguments of the five passes (the caller's parts of `xa` and `xi`
+    // kept: the input / epilogue fields)
+    XfArgs xargs(XfArgs xa, int nin) const
+    {
+        xa.g = g; xa.S = S; xa.pm = pm; xa.tw1 = tw1; xa.nin = nin; xa.rows = rows; xa.has_trac = 1;
+        xa.scale3 = (float)(g.dx1 * g.dx2 * g.dx3);
+        xa.scale2 = (float)(g.dx1 * g.dx2);
+        return xa;
+    }
+    YArgs yargs(int nplanes, int traction, int tile) const { return YArgs{g, S, py, tile, nplanes, traction}; }
+    ZArgs zargs(int nin, int nout, double lambda, double mu, double gam, int tile) const
+    {
+        ZArgs za{};
+        za.g = g; za.S = S; za.pz = pz; za.tw = tile; za.nin = nin; za.nout = nout;
+        za.ratio1 = (float)((lambda + mu) / (lambda + 2.0 * mu) / mu / (4.0 * M_PI * M_PI));
+        za.ratio2 = (float)(mu / (lambda + mu));
+        za.lambda = lambda; za.mu = mu; za.gam = gam;
+        return za;
+    }
+    XiArgs xiargs(XiArgs xi) const
+    {
+        xi.g = g; xi.S = S; xi.pm = pm; xi.tw1 = tw1; xi.rows = rows;
+        xi.scale = (float)(2.0 / ((double)g.sx1 * g.dx1 * g.sx2 * g.dx2 * g.sx3 * g.dx3));
+        return xi;
+    }
+
     // Green's function: forward (x pass from `xa`), y, z spectral, y inverse,
     // x inverse with the epilogue in `xi`.
     int green(XfArgs xa, bool div, int nin, int nout, XiArgs xi, double lambda, double mu, double gam,
               cudaStream_t st)
     {
-        xa.g = g; xa.S = S; xa.pm = pm; xa.tw1 = tw1; xa.nin = nin; xa.rows = rows; xa.has_trac = 1;
-        xa.scale3 = (float)(g.dx1 * g.dx2 * g.dx3);
-        xa.scale2 = (float)(g.dx1 * g.dx2);
+        xa = xargs(xa, nin);
         dim3 gx(g.sx2 / rows, nin + 1);
         bool xr0 = false;
         cudaError_t re0 = cudaSuccess;
@@ -366,7 +446,7 @@ struct Spectral {
             if (div) TIMED(prof, ST_XFWD, st, (k_xfwd<XIN_DIV><<<gx, RELAX_NTHREADS, smx, st>>>(xa)));
             else TIMED(prof, ST_XFWD, st, (k_xfwd<XIN_REAL><<<gx, RELAX_NTHREADS, smx, st>>>(xa)));
         }
-        YArgs ya{g, S, py, twy, nin, 1};
+        YArgs ya = yargs(nin, 1, twy);
         cudaError_t re = cudaSuccess;
         if (use_reg) {
             TIMED(prof, ST_YFWD, st, (ya.tw = kCW, yreg = ypass_reg(ya, -1, st, &re)));
@@ -377,11 +457,7 @@ struct Spectral {
             TIMED(prof, ST_YFWD, st,
                   (k_ypass<-1><<<dim3((g.K1 + twy - 1) / twy, nin + 1, 3), RELAX_NTHREADS, smy, st>>>(ya)));
         }
-        ZArgs za;
-        za.g = g; za.S = S; za.pz = pz; za.tw = twz; za.nin = nin; za.nout = nout;
-        za.ratio1 = (float)((lambda + mu) / (lambda + 2.0 * mu) / mu / (4.0 * M_PI * M_PI));
-        za.ratio2 = (float)(mu / (lambda + mu));
-        za.lambda = lambda; za.mu = mu; za.gam = gam;
+        ZArgs za = zargs(nin, nout, lambda, mu, gam, twz);
         bool zr = false;
         if (use_reg) {
             TIMED(prof, ST_ZSPEC, st, (zr = zspec_reg(za, dim3((g.sx2 * g.K1 + kCW - 1) / kCW), st, &re)));
@@ -391,7 +467,7 @@ struct Spectral {
             za.tw = twz;
             TIMED(prof, ST_ZSPEC, st, (k_zspec<<<dim3((g.K1 + twz - 1) / twz, g.sx2), RELAX_NTHREADS, smz, st>>>(za)));
         }
-        YArgs yb{g, S, py, twy, nout, 0};
+        YArgs yb = yargs(nout, 0, twy);
         bool yr2 = false;
         if (use_reg) {
             yb.tw = kCW;
@@ -403,8 +479,7 @@ struct Spectral {
             TIMED(prof, ST_YINV, st,
                   (k_ypass<+1><<<dim3((g.K1 + twy - 1) / twy, nout, 3), RELAX_NTHREADS, smy, st>>>(yb)));
         }
-        xi.g = g; xi.S = S; xi.pm = pm; xi.tw1 = tw1; xi.rows = rows;
-        xi.scale = (float)(2.0 / ((double)g.sx1 * g.dx1 * g.sx2 * g.dx2 * g.sx3 * g.dx3));
+        xi = xiargs(xi);
         bool xr = false;
         if (use_reg) {
             TIMED(prof, ST_XINV, st, (xr = xinv_reg(xi, nout, st, &re)));
@@ -605,6 +680,7 @@ struct relax_ctx {
     unsigned char *sig_mask = nullptr;
     unsigned *ticket = nullptr;                 // last-block counter of the stress kernels
     StepState *dst = nullptr, *hst = nullptr;   // device state, pinned host mirror
+    bool own_dst = true;                         // false: dst lives in a batch's array
     float *tm_part = nullptr, *fr_part = nullptr;
     double *amp_part = nullptr, *amp_alt = nullptr;
     int *err = nullptr;
@@ -636,7 +712,7 @@ static void free_ctx(relax_ctx *c)
     for (auto p : c->band_imp) if (p) cudaFree(p);
     if (c->sig_mask) cudaFree(c->sig_mask);
     if (c->ticket) cudaFree(c->ticket);
-    if (c->dst) cudaFree(c->dst);
+    if (c->dst && c->own_dst) cudaFree(c->dst);
     if (c->hst) cudaFreeHost(c->hst);
     if (c->amp_part) cudaFree(c->amp_part);
     if (c->amp_alt) cudaFree(c->amp_alt);
@@ -1083,39 +1159,65 @@ static int build_bands(relax_ctx *c)
     return RELAX_OK;
 }
 
+// arguments of frictioneigenstress on the band points of plane k
+static FrictionPtsArgs friction_pts_args(relax_ctx *c, size_t k, bool want_tm)
+{
+    const relax_plane &p = c->planes[k];
+    FrictionArgs fa = plane_args(c, p);
+    FrictionPtsArgs a{};
+    a.g = c->g; a.mu = c->cfg.mu; a.rake = p.rake; a.L = p.width; a.W = p.length;
+    a.n0 = fa.cd * fa.cs; a.n1 = -fa.cd * fa.ss; a.n2 = -fa.sd;
+    a.r0 = fa.ss * fa.cr + fa.cs * fa.sd * fa.sr;
+    a.r1 = fa.cs * fa.cr - fa.ss * fa.sd * fa.sr;
+    a.r2 = fa.cd * fa.sr;
+    a.fc = c->fcd; a.sig = c->sig; a.m = c->m; a.err = c->err;
+    a.idx = c->band_idx[k]; a.imp = c->band_imp[k]; a.npts = c->band_n[k];
+    a.want_tm = want_tm;
+    return a;
+}
+
+// arguments of monitorfriction on the patches of plane k
+static MonitorArgs monitor_args(relax_ctx *c, size_t k, bool with_dt)
+{
+    const relax_plane &p = c->planes[k];
+    MonitorArgs a{};
+    a.g = c->g;
+    a.x = p.x; a.y = p.y; a.z = p.z; a.strike = p.strike; a.dip = p.dip; a.rake = p.rake;
+    a.fc = c->fcd; a.sig = c->sig; a.patch = c->patch + c->patch_off[k];
+    a.px2 = p.px2; a.px3 = p.px3;
+    a.st = with_dt ? c->dst : nullptr;
+    return a;
+}
+
+// Maxwell-time partial slots of the friction kernels: the blocks of each
+// plane in turn.  Grows the partial array when needed.
+static int friction_slots(relax_ctx *c, int *total)
+{
+    int blk = 0;
+    for (size_t k = 0; k < c->planes.size(); k++) blk += (int)nblocks(c->band_n[k]);
+    if (blk > c->nfr) {
+        CK(cudaStreamSynchronize(c->st));
+        float *np = nullptr;
+        TRY(dalloc(&np, (size_t)blk));
+        if (c->fr_part) cudaFree(c->fr_part);
+        c->fr_part = np;
+        c->nfr = blk;
+    }
+    *total = blk;
+    return RELAX_OK;
+}
+
 static int friction_planes(relax_ctx *c, bool want_tm, int *nblk_out)
 {
-    const Grid &g = c->g;
     int blk_total = 0;
     *nblk_out = 0;
+    if (want_tm) TRY(friction_slots(c, &blk_total));
+    blk_total = 0;
     for (size_t k = 0; k < c->planes.size(); k++) {
         if (c->band_n[k] == 0) continue;
-        const relax_plane &p = c->planes[k];
-        FrictionArgs fa = plane_args(c, p);
-        FrictionPtsArgs a{};
-        a.g = g; a.mu = c->cfg.mu; a.rake = p.rake; a.L = p.width; a.W = p.length;
-        a.n0 = fa.cd * fa.cs; a.n1 = -fa.cd * fa.ss; a.n2 = -fa.sd;
-        a.r0 = fa.ss * fa.cr + fa.cs * fa.sd * fa.sr;
-        a.r1 = fa.cs * fa.cr - fa.ss * fa.sd * fa.sr;
-        a.r2 = fa.cd * fa.sr;
-        a.fc = c->fcd; a.sig = c->sig; a.m = c->m; a.err = c->err;
-        a.idx = c->band_idx[k]; a.imp = c->band_imp[k]; a.npts = c->band_n[k];
-        a.want_tm = want_tm;
+        FrictionPtsArgs a = friction_pts_args(c, k, want_tm);
         const int nb = (int)nblocks(a.npts);
-        if (want_tm) {
-            if (blk_total + nb > c->nfr) {
-                CK(cudaStreamSynchronize(c->st));
-                float *np = nullptr;
-                TRY(dalloc(&np, (size_t)(blk_total + nb) * 2));
-                if (c->fr_part) {
-                    CK(cudaMemcpy(np, c->fr_part, c->nfr * sizeof(float), cudaMemcpyDeviceToDevice));
-                    cudaFree(c->fr_part);
-                }
-                c->fr_part = np;
-                c->nfr = (blk_total + nb) * 2;
-            }
-            a.tm_part = c->fr_part + blk_total;
-        }
+        if (want_tm) a.tm_part = c->fr_part + blk_total;
         TIMED(&c->prof, ST_FRICTION, c->st, (k_friction_pts<<<nb, RELAX_NTHREADS, 0, c->st>>>(a)));
         blk_total += nb;
     }
@@ -1129,12 +1231,7 @@ static int monitor_planes(relax_ctx *c, bool with_dt)
         const relax_plane &p = c->planes[k];
         const int n = std::max(0, p.px2) * std::max(0, p.px3);
         if (n == 0) continue;
-        MonitorArgs a{};
-        a.g = c->g;
-        a.x = p.x; a.y = p.y; a.z = p.z; a.strike = p.strike; a.dip = p.dip; a.rake = p.rake;
-        a.fc = c->fcd; a.sig = c->sig; a.patch = c->patch + c->patch_off[k];
-        a.px2 = p.px2; a.px3 = p.px3;
-        a.st = with_dt ? c->dst : nullptr;
+        MonitorArgs a = monitor_args(c, k, with_dt);
         TIMED(&c->prof, ST_MONITOR, c->st, (k_monitor<<<nblocks(n, 128), 128, 0, c->st>>>(a)));
     }
     return RELAX_OK;
@@ -1201,6 +1298,55 @@ static DtPolicy policy(relax_ctx *c)
     p.mech[1] = !c->non.empty();
     p.mech[2] = !c->fc.empty();
     return p;
+}
+
+// The host part of the end of a step, from the step state in c->hst: time,
+// counters, the event branch when k_dt found that t + Dt reaches the next
+// event, isoutput, the error flags and the log line.
+static int finish_step(relax_ctx *c, relax_step_log *log)
+{
+    const Grid &g = c->g;
+    double Dt = 0.0;
+    if (!(c->hst->dt_raw > 0.0) || !std::isfinite(c->hst->dt_raw))
+        return fail(RELAX_ERR_ARG, "invalid time step %g", c->hst->dt_raw);
+    Dt = c->hst->Dt;
+    const double mw[3] = {c->hst->maxwell[0], c->hst->maxwell[1], c->hst->maxwell[2]};
+    c->t = c->t + Dt;
+    c->i++;
+    const int fired = c->hst->fire;
+    if (fired) {
+        // tau += Dt m, then the coseismic event, then the stress
+        k_tau_update<<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(g, c->tau, c->m, c->dst, c->amp_alt);
+        CKL();
+        c->e++;
+        bool any = false, ld = false;
+        TRY(event_sources(c, c->events[c->e], &any));
+        TRY(upload_loads(c, c->events[c->e], c->t, 0.0, false, &ld));
+        TRY(event_green(c, ld));
+        TRY(launch_stress<MODE_INIT>(c, stress_args(c, c->u)));
+        k_reduce_amp<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->amp_part, c->nblk, c->amp_alt,
+                                                        g.dx1 * g.dx2 * g.dx3);
+        CKL();
+        TRY(pull_state(c));
+    }
+    c->m_valid = true;
+    c->sig_valid = c->store_sig && !c->sig_mask;
+    // isoutput, src/relax.f90:1364-1376
+    {
+        const double odt = c->cfg.odt, etime = c->events[c->e].time;
+        if ((0 == c->cfg.skip && fabs(c->t - c->oi * odt) < 1e-6 * odt) ||
+            (0 < c->cfg.skip && ((c->i - 1) % c->cfg.skip) == 0) || fabs(c->t - etime) < 1e-6)
+            c->oi++;
+    }
+    if (!c->fc.empty()) TRY(check_err(c));
+    log->i = c->i;
+    log->event = fired;
+    log->dt = Dt;
+    log->tm_ve = mw[0]; log->tm_pl = mw[1]; log->tm_as = mw[2];
+    log->t = c->t;
+    log->power = c->hst->power;
+    log->cei = c->hst->cei;
+    return RELAX_OK;
 }
 
 static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
@@ -1275,50 +1421,11 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
     }
     // tau += Dt m, sig, next predictor moment; tmin, power and cei reduced by
     // the kernel's last block.  When t + Dt reaches the next event (the test
-    // of src/relax.f90:859, made by k_dt) the kernel does nothing and the
-    // event branch below runs instead.
+    // of src/relax.f90:859, made by k_dt) the kernel does nothing and
+    // finish_step runs the event branch instead.
     TRY(launch_stress<MODE_END>(c, stress_args(c, c->u)));
     TRY(pull_state(c));
-    if (!(c->hst->dt_raw > 0.0) || !std::isfinite(c->hst->dt_raw))
-        return fail(RELAX_ERR_ARG, "invalid time step %g", c->hst->dt_raw);
-    Dt = c->hst->Dt;
-    const double mw[3] = {c->hst->maxwell[0], c->hst->maxwell[1], c->hst->maxwell[2]};
-    c->t = c->t + Dt;
-    c->i++;
-    const int fired = c->hst->fire;
-    if (fired) {
-        // tau += Dt m, then the coseismic event, then the stress
-        k_tau_update<<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(g, c->tau, c->m, c->dst, c->amp_alt);
-        CKL();
-        c->e++;
-        bool any = false, ld = false;
-        TRY(event_sources(c, c->events[c->e], &any));
-        TRY(upload_loads(c, c->events[c->e], c->t, 0.0, false, &ld));
-        TRY(event_green(c, ld));
-        TRY(launch_stress<MODE_INIT>(c, stress_args(c, c->u)));
-        k_reduce_amp<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->amp_part, c->nblk, c->amp_alt,
-                                                        g.dx1 * g.dx2 * g.dx3);
-        CKL();
-        TRY(pull_state(c));
-    }
-    c->m_valid = true;
-    c->sig_valid = c->store_sig && !c->sig_mask;
-    // isoutput, src/relax.f90:1364-1376
-    {
-        const double odt = c->cfg.odt, etime = c->events[c->e].time;
-        if ((0 == c->cfg.skip && fabs(c->t - c->oi * odt) < 1e-6 * odt) ||
-            (0 < c->cfg.skip && ((c->i - 1) % c->cfg.skip) == 0) || fabs(c->t - etime) < 1e-6)
-            c->oi++;
-    }
-    if (!c->fc.empty()) TRY(check_err(c));
-    log->i = c->i;
-    log->event = fired;
-    log->dt = Dt;
-    log->tm_ve = mw[0]; log->tm_pl = mw[1]; log->tm_as = mw[2];
-    log->t = c->t;
-    log->power = c->hst->power;
-    log->cei = c->hst->cei;
-    return RELAX_OK;
+    return finish_step(c, log);
 }
 
 extern "C" int relax_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
@@ -1841,5 +1948,394 @@ extern "C" int relax_launch_count(relax_ctx *c, long long *n)
 {
     if (!c || !n) return fail(RELAX_ERR_ARG, "null argument");
     *n = c->prof.launches;
+    return RELAX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batches: members that share the grid and the elastic constants, stepped
+// together.  Each stage of the RK2 step is one launch for all members (the
+// member is a spare grid dimension, its arguments an entry of a device
+// table); the host synchronises once per batch step.  Members differ in
+// their events, rheology, prestress, weak zones and afterslip planes (the
+// same number of planes).
+// ---------------------------------------------------------------------------
+struct BatchTables {
+    unsigned char *dev = nullptr;
+    StressArgs *corr = nullptr, *end = nullptr;
+    XfArgs *xf = nullptr;
+    YArgs *yf = nullptr, *yi = nullptr;
+    ZArgs *z = nullptr;
+    XiArgs *xip = nullptr, *xic = nullptr;
+    std::vector<FrictionPtsArgs *> frp, frc;
+    std::vector<MonitorArgs *> mon;
+    std::vector<int> frblk, monblk;       // grid.x of plane k's launches
+    DtArgs *dt = nullptr;
+    // member 0's host copies: shapes and kernel choices of the launches
+    StressArgs corr0{}, end0{};
+    XfArgs xf0{};
+    YArgs yf0{}, yi0{};
+    ZArgs z0{};
+    XiArgs xip0{}, xic0{};
+    std::vector<FrictionPtsArgs> frp0, frc0;
+    std::vector<MonitorArgs> mon0;
+};
+
+struct relax_batch {
+    std::vector<relax_ctx *> m;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    bool batched = false;          // register passes instantiated for the grid
+    bool tables_valid = false;
+    BatchTables tab;
+    StepState *dst = nullptr;      // the members' device states, contiguous
+    StepState *hst = nullptr;      // pinned mirror
+    DtArgs *hdt = nullptr;         // pinned: this step's k_dt inputs
+    std::vector<int> nfr;          // friction partial slots per member
+    long long launches = 0;
+};
+
+static void free_batch(relax_batch *b)
+{
+    if (!b) return;
+    for (auto *c : b->m) free_ctx(c);
+    if (b->tab.dev) cudaFree(b->tab.dev);
+    if (b->dst) cudaFree(b->dst);
+    if (b->hst) cudaFreeHost(b->hst);
+    if (b->hdt) cudaFreeHost(b->hdt);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+static int same_shape(const relax_config &a, const relax_config &b)
+{
+    return a.sx1 == b.sx1 && a.sx2 == b.sx2 && a.sx3 == b.sx3 && a.dx1 == b.dx1 && a.dx2 == b.dx2 &&
+           a.dx3 == b.dx3 && a.lambda == b.lambda && a.mu == b.mu && a.gam == b.gam && a.np == b.np;
+}
+
+extern "C" int relax_batch_create(const relax_config *members, int n, int device, relax_batch **out)
+{
+    if (!members || !out || n < 1) return fail(RELAX_ERR_ARG, "null argument or empty batch");
+    *out = nullptr;
+    for (int k = 1; k < n; k++)
+        if (!same_shape(members[0], members[k]))
+            return fail(RELAX_ERR_ARG, "batch member %d: grid, spacing, elastic constants and the number of "
+                                       "afterslip planes must match member 0", k);
+    relax_batch *b = new relax_batch();
+    b->device = device;
+    auto bail = [&](int rc) { free_batch(b); return rc; };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(fail(RELAX_ERR_CUDA, "cudaSetDevice(%d)", device));
+    for (int k = 0; k < n; k++) {
+        relax_ctx *c = new relax_ctx();
+        const int rc = create(&members[k], device, c);
+        if (rc != RELAX_OK) {
+            free_ctx(c);
+            return bail(rc);
+        }
+        b->m.push_back(c);
+        for (const auto &ev : c->events)
+            if (!ev.l.empty())
+                return bail(fail(RELAX_ERR_UNSUPPORTED, "batch member %d: surface loads are evaluated on the host "
+                                                        "at t + Dt; step such members alone", k));
+    }
+    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(RELAX_ERR_CUDA, "stream"));
+    // member states in one array (one read-back per step)
+    if (dalloc(&b->dst, (size_t)n) != RELAX_OK) return bail(RELAX_ERR_NOMEM);
+    if (cudaMemset(b->dst, 0, n * sizeof(StepState)) != cudaSuccess ||
+        cudaMallocHost(&b->hst, n * sizeof(StepState)) != cudaSuccess ||
+        cudaMallocHost(&b->hdt, n * sizeof(DtArgs)) != cudaSuccess)
+        return bail(fail(RELAX_ERR_NOMEM, "batch state"));
+    for (int k = 0; k < n; k++) {
+        relax_ctx *c = b->m[k];
+        cudaFree(c->dst);
+        c->dst = b->dst + k;
+        c->own_dst = false;
+        c->err = &c->dst->error;
+    }
+    b->batched = reg_shape(b->m[0]->g);
+    b->nfr.assign(n, 0);
+    *out = b;
+    return RELAX_OK;
+}
+
+extern "C" int relax_batch_destroy(relax_batch *b)
+{
+    free_batch(b);
+    return RELAX_OK;
+}
+
+extern "C" int relax_batch_size(relax_batch *b, int *n)
+{
+    if (!b || !n) return fail(RELAX_ERR_ARG, "null argument");
+    *n = (int)b->m.size();
+    return RELAX_OK;
+}
+
+extern "C" int relax_batch_member(relax_batch *b, int k, relax_ctx **c)
+{
+    if (!b || !c) return fail(RELAX_ERR_ARG, "null argument");
+    if (k < 0 || k >= (int)b->m.size()) return fail(RELAX_ERR_ARG, "member %d out of range", k);
+    *c = b->m[k];
+    return RELAX_OK;
+}
+
+extern "C" int relax_batch_coseismic(relax_batch *b, relax_step_log *logs)
+{
+    if (!b) return fail(RELAX_ERR_ARG, "null batch");
+    for (size_t k = 0; k < b->m.size(); k++) TRY(relax_coseismic(b->m[k], 0, logs ? &logs[k] : nullptr));
+    b->tables_valid = false;
+    return RELAX_OK;
+}
+
+template <typename T>
+static T *carve(unsigned char *base, size_t *off, size_t n)
+{
+    *off = (*off + 255) & ~(size_t)255;
+    T *p = reinterpret_cast<T *>(base + *off);
+    *off += n * sizeof(T);
+    return p;
+}
+
+// the argument tables of every member (pointers, geometry and constants);
+// rebuilt after an event or a change of plane geometry
+static int build_tables(relax_batch *b)
+{
+    const int n = (int)b->m.size();
+    relax_ctx *c0 = b->m[0];
+    const Grid &g = c0->g;
+    const size_t np = c0->planes.size();
+    std::vector<StressArgs> corr(n), end(n);
+    std::vector<XfArgs> xf(n);
+    std::vector<YArgs> yf(n), yi(n);
+    std::vector<ZArgs> z(n);
+    std::vector<XiArgs> xip(n), xic(n);
+    std::vector<std::vector<FrictionPtsArgs>> frp(np, std::vector<FrictionPtsArgs>(n)),
+        frc(np, std::vector<FrictionPtsArgs>(n));
+    std::vector<std::vector<MonitorArgs>> mon(np, std::vector<MonitorArgs>(n));
+    BatchTables &t = b->tab;
+    t.frblk.assign(np, 0);
+    t.monblk.assign(np, 0);
+    for (int k = 0; k < n; k++) {
+        relax_ctx *c = b->m[k];
+        if (!c->m_valid) TRY(tail_init(c));
+        corr[k] = stress_args(c, c->vp);
+        end[k] = stress_args(c, c->u);
+        xf[k] = c->sp.xargs(xf_div(c), g.sx3h);
+        yf[k] = c->sp.yargs(g.sx3h, 1, kCW);
+        yi[k] = c->sp.yargs(g.sx3h, 0, kCW);
+        z[k] = c->sp.zargs(g.sx3h, g.sx3h, c->cfg.lambda, c->cfg.mu, c->cfg.gam, kCW);
+        xip[k] = c->sp.xiargs(xi_update(c, c->vp, c->u, 0.5f, true));
+        xic[k] = c->sp.xiargs(xi_update(c, c->u, c->u, 1.0f, true));
+        int tot = 0;
+        TRY(friction_slots(c, &tot));
+        b->nfr[k] = tot;
+        int off = 0;
+        for (size_t q = 0; q < np; q++) {
+            frp[q][k] = friction_pts_args(c, q, true);
+            frp[q][k].tm_part = c->fr_part + off;
+            frc[q][k] = friction_pts_args(c, q, false);
+            mon[q][k] = monitor_args(c, q, true);
+            const int nb = (int)nblocks(c->band_n[q]);
+            off += nb;
+            t.frblk[q] = std::max(t.frblk[q], nb);
+            const int npch = std::max(0, c->planes[q].px2) * std::max(0, c->planes[q].px3);
+            t.monblk[q] = std::max(t.monblk[q], (int)nblocks(npch, 128));
+        }
+    }
+    size_t off = 0;
+    unsigned char *nul = nullptr;
+    // sizes first (offsets from a null base), then one allocation
+    auto layout = [&](unsigned char *base) {
+        off = 0;
+        t.corr = carve<StressArgs>(base, &off, n); t.end = carve<StressArgs>(base, &off, n);
+        t.xf = carve<XfArgs>(base, &off, n);
+        t.yf = carve<YArgs>(base, &off, n); t.yi = carve<YArgs>(base, &off, n);
+        t.z = carve<ZArgs>(base, &off, n);
+        t.xip = carve<XiArgs>(base, &off, n); t.xic = carve<XiArgs>(base, &off, n);
+        t.frp.assign(np, nullptr); t.frc.assign(np, nullptr); t.mon.assign(np, nullptr);
+        for (size_t q = 0; q < np; q++) {
+            t.frp[q] = carve<FrictionPtsArgs>(base, &off, n);
+            t.frc[q] = carve<FrictionPtsArgs>(base, &off, n);
+            t.mon[q] = carve<MonitorArgs>(base, &off, n);
+        }
+        t.dt = carve<DtArgs>(base, &off, n);
+    };
+    layout(nul);
+    if (t.dev) cudaFree(t.dev);
+    t.dev = nullptr;
+    TRY(dalloc(&t.dev, off));
+    layout(t.dev);
+    auto up = [&](void *dst, const void *src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, b->st);
+    };
+    cudaError_t e = up(t.corr, corr.data(), n * sizeof(StressArgs));
+    if (e == cudaSuccess) e = up(t.end, end.data(), n * sizeof(StressArgs));
+    if (e == cudaSuccess) e = up(t.xf, xf.data(), n * sizeof(XfArgs));
+    if (e == cudaSuccess) e = up(t.yf, yf.data(), n * sizeof(YArgs));
+    if (e == cudaSuccess) e = up(t.yi, yi.data(), n * sizeof(YArgs));
+    if (e == cudaSuccess) e = up(t.z, z.data(), n * sizeof(ZArgs));
+    if (e == cudaSuccess) e = up(t.xip, xip.data(), n * sizeof(XiArgs));
+    if (e == cudaSuccess) e = up(t.xic, xic.data(), n * sizeof(XiArgs));
+    for (size_t q = 0; q < np && e == cudaSuccess; q++) {
+        e = up(t.frp[q], frp[q].data(), n * sizeof(FrictionPtsArgs));
+        if (e == cudaSuccess) e = up(t.frc[q], frc[q].data(), n * sizeof(FrictionPtsArgs));
+        if (e == cudaSuccess) e = up(t.mon[q], mon[q].data(), n * sizeof(MonitorArgs));
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+    if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "batch tables: %s", cudaGetErrorString(e));
+    t.corr0 = corr[0]; t.corr0.tab = t.corr;
+    t.end0 = end[0]; t.end0.tab = t.end;
+    t.xf0 = xf[0]; t.xf0.tab = t.xf;
+    t.yf0 = yf[0]; t.yf0.tab = t.yf;
+    t.yi0 = yi[0]; t.yi0.tab = t.yi;
+    t.z0 = z[0]; t.z0.tab = t.z;
+    t.xip0 = xip[0]; t.xip0.tab = t.xip;
+    t.xic0 = xic[0]; t.xic0.tab = t.xic;
+    t.frp0.resize(np); t.frc0.resize(np); t.mon0.resize(np);
+    for (size_t q = 0; q < np; q++) {
+        t.frp0[q] = frp[q][0]; t.frp0[q].tab = t.frp[q];
+        t.frc0[q] = frc[q][0]; t.frc0[q].tab = t.frc[q];
+        t.mon0[q] = mon[q][0]; t.mon0[q].tab = t.mon[q];
+    }
+    b->tables_valid = true;
+    return RELAX_OK;
+}
+
+// the batched Green's function: five launches for all members
+static int batch_green(relax_batch *b, const XiArgs &xi0)
+{
+    BatchTables &t = b->tab;
+    const int n = (int)b->m.size();
+    const Grid &g = b->m[0]->g;
+    cudaError_t e = cudaSuccess;
+    if (!xfwd_reg(t.xf0, true, g.sx3h + 1, b->st, &e, n) || e != cudaSuccess)
+        return fail(RELAX_ERR_CUDA, "batched x pass: %s", cudaGetErrorString(e));
+    if (!ypass_reg(t.yf0, -1, b->st, &e, n) || e != cudaSuccess)
+        return fail(RELAX_ERR_CUDA, "batched y pass: %s", cudaGetErrorString(e));
+    if (!zspec_reg(t.z0, dim3((g.sx2 * g.K1 + kCW - 1) / kCW), b->st, &e, n) || e != cudaSuccess)
+        return fail(RELAX_ERR_CUDA, "batched z pass: %s", cudaGetErrorString(e));
+    if (!ypass_reg(t.yi0, +1, b->st, &e, n) || e != cudaSuccess)
+        return fail(RELAX_ERR_CUDA, "batched y pass: %s", cudaGetErrorString(e));
+    if (!xinv_reg(xi0, g.sx3h, b->st, &e, n) || e != cudaSuccess)
+        return fail(RELAX_ERR_CUDA, "batched x inverse: %s", cudaGetErrorString(e));
+    b->launches += 5;
+    return RELAX_OK;
+}
+
+// One RK2 step of every member (the steps of src/relax.f90:555-890 as in
+// relax_step).  Members whose time reached the interval take Dt = 0 on the
+// device and report i = 0.
+extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
+{
+    if (!b || !logs) return fail(RELAX_ERR_ARG, "null argument");
+    CK(cudaSetDevice(b->device));
+    const int n = (int)b->m.size();
+    std::vector<char> live(n, 0);
+    int nlive = 0;
+    for (int k = 0; k < n; k++) {
+        relax_ctx *c = b->m[k];
+        if (!c->cos_done) TRY(relax_coseismic(c, 0, nullptr));
+        memset(&logs[k], 0, sizeof(relax_step_log));
+        live[k] = c->t < c->cfg.interval;
+        nlive += live[k];
+    }
+    if (!nlive) return RELAX_OK;
+    if (!b->batched || n == 1) {
+        // no batched instantiation for this grid: the members in turn
+        for (int k = 0; k < n; k++)
+            if (live[k]) TRY(do_step(b->m[k], nullptr, &logs[k]));
+        return RELAX_OK;
+    }
+    if (!b->tables_valid) TRY(build_tables(b));
+    // the members' own streams carry their set-up and event work
+    for (auto *c : b->m) CK(cudaStreamSynchronize(c->st));
+    BatchTables &t = b->tab;
+    relax_ctx *c0 = b->m[0];
+    const Grid &g = c0->g;
+    const size_t np = c0->planes.size();
+    cudaStream_t st = b->st;
+    // ---- predictor
+    for (int k = 0; k < n; k++) {
+        relax_ctx *c = b->m[k];
+        DtArgs &d = b->hdt[k];
+        d.st = c->dst;
+        d.pol = policy(c);
+        d.in = DtIn{};
+        d.in.t = c->t;
+        d.in.oi = c->oi;
+        d.in.use_override = live[k] ? 0 : 1;   // finished members: Dt = 0
+        d.in.dt_override = 0.0;
+        d.fr_part = c->fr_part;
+        d.nfr = c->fc.empty() ? 0 : b->nfr[k];
+    }
+    CK(cudaMemcpyAsync(t.dt, b->hdt, n * sizeof(DtArgs), cudaMemcpyHostToDevice, st));
+    if (!c0->fc.empty())
+        for (size_t q = 0; q < np; q++)
+            if (t.frblk[q] > 0) {
+                k_friction_pts<true><<<dim3(t.frblk[q], n), RELAX_NTHREADS, 0, st>>>(t.frp0[q]);
+                b->launches++;
+            }
+    k_dt_batch<<<n, RELAX_NTHREADS, 0, st>>>(t.dt);
+    b->launches++;
+    CKL();
+    TRY(batch_green(b, t.xip0));
+    // ---- corrector
+    k_stress<MODE_CORR, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.corr0);
+    b->launches++;
+    if (!c0->fc.empty())
+        for (size_t q = 0; q < np; q++) {
+            if (t.frblk[q] > 0) {
+                k_friction_pts<true><<<dim3(t.frblk[q], n), RELAX_NTHREADS, 0, st>>>(t.frc0[q]);
+                b->launches++;
+            }
+            if (t.monblk[q] > 0) {
+                k_monitor<true><<<dim3(t.monblk[q], n), 128, 0, st>>>(t.mon0[q]);
+                b->launches++;
+            }
+        }
+    for (int k = 0; k < n; k++) {
+        relax_ctx *c = b->m[k];
+        for (const auto &s : c->inter.s) {
+            SrcArgs a{};
+            a.g = g; a.mu = c->cfg.mu; a.s = s.slip; a.x = s.x; a.y = s.y; a.z = s.z;
+            a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.rake = s.rake; a.beta = s.beta;
+            a.tau = c->m;
+            k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(a);
+            a.tau = c->tau;   // src/relax.f90:1228-1235 also adds it to tau
+            k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(a);
+            b->launches += 2;
+        }
+    }
+    CKL();
+    TRY(batch_green(b, t.xic0));
+    k_stress<MODE_END, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.end0);
+    b->launches++;
+    CKL();
+    CK(cudaMemcpyAsync(b->hst, b->dst, n * sizeof(StepState), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // ---- host part of each member's step end
+    for (int k = 0; k < n; k++) {
+        if (!live[k]) continue;
+        relax_ctx *c = b->m[k];
+        *c->hst = b->hst[k];
+        const int e0 = c->e;
+        TRY(finish_step(c, &logs[k]));
+        if (c->e != e0) b->tables_valid = false;   // the event branch ran on the member's stream
+    }
+    return RELAX_OK;
+}
+
+extern "C" int relax_batch_launch_count(relax_batch *b, long long *n)
+{
+    if (!b || !n) return fail(RELAX_ERR_ARG, "null argument");
+    *n = b->launches;
+    for (auto *c : b->m) *n += c->prof.launches;
+    return RELAX_OK;
+}
+
+extern "C" int relax_batch_get_stream(relax_batch *b, void **s)
+{
+    if (!b || !s) return fail(RELAX_ERR_ARG, "null argument");
+    *s = (void *)b->st;
     return RELAX_OK;
 }
