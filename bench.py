@@ -330,6 +330,87 @@ def run_gpu(args, rank, world, local_rank):
     return 0
 
 
+# --------------------------------------------------------------------------
+# the batched ensemble (64 members, uneven grids), against a loop of plain solves
+# --------------------------------------------------------------------------
+def run_ensemble(args):
+    import collections
+    import torch
+    from relax_b200.api import Batch, Relax
+    from relax_b200.config import ensemble_uneven
+
+    torch.cuda.set_device(0)
+    sims = ensemble_uneven(seed=4, n=64)
+    groups = collections.OrderedDict()
+    for s in sims:
+        groups.setdefault((s.sx1, s.sx2, s.sx3), []).append(s)
+    npts = sum(s.npoints for s in sims)
+    K, W = args.steps, args.warmup
+
+    # batched: one batch per grid shape, every batch stepped once per step
+    batches = [Batch(g) for g in groups.values()]
+    for b in batches:
+        b.coseismic()
+    for _ in range(W):
+        for b in batches:
+            b.step()
+    n0 = sum(b.launch_count() for b in batches)
+    per_batch = [0.0] * len(batches)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        for j, b in enumerate(batches):
+            tb = time.perf_counter()
+            b.step()             # ends with the batch's host synchronisation
+            per_batch[j] += time.perf_counter() - tb
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    launches = sum(b.launch_count() for b in batches) - n0
+    for b in batches:
+        b.close()
+
+    # the loop of plain solves: each member alone through relax_step
+    t_loop = 0.0
+    per_shape_loop = collections.Counter()
+    for s in sims:
+        with Relax(s) as r:
+            r.coseismic()
+            for _ in range(W):
+                r.step()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(K):
+                r.step()
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            t_loop += dt
+            per_shape_loop[(s.sx1, s.sx2, s.sx3)] += dt
+
+    steps_per_solve = 100
+    solves = len(sims) * K / steps_per_solve
+    line = {
+        "metric": "ensemble solves/s (100 RK2 steps per member)", "value": solves / t_batch,
+        "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": W, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "uneven ensemble of 64 members, grids {64^3, 128^2x64, 128^3, 192^2x96}, "
+                               "power-law n U[1,3.5], prefactor 10^U[-1,1], lid U[15,40] km, one fault each",
+                   "members": {f"{a}x{b}x{c}": len(g) for (a, b, c), g in groups.items()},
+                   "grid_points_total": npts, "parallelism": "one batch per grid shape",
+                   "timing": "host wall clock around K steps of every member, after W warm-up steps"},
+        "grid_pt_steps_per_s": npts * K / t_batch,
+        "loop_of_plain_solves": {"value": solves / t_loop, "unit": "solves/s",
+                                 "grid_pt_steps_per_s": npts * K / t_loop},
+        "speedup_vs_loop": t_loop / t_batch,
+        "per_shape": {f"{a}x{b}x{c}": {"members": len(g), "batch_ms_per_step": 1e3 * per_batch[j] / K,
+                                       "loop_ms_per_step": 1e3 * per_shape_loop[(a, b, c)] / K,
+                                       "speedup": per_shape_loop[(a, b, c)] / per_batch[j]}
+                      for j, ((a, b, c), g) in enumerate(groups.items())},
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -337,6 +418,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--ensemble", action="store_true",
+                    help="the batched 64-member ensemble against a loop of plain solves (1 GPU)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -349,6 +432,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.ensemble:
+        return run_ensemble(args)
     try:
         if args.impl == "reference":
             rc = run_reference(args, rank, world)

@@ -343,6 +343,39 @@ def random_faults(seed: int, sx: int = 512, sz: int = 256, dx: float = 0.4, nfau
         name=f"random-faults-{sx}x{sx}x{sz}-seed{seed}")
 
 
+ENSEMBLE_SHAPES = ((64, 64, 64), (128, 128, 64), (128, 128, 128), (192, 192, 96))
+
+
+def ensemble_uneven(seed: int = 4, n: int = 64) -> List[Simulation]:
+    """Batched ensemble of `n` members with uneven grids drawn from
+    {64^3, 128^2 x 64, 128^3, 192^2 x 96}.  Per member: stress exponent
+    U[1, 3.5], log10 of the fluidity prefactor U[-1, 1], elastic lid depth
+    U[15, 40] km, one strike-slip (dip 90, rake 0) or thrust (dip 25, rake 90)
+    fault with slip lognormal of median 1 (sigma 0.5), length U[10, 30] km,
+    width L/2.  The grid spacing makes every box 64 km deep (128 km / sx3),
+    so the lid lies inside the physical half-space.  Skip mode, Dt = tm/10."""
+    rng = np.random.default_rng(seed)
+    sims = []
+    for k in range(n):
+        sx1, sx2, sx3 = ENSEMBLE_SHAPES[int(rng.integers(len(ENSEMBLE_SHAPES)))]
+        dx = 128.0 / sx3
+        nexp = float(rng.uniform(1.0, 3.5))
+        g0 = float(10.0 ** rng.uniform(-1.0, 1.0))
+        lid = float(rng.uniform(15.0, 40.0))
+        L = float(rng.uniform(10.0, 30.0))
+        slip = float(np.exp(rng.normal(0.0, 0.5)))
+        if rng.integers(2):
+            f = Fault(slip, -L / 2, 0.0, 0.0, L, L / 2, 0.0, 90.0, 0.0)
+        else:
+            f = Fault(slip, -L / 2, 0.0, 1.0, L, L / 2, 0.0, 25.0, 90.0)
+        sims.append(Simulation(
+            sx1=sx1, sx2=sx2, sx3=sx3, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0, lambda_=1.0,
+            mu=1.0, gam=0.0, interval=1.0e6, odt=-1, tscale=1.0,
+            nonlinear=[(lid, g0, nexp, 0.0)], events=[Event(0.0, [f])],
+            name=f"ensemble-{k}-{sx1}x{sx2}x{sx3}"))
+    return sims
+
+
 def reference_output2() -> Simulation:
     """The input echoed in examples/tutorials/output2.param:8-62 (power-law
     n=3 relaxation after a strike-slip fault, 256^3)."""
