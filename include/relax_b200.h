@@ -118,14 +118,25 @@ typedef struct relax_config {
     int ne;                             /* coseismic events            */
     const relax_event *events;
     relax_event inter;                  /* interseismic loading rates  */
+    /* transient (Burgers) rheology, src/viscoelastic3d.f90:123-202 (the
+     * reference's --with-transient): linear and nonlinear per-layer
+     * structures (gammadot0, stressexponent, Gk; nz = sx3/2 entries) and
+     * optional weak-zone fields, or NULL */
+    const relax_layer *ltransientstruc;
+    const relax_layer *nltransientstruc;
+    const float *ltransientdgammadot0;
+    const float *nltransientdgammadot0;
 } relax_config;
 
 /* One line of RELAX's step log (src/relax.f90:1027-1047, format 1100):
- * I, Dt, tm(ve), tm(pl), tm(as), t, power, C:E^i. */
+ * I, Dt, tm(ve), tm(pl), tm(as), t, power, C:E^i; with the transient
+ * rheology (formats 1102/1103) also the Maxwell times of the linear and
+ * nonlinear transient mechanisms. */
 typedef struct relax_step_log {
     int i;
     int event;         /* 1 when a coseismic event fired after the step */
     double dt, tm_ve, tm_pl, tm_as, t, power, cei;
+    double tm_tl, tm_tnl;
 } relax_step_log;
 
 /* field selectors for relax_get_field / relax_set_field */

@@ -163,6 +163,7 @@ class Oracle:
             if rc:
                 raise RuntimeError(f"orc_coseismic failed ({rc})")
             logs.append(lg.as_tuple())
+            tmt = [(lg.tm_tl, lg.tm_tnl)]
             for k in range(nsteps):
                 dtp = C.byref(C.c_double(dt_schedule[k])) if dt_schedule is not None else None
                 rc = self.lib.orc_step(st, dtp, C.byref(lg))
@@ -171,9 +172,10 @@ class Oracle:
                 if lg.i == 0:
                     break
                 logs.append(lg.as_tuple())
-            out = {}
+                tmt.append((lg.tm_tl, lg.tm_tnl))
+            out = {"tm_transient": tmt}
             if fields:
-                out = self.get_fields(st, sim)
+                out.update(self.get_fields(st, sim))
                 out["patches"] = [self.get_patches(st, k, cfg.planes[k].px2 * cfg.planes[k].px3)
                                   for k in range(cfg.np)]
             return logs, out

@@ -508,6 +508,46 @@ int orc_viscouseigenstress(double mu, const relax_layer *structure,
 }
 
 /* ------------------------------------------------------------------ */
+/* transienteigenstress, src/viscoelastic3d.f90:123-202: Burgers creep    */
+/* with the transient strain epsilonik.  epsilonik and epsilonikdot may   */
+/* be the same array (the corrector's call, src/relax.f90:768-786): each  */
+/* point reads epsilonik before it writes epsilonikdot.                   */
+/* ------------------------------------------------------------------ */
+int orc_transienteigenstress(double mu, const relax_layer *structure, const otensor *sig,
+                             const otensor *epsilonik, int sx1, int sx2, int sx3, otensor *moment,
+                             otensor *epsilonikdot, double *maxwelltime, const real *dgammadot0)
+{
+    real tm = maxwelltime ? (real)*maxwelltime : (real)1e30;
+    for (int i3 = 0; i3 < sx3; i3++)
+        if (structure[i3].stressexponent < 0.999999) return ORC_ERR_POWER;
+#pragma omp parallel for schedule(static) reduction(min : tm)
+    for (int i3 = 0; i3 < sx3; i3++) {
+        double power = structure[i3].stressexponent, muk = structure[i3].Gk;
+        for (int i2 = 0; i2 < sx2; i2++) {
+            for (int i1 = 0; i1 < sx1; i1++) {
+                size_t o = IDX3(i1, i2, i3, sx1, sx2);
+                double gammadot0 = structure[i3].gammadot0;
+                if (dgammadot0) gammadot0 = gammadot0 + dgammadot0[o];
+                if (1.0e-20 > gammadot0) {
+                    memset(&epsilonikdot[o], 0, sizeof(otensor));
+                    continue;
+                }
+                otensor s = tdev(&sig[o]);
+                otensor Q = tminus(s, ttimes((real)(2.0 * muk), epsilonik[o]));
+                double nq = tnorm(&Q);
+                double gammadot = gammadot0 * pow(nq / mu, power - 1);
+                epsilonikdot[o] = ttimes((real)(gammadot / mu), Q);
+                moment[o] = tplus(moment[o], ttimes((real)(2.0 * gammadot), Q));
+                real r = (real)(1.0 / gammadot);
+                tm = tm < r ? tm : r;
+            }
+        }
+    }
+    if (maxwelltime) *maxwelltime = (double)tm < *maxwelltime ? (double)tm : *maxwelltime;
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------ */
 /* frictioneigenstress, src/friction3d.f90:82-241 (CPU branch)          */
 /* ------------------------------------------------------------------ */
 int orc_frictioneigenstress(double x, double y, double z, double L, double W, double strike,
@@ -1221,6 +1261,7 @@ typedef struct orc_state {
     size_t nv, nu, nt, n2;
     real *v[3], *u[3], *t[3], *gamma;
     otensor *tau, *sig, *moment;
+    otensor *eps, *epsdot;          /* transient strain and its rate (with a transient structure) */
     relax_slippatch **patch;
     double time;
     int i, e, oi;
@@ -1319,6 +1360,7 @@ void orc_state_free(orc_state *S)
     if (!S) return;
     for (int k = 0; k < 3; k++) { free(S->v[k]); free(S->u[k]); free(S->t[k]); }
     free(S->gamma); free(S->tau); free(S->sig); free(S->moment);
+    free(S->eps); free(S->epsdot);
     if (S->patch) for (int k = 0; k < S->cfg.np; k++) free(S->patch[k]);
     free(S->patch);
     free(S);
@@ -1344,6 +1386,11 @@ orc_state *orc_state_create(const relax_config *cfg)
     ok &= (S->tau = calloc(S->nt, sizeof(otensor))) != NULL;
     ok &= (S->sig = calloc(S->nt, sizeof(otensor))) != NULL;
     ok &= (S->moment = calloc(S->nt, sizeof(otensor))) != NULL;
+    /* epsilonik starts at zero (allocated, src/relax.f90:299-302) */
+    if (cfg->ltransientstruc || cfg->nltransientstruc) {
+        ok &= (S->eps = calloc(S->nt, sizeof(otensor))) != NULL;
+        ok &= (S->epsdot = calloc(S->nt, sizeof(otensor))) != NULL;
+    }
     if (cfg->np > 0) {
         S->patch = calloc((size_t)cfg->np, sizeof(relax_slippatch *));
         for (int k = 0; k < cfg->np && S->patch; k++) {
@@ -1390,6 +1437,30 @@ int orc_coseismic(orc_state *S, relax_step_log *log)
     return ORC_OK;
 }
 
+/* the linear and nonlinear transient mechanisms in turn (src/relax.f90:614-645
+ * in the predictor, :764-790 in the corrector): the input strain is `in`,
+ * the rate goes to S->epsdot (each call overwrites it) */
+static int transient_all(orc_state *S, const otensor *in, double *maxwell)
+{
+    const relax_config *c = &S->cfg;
+    const relax_layer *st[2] = {c->ltransientstruc, c->nltransientstruc};
+    const float *dg[2] = {c->ltransientdgammadot0, c->nltransientdgammadot0};
+    for (int m = 0; m < 2; m++) {
+        if (!st[m]) continue;
+        real *dgr = NULL;
+        if (dg[m]) {
+            dgr = malloc(sizeof(real) * S->nt);
+            if (!dgr) return ORC_ERR_ARG;
+            for (size_t q = 0; q < S->nt; q++) dgr[q] = (real)dg[m][q];
+        }
+        int err = orc_transienteigenstress(c->mu, st[m], S->sig, in, S->sx1, S->sx2, S->sx3h, S->moment,
+                                           S->epsdot, maxwell ? &maxwell[3 + m] : NULL, dgr);
+        free(dgr);
+        if (err) return err;
+    }
+    return ORC_OK;
+}
+
 /* one RK2 step, src/relax.f90:555-890 */
 int orc_step(orc_state *S, const double *dt_override, relax_step_log *log)
 {
@@ -1416,6 +1487,11 @@ int orc_step(orc_state *S, const double *dt_override, relax_step_log *log)
         }
         mech[2] = 1;
     }
+    if (S->eps) {
+        if ((err = transient_all(S, S->eps, maxwell))) return err;
+        if (c->ltransientstruc) mech[3] = 1;
+        if (c->nltransientstruc) mech[4] = 1;
+    }
     double tm = 1.0 / (mech[0] / maxwell[0] + mech[1] / maxwell[1] + mech[2] / maxwell[2] +
                        mech[3] / maxwell[3] + mech[4] / maxwell[4]);
     if (tm > STEP_MAX) tm = STEP_MAX;
@@ -1432,6 +1508,8 @@ int orc_step(orc_state *S, const double *dt_override, relax_step_log *log)
     orc_traction(c->mu, &c->events[S->e], S->sx1, S->sx2, c->dx1, c->dx2, S->time, Dt / 2.0e8, S->t[2], 1);
     if ((err = green(S))) return err;
     for (int k = 0; k < 3; k++) orc_fieldadd(S->v[k], S->u[k], S->nu, 1, (real)(Dt / 2), 0, 0);
+    /* epsilonikdot = Dt/2 epsilonikdot + epsilonik, src/relax.f90:693-695 */
+    if (S->eps) orc_tensorfieldadd(S->epsdot, S->eps, S->nt, 1, (real)(Dt / 2), 1, 1);
     orc_tensorfieldadd(S->sig, S->tau, S->nt, 1, -(real)(Dt / 2), 1, -1);
 
     /* corrector */
@@ -1450,6 +1528,13 @@ int orc_step(orc_state *S, const double *dt_override, relax_step_log *log)
                                 c->beta, S->sx1, S->sx2, S->sx3h, c->dx1, c->dx2, c->dx3, S->sig,
                                 c->faultcreepstruc, p->px2, p->px3, S->patch[k]);
         }
+    }
+    if (S->eps) {
+        /* both calls read epsilonikdot (src/relax.f90:768-786), then
+         * epsilonik += Dt epsilonikdot and epsilonikdot = 0 (:789-790) */
+        if ((err = transient_all(S, S->epsdot, NULL))) return err;
+        orc_tensorfieldadd(S->eps, S->epsdot, S->nt, 0, 0, 1, (real)Dt);
+        orc_tensorfieldadd(S->epsdot, S->epsdot, S->nt, 1, 0, 1, 0);
     }
     if (c->inter.ns > 0) {
         for (int i = 0; i < c->inter.ns; i++) {
@@ -1496,6 +1581,7 @@ int orc_step(orc_state *S, const double *dt_override, relax_step_log *log)
     if (log) {
         log->i = S->i; log->event = fired; log->dt = Dt;
         log->tm_ve = maxwell[0]; log->tm_pl = maxwell[1]; log->tm_as = maxwell[2];
+        log->tm_tl = maxwell[3]; log->tm_tnl = maxwell[4];
         log->t = S->time;
         log->power = orc_tensoramplitude(S->moment, S->nt, c->dx1, c->dx2, c->dx3);
         log->cei = orc_tensoramplitude(S->tau, S->nt, c->dx1, c->dx2, c->dx3);

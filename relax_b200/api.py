@@ -59,6 +59,7 @@ class Relax:
         lg = relax_step_log()
         dtp = C.byref(C.c_double(dt)) if dt is not None else None
         _lib.check(self.lib.relax_step(self.h, dtp, C.byref(lg)))
+        self.last_log = lg        # the full record (transient Maxwell times included)
         return lg.as_tuple()
 
     def run(self, nsteps: int, dt_schedule: Optional[Sequence[float]] = None) -> List[tuple]:

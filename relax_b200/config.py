@@ -78,12 +78,17 @@ class relax_config(C.Structure):
                 ("nonlineardgammadot0", C.POINTER(C.c_float)),
                 ("np", C.c_int), ("planes", C.POINTER(relax_plane)),
                 ("ne", C.c_int), ("events", C.POINTER(relax_event)),
-                ("inter", relax_event)]
+                ("inter", relax_event),
+                ("ltransientstruc", C.POINTER(relax_layer)),
+                ("nltransientstruc", C.POINTER(relax_layer)),
+                ("ltransientdgammadot0", C.POINTER(C.c_float)),
+                ("nltransientdgammadot0", C.POINTER(C.c_float))]
 
 
 class relax_step_log(C.Structure):
     _fields_ = [("i", C.c_int), ("event", C.c_int)] + \
-               [(n, C.c_double) for n in ("dt", "tm_ve", "tm_pl", "tm_as", "t", "power", "cei")]
+               [(n, C.c_double) for n in ("dt", "tm_ve", "tm_pl", "tm_as", "t", "power", "cei",
+                                          "tm_tl", "tm_tnl")]
 
     def as_tuple(self):
         return (self.i, self.dt, self.tm_ve, self.tm_pl, self.tm_as, self.t, self.power,
@@ -181,6 +186,10 @@ class Simulation:
     linear: List[Tuple[float, ...]] = field(default_factory=list)
     nonlinear: List[Tuple[float, ...]] = field(default_factory=list)
     faultcreep: List[Tuple[float, ...]] = field(default_factory=list)
+    # transient (Burgers) interfaces, src/input.f90:738-900:
+    # linear (depth, gammadot0, Gk), nonlinear (depth, gammadot0, power, Gk)
+    ltransient: List[Tuple[float, ...]] = field(default_factory=list)
+    nltransient: List[Tuple[float, ...]] = field(default_factory=list)
     planes: List[Plane] = field(default_factory=list)
     events: List[Event] = field(default_factory=list)
     name: str = "relax"
@@ -209,6 +218,14 @@ class Simulation:
               for (d, v0, ab, f, c) in self.faultcreep]
         return lin, non, fc
 
+    def transient_lists(self):
+        # the linear transient exponent is 1 (src/input.f90:760)
+        lt = [relax_layer(z=d, gammadot0=g, stressexponent=1.0, cohesion=0.0, friction=0.0, Gk=gk)
+              for (d, g, gk) in self.ltransient]
+        nlt = [relax_layer(z=d, gammadot0=g, stressexponent=n, cohesion=0.0, friction=0.0, Gk=gk)
+               for (d, g, n, gk) in self.nltransient]
+        return lt, nlt
+
     def to_c(self, structure_fn: Callable[[Sequence[relax_layer], float, int], C.Array]):
         """Returns (relax_config, keepalive) for this deck."""
         keep = []
@@ -222,8 +239,9 @@ class Simulation:
         cfg.odt = self.odt
         cfg.skip = self.skip
         lin, non, fc = self.layer_lists()
+        lt, nlt = self.transient_lists()
         for name, lst in (("linearstruc", lin), ("nonlinearstruc", non),
-                          ("faultcreepstruc", fc)):
+                          ("faultcreepstruc", fc), ("ltransientstruc", lt), ("nltransientstruc", nlt)):
             if lst:
                 arr = structure_fn(lst, self.dx3, nz)
                 keep.append(arr)

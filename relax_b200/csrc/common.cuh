@@ -38,9 +38,9 @@ struct DepthVisc {
 // Device-resident time-step state (src/relax.f90:555-890 host scalars).
 struct StepState {
     double t, Dt, tm;          // time, current step, combined Maxwell time
-    double maxwell[3];         // tm(ve), tm(pl), tm(as)
+    double maxwell[5];         // tm(ve), tm(pl), tm(as), transient linear / nonlinear
     double power, cei;         // log amplitudes of the last step
-    float tmin[2];             // Maxwell-time minima of the last stress pass
+    float tmin[4];             // Maxwell-time minima of the last stress pass (viscous 2, transient 2)
     double dt_raw;             // the step chosen by k_dt before validation
     int fire;                  // t + Dt reaches the next event
     double dt_override;        // used when use_override != 0
@@ -53,9 +53,15 @@ struct StepState {
 struct DtPolicy {
     double interval, odt, tscale, next_event_time;
     int skip, has_next_event, has_inter;
-    int mech[3];               // linear, nonlinear, fault creep present
+    int mech[5];               // linear, nonlinear, fault creep, transient linear / nonlinear present
 };
 
 #define RELAX_NTHREADS 256
+
+// one layer of a transient (Burgers) structure: gammadot0, stress exponent
+// and REAL(2 Gk) (src/viscoelastic3d.f90:171-181)
+struct TransLayer {
+    float g0, power, gk2, pad;
+};
 
 }  // namespace relax

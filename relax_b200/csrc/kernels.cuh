@@ -112,11 +112,21 @@ struct StressArgs {
     StepState *fin;          // with ticket: receives tmin, power, cei
     double dv;               // cell volume dx1 dx2 dx3 (amplitude scale)
     const struct StressArgs *tab;   // batched launch: one entry per member (blockIdx.y)
+    // transient (Burgers) rheology, TRANS instantiations only
+    const TransLayer *trans[2];      // linear / nonlinear transient structures or null
+    const float *tdg0[2];            // their weak-zone perturbations or null
+    float *eps, *epsdot;             // epsilonik, epsilonikdot (6 x nh each)
 };
 
-// BATCH: blockIdx.y selects a member of a batch, whose arguments are a0.tab[blockIdx.y]
-template <int MODE, bool BATCH = false>
-__global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(const __grid_constant__ StressArgs a0)
+// BATCH: blockIdx.y selects a member of a batch, whose arguments are a0.tab[blockIdx.y].
+// TRANS: also the transient rheology (transienteigenstress,
+// src/viscoelastic3d.f90:123-202): in INIT/END the predictor's calls
+// (src/relax.f90:614-645: epsilonikdot from epsilonik, two more Maxwell-time
+// minima), in CORR the predicted strain epsilonikdot = Dt/2 epsilonikdot +
+// epsilonik (:693-695), the corrector's calls on it (:764-787) and
+// epsilonik += Dt epsilonikdot (:789).
+template <int MODE, bool BATCH = false, bool TRANS = false>
+__global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const __grid_constant__ StressArgs a0)
 {
     const StressArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     __shared__ float shf[32];
@@ -127,7 +137,8 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(const __grid_const
     const size_t nq = g.nh >> 2;
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = q < nq;
-    float tmin[2] = {3.0e38f, 3.0e38f};
+    constexpr int NTM = TRANS ? 4 : 2;        // Maxwell-time minima: viscous 2 (+ transient 2)
+    float tmin[4] = {3.0e38f, 3.0e38f, 3.0e38f, 3.0e38f};
     double amp_m = 0.0, amp_t = 0.0;
 
     if (live) {
@@ -318,6 +329,85 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(const __grid_const
                     for (int j = 0; j < 4; j++) gacc[j] = gacc[j] + dtf * gsum[j];
                 }
             }
+            if (TRANS && (MODE == MODE_INIT || MODE == MODE_END || MODE == MODE_CORR) && a.eps) {
+                float ep[6][4], in[6][4], rate[6][4];
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    const float4 e = ldc4(a.eps + c * nh + idx);
+                    ep[c][0] = e.x; ep[c][1] = e.y; ep[c][2] = e.z; ep[c][3] = e.w;
+                }
+                if (MODE == MODE_CORR) {
+                    const float h = (float)(a.st->Dt / 2);
+#pragma unroll
+                    for (int c = 0; c < 6; c++) {
+                        const float4 r = ldc4(a.epsdot + c * nh + idx);
+                        in[c][0] = h * r.x + ep[c][0]; in[c][1] = h * r.y + ep[c][1];
+                        in[c][2] = h * r.z + ep[c][2]; in[c][3] = h * r.w + ep[c][3];
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 6; c++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) in[c][j] = ep[c][j];
+                }
+#pragma unroll
+                for (int c = 0; c < 6; c++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) rate[c][j] = 0.f;
+#pragma unroll
+                for (int tm = 0; tm < 2; tm++) {
+                    if (!a.trans[tm]) continue;
+                    const TransLayer L = a.trans[tm][i3];
+                    float g0v[4] = {L.g0, L.g0, L.g0, L.g0};
+                    if (a.tdg0[tm]) {
+                        const float4 d = ld4(a.tdg0[tm] + idx);
+                        g0v[0] += d.x; g0v[1] += d.y; g0v[2] += d.z; g0v[3] += d.w;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+#pragma unroll
+                        for (int c = 0; c < 6; c++) rate[c][j] = 0.f;
+                        if (1.0e-20f > g0v[j]) continue;
+                        const float tr3 = (s[0][j] + s[3][j] + s[5][j]) * (1.f / 3.f);
+                        // Q = s' - 2 Gk epsilonik
+                        const float Q[6] = {(s[0][j] - tr3) - L.gk2 * in[0][j], s[1][j] - L.gk2 * in[1][j],
+                                            s[2][j] - L.gk2 * in[2][j], (s[3][j] - tr3) - L.gk2 * in[3][j],
+                                            s[4][j] - L.gk2 * in[4][j], (s[5][j] - tr3) - L.gk2 * in[5][j]};
+                        const float x = tnorm6(Q[0], Q[1], Q[2], Q[3], Q[4], Q[5]) * a.muinv;
+                        const float pe = L.power - 1.f;
+                        float gd;
+                        if (pe == 0.f) gd = g0v[j];
+                        else if (pe == 1.f) gd = g0v[j] * x;
+                        else if (pe == 2.f) gd = g0v[j] * x * x;
+                        else gd = g0v[j] * powf(x, pe);
+                        const float rq = gd * a.muinv, gd2 = 2.f * gd;
+#pragma unroll
+                        for (int c = 0; c < 6; c++) {
+                            rate[c][j] = rq * Q[c];
+                            mo[c][j] += gd2 * Q[c];
+                        }
+                        if (MODE != MODE_CORR) tmin[2 + tm] = fminf(tmin[2 + tm], 1.f / gd);
+                    }
+                    if (MODE == MODE_CORR) {
+                        // the corrector's next call reads epsilonikdot, i.e. this rate
+#pragma unroll
+                        for (int c = 0; c < 6; c++)
+#pragma unroll
+                            for (int j = 0; j < 4; j++) in[c][j] = rate[c][j];
+                    }
+                }
+                if (MODE == MODE_CORR) {
+#pragma unroll
+                    for (int c = 0; c < 6; c++)
+                        st4(a.eps + c * nh + idx,
+                            make_float4(ep[c][0] + dtf * rate[c][0], ep[c][1] + dtf * rate[c][1],
+                                        ep[c][2] + dtf * rate[c][2], ep[c][3] + dtf * rate[c][3]));
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 6; c++)
+                        st4(a.epsdot + c * nh + idx, make_float4(rate[c][0], rate[c][1], rate[c][2], rate[c][3]));
+                }
+            }
 #pragma unroll
             for (int c = 0; c < 6; c++)
                 st4(a.m + c * nh + idx, make_float4(mo[c][0], mo[c][1], mo[c][2], mo[c][3]));
@@ -327,24 +417,30 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(const __grid_const
     }
 
     if (MODE == MODE_INIT || MODE == MODE_END || MODE == MODE_EIGEN) {
-        // the four block reductions in one pass (fixed order, one barrier)
-        float t0 = warp_min(tmin[0]), t1 = warp_min(tmin[1]);
+        // the block reductions in one pass (fixed order, one barrier); 8 warps
+        float tq[4];
+#pragma unroll
+        for (int q = 0; q < NTM; q++) tq[q] = warp_min(tmin[q]);
         double am = warp_sum(amp_m), at = warp_sum(amp_t);
         {
             const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
-            if (l == 0) { shf[w] = t0; shf[16 + w] = t1; shd[w] = am; shd[16 + w] = at; }
+            if (l == 0) {
+#pragma unroll
+                for (int q = 0; q < NTM; q++) shf[8 * q + w] = tq[q];
+                shd[w] = am; shd[16 + w] = at;
+            }
             __syncthreads();
             if (w == 0) {
-                t0 = warp_min(l < nw ? shf[l] : 3.0e38f);
-                t1 = warp_min(l < nw ? shf[16 + l] : 3.0e38f);
+#pragma unroll
+                for (int q = 0; q < NTM; q++) tq[q] = warp_min(l < nw ? shf[8 * q + l] : 3.0e38f);
                 am = warp_sum(l < nw ? shd[l] : 0.0);
                 at = warp_sum(l < nw ? shd[16 + l] : 0.0);
             }
         }
         __shared__ unsigned last;
         if (threadIdx.x == 0) {
-            a.tm_part[blockIdx.x] = t0;
-            a.tm_part[gridDim.x + blockIdx.x] = t1;
+#pragma unroll
+            for (int q = 0; q < NTM; q++) a.tm_part[q * gridDim.x + blockIdx.x] = tq[q];
             a.amp_part[blockIdx.x] = am;
             a.amp_part[gridDim.x + blockIdx.x] = at;
             if (a.ticket) {
@@ -359,38 +455,39 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, 3) k_stress(const __grid_const
             if (last) {
                 __threadfence();
                 const int n = gridDim.x, nt = blockDim.x;
-                float m0 = 3.0e38f, m1 = 3.0e38f;
+                float mq[4] = {3.0e38f, 3.0e38f, 3.0e38f, 3.0e38f};
                 double s0 = 0.0, s1 = 0.0;
                 for (int b = 0; b < n; b += 8 * nt) {
-                    float v0[8], v1[8];
+                    float v[4][8];
                     double w0[8], w1[8];
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
                         const int i = b + u * nt + threadIdx.x;
                         const bool in = i < n;
-                        v0[u] = in ? __ldcg(a.tm_part + i) : 3.0e38f;
-                        v1[u] = in ? __ldcg(a.tm_part + n + i) : 3.0e38f;
+#pragma unroll
+                        for (int q = 0; q < NTM; q++) v[q][u] = in ? __ldcg(a.tm_part + q * n + i) : 3.0e38f;
                         w0[u] = in ? __ldcg(a.amp_part + i) : 0.0;
                         w1[u] = in ? __ldcg(a.amp_part + n + i) : 0.0;
                     }
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
-                        m0 = fminf(m0, v0[u]);
-                        m1 = fminf(m1, v1[u]);
+#pragma unroll
+                        for (int q = 0; q < NTM; q++) mq[q] = fminf(mq[q], v[q][u]);
                         s0 += w0[u];
                         s1 += w1[u];
                     }
                 }
-                m0 = block_min(m0, shf);
-                __syncthreads();
-                m1 = block_min(m1, shf);
-                __syncthreads();
+#pragma unroll
+                for (int q = 0; q < NTM; q++) {
+                    mq[q] = block_min(mq[q], shf);
+                    __syncthreads();
+                }
                 s0 = block_sum(s0, shd);
                 __syncthreads();
                 s1 = block_sum(s1, shd);
                 if (threadIdx.x == 0) {
-                    a.fin->tmin[0] = m0;
-                    a.fin->tmin[1] = m1;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) a.fin->tmin[q] = q < NTM ? mq[q] : 3.0e38f;
                     a.fin->power = s0 * a.dv;
                     a.fin->cei = s1 * a.dv;
                     *a.ticket = 0u;
@@ -1690,16 +1787,19 @@ __device__ __forceinline__ void dt_body(StepState *st, const DtPolicy &pol, cons
     m2 = block_min(m2, shf);
     if (threadIdx.x == 0) {
         const double STEP_MAX = 1e7;
-        double mw[3];
-        const float mf[3] = {m0, m1, m2};
-        for (int k = 0; k < 3; k++) {
+        // mechanisms of src/relax.f90:660-664: linear, power law, fault
+        // creep, linear and nonlinear transient
+        double mw[5];
+        const float mf[5] = {m0, m1, m2, ntm == 0 ? st->tmin[2] : 3.0e38f, ntm == 0 ? st->tmin[3] : 3.0e38f};
+        for (int k = 0; k < 5; k++) {
             // tm = min(REAL(STEP_MAX), min over cells), src/viscoelastic3d.f90:242-245
             const float v = fminf((float)STEP_MAX, mf[k]);
             mw[k] = pol.mech[k] ? (double)v : STEP_MAX;
             st->maxwell[k] = mw[k];
         }
         double tm = 1.0 / ((double)pol.mech[0] / mw[0] + (double)pol.mech[1] / mw[1] +
-                           (double)pol.mech[2] / mw[2]);
+                           (double)pol.mech[2] / mw[2] + (double)pol.mech[3] / mw[3] +
+                           (double)pol.mech[4] / mw[4]);
         if (tm > STEP_MAX) tm = STEP_MAX;
         if (pol.has_inter && tm == STEP_MAX) tm = pol.interval / 20.0;
         st->tm = tm;

@@ -667,6 +667,12 @@ struct relax_ctx {
     float *tau = nullptr, *m = nullptr, *sig = nullptr, *u = nullptr, *vp = nullptr, *gamma = nullptr;
     float *work = nullptr, *twork = nullptr, *tload = nullptr;
     DepthVisc *visc[2] = {nullptr, nullptr};
+    // transient (Burgers) rheology: structures, weak zones, epsilonik, epsilonikdot
+    std::vector<relax_layer> lt, nlt;
+    TransLayer *tvisc[2] = {nullptr, nullptr};
+    float *tdg0[2] = {nullptr, nullptr};
+    float *eps = nullptr, *epsdot = nullptr;
+    bool trans = false;
     float *spdev = nullptr, *dg0[2] = {nullptr, nullptr};
     double *fcd = nullptr;
     relax_slippatch *patch = nullptr;
@@ -711,6 +717,12 @@ static void free_ctx(relax_ctx *c)
     for (auto p : c->band_idx) if (p) cudaFree(p);
     for (auto p : c->band_imp) if (p) cudaFree(p);
     if (c->sig_mask) cudaFree(c->sig_mask);
+    for (int k = 0; k < 2; k++) {
+        if (c->tvisc[k]) cudaFree(c->tvisc[k]);
+        if (c->tdg0[k]) cudaFree(c->tdg0[k]);
+    }
+    if (c->eps) cudaFree(c->eps);
+    if (c->epsdot) cudaFree(c->epsdot);
     if (c->ticket) cudaFree(c->ticket);
     if (c->dst && c->own_dst) cudaFree(c->dst);
     if (c->hst) cudaFreeHost(c->hst);
@@ -752,6 +764,9 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     copyv(cfg->linearstruc, c->lin);
     copyv(cfg->nonlinearstruc, c->non);
     copyv(cfg->faultcreepstruc, c->fc);
+    copyv(cfg->ltransientstruc, c->lt);
+    copyv(cfg->nltransientstruc, c->nlt);
+    c->trans = !c->lt.empty() || !c->nlt.empty();
     if (cfg->stressstruc) c->pre.assign(cfg->stressstruc, cfg->stressstruc + nz);
     if (cfg->np > 0) c->planes.assign(cfg->planes, cfg->planes + cfg->np);
     auto copye = [](const relax_event &e, EventCopy &o) {
@@ -768,13 +783,15 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
             return fail(RELAX_ERR_UNSUPPORTED, "tensile and dilatation sources are not supported");
     }
     copye(cfg->inter, c->inter);
-    for (const auto *v : {&c->lin, &c->non})
+    for (const auto *v : {&c->lin, &c->non, &c->lt, &c->nlt})
         for (const auto &l : *v)
             if (l.stressexponent < 0.999999)
                 return fail(RELAX_ERR_POWER, "invalid power exponent %g", l.stressexponent);
     c->cfg.stressstruc = nullptr; c->cfg.linearstruc = nullptr; c->cfg.nonlinearstruc = nullptr;
     c->cfg.faultcreepstruc = nullptr; c->cfg.planes = nullptr; c->cfg.events = nullptr;
     c->cfg.lineardgammadot0 = nullptr; c->cfg.nonlineardgammadot0 = nullptr;
+    c->cfg.ltransientstruc = nullptr; c->cfg.nltransientstruc = nullptr;
+    c->cfg.ltransientdgammadot0 = nullptr; c->cfg.nltransientdgammadot0 = nullptr;
 
     const size_t nh = g.nh;
     TRY(dalloc(&c->tau, 6 * nh));
@@ -822,6 +839,30 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
             CK(cudaMemcpy(c->dg0[k], dgs[k], nh * sizeof(float), cudaMemcpyHostToDevice));
         }
     }
+    // transient structures (gammadot0, exponent, REAL(2 Gk) per layer), weak
+    // zones, and epsilonik = epsilonikdot = 0 (allocated, src/relax.f90:299-302)
+    if (c->trans) {
+        const std::vector<relax_layer> *ts[2] = {&c->lt, &c->nlt};
+        const float *tdg[2] = {cfg->ltransientdgammadot0, cfg->nltransientdgammadot0};
+        for (int k = 0; k < 2; k++) {
+            if (ts[k]->empty()) continue;
+            std::vector<TransLayer> tl(nz);
+            for (int i3 = 0; i3 < nz; i3++) {
+                const relax_layer &l = (*ts[k])[i3];
+                tl[i3] = TransLayer{(float)l.gammadot0, (float)l.stressexponent, (float)(2.0 * l.Gk), 0.f};
+            }
+            TRY(dalloc(&c->tvisc[k], nz));
+            CK(cudaMemcpy(c->tvisc[k], tl.data(), nz * sizeof(TransLayer), cudaMemcpyHostToDevice));
+            if (tdg[k]) {
+                TRY(dalloc(&c->tdg0[k], nh));
+                CK(cudaMemcpy(c->tdg0[k], tdg[k], nh * sizeof(float), cudaMemcpyHostToDevice));
+            }
+        }
+        TRY(dalloc(&c->eps, 6 * nh));
+        TRY(dalloc(&c->epsdot, 6 * nh));
+        CK(cudaMemsetAsync(c->eps, 0, 6 * nh * sizeof(float), c->st));
+        CK(cudaMemsetAsync(c->epsdot, 0, 6 * nh * sizeof(float), c->st));
+    }
     if (pre) {
         if (spdev.empty()) {
             std::vector<DepthVisc> dv;
@@ -855,7 +896,7 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     }
     // reductions
     c->nblk = (int)nblocks(nh / 4);
-    TRY(dalloc(&c->tm_part, 2 * (size_t)c->nblk));
+    TRY(dalloc(&c->tm_part, 4 * (size_t)c->nblk));
     TRY(dalloc(&c->amp_part, 2 * (size_t)c->nblk));
     TRY(dalloc(&c->amp_alt, 2 * (size_t)c->nblk));
     c->nfr = 1;
@@ -929,6 +970,8 @@ static StressArgs stress_args(relax_ctx *c, const float *w)
     a.ticket = c->ticket;
     a.fin = c->dst;
     a.dv = g.dx1 * g.dx2 * g.dx3;
+    for (int k = 0; k < 2; k++) { a.trans[k] = c->tvisc[k]; a.tdg0[k] = c->tdg0[k]; }
+    a.eps = c->eps; a.epsdot = c->epsdot;
     a.tm_part = c->tm_part;
     a.amp_part = c->amp_part;
     return a;
@@ -939,7 +982,10 @@ static int launch_stress(relax_ctx *c, StressArgs a)
 {
     const int stage = MODE == MODE_END ? ST_STRESS_END : MODE == MODE_CORR ? ST_STRESS_CORR
                       : MODE == MODE_INIT ? ST_STRESS_INIT : ST_OTHER;
-    TIMED(&c->prof, stage, c->st, (k_stress<MODE><<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(a)));
+    if (c->trans && MODE != MODE_OP && MODE != MODE_EIGEN)
+        TIMED(&c->prof, stage, c->st, (k_stress<MODE, false, true><<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(a)));
+    else
+        TIMED(&c->prof, stage, c->st, (k_stress<MODE><<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(a)));
     return RELAX_OK;
 }
 
@@ -1297,6 +1343,8 @@ static DtPolicy policy(relax_ctx *c)
     p.mech[0] = !c->lin.empty();
     p.mech[1] = !c->non.empty();
     p.mech[2] = !c->fc.empty();
+    p.mech[3] = !c->lt.empty();
+    p.mech[4] = !c->nlt.empty();
     return p;
 }
 
@@ -1310,7 +1358,8 @@ static int finish_step(relax_ctx *c, relax_step_log *log)
     if (!(c->hst->dt_raw > 0.0) || !std::isfinite(c->hst->dt_raw))
         return fail(RELAX_ERR_ARG, "invalid time step %g", c->hst->dt_raw);
     Dt = c->hst->Dt;
-    const double mw[3] = {c->hst->maxwell[0], c->hst->maxwell[1], c->hst->maxwell[2]};
+    const double mw[5] = {c->hst->maxwell[0], c->hst->maxwell[1], c->hst->maxwell[2], c->hst->maxwell[3],
+                          c->hst->maxwell[4]};
     c->t = c->t + Dt;
     c->i++;
     const int fired = c->hst->fire;
@@ -1343,6 +1392,7 @@ static int finish_step(relax_ctx *c, relax_step_log *log)
     log->event = fired;
     log->dt = Dt;
     log->tm_ve = mw[0]; log->tm_pl = mw[1]; log->tm_as = mw[2];
+    log->tm_tl = mw[3]; log->tm_tnl = mw[4];
     log->t = c->t;
     log->power = c->hst->power;
     log->cei = c->hst->cei;
@@ -1985,6 +2035,7 @@ struct relax_batch {
     int device = 0;
     cudaStream_t st = nullptr;
     bool batched = false;          // register passes instantiated for the grid
+    bool trans = false;            // a member has the transient rheology
     bool tables_valid = false;
     BatchTables tab;
     StepState *dst = nullptr;      // the members' device states, contiguous
@@ -2053,6 +2104,7 @@ extern "C" int relax_batch_create(const relax_config *members, int n, int device
         c->err = &c->dst->error;
     }
     b->batched = reg_shape(b->m[0]->g);
+    for (auto *c : b->m) b->trans = b->trans || c->trans;
     b->nfr.assign(n, 0);
     *out = b;
     return RELAX_OK;
@@ -2280,7 +2332,8 @@ extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
     CKL();
     TRY(batch_green(b, t.xip0));
     // ---- corrector
-    k_stress<MODE_CORR, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.corr0);
+    if (b->trans) k_stress<MODE_CORR, true, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.corr0);
+    else k_stress<MODE_CORR, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.corr0);
     b->launches++;
     if (!c0->fc.empty())
         for (size_t q = 0; q < np; q++) {
@@ -2308,7 +2361,8 @@ extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
     }
     CKL();
     TRY(batch_green(b, t.xic0));
-    k_stress<MODE_END, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.end0);
+    if (b->trans) k_stress<MODE_END, true, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.end0);
+    else k_stress<MODE_END, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.end0);
     b->launches++;
     CKL();
     CK(cudaMemcpyAsync(b->hst, b->dst, n * sizeof(StepState), cudaMemcpyDeviceToHost, st));

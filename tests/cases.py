@@ -60,3 +60,20 @@ def two_events(sx=64, sz=32, dx=1.0):
     s.events.append(Event(1.0, [Fault(0.5, -5.0, 8.0, 0.0, 10.0, 5.0, 30.0, 60.0, 45.0)]))
     s.name = "two-events"
     return s
+
+
+def transient_small(linear=True, nonlinear=False, viscous=False, sx=64, sz=32):
+    """Transient (Burgers) rheology below 6 km: linear (gammadot0 1, Gk 0.5)
+    and/or nonlinear (gammadot0 2, n 3, Gk 1) transient layers, optionally a
+    linear Maxwell layer as well; the vertical strike-slip fault of
+    linear_small."""
+    s = linear_small(sx, sz, steps=4)
+    s.name = "transient-small"
+    s.interval = 1.0e6       # the nonlinear transient's first steps are long
+    if not viscous:
+        s.linear = []
+    if linear:
+        s.ltransient = [(6.0, 1.0, 0.5)]
+    if nonlinear:
+        s.nltransient = [(6.0, 2.0, 3.0, 1.0)]
+    return s
