@@ -85,6 +85,15 @@ typedef struct relax_slippatch {
     relax_tensor sig;
 } relax_slippatch;
 
+/* WEAK_STRUCT, src/types.f90:46-50: a ductile (weak) zone in the internal
+ * convention (after wangconvention, src/input.f90:574-583).  Negative
+ * dimensions select spherical / cylindrical zones (src/viscoelastic3d.f90:
+ * 403-430). */
+typedef struct relax_weakzone {
+    double dgammadot0, x, y, z, width, length, thickness, strike, dip;
+    relax_tensor e;
+} relax_weakzone;
+
 /* EVENT_STRUC, src/types.f90:99-106 (shear, tensile, point and load
  * sources; cuboid/tetrahedron eigenstrain sources are not supported). */
 typedef struct relax_event {
@@ -290,6 +299,25 @@ int relax_op_viscouseigenstress(double mu, const relax_layer *structure,
                                 double *maxwelltime, float *gamma,
                                 const float *dgammadot0, void *stream);
 
+/* transienteigenstress, src/viscoelastic3d.f90:123-202: moment +=
+ * 2 gammadot Q and epsilonikdot = gammadot/mu Q with Q = s' - 2 Gk
+ * epsilonik, per layer of `structure` (gammadot0, stressexponent, Gk; sx3h
+ * entries); epsilonik and epsilonikdot may be the same buffer (the
+ * reference's corrector call).  dgammadot0 optional (sx1, sx2, sx3h).
+ * *maxwelltime = min(*maxwelltime, min 1/gammadot) when non-NULL
+ * (synchronous then). */
+int relax_op_transienteigenstress(double mu, const relax_layer *structure, const relax_tensor *sig,
+                                  const relax_tensor *epsilonik, int sx1, int sx2, int sx3h,
+                                  relax_tensor *moment, relax_tensor *epsilonikdot,
+                                  double *maxwelltime, const float *dgammadot0, void *stream);
+
+/* builddgammadot0, src/viscoelastic3d.f90:320-435: the fluidity
+ * perturbation of `nz` weak zones (host array) at the physical points,
+ * out (sx1, sx2, sx3h) on the device.  RELAX builds with beta = 0
+ * (src/relax.f90:487-541). */
+int relax_op_dgammadot0(const relax_weakzone *zones, int nz, int sx1, int sx2, int sx3h,
+                        double dx1, double dx2, double dx3, double beta, float *out, void *stream);
+
 /* frictioneigenstress, src/friction3d.f90:82-241 for one afterslip plane
  * (x..rake in the internal convention; L = plane width, W = plane length
  * as the reference call sites pass them).  Synchronous when maxwelltime
@@ -406,6 +434,22 @@ void cusource_(double mu, double s, double x, double y, double z, double L,
                double beta, int sx1, int sx2, int sx3, double dx1,
                double dx2, double dx3, float *f1, float *f2, float *f3,
                float *t1, float *t2, float *t3);
+/* src/cuelastic.cu:1085 -- transient eigenstress on epsilonik (eType 4) or,
+ * in place, on epsilonikdot (eType 5); bgammadot 3/4 = transient weak zones */
+void cutransienteigenwrapper_(int eType, relax_layer *structure, double mu,
+                              int sx1, int sx2, int sx3h, double dx1,
+                              double dx2, double dx3, int bMaxwell,
+                              double *dMaxwell, int bgammadot);
+/* src/cuelastic.cu:1689 -- weak-zone fluidity field of one mechanism
+ * (gammadotType 1..4: linear, nonlinear, linear / nonlinear transient) */
+void cubuildgammadot_(int sx1, int sx2, int sx3h, double dx1, double dx2,
+                      double dx3, int nz, relax_weakzone *zones,
+                      int gammadotType);
+/* src/cuelastic.cu:1629 -- one x3-plane of the padded displacement */
+void cuexportspatial_(float *u1, float *u2, float *u3, int i3);
+/* src/cuelastic.cu:1652 -- displacement and stress at one point (0-based) */
+void cuexportpoints_(double *u1, double *u2, double *u3, ST_TENSOR_C *sig,
+                     int i1, int i2, int i3);
 
 #ifdef __cplusplus
 }

@@ -42,6 +42,8 @@ def load(precision: int = 32) -> C.CDLL:
         "orc_stressupdate": (I, [P, P, P, D, D, D, D, D, I, I, I, P]),
         "orc_equivalentbodyforce": (I, [P, D, D, D, I, I, I, P, P, P, P, P, P]),
         "orc_viscouseigenstress": (I, [D, P, P, P, I, I, I, P, P, P, P]),
+        "orc_transienteigenstress": (I, [D, P, P, P, I, I, I, P, P, P, P]),
+        "orc_builddgammadot0": (None, [I, I, I, D, D, D, D, I, P, P]),
         "orc_frictioneigenstress": (I, [D, D, D, D, D, D, D, D, D, P, D, P, I, I, I, D, D, D, P, P]),
         "orc_fft3": (None, [P, I, I, I, D, D, D, I]),
         "orc_fft2": (None, [P, I, I, D, D, I]),
@@ -129,6 +131,21 @@ class Oracle:
             ptr(sig), sx1, sx2, sx3h, ptr(moment), None if tm is None else C.byref(tm), ptr(gamma),
             ptr(dgammadot0))
         return rc, (tm.value if tm is not None else None)
+
+    def transienteigenstress(self, mu, structure, sig, eps, sx1, sx2, sx3h, moment, epsdot,
+                             maxwell: Optional[float] = None, dgammadot0=None):
+        """eps and epsdot may be the same array"""
+        tm = C.c_double(maxwell) if maxwell is not None else None
+        rc = self.lib.orc_transienteigenstress(
+            mu, C.cast(structure, C.c_void_p), ptr(sig), ptr(eps), sx1, sx2, sx3h, ptr(moment), ptr(epsdot),
+            None if tm is None else C.byref(tm), ptr(dgammadot0))
+        return rc, (tm.value if tm is not None else None)
+
+    def builddgammadot0(self, zones, sx1, sx2, sx3h, dx, beta):
+        out = np.zeros((sx3h, sx2, sx1), self.real)
+        arr = C.cast(zones, C.c_void_p) if len(zones) else None
+        self.lib.orc_builddgammadot0(sx1, sx2, sx3h, *dx, beta, len(zones), arr, ptr(out))
+        return out
 
     def frictioneigenstress(self, plane, beta, sig, mu, structure, sx1, sx2, sx3h, dx, moment,
                             maxwell: Optional[float] = None):

@@ -548,6 +548,57 @@ int orc_transienteigenstress(double mu, const relax_layer *structure, const oten
 }
 
 /* ------------------------------------------------------------------ */
+/* builddgammadot0 / fdgammadot0, src/viscoelastic3d.f90:320-435        */
+/* ------------------------------------------------------------------ */
+void orc_builddgammadot0(int sx1, int sx2, int sx3, double dx1, double dx2, double dx3, double beta,
+                         int nz, const relax_weakzone *zones, real *dgammadot0)
+{
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3; i3++) {
+        double x3 = (double)(i3 - 1) * dx3;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                double x1, x2, dum;
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &dum);
+                double f = 0.0;
+                for (int i = 0; i < nz; i++) {
+                    const relax_weakzone *z = &zones[i];
+                    double dg = z->dgammadot0, x = z->x, y = z->y, zz = z->z;
+                    double W = z->length, L = z->width, D = z->thickness;
+                    double Wp = W * (1.0 + 2.0 * beta) / 2.0, Lp = L * (1.0 + 2.0 * beta) / 2.0;
+                    double Dp = D * (1.0 + 2.0 * beta) / 2.0;
+                    double LM = Wp > Lp ? Wp : Lp;
+                    if (Dp > LM) LM = Dp;
+                    if (fabs(x3 - zz) > LM || fabs(x1 - x) > LM || fabs(x2 - y) > LM) continue;
+                    double cs = cos(z->strike), ss = sin(z->strike), cd = cos(z->dip), sd = sin(z->dip);
+                    double x2r = cs * x - ss * y;
+                    double xr = cd * x2r - sd * zz, yr = ss * x + cs * y, zr = sd * x2r + cd * zz;
+                    x2r = cs * x1 - ss * x2;
+                    double x1s = cd * x2r - sd * x3, x2s = ss * x1 + cs * x2, x3s = sd * x2r + cd * x3;
+                    if (D >= 0 && W >= 0 && L >= 0) {
+                        f = f + omega((x1s - xr) / D, beta) * omega((x2s - yr) / W, beta) *
+                                    omega((x3s - zr) / L, beta) * dg;
+                    } else if (D < 0 && W < 0 && L < 0) {
+                        double r = sqrt(SQ((x1s - xr) / D) + SQ((x2s - yr) / W) + SQ((x3s - zr) / L));
+                        f = f + omega(r, beta) * dg;
+                    } else if (D < 0 && W < 0) {
+                        double rho = sqrt(SQ((x1s - xr) / D) + SQ((x2s - yr) / W));
+                        f = f + omega(rho, beta) * omega((x3s - zr) / L, beta) * dg;
+                    } else if (D < 0 && L < 0) {
+                        double rho = sqrt(SQ((x1s - xr) / D) + SQ((x3s - zr) / L));
+                        f = f + omega(rho, beta) * omega((x2s - yr) / W, beta) * dg;
+                    } else if (W < 0 && L < 0) {
+                        double rho = sqrt(SQ((x2s - yr) / W) + SQ((x3s - zr) / L));
+                        f = f + omega(rho, beta) * omega((x1s - xr) / D, beta) * dg;
+                    }
+                }
+                dgammadot0[IDX3(i1 - 1, i2 - 1, i3 - 1, sx1, sx2)] = (real)f;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* frictioneigenstress, src/friction3d.f90:82-241 (CPU branch)          */
 /* ------------------------------------------------------------------ */
 int orc_frictioneigenstress(double x, double y, double z, double L, double W, double strike,

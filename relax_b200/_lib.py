@@ -84,6 +84,8 @@ def load() -> C.CDLL:
         "relax_op_stressupdate": (I, [P, P, P, D, D, D, D, D, I, I, I, P, P]),
         "relax_op_bodyforce": (I, [P, D, D, D, I, I, I, P, P, P, P, P, P, P]),
         "relax_op_viscouseigenstress": (I, [D, P, P, P, I, I, I, P, C.POINTER(D), P, P, P]),
+        "relax_op_transienteigenstress": (I, [D, P, P, P, I, I, I, P, P, C.POINTER(D), P, P]),
+        "relax_op_dgammadot0": (I, [P, I, I, I, I, D, D, D, D, P, P]),
         "relax_op_frictioneigenstress": (I, [D, D, D, D, D, D, D, D, D, P, D, P, I, I, I, D, D, D, P,
                                              C.POINTER(D), P]),
         "relax_op_green": (I, [P, P, P, P, P, P, I, I, I, D, D, D, D, D, D, P]),

@@ -56,6 +56,12 @@ class relax_slippatch(C.Structure):
                  "taus")] + [("sig", relax_tensor)]
 
 
+class relax_weakzone(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("dgammadot0", "x", "y", "z", "width", "length", "thickness", "strike", "dip")] + \
+               [("e", relax_tensor)]
+
+
 class relax_event(C.Structure):
     _fields_ = [("time", C.c_double), ("ns", C.c_int), ("nt", C.c_int), ("nm", C.c_int),
                 ("nl", C.c_int), ("s", C.POINTER(relax_source)),

@@ -868,6 +868,103 @@ __global__ void k_monitor(const __grid_constant__ MonitorArgs a0)
     p->slip = sqrt(p->ds * p->ds + p->ss * p->ss);
 }
 
+// transienteigenstress (src/viscoelastic3d.f90:123-202) on SoA tensors, one
+// point per thread (operator API): moment += 2 gd Q, epsilonikdot = gd/mu Q
+// with Q = s' - 2 Gk epsilonik.  eps and epsdot may be the same array (each
+// point reads before it writes), as in the reference's corrector call.
+struct TransArgs {
+    Grid g;
+    const TransLayer *L;
+    const float *dg0;        // weak-zone perturbation or null
+    const float *sig;        // 6 x nh
+    const float *eps;        // 6 x nh
+    float *m;                // 6 x nh, accumulated
+    float *epsdot;           // 6 x nh
+    float muinv;
+    float *tm_part;          // [gridDim.x]
+};
+
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_transient(TransArgs a)
+{
+    __shared__ float shf[32];
+    const Grid &g = a.g;
+    const size_t nh = g.nh;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float tm = 3.0e38f;
+    if (q < nh) {
+        const TransLayer L = a.L[q / g.plane];
+        const float g0 = a.dg0 ? L.g0 + a.dg0[q] : L.g0;
+        if (1.0e-20f > g0) {
+            for (int c = 0; c < 6; c++) a.epsdot[c * nh + q] = 0.f;
+        } else {
+            float s[6], e[6];
+            for (int c = 0; c < 6; c++) { s[c] = a.sig[c * nh + q]; e[c] = a.eps[c * nh + q]; }
+            const float tr3 = (s[0] + s[3] + s[5]) * (1.f / 3.f);
+            const float Q[6] = {(s[0] - tr3) - L.gk2 * e[0], s[1] - L.gk2 * e[1], s[2] - L.gk2 * e[2],
+                                (s[3] - tr3) - L.gk2 * e[3], s[4] - L.gk2 * e[4], (s[5] - tr3) - L.gk2 * e[5]};
+            const float x = tnorm6(Q[0], Q[1], Q[2], Q[3], Q[4], Q[5]) * a.muinv;
+            const float pe = L.power - 1.f;
+            float gd;
+            if (pe == 0.f) gd = g0;
+            else if (pe == 1.f) gd = g0 * x;
+            else if (pe == 2.f) gd = g0 * x * x;
+            else gd = g0 * powf(x, pe);
+            const float rq = gd * a.muinv, gd2 = 2.f * gd;
+            for (int c = 0; c < 6; c++) {
+                a.epsdot[c * nh + q] = rq * Q[c];
+                a.m[c * nh + q] += gd2 * Q[c];
+            }
+            tm = 1.f / gd;
+        }
+    }
+    tm = block_min(tm, shf);
+    if (threadIdx.x == 0) a.tm_part[blockIdx.x] = tm;
+}
+
+// builddgammadot0 (src/viscoelastic3d.f90:320-435): the fluidity perturbation
+// of tapered ductile zones (bricks, spheres, cylinders) at the physical
+// points, one point per thread
+__global__ void k_dgammadot0(Grid g, const relax_weakzone *zones, int nz, double beta, float *out)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int j1 = (int)(q % g.sx1), j2 = (int)((q / g.sx1) % g.sx2), j3 = (int)(q / g.plane);
+    const double x1 = (j1 < g.sx1 / 2 ? j1 : j1 - g.sx1) * g.dx1;
+    const double x2 = (j2 < g.sx2 / 2 ? j2 : j2 - g.sx2) * g.dx2;
+    const double x3 = (double)j3 * g.dx3;
+    double f = 0.0;
+    for (int i = 0; i < nz; i++) {
+        const relax_weakzone &z = zones[i];
+        const double dg = z.dgammadot0, W = z.length, L = z.width, D = z.thickness;
+        const double Wp = W * (1.0 + 2.0 * beta) / 2.0, Lp = L * (1.0 + 2.0 * beta) / 2.0,
+                     Dp = D * (1.0 + 2.0 * beta) / 2.0;
+        const double LM = fmax(Wp, fmax(Lp, Dp));
+        if (fabs(x3 - z.z) > LM || fabs(x1 - z.x) > LM || fabs(x2 - z.y) > LM) continue;
+        const double cs = cos(z.strike), ss = sin(z.strike), cd = cos(z.dip), sd = sin(z.dip);
+        double x2r = cs * z.x - ss * z.y;
+        const double xr = cd * x2r - sd * z.z, yr = ss * z.x + cs * z.y, zr = sd * x2r + cd * z.z;
+        x2r = cs * x1 - ss * x2;
+        const double x1s = cd * x2r - sd * x3, x2s = ss * x1 + cs * x2, x3s = sd * x2r + cd * x3;
+        if (D >= 0 && W >= 0 && L >= 0) {
+            f = f + d_omega((x1s - xr) / D, beta) * d_omega((x2s - yr) / W, beta) * d_omega((x3s - zr) / L, beta) * dg;
+        } else if (D < 0 && W < 0 && L < 0) {
+            const double r = sqrt(((x1s - xr) / D) * ((x1s - xr) / D) + ((x2s - yr) / W) * ((x2s - yr) / W) +
+                                  ((x3s - zr) / L) * ((x3s - zr) / L));
+            f = f + d_omega(r, beta) * dg;
+        } else if (D < 0 && W < 0) {
+            const double rho = sqrt(((x1s - xr) / D) * ((x1s - xr) / D) + ((x2s - yr) / W) * ((x2s - yr) / W));
+            f = f + d_omega(rho, beta) * d_omega((x3s - zr) / L, beta) * dg;
+        } else if (D < 0 && L < 0) {
+            const double rho = sqrt(((x1s - xr) / D) * ((x1s - xr) / D) + ((x3s - zr) / L) * ((x3s - zr) / L));
+            f = f + d_omega(rho, beta) * d_omega((x2s - yr) / W, beta) * dg;
+        } else if (W < 0 && L < 0) {
+            const double rho = sqrt(((x2s - yr) / W) * ((x2s - yr) / W) + ((x3s - zr) / L) * ((x3s - zr) / L));
+            f = f + d_omega(rho, beta) * d_omega((x1s - xr) / D, beta) * dg;
+        }
+    }
+    out[q] = (float)f;
+}
+
 // ------------------------------------------------------------------------
 // 3-D transform, pass 1: R2C along x1.
 //   MODE_DIV: the input is the equivalent body force -div(m) of the moment

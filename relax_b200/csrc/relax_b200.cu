@@ -1757,6 +1757,71 @@ extern "C" int relax_op_viscouseigenstress(double mu, const relax_layer *structu
     return RELAX_OK;
 }
 
+extern "C" int relax_op_transienteigenstress(double mu, const relax_layer *structure, const relax_tensor *sig,
+                                             const relax_tensor *epsilonik, int sx1, int sx2, int sx3h,
+                                             relax_tensor *moment, relax_tensor *epsilonikdot,
+                                             double *maxwelltime, const float *dgammadot0, void *stream)
+{
+    Grid g;
+    TRY(make_grid(g, sx1, sx2, 2 * sx3h, 1.0, 1.0, 1.0));
+    if (!structure || !sig || !epsilonik || !moment || !epsilonikdot) return fail(RELAX_ERR_ARG, "null argument");
+    for (int i = 0; i < sx3h; i++)
+        if (structure[i].stressexponent < 0.999999) return fail(RELAX_ERR_POWER, "invalid power exponent");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc(st);
+    std::vector<TransLayer> tl(sx3h);
+    for (int i = 0; i < sx3h; i++)
+        tl[i] = TransLayer{(float)structure[i].gammadot0, (float)structure[i].stressexponent,
+                           (float)(2.0 * structure[i].Gk), 0.f};
+    float *s, *e, *mo, *ed, *tmp;
+    TransLayer *tld;
+    const int nb = (int)nblocks(g.nh);
+    TRY(sc.get(&s, 6 * g.nh));
+    TRY(sc.get(&e, 6 * g.nh));
+    TRY(sc.get(&mo, 6 * g.nh));
+    TRY(sc.get(&ed, 6 * g.nh));
+    TRY(sc.get(&tld, sx3h));
+    TRY(sc.get(&tmp, (size_t)nb));
+    CK(cudaMemcpyAsync(tld, tl.data(), sx3h * sizeof(TransLayer), cudaMemcpyHostToDevice, st));
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(sig, s, g.nh);
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(epsilonik, e, g.nh);
+    k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(moment, mo, g.nh);
+    TransArgs a{};
+    a.g = g; a.L = tld; a.dg0 = dgammadot0; a.sig = s; a.eps = e; a.m = mo; a.epsdot = ed;
+    a.muinv = (float)(1.0 / mu); a.tm_part = tmp;
+    k_transient<<<nb, RELAX_NTHREADS, 0, st>>>(a);
+    k_soa_to_aos<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(mo, moment, g.nh);
+    k_soa_to_aos<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(ed, epsilonikdot, g.nh);
+    CKL();
+    if (maxwelltime) {
+        std::vector<float> h(nb);
+        CK(cudaMemcpyAsync(h.data(), tmp, nb * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        float tm = (float)*maxwelltime;
+        for (float v : h) tm = std::min(tm, v);
+        *maxwelltime = std::min((double)tm, *maxwelltime);
+    }
+    return RELAX_OK;
+}
+
+extern "C" int relax_op_dgammadot0(const relax_weakzone *zones, int nz, int sx1, int sx2, int sx3h, double dx1,
+                                   double dx2, double dx3, double beta, float *out, void *stream)
+{
+    if (!out || (nz > 0 && !zones) || nz < 0) return fail(RELAX_ERR_ARG, "null argument");
+    if (sx1 < 1 || sx2 < 1 || sx3h < 1) return fail(RELAX_ERR_ARG, "grid");
+    Grid g{};
+    g.sx1 = sx1; g.sx2 = sx2; g.sx3 = 2 * sx3h; g.sx3h = sx3h; g.dx1 = dx1; g.dx2 = dx2; g.dx3 = dx3;
+    g.plane = (size_t)sx1 * sx2; g.nh = g.plane * sx3h;
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc(st);
+    relax_weakzone *zd = nullptr;
+    TRY(sc.get(&zd, (size_t)std::max(nz, 1)));
+    if (nz > 0) CK(cudaMemcpyAsync(zd, zones, nz * sizeof(relax_weakzone), cudaMemcpyHostToDevice, st));
+    k_dgammadot0<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(g, zd, nz, beta, out);
+    CKL();
+    return RELAX_OK;
+}
+
 extern "C" int relax_op_frictioneigenstress(double x, double y, double z, double L, double W, double strike,
                                             double dip, double rake, double beta, const relax_tensor *sig,
                                             double mu, const relax_layer *structure, int sx1, int sx2,

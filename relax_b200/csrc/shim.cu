@@ -29,6 +29,11 @@ struct ShimState {
     float *t[3] = {nullptr, nullptr, nullptr};   // (sx1+2, sx2)
     relax_tensor *sig = nullptr, *mom = nullptr, *tau = nullptr;
     float *work = nullptr;                        // 3 x sx1 sx2 sx3/2 + 3 x sx1 sx2
+    // transient rheology (cuinflags_) and weak-zone fluidity fields
+    // (E_GAMMADOT0_TYPE 1..4: linear, nonlinear, linear / nonlinear transient)
+    bool transient = false;
+    relax_tensor *eps = nullptr, *epsdot = nullptr;
+    float *dg[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t nvec() const { return (size_t)(sx1 + 2) * sx2 * sx3; }
     size_t nhalf() const { return (size_t)(sx1 + 2) * sx2 * (sx3 / 2); }
     size_t ntens() const { return (size_t)sx1 * sx2 * (sx3 / 2); }
@@ -49,6 +54,13 @@ void release()
     if (S.mom) cudaFree(S.mom);
     if (S.tau) cudaFree(S.tau);
     if (S.work) cudaFree(S.work);
+    if (S.eps) cudaFree(S.eps);
+    if (S.epsdot) cudaFree(S.epsdot);
+    for (int k = 0; k < 4; k++) {
+        if (S.dg[k]) cudaFree(S.dg[k]);
+        S.dg[k] = nullptr;
+    }
+    S.eps = S.epsdot = nullptr;
     S.sig = S.mom = S.tau = nullptr;
     S.work = nullptr;
     S.init = false;
@@ -57,7 +69,8 @@ void release()
 relax_tensor *tensor_of(int type)
 {
     // E_TENSOR_TYPE, src/cuinclude.h:121-129
-    return type == 1 ? S.sig : type == 2 ? S.mom : type == 3 ? S.tau : nullptr;
+    return type == 1 ? S.sig : type == 2 ? S.mom : type == 3 ? S.tau : type == 4 ? S.eps
+                                                                   : type == 5 ? S.epsdot : nullptr;
 }
 
 __global__ void k_axpby_vec(float *a, const float *b, size_t n, float c1, float c2)
@@ -101,8 +114,10 @@ void cuinflags_(int *istransient, int *nlwz, int *nnlwz, int *nltwz, int *nnltwz
 {
     (void)nlwz; (void)nnlwz; (void)nltwz; (void)nnltwz; (void)islinear; (void)isnonlinear;
     (void)isltransient; (void)isnltransient;
-    // the transient (Burgers) rheology is not part of this library
-    if (iRet) *iRet = (istransient && *istransient) ? 1 : 0;
+    // the weak-zone fields are allocated by cubuildgammadot_; epsilonik and
+    // epsilonikdot by cuinit_ when the transient rheology is on
+    S.transient = istransient && *istransient;
+    if (iRet) *iRet = 0;
 }
 
 void cuinit_(int sx1, int sx2, int sx3, double dx1, double dx2, double dx3, int *iRet)
@@ -125,6 +140,14 @@ void cuinit_(int sx1, int sx2, int sx3, double dx1, double dx2, double dx3, int 
         ok &= cudaMalloc(&S.mom, S.ntens() * sizeof(relax_tensor)) == cudaSuccess;
         ok &= cudaMalloc(&S.tau, S.ntens() * sizeof(relax_tensor)) == cudaSuccess;
         ok &= cudaMalloc(&S.work, (3 * (size_t)sx1 * sx2 * (sx3 / 2) + 3 * (size_t)sx1 * sx2) * sizeof(float)) == cudaSuccess;
+    }
+    if (ok && S.transient) {
+        ok &= cudaMalloc(&S.eps, S.ntens() * sizeof(relax_tensor)) == cudaSuccess;
+        ok &= cudaMalloc(&S.epsdot, S.ntens() * sizeof(relax_tensor)) == cudaSuccess;
+        if (ok) {
+            cudaMemset(S.eps, 0, S.ntens() * sizeof(relax_tensor));
+            cudaMemset(S.epsdot, 0, S.ntens() * sizeof(relax_tensor));
+        }
     }
     if (ok) {
         cudaMemset(S.sig, 0, S.ntens() * sizeof(relax_tensor));
@@ -199,9 +222,10 @@ void cutensorfieldadd_(int eField, int sx1, int sx2, int sx3h, float c1, float c
 {
     if (!S.init) return;
     // E_TENSOR_FIELD, src/cuinclude.h:100-111
-    relax_tensor *pairs[6][2] = {{nullptr, nullptr}, {S.tau, S.tau}, {S.sig, S.tau},
-                                 {S.mom, S.mom}, {S.sig, S.mom}, {S.tau, S.mom}};
-    if (eField < 1 || eField > 5) return;
+    relax_tensor *pairs[9][2] = {{nullptr, nullptr}, {S.tau, S.tau}, {S.sig, S.tau},
+                                 {S.mom, S.mom}, {S.sig, S.mom}, {S.tau, S.mom},
+                                 {S.eps, S.epsdot}, {S.epsdot, S.eps}, {S.epsdot, S.epsdot}};
+    if (eField < 1 || eField > 8 || !pairs[eField][0] || !pairs[eField][1]) return;
     const size_t n = (size_t)sx1 * sx2 * sx3h;
     k_axpby_tensor<<<nb(n), 256>>>(pairs[eField][0], pairs[eField][1], n, c1, c2);
     cudaDeviceSynchronize();
@@ -244,10 +268,12 @@ void calfftnelasic_(float *c1, float *c2, float *c3, float *t1, float *t2, float
 void cuviscouseigen_(relax_layer *structure, relax_tensor_layer *prestress, double mu, int sx1, int sx2, int sx3h,
                      double dx1, double dx2, double dx3, int bMaxwell, double *tm, int gammadot0type)
 {
-    (void)dx1; (void)dx2; (void)dx3; (void)gammadot0type;
+    (void)dx1; (void)dx2; (void)dx3;
     if (!S.init) return;
+    // E_GAMMADOT0_TYPE_LINEAR / _NONLINEAR: the field of cubuildgammadot_
+    const float *dg = (gammadot0type == 1 || gammadot0type == 2) ? S.dg[gammadot0type - 1] : nullptr;
     relax_op_viscouseigenstress(mu, structure, prestress, S.sig, sx1, sx2, sx3h, S.mom, bMaxwell ? tm : nullptr,
-                                nullptr, nullptr, nullptr);
+                                nullptr, dg, nullptr);
     cudaDeviceSynchronize();
 }
 
@@ -296,6 +322,67 @@ void cusource_(double mu, double s, double x, double y, double z, double L, doub
         k_add_padded<<<nb(g.plane), 256>>>(S.t[k], a.t[k], sx1, (size_t)sx2);
     }
     cudaDeviceSynchronize();
+}
+
+
+// cutransienteigenwrapper_, src/cuelastic.cu:1085-1118: transienteigenstress
+// on epsilonik (E_TENSOR_IK) or epsilonikdot (E_TENSOR_IKDOT, the
+// corrector's in-place call) into epsilonikdot and the moment;
+// E_GAMMADOT0_TYPE 3 / 4 select the transient weak-zone fields
+void cutransienteigenwrapper_(int eType, relax_layer *structure, double mu, int sx1, int sx2, int sx3h,
+                              double dx1, double dx2, double dx3, int bMaxwell, double *dMaxwell, int bgammadot)
+{
+    (void)dx1; (void)dx2; (void)dx3;
+    if (!S.init || !S.eps) return;
+    const relax_tensor *in = eType == 4 ? S.eps : eType == 5 ? S.epsdot : nullptr;
+    if (!in) return;
+    const float *dg = (bgammadot == 3 || bgammadot == 4) ? S.dg[bgammadot - 1] : nullptr;
+    relax_op_transienteigenstress(mu, structure, S.sig, in, sx1, sx2, sx3h, S.mom, S.epsdot,
+                                  bMaxwell ? dMaxwell : nullptr, dg, nullptr);
+    cudaDeviceSynchronize();
+}
+
+// cubuildgammadot_, src/cuelastic.cu:1689-1750: the weak-zone field of one
+// mechanism (beta = 0, as src/relax.f90:487-541 and the reference kernel)
+void cubuildgammadot_(int sx1, int sx2, int sx3h, double dx1, double dx2, double dx3, int nz,
+                      relax_weakzone *zones, int gammadotType)
+{
+    if (!S.init || gammadotType < 1 || gammadotType > 4) return;
+    float *&d = S.dg[gammadotType - 1];
+    const size_t n = (size_t)sx1 * sx2 * sx3h;
+    if (!d && cudaMalloc(&d, n * sizeof(float)) != cudaSuccess) {
+        d = nullptr;
+        return;
+    }
+    relax_op_dgammadot0(zones, nz, sx1, sx2, sx3h, dx1, dx2, dx3, 0.0, d, nullptr);
+    cudaDeviceSynchronize();
+}
+
+// cuexportspatial_, src/cuelastic.cu:1629-1650: one x3-plane of the padded
+// displacement components to the host
+void cuexportspatial_(float *u1, float *u2, float *u3, int i3)
+{
+    if (!S.init || i3 < 0 || i3 >= S.sx3 / 2) return;
+    const size_t off = (size_t)i3 * S.n2();
+    float *h[3] = {u1, u2, u3};
+    for (int k = 0; k < 3; k++)
+        if (h[k]) cudaMemcpy(h[k], S.u[k] + off, S.n2() * sizeof(float), cudaMemcpyDeviceToHost);
+}
+
+// cuexportpoints_, src/cuelastic.cu:1652-1687: displacement and stress at
+// one grid point (0-based indices)
+void cuexportpoints_(double *u1, double *u2, double *u3, ST_TENSOR_C *sig, int i1, int i2, int i3)
+{
+    if (!S.init || i1 < 0 || i1 >= S.sx1 || i2 < 0 || i2 >= S.sx2 || i3 < 0 || i3 >= S.sx3 / 2) return;
+    const size_t iu = ((size_t)i3 * S.sx2 + i2) * (S.sx1 + 2) + i1;
+    const size_t is = ((size_t)i3 * S.sx2 + i2) * S.sx1 + i1;
+    double *h[3] = {u1, u2, u3};
+    for (int k = 0; k < 3; k++) {
+        float v = 0.f;
+        cudaMemcpy(&v, S.u[k] + iu, sizeof(float), cudaMemcpyDeviceToHost);
+        if (h[k]) *h[k] = (double)v;
+    }
+    if (sig) cudaMemcpy(sig, S.sig + is, sizeof(relax_tensor), cudaMemcpyDeviceToHost);
 }
 
 }  // extern "C"

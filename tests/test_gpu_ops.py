@@ -272,3 +272,70 @@ def test_unsupported_grid_is_rejected():
     d = dev(np.zeros((20, 10, 14), np.float32))
     rc = lib.relax_op_fft3(ptr(d), 12, 10, 20, 1.0, 1.0, 1.0, -1, None)   # sx1/2 = 6 ok, sx2=10 no
     assert rc == 4
+
+
+@pytest.mark.parametrize("power", [1.0, 3.0])
+@pytest.mark.parametrize("inplace", [False, True])
+def test_transient_eigenstress_matches_oracle(oracle32, power, inplace):
+    """transienteigenstress, separate and aliased epsilonik / epsilonikdot"""
+    lib = _lib.load()
+    sx1, sx2, sx3 = 64, 32, 32
+    sx3h = sx3 // 2
+    rng = np.random.default_rng(21)
+    sig = tensors_random(rng, (sx3h, sx2, sx1), 0.3)
+    eps = tensors_random(rng, (sx3h, sx2, sx1), 0.05)
+    mom = tensors_random(rng, (sx3h, sx2, sx1), 0.1)
+    epsdot = tensors_random(rng, (sx3h, sx2, sx1), 1.0)
+    dg0 = (0.2 * rng.standard_normal((sx3h, sx2, sx1))).astype(np.float32)
+    st = (relax_layer * sx3h)()
+    for k in range(sx3h):
+        st[k] = relax_layer(z=0, gammadot0=(0.0 if k < 3 else 10 ** rng.uniform(-1, 1)),
+                            stressexponent=power, cohesion=0.0, friction=0, Gk=0.25 + 0.05 * k)
+    mref = mom.copy()
+    eref = eps.copy()
+    dref = eref if inplace else epsdot.copy()
+    rc, tref = oracle32.transienteigenstress(1.0, st, sig, eref, sx1, sx2, sx3h, mref, dref, maxwell=1e7,
+                                             dgammadot0=dg0)
+    assert rc == 0
+    dm = dev(mom.view(np.float32))
+    de = dev(eps.view(np.float32))
+    dd = de if inplace else dev(epsdot.view(np.float32))
+    ddg = dev(dg0)
+    tm = C.c_double(1e7)
+    _lib.check(lib.relax_op_transienteigenstress(
+        1.0, C.cast(st, C.c_void_p), ptr(dev(sig.view(np.float32))), ptr(de), sx1, sx2, sx3h, ptr(dm),
+        ptr(dd), C.byref(tm), ptr(ddg), None))
+    torch.cuda.synchronize()
+    gm = dm.cpu().numpy().view(TENSOR_DTYPE).reshape(mom.shape)
+    gd = dd.cpu().numpy().view(TENSOR_DTYPE).reshape(mom.shape)
+    assert rel_l2(tensor_array(gm), tensor_array(mref)) < 1e-5
+    assert rel_l2(tensor_array(gd), tensor_array(dref)) < 1e-5
+    assert abs(tm.value - tref) <= 1e-5 * tref
+
+
+@pytest.mark.parametrize("beta", [0.0, 0.2])
+def test_weak_zones_match_oracle(oracle32, beta):
+    """builddgammadot0: a rotated brick, a sphere and two cylinders"""
+    from relax_b200.config import relax_weakzone
+    lib = _lib.load()
+    sx1, sx2, sx3h = 64, 48, 24
+    dx = (1.0, 1.0, 0.5)
+    zones = (relax_weakzone * 4)()
+    zones[0] = relax_weakzone(dgammadot0=2.0, x=-5.0, y=3.0, z=4.0, width=6.0, length=10.0, thickness=3.0,
+                              strike=0.4, dip=1.1)
+    zones[1] = relax_weakzone(dgammadot0=1.5, x=10.0, y=-8.0, z=6.0, width=-4.0, length=-4.0, thickness=-4.0,
+                              strike=0.0, dip=0.0)
+    zones[2] = relax_weakzone(dgammadot0=-0.5, x=0.0, y=12.0, z=3.0, width=5.0, length=-3.0, thickness=-3.0,
+                              strike=1.0, dip=0.3)
+    zones[3] = relax_weakzone(dgammadot0=0.7, x=-15.0, y=-15.0, z=8.0, width=-3.5, length=7.0,
+                              thickness=-3.5, strike=-0.6, dip=0.8)
+    ref = oracle32.builddgammadot0(zones, sx1, sx2, sx3h, dx, beta)
+    out = torch.zeros((sx3h, sx2, sx1), dtype=torch.float32, device="cuda")
+    _lib.check(lib.relax_op_dgammadot0(C.cast(zones, C.c_void_p), 4, sx1, sx2, sx3h, *dx, beta, ptr(out), None))
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert np.abs(ref).max() > 0.5
+    # the taper is a step for beta = 0: a rotated coordinate landing on a zone's edge may
+    # round to either side; away from the edges the fields agree to rounding
+    bad = np.abs(got - ref) > 1e-5 * np.abs(ref).max()
+    assert bad.mean() <= (2e-3 if beta == 0.0 else 0.0), bad.mean()
