@@ -548,6 +548,163 @@ int orc_transienteigenstress(double mu, const relax_layer *structure, const oten
 }
 
 /* ------------------------------------------------------------------ */
+/* tensile cracks and dilatation point sources                          */
+/* ------------------------------------------------------------------ */
+
+/* tensilesource, src/elastic3d.f90:2315-2411: equivalent body force of an
+ * opening crack over the whole box (sx3 layers: the image lies in the
+ * lower half), padded (sx1+2, sx2, sx3) arrays */
+void orc_tensilesource(double lambda, double mu, double s, double x, double y, double z, double L,
+                       double W, double strike, double dip, double beta, int sx1, int sx2, int sx3,
+                       double dx1, double dx2, double dx3, real *f1, real *f2, real *f3)
+{
+    const int n1 = sx1 + 2;
+    double cstrike = cos(strike), sstrike = sin(strike), cdip = cos(dip), sdip = sin(dip);
+    double Wp = W * (1.0 + 2.0 * beta) / 2.0, Lp = L * (1.0 + 2.0 * beta) / 2.0;
+    double x2r0 = cstrike * x - sstrike * y;
+    double xr = cdip * x2r0 - sdip * z, yr = sstrike * x + cstrike * y, zr = sdip * x2r0 + cdip * z;
+    double scale1 = -s * (lambda + 2.0 * mu), scale2 = -s * lambda;
+    const double w701 = (double)7.01f;   /* default-real literal */
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3; i3++) {
+        double x1, x2, x3;
+        shiftedcoordinates(1, 1, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &x3);
+        if (fabs(x3 - z) > Lp && fabs(x3 + z) > Lp) continue;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &x3);
+                if (fabs(x1 - x) > Wp || fabs(x2 - y) > Wp) continue;
+                double x2r = cstrike * x1 - sstrike * x2;
+                double x1s = cdip * x2r - sdip * x3, x1i = cdip * x2r + sdip * x3;
+                if (fabs(x1s - xr) > w701 * dx1 && fabs(x1i - xr) > w701 * dx1) continue;
+                double x2s = sstrike * x1 + cstrike * x2;
+                double x3s = sdip * x2r + cdip * x3, x3i = -sdip * x2r + cdip * x3;
+                double temp1 = gauss(x1s - xr, dx1), temp2 = omega((x2s - yr) / W, beta);
+                double temp3 = omega((x3s - zr) / L, beta);
+                double sourc = scale1 * gaussp(x1s - xr, dx1) * temp2 * temp3;
+                double dblcp = scale2 / W * temp1 * omegap((x2s - yr) / W, beta) * temp3;
+                double dipcs = scale2 / L * temp1 * temp2 * omegap((x3s - zr) / L, beta);
+                temp1 = gauss(x1i - xr, dx1);
+                temp3 = omega((x3i + zr) / L, beta);
+                double image = scale1 * gaussp(x1i - xr, dx1) * temp2 * temp3;
+                double cplei = scale2 / W * temp1 * omegap((x2s - yr) / W, beta) * temp3;
+                double dipci = scale2 / L * temp1 * temp2 * omegap((x3i + zr) / L, beta);
+                size_t o = IDX3(i1 - 1, i2 - 1, i3 - 1, n1, sx2);
+                f1[o] = (real)(f1[o] + cstrike * cdip * (sourc + image) + sstrike * (dblcp + cplei) +
+                               cstrike * sdip * (dipcs + dipci));
+                f2[o] = (real)(f2[o] - sstrike * cdip * (sourc + image) + cstrike * (dblcp + cplei) -
+                               sstrike * sdip * (dipcs + dipci));
+                f3[o] = (real)(f3[o] - sdip * (sourc - image) + cdip * (dipcs - dipci));
+            }
+        }
+    }
+}
+
+/* mogisource, src/elastic3d.f90:2458-2509: equivalent body force of a
+ * dilatation point source and its image over the whole box */
+void orc_mogisource(double lambda, double mu, double o, double xs, double ys, double zs, int sx1, int sx2,
+                    int sx3, double dx1, double dx2, double dx3, real *f1, real *f2, real *f3)
+{
+    const int n1 = sx1 + 2;
+    double scale = -(lambda + 2.0 * mu / 3.0) * o;
+    double mx = dx1 > dx2 ? dx1 : dx2;
+    if (dx3 > mx) mx = dx3;
+    double Wp = 6.0 * mx, Lp = 6.0 * mx;
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3; i3++) {
+        double x1, x2, x3;
+        shiftedcoordinates(1, 1, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &x3);
+        if (fabs(x3 - zs) > Lp && fabs(x3 + zs) > Lp) continue;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &x3);
+                if (fabs(x1 - xs) > Wp || fabs(x2 - ys) > Wp) continue;
+                double temp1 = gauss(x1 - xs, dx1), temp2 = gauss(x2 - ys, dx2), temp3 = gauss(x3 - zs, dx3);
+                double source1 = scale * gaussp(x1 - xs, dx1) * temp2 * temp3;
+                double source2 = scale * temp1 * gaussp(x2 - ys, dx2) * temp3;
+                double source3 = scale * temp1 * temp2 * gaussp(x3 - zs, dx3);
+                temp3 = gauss(x3 + zs, dx3);
+                double image1 = scale * gaussp(x1 - xs, dx1) * temp2 * temp3;
+                double image2 = scale * temp1 * gaussp(x2 - ys, dx2) * temp3;
+                double image3 = scale * temp1 * temp2 * gaussp(x3 + zs, dx3);
+                size_t q = IDX3(i1 - 1, i2 - 1, i3 - 1, n1, sx2);
+                f1[q] = (real)(f1[q] + (source1 + image1));
+                f2[q] = (real)(f2[q] + (source2 + image2));
+                f3[q] = (real)(f3[q] + (source3 - image3));
+            }
+        }
+    }
+}
+
+/* momentdensitytensile, src/elastic3d.f90:3137-3215 (physical layers) */
+void orc_momentdensitytensile(double lambda, double mu, double slip, double x, double y, double z, double L,
+                              double W, double strike, double dip, double beta, int sx1, int sx2, int sx3,
+                              double dx1, double dx2, double dx3, otensor *sig)
+{
+    double cstrike = cos(strike), sstrike = sin(strike), cdip = cos(dip), sdip = sin(dip);
+    double Wp = W * (1.0 + 2.0 * beta) / 2.0, Lp = L * (1.0 + 2.0 * beta) / 2.0;
+    double x2r0 = cstrike * x - sstrike * y;
+    double xr = cdip * x2r0 - sdip * z, yr = sstrike * x + cstrike * y, zr = sdip * x2r0 + cdip * z;
+    const double w701 = (double)7.01f;
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3; i3++) {
+        double x3 = (double)(i3 - 1) * dx3;
+        if (fabs(x3 - z) > Lp) continue;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                double x1, x2, dum;
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &dum);
+                if (fabs(x1 - x) > Wp || fabs(x2 - y) > Wp) continue;
+                double x2r = cstrike * x1 - sstrike * x2;
+                double x1s = cdip * x2r - sdip * x3, x1i = cdip * x2r + sdip * x3;
+                if (fabs(x1s - xr) > w701 * dx1 && fabs(x1i - xr) > w701 * dx1) continue;
+                double x2s = sstrike * x1 + cstrike * x2;
+                double x3s = sdip * x2r + cdip * x3, x3i = -sdip * x2r + cdip * x3;
+                double temp1 = gauss(x1s - xr, dx1), temp2 = omega((x2s - yr) / W, beta);
+                double temp3 = omega((x3s - zr) / L, beta);
+                double aperture = temp1 * temp2 * temp3;
+                temp1 = gauss(x1i - xr, dx1);
+                temp3 = omega((x3i + zr) / L, beta);
+                aperture = aperture + temp1 * temp2 * temp3;
+                double n[3] = {+cdip * cstrike * aperture, -cdip * sstrike * aperture, -sdip * aperture};
+                double sn[3] = {slip * n[0], slip * n[1], slip * n[2]};
+                otensor Ei = sdyad(n, sn);
+                isotropic(&Ei, lambda, mu);
+                size_t o = IDX3(i1 - 1, i2 - 1, i3 - 1, sx1, sx2);
+                sig[o] = tplus(sig[o], Ei);
+            }
+        }
+    }
+}
+
+/* momentdensitymogi, src/elastic3d.f90:3240-3286 (physical layers) */
+void orc_momentdensitymogi(double lambda, double mu, double o, double xs, double ys, double zs, int sx1,
+                           int sx2, int sx3, double dx1, double dx2, double dx3, otensor *sig)
+{
+    double kappa = lambda + 2.0 / 3.0 * mu;
+    double mx = dx1 > dx2 ? dx1 : dx2;
+    if (dx3 > mx) mx = dx3;
+    double Wp = 6.0 * mx, Lp = 6.0 * mx;
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3; i3++) {
+        double x3 = (double)(i3 - 1) * dx3;
+        if (fabs(x3 - zs) > Lp) continue;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                double x1, x2, dum;
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &dum);
+                if (fabs(x1 - xs) > Wp || fabs(x2 - ys) > Wp) continue;
+                double gamma = o * gauss(x1 - xs, dx1) * gauss(x2 - ys, dx2) * gauss(x3 - zs, dx3);
+                gamma = kappa * gamma;
+                otensor m = {(real)gamma, 0, 0, (real)gamma, 0, (real)gamma};
+                size_t q = IDX3(i1 - 1, i2 - 1, i3 - 1, sx1, sx2);
+                sig[q] = tplus(sig[q], m);
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* builddgammadot0 / fdgammadot0, src/viscoelastic3d.f90:320-435        */
 /* ------------------------------------------------------------------ */
 void orc_builddgammadot0(int sx1, int sx2, int sx3, double dx1, double dx2, double dx3, double beta,
@@ -1338,7 +1495,6 @@ static int orc_dislocations(orc_state *S, const relax_event *ev)
     const relax_config *c = &S->cfg;
     double mind = c->dx1 < c->dx2 ? c->dx1 : c->dx2;
     if (c->dx3 < mind) mind = c->dx3;
-    if (ev->nt || ev->nm) return ORC_ERR_UNSUPPORTED;
     for (int i = 0; i < ev->ns; i++) {
         const relax_source *s = &ev->s[i];
         if (c->nyquist * mind < s->length || c->nyquist * mind < s->width)
@@ -1351,6 +1507,32 @@ static int orc_dislocations(orc_state *S, const relax_event *ev)
         orc_momentdensityshear(c->mu, s->slip, s->x, s->y, s->z, s->width, s->length, s->strike,
                                s->dip, s->rake, s->beta, S->sx1, S->sx2, S->sx3h, c->dx1, c->dx2,
                                c->dx3, S->tau);
+    }
+    /* tensile cracks (src/relax.f90:1226-1260): L = width, W = length, the
+     * global beta, the crack's opening */
+    for (int i = 0; i < ev->nt; i++) {
+        const relax_source *s = &ev->ts[i];
+        if (c->nyquist * mind < s->length || c->nyquist * mind < s->width)
+            orc_tensilesource(c->lambda, c->mu, s->opening, s->x, s->y, s->z, s->width, s->length,
+                              s->strike, s->dip, c->beta, S->sx1, S->sx2, S->sx3, c->dx1, c->dx2, c->dx3,
+                              S->v[0], S->v[1], S->v[2]);
+    }
+    for (int i = 0; i < ev->nt; i++) {
+        const relax_source *s = &ev->ts[i];
+        orc_momentdensitytensile(c->lambda, c->mu, s->opening, s->x, s->y, s->z, s->width, s->length,
+                                 s->strike, s->dip, c->beta, S->sx1, S->sx2, S->sx3h, c->dx1, c->dx2,
+                                 c->dx3, S->tau);
+    }
+    /* dilatation point sources (src/relax.f90:1262-1287): amplitude in slip */
+    for (int i = 0; i < ev->nm; i++) {
+        const relax_source *s = &ev->m[i];
+        orc_mogisource(c->lambda, c->mu, s->slip, s->x, s->y, s->z, S->sx1, S->sx2, S->sx3, c->dx1, c->dx2,
+                       c->dx3, S->v[0], S->v[1], S->v[2]);
+    }
+    for (int i = 0; i < ev->nm; i++) {
+        const relax_source *s = &ev->m[i];
+        orc_momentdensitymogi(c->lambda, c->mu, s->slip, s->x, s->y, s->z, S->sx1, S->sx2, S->sx3h, c->dx1,
+                              c->dx2, c->dx3, S->tau);
     }
     return ORC_OK;
 }
@@ -1587,6 +1769,8 @@ int orc_step(orc_state *S, const double *dt_override, relax_step_log *log)
         orc_tensorfieldadd(S->eps, S->epsdot, S->nt, 0, 0, 1, (real)Dt);
         orc_tensorfieldadd(S->epsdot, S->epsdot, S->nt, 1, 0, 1, 0);
     }
+    /* interseismic loading, src/relax.f90:796-800: dislocations(..., eigenstress=moment)
+     * adds the moment densities to the moment and to tau */
     if (c->inter.ns > 0) {
         for (int i = 0; i < c->inter.ns; i++) {
             const relax_source *s = &c->inter.s[i];
@@ -1597,6 +1781,18 @@ int orc_step(orc_state *S, const double *dt_override, relax_step_log *log)
                                    s->strike, s->dip, s->rake, s->beta, S->sx1, S->sx2, S->sx3h,
                                    c->dx1, c->dx2, c->dx3, S->tau);
         }
+    }
+    for (int i = 0; i < c->inter.nt; i++) {
+        const relax_source *s = &c->inter.ts[i];
+        orc_momentdensitytensile(c->lambda, c->mu, s->opening, s->x, s->y, s->z, s->width, s->length,
+                                 s->strike, s->dip, c->beta, S->sx1, S->sx2, S->sx3h, c->dx1, c->dx2,
+                                 c->dx3, S->moment);
+    }
+    for (int i = 0; i < c->inter.nt; i++) {
+        const relax_source *s = &c->inter.ts[i];
+        orc_momentdensitytensile(c->lambda, c->mu, s->opening, s->x, s->y, s->z, s->width, s->length,
+                                 s->strike, s->dip, c->beta, S->sx1, S->sx2, S->sx3h, c->dx1, c->dx2,
+                                 c->dx3, S->tau);
     }
     zero_vt(S);
     orc_equivalentbodyforce(S->moment, c->dx1, c->dx2, c->dx3, S->sx1, S->sx2, S->sx3h, S->v[0],

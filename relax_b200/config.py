@@ -127,6 +127,19 @@ def wang_convention(slip, x, y, z, length, width, strike, dip, rake, x0=0.0, y0=
     return slip, x, y, z, strike, dip, rake
 
 
+def antialiasing_filter(slip, length, width, dx1, dx2, dx3, nyquist):
+    """antialiasingfilter, src/input.f90:1836-1856: segments smaller than
+    nyquist * min(dx) are widened with their slip scaled down."""
+    dx = min(dx1, dx2, dx3) * nyquist
+    if length < dx:
+        slip = slip * length / dx
+        length = dx
+    if width < dx:
+        slip = slip * width / dx
+        width = dx
+    return slip, length, width
+
+
 def fix(number: float) -> int:
     """fix, src/elastic3d.f90:69-80 (round half down)."""
     f, c = math.floor(number), math.ceil(number)
@@ -162,9 +175,33 @@ class Plane:
 
 
 @dataclass
+class Tensile:
+    """An opening crack in input-file convention (src/input.f90:1389-1440)."""
+    opening: float
+    x: float
+    y: float
+    z: float
+    length: float
+    width: float
+    strike: float
+    dip: float
+
+
+@dataclass
+class Point:
+    """A dilatation (Mogi) point source (src/input.f90:1460-1484)."""
+    amplitude: float
+    x: float
+    y: float
+    z: float
+
+
+@dataclass
 class Event:
     time: float
     faults: List[Fault] = field(default_factory=list)
+    tensile: List[Tensile] = field(default_factory=list)
+    points: List[Point] = field(default_factory=list)
 
 
 @dataclass
@@ -198,6 +235,9 @@ class Simulation:
     nltransient: List[Tuple[float, ...]] = field(default_factory=list)
     planes: List[Plane] = field(default_factory=list)
     events: List[Event] = field(default_factory=list)
+    # interseismic loading rates (src/input.f90:1107-1240): shear (faults)
+    # and tensile segments; the time is not used
+    inter: Optional[Event] = None
     name: str = "relax"
 
     @property
@@ -284,9 +324,59 @@ class Simulation:
                 keep.append(sarr)
                 earr[e].ns = len(ev.faults)
                 earr[e].s = C.cast(sarr, C.POINTER(relax_source))
+            if ev.tensile:
+                tarr = (relax_source * len(ev.tensile))()
+                for k, t in enumerate(ev.tensile):
+                    # slip = opening goes through wangconvention; the opening stays
+                    slip, x, y, z, strike, dip, _ = wang_convention(
+                        t.opening, t.x, t.y, t.z, t.length, t.width, t.strike, t.dip, 0.0,
+                        self.x0, self.y0, self.rot)
+                    tarr[k] = relax_source(slip=slip, x=x, y=y, z=z, width=t.width, length=t.length,
+                                           strike=strike, dip=dip, rake=0.0, period=0.0, phase=0.0,
+                                           beta=self.beta, opening=t.opening)
+                keep.append(tarr)
+                earr[e].nt = len(ev.tensile)
+                earr[e].ts = C.cast(tarr, C.POINTER(relax_source))
+            if ev.points:
+                marr = (relax_source * len(ev.points))()
+                for k, m in enumerate(ev.points):
+                    # rotation only (src/input.f90:1481)
+                    a = self.rot * DEG2RAD
+                    x = m.x * math.cos(a) + m.y * math.sin(a)
+                    y = -m.x * math.sin(a) + m.y * math.cos(a)
+                    marr[k] = relax_source(slip=m.amplitude, x=x, y=y, z=m.z, beta=self.beta)
+                keep.append(marr)
+                earr[e].nm = len(ev.points)
+                earr[e].m = C.cast(marr, C.POINTER(relax_source))
         keep.append(earr)
         cfg.ne = len(self.events)
         cfg.events = C.cast(earr, C.POINTER(relax_event))
+        if self.inter is not None:
+            d = (self.dx1, self.dx2, self.dx3, self.nyquist)
+            if self.inter.faults:
+                sarr = (relax_source * len(self.inter.faults))()
+                for k, f in enumerate(self.inter.faults):
+                    slip, length, width = antialiasing_filter(f.slip, f.length, f.width, *d)
+                    slip, x, y, z, strike, dip, rake = wang_convention(
+                        slip, f.x, f.y, f.z, length, width, f.strike, f.dip, f.rake, self.x0, self.y0, self.rot)
+                    sarr[k] = relax_source(slip=slip, x=x, y=y, z=z, width=width, length=length, strike=strike,
+                                           dip=dip, rake=rake, beta=self.beta if f.beta is None else f.beta)
+                keep.append(sarr)
+                cfg.inter.ns = len(self.inter.faults)
+                cfg.inter.s = C.cast(sarr, C.POINTER(relax_source))
+            if self.inter.tensile:
+                tarr = (relax_source * len(self.inter.tensile))()
+                for k, t in enumerate(self.inter.tensile):
+                    # the filter acts on slip = 0 (src/input.f90:1205, :1233-1235): only the
+                    # dimensions change; the opening rate stays
+                    _, length, width = antialiasing_filter(0.0, t.length, t.width, *d)
+                    slip, x, y, z, strike, dip, _ = wang_convention(
+                        0.0, t.x, t.y, t.z, length, width, t.strike, t.dip, 0.0, self.x0, self.y0, self.rot)
+                    tarr[k] = relax_source(slip=slip, x=x, y=y, z=z, width=width, length=length,
+                                           strike=strike, dip=dip, beta=self.beta, opening=t.opening)
+                keep.append(tarr)
+                cfg.inter.nt = len(self.inter.tensile)
+                cfg.inter.ts = C.cast(tarr, C.POINTER(relax_source))
         return cfg, keep
 
     # field sizes in the reference layout

@@ -1972,7 +1972,8 @@ __global__ void k_reduce_amp(StepState *st, const double *amp_part, int n, const
 struct SrcArgs {
     Grid g;
     double mu, s, x, y, z, L, W, strike, dip, rake, beta;
-    float *f[3];             // body force (3 x nh, physical layers)
+    double lambda;           // tensile and point sources
+    float *f[3];             // body force (3 x nh, physical layers; whole box: 3 x 2 nh)
     float *t[3];             // traction (3 x plane)
     float *tau;              // 6 x nh (momentdensityshear)
 };
@@ -2094,6 +2095,141 @@ __global__ void k_moment_shear(SrcArgs a)
                         (float)((n[0] * s[2] + n[2] * s[0]) / 2.0), (float)(n[1] * s[1]),
                         (float)((n[1] * s[2] + n[2] * s[1]) / 2.0), (float)(n[2] * s[2])};
     for (int c = 0; c < 6; c++) a.tau[c * g.nh + q] += rmu * e[c];
+}
+
+// tensilesource (src/elastic3d.f90:2315-2411): equivalent body force of an
+// opening crack (a.s = opening) over the whole box, sx3 layers (x3 < 0
+// holds the image), f[k] of sx1 sx2 sx3 floats each
+__global__ void k_source_tensile(SrcArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 2 * g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = (i3 < g.sx3 / 2 ? i3 : i3 - g.sx3) * g.dx3;
+    const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+    if (fabs(x3 - a.z) > Lp && fabs(x3 + a.z) > Lp) return;
+    if (fabs(x1 - a.x) > Wp || fabs(x2 - a.y) > Wp) return;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double x2r0 = cs * a.x - ss * a.y;
+    const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+    const double scale1 = -a.s * (a.lambda + 2.0 * a.mu), scale2 = -a.s * a.lambda;
+    const double x2r = cs * x1 - ss * x2;
+    const double x1s = cd * x2r - sd * x3, x1i = cd * x2r + sd * x3;
+    const double w701 = (double)7.01f;   // default-real literal
+    if (fabs(x1s - xr) > w701 * g.dx1 && fabs(x1i - xr) > w701 * g.dx1) return;
+    const double x2s = ss * x1 + cs * x2;
+    const double x3s = sd * x2r + cd * x3, x3i = -sd * x2r + cd * x3;
+    double temp1 = d_gauss(x1s - xr, g.dx1), temp2 = d_omega((x2s - yr) / a.W, a.beta);
+    double temp3 = d_omega((x3s - zr) / a.L, a.beta);
+    const double sourc = scale1 * d_gaussp(x1s - xr, g.dx1) * temp2 * temp3;
+    const double dblcp = scale2 / a.W * temp1 * d_omegap((x2s - yr) / a.W, a.beta) * temp3;
+    const double dipcs = scale2 / a.L * temp1 * temp2 * d_omegap((x3s - zr) / a.L, a.beta);
+    temp1 = d_gauss(x1i - xr, g.dx1);
+    temp3 = d_omega((x3i + zr) / a.L, a.beta);
+    const double image = scale1 * d_gaussp(x1i - xr, g.dx1) * temp2 * temp3;
+    const double cplei = scale2 / a.W * temp1 * d_omegap((x2s - yr) / a.W, a.beta) * temp3;
+    const double dipci = scale2 / a.L * temp1 * temp2 * d_omegap((x3i + zr) / a.L, a.beta);
+    a.f[0][q] = (float)(a.f[0][q] + cs * cd * (sourc + image) + ss * (dblcp + cplei) + cs * sd * (dipcs + dipci));
+    a.f[1][q] = (float)(a.f[1][q] - ss * cd * (sourc + image) + cs * (dblcp + cplei) - ss * sd * (dipcs + dipci));
+    a.f[2][q] = (float)(a.f[2][q] - sd * (sourc - image) + cd * (dipcs - dipci));
+}
+
+// mogisource (src/elastic3d.f90:2458-2509): a dilatation point source of
+// amplitude a.s and its image over the whole box
+__global__ void k_source_mogi(SrcArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 2 * g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = (i3 < g.sx3 / 2 ? i3 : i3 - g.sx3) * g.dx3;
+    const double W6 = 6.0 * fmax(g.dx1, fmax(g.dx2, g.dx3));
+    if (fabs(x3 - a.z) > W6 && fabs(x3 + a.z) > W6) return;
+    if (fabs(x1 - a.x) > W6 || fabs(x2 - a.y) > W6) return;
+    const double scale = -(a.lambda + 2.0 * a.mu / 3.0) * a.s;
+    const double temp1 = d_gauss(x1 - a.x, g.dx1), temp2 = d_gauss(x2 - a.y, g.dx2);
+    double temp3 = d_gauss(x3 - a.z, g.dx3);
+    const double source1 = scale * d_gaussp(x1 - a.x, g.dx1) * temp2 * temp3;
+    const double source2 = scale * temp1 * d_gaussp(x2 - a.y, g.dx2) * temp3;
+    const double source3 = scale * temp1 * temp2 * d_gaussp(x3 - a.z, g.dx3);
+    temp3 = d_gauss(x3 + a.z, g.dx3);
+    const double image1 = scale * d_gaussp(x1 - a.x, g.dx1) * temp2 * temp3;
+    const double image2 = scale * temp1 * d_gaussp(x2 - a.y, g.dx2) * temp3;
+    const double image3 = scale * temp1 * temp2 * d_gaussp(x3 + a.z, g.dx3);
+    a.f[0][q] = (float)(a.f[0][q] + (source1 + image1));
+    a.f[1][q] = (float)(a.f[1][q] + (source2 + image2));
+    a.f[2][q] = (float)(a.f[2][q] + (source3 - image3));
+}
+
+// momentdensitytensile (src/elastic3d.f90:3137-3215): isotropic Hooke's law
+// of the crack's eigenstrain n (x) (opening n), added to a.tau (6 x nh)
+__global__ void k_moment_tensile(SrcArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = i3 * g.dx3;
+    const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0;
+    if (fabs(x3 - a.z) > Lp) return;
+    if (fabs(x1 - a.x) > Wp || fabs(x2 - a.y) > Wp) return;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double x2r0 = cs * a.x - ss * a.y;
+    const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+    const double x2r = cs * x1 - ss * x2;
+    const double x1s = cd * x2r - sd * x3, x1i = cd * x2r + sd * x3;
+    const double w701 = (double)7.01f;
+    if (fabs(x1s - xr) > w701 * g.dx1 && fabs(x1i - xr) > w701 * g.dx1) return;
+    const double x2s = ss * x1 + cs * x2;
+    const double x3s = sd * x2r + cd * x3, x3i = -sd * x2r + cd * x3;
+    double temp1 = d_gauss(x1s - xr, g.dx1), temp2 = d_omega((x2s - yr) / a.W, a.beta);
+    double temp3 = d_omega((x3s - zr) / a.L, a.beta);
+    double ap = temp1 * temp2 * temp3;
+    temp1 = d_gauss(x1i - xr, g.dx1);
+    temp3 = d_omega((x3i + zr) / a.L, a.beta);
+    ap = ap + temp1 * temp2 * temp3;
+    const double n[3] = {cd * cs * ap, -cd * ss * ap, -sd * ap};
+    const double s[3] = {a.s * n[0], a.s * n[1], a.s * n[2]};
+    float e[6] = {(float)(n[0] * s[0]), (float)((n[0] * s[1] + n[1] * s[0]) / 2.0),
+                  (float)((n[0] * s[2] + n[2] * s[0]) / 2.0), (float)(n[1] * s[1]),
+                  (float)((n[1] * s[2] + n[2] * s[1]) / 2.0), (float)(n[2] * s[2])};
+    // isotropicstressstrain, src/elastic3d.f90:129-142
+    const double epskk = (double)(e[0] + e[3] + e[5]);
+    const float mu2 = (float)(2.0 * a.mu);
+    for (int c = 0; c < 6; c++) e[c] = mu2 * e[c];
+    e[0] = (float)(e[0] + a.lambda * epskk);
+    e[3] = (float)(e[3] + a.lambda * epskk);
+    e[5] = (float)(e[5] + a.lambda * epskk);
+    for (int c = 0; c < 6; c++) a.tau[c * g.nh + q] += e[c];
+}
+
+// momentdensitymogi (src/elastic3d.f90:3240-3286): kappa o delta_ij at the
+// point source, added to a.tau (6 x nh)
+__global__ void k_moment_mogi(SrcArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = i3 * g.dx3;
+    const double W6 = 6.0 * fmax(g.dx1, fmax(g.dx2, g.dx3));
+    if (fabs(x3 - a.z) > W6) return;
+    if (fabs(x1 - a.x) > W6 || fabs(x2 - a.y) > W6) return;
+    const double kappa = a.lambda + 2.0 / 3.0 * a.mu;
+    const float gm = (float)(kappa * (a.s * d_gauss(x1 - a.x, g.dx1) * d_gauss(x2 - a.y, g.dx2) *
+                                      d_gauss(x3 - a.z, g.dx3)));
+    a.tau[0 * g.nh + q] += gm;
+    a.tau[3 * g.nh + q] += gm;
+    a.tau[5 * g.nh + q] += gm;
 }
 
 // ------------------------------------------------------------------------

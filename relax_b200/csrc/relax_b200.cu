@@ -777,11 +777,7 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
         if (e.nl > 0 && e.l) o.l.assign(e.l, e.l + e.nl);
     };
     c->events.resize(cfg->ne);
-    for (int k = 0; k < cfg->ne; k++) {
-        copye(cfg->events[k], c->events[k]);
-        if (!c->events[k].ts.empty() || !c->events[k].m.empty())
-            return fail(RELAX_ERR_UNSUPPORTED, "tensile and dilatation sources are not supported");
-    }
+    for (int k = 0; k < cfg->ne; k++) copye(cfg->events[k], c->events[k]);
     copye(cfg->inter, c->inter);
     for (const auto *v : {&c->lin, &c->non, &c->lt, &c->nlt})
         for (const auto &l : *v)
@@ -800,7 +796,7 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     TRY(dalloc(&c->u, 3 * nh));
     TRY(dalloc(&c->vp, 3 * nh));
     TRY(dalloc(&c->gamma, nh));
-    TRY(dalloc(&c->work, 3 * nh));
+    TRY(dalloc(&c->work, 6 * nh));   // coseismic body force over the whole box (3 x sx3 layers)
     TRY(dalloc(&c->twork, 3 * g.plane));
     TRY(dalloc(&c->tload, g.plane));
     CK(cudaMemsetAsync(c->m, 0, 6 * nh * sizeof(float), c->st));
@@ -1059,18 +1055,29 @@ static int upload_loads(relax_ctx *c, const EventCopy &ev, double t, double Dt, 
 
 // shear sources of one event: body force + traction into work/twork, and
 // the relaxed moment density into tau (dislocations, src/relax.f90:1116-1289)
-static int event_sources(relax_ctx *c, const EventCopy &ev, bool *any)
+// dislocations, src/relax.f90:1116-1289: body forces of the event's
+// shear, tensile and point sources into c->work (3 components of the whole
+// box, sx1 sx2 sx3 each; shear sources only touch the physical layers,
+// tensile and point sources also their images below the surface), the
+// surface traction into c->twork, and the moment densities into tau.
+// *full: the lower half of the box is non-zero.
+static int event_sources(relax_ctx *c, const EventCopy &ev, bool *any, bool *full)
 {
     const Grid &g = c->g;
-    CK(cudaMemsetAsync(c->work, 0, 3 * g.nh * sizeof(float), c->st));
+    const size_t nb = 2 * g.nh;            // one component of the whole box
+    CK(cudaMemsetAsync(c->work, 0, 3 * nb * sizeof(float), c->st));
     CK(cudaMemsetAsync(c->twork, 0, 3 * g.plane * sizeof(float), c->st));
     const double mind = std::min(std::min(g.dx1, g.dx2), g.dx3);
-    for (const auto &s : ev.s) {
+    auto args = [&](const relax_source &s) {
         SrcArgs a{};
-        a.g = g; a.mu = c->cfg.mu; a.s = s.slip; a.x = s.x; a.y = s.y; a.z = s.z;
+        a.g = g; a.mu = c->cfg.mu; a.lambda = c->cfg.lambda; a.s = s.slip; a.x = s.x; a.y = s.y; a.z = s.z;
         a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.rake = s.rake; a.beta = s.beta;
-        for (int k = 0; k < 3; k++) { a.f[k] = c->work + k * g.nh; a.t[k] = c->twork + k * g.plane; }
+        for (int k = 0; k < 3; k++) { a.f[k] = c->work + k * nb; a.t[k] = c->twork + k * g.plane; }
         a.tau = c->tau;
+        return a;
+    };
+    for (const auto &s : ev.s) {
+        SrcArgs a = args(s);
         if (c->cfg.nyquist * mind < s.length || c->cfg.nyquist * mind < s.width) {
             k_source_traction<<<nblocks(g.plane), RELAX_NTHREADS, 0, c->st>>>(a);
             CKL();
@@ -1079,30 +1086,55 @@ static int event_sources(relax_ctx *c, const EventCopy &ev, bool *any)
         }
     }
     for (const auto &s : ev.s) {
-        SrcArgs a{};
-        a.g = g; a.mu = c->cfg.mu; a.s = s.slip; a.x = s.x; a.y = s.y; a.z = s.z;
-        a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.rake = s.rake; a.beta = s.beta;
-        a.tau = c->tau;
+        SrcArgs a = args(s);
         k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
         CKL();
     }
-    *any = !ev.s.empty() || !ev.l.empty();
+    // tensile cracks: the opening, the global beta (src/relax.f90:1226-1260)
+    for (const auto &s : ev.ts) {
+        SrcArgs a = args(s);
+        a.s = s.opening; a.beta = c->cfg.beta;
+        if (c->cfg.nyquist * mind < s.length || c->cfg.nyquist * mind < s.width) {
+            k_source_tensile<<<nblocks(nb), RELAX_NTHREADS, 0, c->st>>>(a);
+            CKL();
+        }
+    }
+    for (const auto &s : ev.ts) {
+        SrcArgs a = args(s);
+        a.s = s.opening; a.beta = c->cfg.beta;
+        k_moment_tensile<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
+    }
+    // dilatation point sources (src/relax.f90:1262-1287)
+    for (const auto &s : ev.m) {
+        SrcArgs a = args(s);
+        k_source_mogi<<<nblocks(nb), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
+    }
+    for (const auto &s : ev.m) {
+        SrcArgs a = args(s);
+        k_moment_mogi<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
+    }
+    *any = !ev.s.empty() || !ev.ts.empty() || !ev.m.empty() || !ev.l.empty();
+    *full = !ev.ts.empty() || !ev.m.empty();
     return RELAX_OK;
 }
 
-// coseismic Green's function of work/twork; u += result
-static int event_green(relax_ctx *c, bool loads)
+// the coseismic Green's function of c->work (the whole box when `full`,
+// else its physical half), u += the displacement
+static int event_green(relax_ctx *c, bool loads, bool full)
 {
     const Grid &g = c->g;
     XfArgs xa{};
     for (int k = 0; k < 3; k++) {
-        xa.in[k] = c->work + k * g.nh;
+        xa.in[k] = c->work + k * 2 * g.nh;
         xa.tin[k] = c->twork + k * g.plane;
     }
     xa.rp = g.sx1; xa.pp = g.plane; xa.trp = g.sx1;
     xa.tload = loads ? c->tload : nullptr;
     XiArgs xi = xi_update(c, c->u, c->u, 1.0f, false);
-    return c->sp.green(xa, false, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st);
+    return c->sp.green(xa, false, full ? g.sx3 : g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st);
 }
 
 // strike/dip/rake trigonometry and the rotated plane centre of
@@ -1315,10 +1347,10 @@ extern "C" int relax_coseismic(relax_ctx *c, int e, relax_step_log *log0)
     if (!c) return fail(RELAX_ERR_ARG, "null context");
     if (e < 0 || e >= (int)c->events.size()) return fail(RELAX_ERR_ARG, "event %d out of range", e);
     CK(cudaSetDevice(c->device));
-    bool any = false, loads = false;
-    TRY(event_sources(c, c->events[e], &any));
+    bool any = false, loads = false, full = false;
+    TRY(event_sources(c, c->events[e], &any, &full));
     TRY(upload_loads(c, c->events[e], c->t, 0.0, false, &loads));
-    if (any) TRY(event_green(c, loads));
+    if (any) TRY(event_green(c, loads, full));
     TRY(tail_init(c));
     CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -1368,10 +1400,10 @@ static int finish_step(relax_ctx *c, relax_step_log *log)
         k_tau_update<<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(g, c->tau, c->m, c->dst, c->amp_alt);
         CKL();
         c->e++;
-        bool any = false, ld = false;
-        TRY(event_sources(c, c->events[c->e], &any));
+        bool any = false, ld = false, full = false;
+        TRY(event_sources(c, c->events[c->e], &any, &full));
         TRY(upload_loads(c, c->events[c->e], c->t, 0.0, false, &ld));
-        TRY(event_green(c, ld));
+        TRY(event_green(c, ld, full));
         TRY(launch_stress<MODE_INIT>(c, stress_args(c, c->u)));
         k_reduce_amp<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->amp_part, c->nblk, c->amp_alt,
                                                         g.dx1 * g.dx2 * g.dx3);
@@ -1457,10 +1489,21 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
             a.tau = c->m;
             k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
             CKL();
-            a.tau = c->tau;   // src/relax.f90:1228-1235 also adds it to tau
+            a.tau = c->tau;   // src/relax.f90:1199-1206 also adds it to tau
             k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
             CKL();
         }
+    }
+    // interseismic tensile segments (src/relax.f90:1242-1260), opening rates
+    for (const auto &s : c->inter.ts) {
+        SrcArgs a{};
+        a.g = g; a.mu = c->cfg.mu; a.lambda = c->cfg.lambda; a.s = s.opening; a.x = s.x; a.y = s.y; a.z = s.z;
+        a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.beta = c->cfg.beta;
+        a.tau = c->m;
+        k_moment_tensile<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        a.tau = c->tau;
+        k_moment_tensile<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
     }
     TRY(upload_loads(c, ev, c->t, Dt, true, &loads));
     {
@@ -2419,8 +2462,18 @@ extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
             a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.rake = s.rake; a.beta = s.beta;
             a.tau = c->m;
             k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(a);
-            a.tau = c->tau;   // src/relax.f90:1228-1235 also adds it to tau
+            a.tau = c->tau;   // src/relax.f90:1199-1206 also adds it to tau
             k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(a);
+            b->launches += 2;
+        }
+        for (const auto &s : c->inter.ts) {
+            SrcArgs a{};
+            a.g = g; a.mu = c->cfg.mu; a.lambda = c->cfg.lambda; a.s = s.opening; a.x = s.x; a.y = s.y;
+            a.z = s.z; a.L = s.width; a.W = s.length; a.strike = s.strike; a.dip = s.dip; a.beta = c->cfg.beta;
+            a.tau = c->m;
+            k_moment_tensile<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(a);
+            a.tau = c->tau;
+            k_moment_tensile<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(a);
             b->launches += 2;
         }
     }

@@ -77,3 +77,18 @@ def transient_small(linear=True, nonlinear=False, viscous=False, sx=64, sz=32):
     if nonlinear:
         s.nltransient = [(6.0, 2.0, 3.0, 1.0)]
     return s
+
+
+def sources_small(sx=64, sz=32, interseismic=False):
+    """Linear Maxwell below 6 km with a coseismic tensile crack and a
+    dilatation point source (their images lie in the lower half of the box),
+    optionally interseismic shear and tensile loading."""
+    from relax_b200.config import Point, Tensile
+    s = linear_small(sx, sz, steps=4)
+    s.name = "sources-small"
+    s.events[0].tensile = [Tensile(0.5, 6.0, -4.0, 2.0, 12.0, 6.0, 20.0, 60.0)]
+    s.events[0].points = [Point(0.8, -8.0, 6.0, 5.0)]
+    if interseismic:
+        s.inter = Event(0.0, [Fault(0.1, -15.0, 10.0, 8.0, 10.0, 4.0, 0.0, 30.0, 90.0)],
+                        tensile=[Tensile(0.05, 10.0, 10.0, 6.0, 1.0, 5.0, 0.0, 90.0)])
+    return s
