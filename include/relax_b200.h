@@ -140,22 +140,25 @@ typedef struct relax_config {
 /* One line of RELAX's step log (src/relax.f90:1027-1047, format 1100):
  * I, Dt, tm(ve), tm(pl), tm(as), t, power, C:E^i; with the transient
  * rheology (formats 1102/1103) also the Maxwell times of the linear and
- * nonlinear transient mechanisms. */
+ * nonlinear transient mechanisms.  `output` is isoutput of the step
+ * (src/relax.f90:907): the reference then prints format 1101/1103 ("*")
+ * and writes its output files. */
 typedef struct relax_step_log {
     int i;
     int event;         /* 1 when a coseismic event fired after the step */
     double dt, tm_ve, tm_pl, tm_as, t, power, cei;
     double tm_tl, tm_tnl;
+    int output;
 } relax_step_log;
 
-/* field selectors for relax_get_field / relax_set_field */
+/* field selectors for relax_get_field / relax_set_field / relax_get_plane */
 #define RELAX_FIELD_U       1   /* 3 x float (sx1+2, sx2, sx3/2)         */
 #define RELAX_FIELD_SIG     2   /* relax_tensor (sx1, sx2, sx3/2)        */
 #define RELAX_FIELD_TAU     3   /* relax_tensor (sx1, sx2, sx3/2)        */
 #define RELAX_FIELD_MOMENT  4   /* relax_tensor (sx1, sx2, sx3/2)        */
 #define RELAX_FIELD_GAMMA   5   /* float (sx1+2, sx2, sx3/2)             */
-#define RELAX_FIELD_V       6   /* 3 x float (sx1+2, sx2, sx3) work field */
-#define RELAX_FIELD_T       7   /* 3 x float (sx1+2, sx2) surface traction */
+#define RELAX_FIELD_EPS     6   /* relax_tensor (sx1, sx2, sx3/2): the
+                                   transient strain epsilonik            */
 
 /* ------------------------------------------------------------------ */
 /* host helpers (no device work)                                      */
@@ -219,6 +222,75 @@ int relax_set_field(relax_ctx *ctx, int which, const void *host, size_t bytes);
 int relax_get_patches(relax_ctx *ctx, int k, relax_slippatch *host, size_t n);
 /* Current time, step counter, event index. */
 int relax_get_time(relax_ctx *ctx, double *t, int *i, int *e);
+/* Grid sizes (sx1, sx2, sx3) and sampling (dx1, dx2, dx3); either may be NULL. */
+int relax_get_grid(relax_ctx *ctx, int *sx, double *dx);
+/* One x3-plane i3 (0-based, < sx3/2) of a field: its components one after
+ * the other (3 for U, 1 for GAMMA, 6 for the tensor fields in the order
+ * s11 s12 s13 s22 s23 s33), each sx1 x sx2 floats, x1 fastest, unpadded.
+ * The read-back of cuexportspatial_ (src/cuelastic.cu:1629). */
+int relax_get_plane(relax_ctx *ctx, int which, int i3, float *host, size_t bytes);
+/* Displacement and stress at n grid points given as 0-based (i1, i2, i3)
+ * triples: cuexportpoints_ (src/cuelastic.cu:1652) for many points. */
+int relax_get_points(relax_ctx *ctx, int n, const int *index, double *u,
+                     relax_tensor *sig);
+
+/* ------------------------------------------------------------------ */
+/* output files (host code, fed from the device fields)               */
+/* ------------------------------------------------------------------ */
+
+/* writegrd / writeNetcdf, src/exportnetcdf.f90:17-127: a GMT grid in the
+ * netCDF classic format, pixel registration; z: nx x ny floats, x fastest;
+ * x_i = x0 + i dx, y_j = y0 + j dy. */
+int relax_write_grd(const float *z, int nx, int ny, double x0, double y0,
+                    double dx, double dy, const char *title,
+                    const char *filename);
+/* exportgrd, src/export.f90:917-1057: three unpadded (sx1, sx2) planes ->
+ * wdir/NNN-<suffix>.grd with the suffixes of `convention` (1 north/east/up,
+ * 2 relax-*, 3 eqbf-*, 4 s11/s12/s13, 5 s22/s23/s33, 6 e11/e12/e13,
+ * 7 e22/e23/e33); the third component is negated for 1..3 (positive up). */
+int relax_write_grd3(const float *c1, const float *c2, const float *c3,
+                     int sx1, int sx2, double dx1, double dx2, double origx,
+                     double origy, const char *wdir, int index,
+                     int convention);
+/* The grids of a context's field: RELAX_FIELD_U at plane int(oz/dx3)
+ * (exportgrd, convention 1), RELAX_FIELD_SIG / RELAX_FIELD_EPS at plane
+ * fix(oz/dx3) (exportstressgrd, src/export.f90:860-908: 4/5, 6/7). */
+int relax_export_grd(relax_ctx *ctx, int which, double oz, double origx,
+                     double origy, const char *wdir, int index);
+/* exportvtk_vectors_legacy / exportvtk_tensors_legacy (src/writevtk.c:72,
+ * :151): VTK legacy binary structured points, big-endian floats.  comp:
+ * 3 vector or 6 tensor component arrays of sx1 x sx2 x sx3 floats. */
+int relax_write_vtk(const float *const *comp, int ncomp, int sx1, int sx2,
+                    int sx3, double dx1, double dx2, double dx3, int j1,
+                    int j2, int j3, const char *filename, const char *title,
+                    const char *name);
+/* The same for a context's U or tensor field over its first sx3 planes. */
+int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int j2,
+                     int j3, const char *filename, const char *title,
+                     const char *name);
+/* shiftedindex, src/elastic3d.f90:4063-4101, 0-based indices; sx3 is the
+ * number of x3-planes held (sx3/2 of the grid). */
+int relax_shifted_index(double x1, double x2, double x3, int sx1, int sx2,
+                        int sx3, double dx1, double dx2, double dx3,
+                        int *i1, int *i2, int *i3);
+/* exportpoints, src/util.f90:59-170: x holds n (x1, x2, x3) observation
+ * points in the computational frame; appends one line to each
+ * wdir/<name>.ned (creates it with its header when isnew) and, when
+ * rot != 0, to wdir/<name>.c.txt. */
+int relax_export_points(relax_ctx *ctx, int n, const double *x,
+                        const char *const *names, double time, double rot,
+                        const char *wdir, int isnew);
+/* The step log line, formats 1100-1103 (src/relax.f90:1102-1105), and the
+ * column headers 0990/0991. */
+int relax_format_log(const relax_step_log *log, double interval,
+                     int transient, char *buf, size_t size);
+const char *relax_log_header(int transient);
+/* One .ned row (14ES16.8E2) and the .ned header line. */
+int relax_format_ned(double time, const double *u, const relax_tensor *sig,
+                     char *buf, size_t size);
+const char *relax_ned_header(void);
+/* Fortran ESw.dEe of one value. */
+int relax_es_format(double v, int w, int d, int e, char *buf, size_t size);
 
 /* Waits for the context's stream. */
 int relax_synchronize(relax_ctx *ctx);

@@ -92,6 +92,22 @@ def load() -> C.CDLL:
         "relax_op_green_noalloc": (I, [P, P, P, P, P, P, I, I, I, D, D, D, D, D, D, P]),
         "relax_op_fft3": (I, [P, I, I, I, D, D, D, I, P]),
         "relax_op_tensoramplitude": (I, [P, I, I, I, D, D, D, C.POINTER(D), P]),
+        "relax_get_grid": (I, [P, C.POINTER(I), C.POINTER(D)]),
+        "relax_get_plane": (I, [P, I, I, P, S]),
+        "relax_get_points": (I, [P, I, C.POINTER(I), C.POINTER(D), C.POINTER(relax_tensor)]),
+        "relax_write_grd": (I, [FP, I, I, D, D, D, D, C.c_char_p, C.c_char_p]),
+        "relax_write_grd3": (I, [FP, FP, FP, I, I, D, D, D, D, C.c_char_p, I, I]),
+        "relax_export_grd": (I, [P, I, D, D, D, C.c_char_p, I]),
+        "relax_write_vtk": (I, [C.POINTER(FP), I, I, I, I, D, D, D, I, I, I, C.c_char_p, C.c_char_p,
+                                C.c_char_p]),
+        "relax_export_vtk": (I, [P, I, I, I, I, I, C.c_char_p, C.c_char_p, C.c_char_p]),
+        "relax_shifted_index": (I, [D, D, D, I, I, I, D, D, D, C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
+        "relax_export_points": (I, [P, I, C.POINTER(D), C.POINTER(C.c_char_p), D, D, C.c_char_p, I]),
+        "relax_format_log": (I, [C.POINTER(relax_step_log), D, I, C.c_char_p, S]),
+        "relax_log_header": (C.c_char_p, [I]),
+        "relax_format_ned": (I, [D, C.POINTER(D), C.POINTER(relax_tensor), C.c_char_p, S]),
+        "relax_ned_header": (C.c_char_p, []),
+        "relax_es_format": (I, [D, I, I, I, C.c_char_p, S]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

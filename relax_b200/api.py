@@ -13,14 +13,74 @@ Every call goes through ``librelax_b200.so``; host arrays use RELAX's layout
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import List, Optional, Sequence
 
 import numpy as np
 
 from . import _lib
-from .config import TENSOR_DTYPE, Simulation, relax_slippatch, relax_step_log
+from .config import TENSOR_DTYPE, Simulation, relax_slippatch, relax_step_log, relax_tensor
 
-FIELDS = {"u": 1, "sig": 2, "tau": 3, "moment": 4, "gamma": 5}
+FIELDS = {"u": 1, "sig": 2, "tau": 3, "moment": 4, "gamma": 5, "eps": 6}
+NCOMP = {"u": 3, "gamma": 1, "sig": 6, "tau": 6, "moment": 6, "eps": 6}
+
+
+def _path(p) -> bytes:
+    return os.fsencode(p)
+
+
+def format_log(log: relax_step_log, interval: float, transient: bool = False) -> str:
+    """The step log line of RELAX (formats 1100-1103, src/relax.f90:1102-1105)."""
+    buf = C.create_string_buffer(256)
+    _lib.check(_lib.load().relax_format_log(C.byref(log), interval, 1 if transient else 0, buf, 256))
+    return buf.value.decode()
+
+
+def log_header(transient: bool = False) -> str:
+    """The column header printed before the log (formats 0990/0991)."""
+    return _lib.load().relax_log_header(1 if transient else 0).decode()
+
+
+def es_format(v: float, w: int, d: int, e: int) -> str:
+    """Fortran ESw.dEe of one value."""
+    buf = C.create_string_buffer(128)
+    _lib.check(_lib.load().relax_es_format(v, w, d, e, buf, 128))
+    return buf.value.decode()
+
+
+def write_grd(z: np.ndarray, x0: float, y0: float, dx: float, dy: float, title: str, filename):
+    """A GMT netCDF grid of z (ny, nx), x_i = x0 + i dx, y_j = y0 + j dy."""
+    z = np.ascontiguousarray(z, np.float32)
+    ny, nx = z.shape
+    _lib.check(_lib.load().relax_write_grd(z.ctypes.data_as(C.POINTER(C.c_float)), nx, ny, x0, y0, dx, dy,
+                                           title.encode(), _path(filename)))
+
+
+def write_grd3(planes, dx1: float, dx2: float, origx: float, origy: float, wdir, index: int, convention: int):
+    """exportgrd of three (sx2, sx1) planes (x1 fastest) into wdir."""
+    ps = [np.ascontiguousarray(p, np.float32) for p in planes]
+    sx2, sx1 = ps[0].shape
+    fp = C.POINTER(C.c_float)
+    _lib.check(_lib.load().relax_write_grd3(*[p.ctypes.data_as(fp) for p in ps], sx1, sx2, dx1, dx2, origx, origy,
+                                            _path(wdir), index, convention))
+
+
+def write_vtk(comps, dx: Sequence[float], strides: Sequence[int], filename, title: str = "", name: str = "field"):
+    """VTK legacy binary file of 3 vector or 6 tensor components, each (sx3, sx2, sx1)."""
+    cs = [np.ascontiguousarray(c, np.float32) for c in comps]
+    sx3, sx2, sx1 = cs[0].shape
+    fp = C.POINTER(C.c_float)
+    arr = (fp * len(cs))(*[c.ctypes.data_as(fp) for c in cs])
+    _lib.check(_lib.load().relax_write_vtk(arr, len(cs), sx1, sx2, sx3, *dx, *strides, _path(filename),
+                                           title.encode(), name.encode()))
+
+
+def shifted_index(x, sx, dx):
+    """shiftedindex (src/elastic3d.f90:4063-4101): 0-based (i1, i2, i3) of a
+    point; sx[2] is the number of x3-planes held."""
+    i = [C.c_int() for _ in range(3)]
+    _lib.check(_lib.load().relax_shifted_index(*x, *sx, *dx, *[C.byref(v) for v in i]))
+    return tuple(v.value for v in i)
 
 
 class Relax:
@@ -113,6 +173,41 @@ class Relax:
         a = np.ascontiguousarray(a)
         _lib.check(self.lib.relax_set_field(self.h, FIELDS[name], a.ctypes.data_as(C.c_void_p),
                                             a.nbytes))
+
+    def plane(self, name: str, i3: int) -> np.ndarray:
+        """Plane i3 of a field as (ncomp, sx2, sx1), unpadded."""
+        s = self.sim
+        a = np.zeros((NCOMP[name], s.sx2, s.sx1), np.float32)
+        _lib.check(self.lib.relax_get_plane(self.h, FIELDS[name], i3, a.ctypes.data_as(C.c_void_p), a.nbytes))
+        return a
+
+    def points(self, index) -> tuple:
+        """Displacement (n, 3) and stress (n,) TENSOR_DTYPE at 0-based (i1, i2, i3) points."""
+        idx = np.ascontiguousarray(index, np.int32).reshape(-1, 3)
+        n = idx.shape[0]
+        u = np.zeros((n, 3), np.float64)
+        sig = (relax_tensor * max(n, 1))()
+        _lib.check(self.lib.relax_get_points(self.h, n, idx.ctypes.data_as(C.POINTER(C.c_int)),
+                                             u.ctypes.data_as(C.POINTER(C.c_double)), sig))
+        out = np.zeros(n, TENSOR_DTYPE)
+        for k in range(n):
+            out[k] = tuple(getattr(sig[k], f) for f in TENSOR_DTYPE.names)
+        return u, out
+
+    def export_grd(self, name: str, wdir, index: int, oz: float = 0.0, origx: float = 0.0, origy: float = 0.0):
+        """exportgrd (u) / exportstressgrd (sig, eps) of the current state into wdir."""
+        _lib.check(self.lib.relax_export_grd(self.h, FIELDS[name], oz, origx, origy, _path(wdir), index))
+
+    def export_vtk(self, name: str, filename, sx3: int, strides=(4, 4, 8), title: str = "", vname: str = "field"):
+        _lib.check(self.lib.relax_export_vtk(self.h, FIELDS[name], sx3, *strides, _path(filename), title.encode(),
+                                             vname.encode()))
+
+    def export_points(self, xyz, names: Sequence[str], time: float, wdir, isnew: bool, rot: float = 0.0):
+        """exportpoints: one .ned line per observation point (x1, x2, x3 in the computational frame)."""
+        x = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        nm = (C.c_char_p * len(names))(*[n.encode() for n in names])
+        _lib.check(self.lib.relax_export_points(self.h, x.shape[0], x.ctypes.data_as(C.POINTER(C.c_double)), nm,
+                                                time, rot, _path(wdir), 1 if isnew else 0))
 
     def patches(self, k: int):
         p = self.cfg.planes[k]

@@ -94,7 +94,8 @@ class relax_config(C.Structure):
 class relax_step_log(C.Structure):
     _fields_ = [("i", C.c_int), ("event", C.c_int)] + \
                [(n, C.c_double) for n in ("dt", "tm_ve", "tm_pl", "tm_as", "t", "power", "cei",
-                                          "tm_tl", "tm_tnl")]
+                                          "tm_tl", "tm_tnl")] + \
+               [("output", C.c_int)]
 
     def as_tuple(self):
         return (self.i, self.dt, self.tm_ve, self.tm_pl, self.tm_as, self.t, self.power,

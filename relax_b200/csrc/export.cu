@@ -1,0 +1,542 @@
+// export.cu -- RELAX's output files written from the device fields:
+//
+//   * GMT grids: netCDF classic (CDF-1) files with the layout of
+//     writeNetcdf, src/exportnetcdf.f90:54-127 (x, y double coordinates,
+//     z float, long_name / actual_range attributes, node_offset = 1,
+//     COARDS conventions), for the slices of exportgrd, src/export.f90:917-1057;
+//   * VTK legacy binary files of a vector or a tensor field,
+//     src/writevtk.c:72-141 and the tensor variant that follows it;
+//   * the .ned time series at observation points, src/util.f90:83-124;
+//   * the step log line, formats 1100-1103 of src/relax.f90:1102-1105.
+//
+// The netCDF classic format is written directly (big-endian header and
+// data, 4-byte alignment) from its published specification; no netCDF
+// library is involved.
+#include <cuda_runtime.h>
+
+#include <cerrno>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/relax_b200.h"
+
+extern "C" __attribute__((visibility("hidden"))) int relax_noalloc_fail(int code, const char *msg);
+
+namespace {
+
+int fail(int code, const char *fmt, ...)
+{
+    char msg[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(msg, sizeof msg, fmt, ap);
+    va_end(ap);
+    return relax_noalloc_fail(code, msg);
+}
+
+// ---------------------------------------------------------------------------
+// netCDF classic (CDF-1) writer for one 2-D grid
+// ---------------------------------------------------------------------------
+enum { NC_CHAR = 2, NC_INT = 4, NC_FLOAT = 5, NC_DOUBLE = 6 };
+enum { NC_DIMENSION = 0x0A, NC_VARIABLE = 0x0B, NC_ATTRIBUTE = 0x0C };
+
+struct Buf {
+    std::vector<unsigned char> b;
+    void u32(uint32_t v)
+    {
+        for (int s = 24; s >= 0; s -= 8) b.push_back((unsigned char)(v >> s));
+    }
+    void f32(float v)
+    {
+        uint32_t u;
+        memcpy(&u, &v, 4);
+        u32(u);
+    }
+    void f64(double v)
+    {
+        uint64_t u;
+        memcpy(&u, &v, 8);
+        u32((uint32_t)(u >> 32));
+        u32((uint32_t)u);
+    }
+    void pad()
+    {
+        while (b.size() % 4) b.push_back(0);
+    }
+    void name(const char *s)
+    {
+        const size_t n = strlen(s);
+        u32((uint32_t)n);
+        b.insert(b.end(), s, s + n);
+        pad();
+    }
+};
+
+struct Att {
+    std::string name;
+    int type;
+    std::string text;
+    std::vector<double> vals;
+};
+
+void put_atts(Buf &h, const std::vector<Att> &atts)
+{
+    if (atts.empty()) {
+        h.u32(0);
+        h.u32(0);
+        return;
+    }
+    h.u32(NC_ATTRIBUTE);
+    h.u32((uint32_t)atts.size());
+    for (const Att &a : atts) {
+        h.name(a.name.c_str());
+        h.u32((uint32_t)a.type);
+        if (a.type == NC_CHAR) {
+            h.u32((uint32_t)a.text.size());
+            h.b.insert(h.b.end(), a.text.begin(), a.text.end());
+            h.pad();
+        } else {
+            h.u32((uint32_t)a.vals.size());
+            for (double v : a.vals) {
+                if (a.type == NC_INT) h.u32((uint32_t)(int32_t)v);
+                else if (a.type == NC_FLOAT) h.f32((float)v);
+                else h.f64(v);
+            }
+            h.pad();
+        }
+    }
+}
+
+// writeNetcdf with registration 1: z(nx, ny), x fastest
+int write_grd(const float *z, int nx, int ny, double x0, double y0, double dx, double dy, const char *title,
+              const char *filename)
+{
+    if (!z || !filename || nx < 2 || ny < 2) return fail(RELAX_ERR_ARG, "grid: null argument or size < 2");
+    std::vector<double> x(nx), y(ny);
+    for (int i = 0; i < nx; i++) x[i] = x0 + (double)i * dx;
+    for (int i = 0; i < ny; i++) y[i] = y0 + (double)i * dy;
+    float zmin = z[0], zmax = z[0];
+    for (size_t i = 0; i < (size_t)nx * ny; i++) {
+        zmin = std::fmin(zmin, z[i]);
+        zmax = std::fmax(zmax, z[i]);
+    }
+    const std::vector<Att> gatts = {
+        {"node_offset", NC_INT, "", {1.0}},
+        {"title", NC_CHAR, title ? title : "", {}},
+        {"history", NC_CHAR, "Relax output", {}},
+        {"Conventions", NC_CHAR, "COARDS/CF-1.0", {}}};
+    const std::vector<Att> xatts = {
+        {"long_name", NC_CHAR, "x", {}},
+        {"actual_range", NC_DOUBLE, "", {x[0] - 0.5 * (x[1] - x[0]), x[nx - 1] + 0.5 * (x[nx - 1] - x[nx - 2])}}};
+    const std::vector<Att> yatts = {
+        {"long_name", NC_CHAR, "y", {}},
+        {"actual_range", NC_DOUBLE, "", {y[0] - 0.5 * (y[1] - y[0]), y[ny - 1] + 0.5 * (y[ny - 1] - y[ny - 2])}}};
+    const std::vector<Att> zatts = {{"long_name", NC_CHAR, "z", {}},
+                                    {"actual_range", NC_FLOAT, "", {(double)zmin, (double)zmax}}};
+    const uint32_t xsize = 8u * nx, ysize = 8u * ny, zsize = 4u * (uint32_t)nx * ny;
+    // the header twice: once to size it, once with the data offsets
+    auto header = [&](uint32_t begin0) {
+        Buf h;
+        h.b = {'C', 'D', 'F', 1};
+        h.u32(0);                       // numrecs
+        h.u32(NC_DIMENSION);
+        h.u32(2);
+        h.name("x");
+        h.u32((uint32_t)nx);
+        h.name("y");
+        h.u32((uint32_t)ny);
+        put_atts(h, gatts);
+        h.u32(NC_VARIABLE);
+        h.u32(3);
+        uint32_t begin = begin0;
+        // x(x)
+        h.name("x"); h.u32(1); h.u32(0); put_atts(h, xatts); h.u32(NC_DOUBLE); h.u32(xsize); h.u32(begin);
+        begin += xsize;
+        // y(y)
+        h.name("y"); h.u32(1); h.u32(1); put_atts(h, yatts); h.u32(NC_DOUBLE); h.u32(ysize); h.u32(begin);
+        begin += ysize;
+        // z(y, x)
+        h.name("z"); h.u32(2); h.u32(1); h.u32(0); put_atts(h, zatts); h.u32(NC_FLOAT); h.u32(zsize);
+        h.u32(begin);
+        return h;
+    };
+    const uint32_t hsize = (uint32_t)header(0).b.size();
+    Buf f = header(hsize);
+    for (double v : x) f.f64(v);
+    for (double v : y) f.f64(v);
+    for (size_t i = 0; i < (size_t)nx * ny; i++) f.f32(z[i]);
+    FILE *fp = fopen(filename, "wb");
+    if (!fp) return fail(RELAX_ERR_ARG, "cannot open %s: %s", filename, strerror(errno));
+    const size_t w = fwrite(f.b.data(), 1, f.b.size(), fp);
+    const int rc = fclose(fp);
+    if (w != f.b.size() || rc != 0) return fail(RELAX_ERR_ARG, "writing %s failed", filename);
+    return RELAX_OK;
+}
+
+// exportspatial with doflip, src/elastic3d.f90:4166-4207: fftshift and
+// transpose of one (sx1, sx2) plane into p(sx2, sx1), x2 fastest
+void exportspatial(const float *data, int sx1, int sx2, float *p)
+{
+    for (int j2 = 0; j2 < sx2; j2++) {
+        const int j2s = j2 < sx2 / 2 ? sx2 / 2 + j2 : j2 - sx2 / 2;
+        for (int j1 = 0; j1 < sx1; j1++) {
+            const int j1s = j1 < sx1 / 2 ? sx1 / 2 + j1 : j1 - sx1 / 2;
+            p[(size_t)j1s * sx2 + j2s] = data[(size_t)j2 * sx1 + j1];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// VTK legacy binary
+// ---------------------------------------------------------------------------
+void put_be(std::vector<unsigned char> &o, float v)
+{
+    uint32_t u;
+    memcpy(&u, &v, 4);
+    o.push_back((unsigned char)(u >> 24));
+    o.push_back((unsigned char)(u >> 16));
+    o.push_back((unsigned char)(u >> 8));
+    o.push_back((unsigned char)u);
+}
+
+// Writes a structured-points file; plane(k3, pc) fills pc[0..ncomp) with
+// the components of plane k3 (sx1 x sx2, x1 fastest) and returns a status.
+template <class Plane>
+int write_vtk(const char *filename, const char *title, const char *name, int ncomp, int sx1, int sx2, int sx3,
+              double dx1, double dx2, double dx3, int j1, int j2, int j3, Plane plane)
+{
+    if (!filename || (ncomp != 3 && ncomp != 6)) return fail(RELAX_ERR_ARG, "vtk: 3 or 6 components");
+    if (j1 < 1 || j2 < 1 || j3 < 1 || sx1 < 2 || sx2 < 2 || sx3 < 1) return fail(RELAX_ERR_ARG, "vtk: sizes");
+    FILE *fp = fopen(filename, "wb");
+    if (!fp) return fail(RELAX_ERR_ARG, "cannot open %s: %s", filename, strerror(errno));
+    fprintf(fp, "# vtk DataFile Version 3.0\n");
+    fprintf(fp, "%s\n", title ? title : "");
+    fprintf(fp, "BINARY\n");
+    fprintf(fp, "DATASET STRUCTURED_POINTS\n");
+    fprintf(fp, "DIMENSIONS %i %i %i\n", sx1 / j1, sx2 / j2, sx3 / j3);
+    fprintf(fp, "ORIGIN %f %f %f\n", -dx1 * (sx1 / 2), -dx2 * (sx2 / 2), 0.0);
+    fprintf(fp, "SPACING %f %f %f\n", dx1 * j1, dx2 * j2, dx3 * j3);
+    fprintf(fp, "POINT_DATA %i\n", (sx1 / j1) * (sx2 / j2) * (sx3 / j3));
+    fprintf(fp, "%s %s float\n", ncomp == 3 ? "VECTORS" : "TENSORS", name ? name : "field");
+    std::vector<unsigned char> o;
+    const float *pc[6] = {};
+    int rc = RELAX_OK;
+    for (int k3 = 0; k3 < sx3 && rc == RELAX_OK; k3 += j3) {
+        rc = plane(k3, pc);
+        if (rc != RELAX_OK) break;
+        o.clear();
+        // x2 and x1 from -sx/2: the origin in the middle of the box
+        for (int k2 = -sx2 / 2; k2 < sx2 / 2; k2 += j2) {
+            const int i2 = (sx2 + k2) % sx2;
+            for (int k1 = -sx1 / 2; k1 < sx1 / 2; k1 += j1) {
+                const size_t q = (size_t)((sx1 + k1) % sx1) + (size_t)i2 * sx1;
+                if (ncomp == 3) {
+                    for (int k = 0; k < 3; k++) put_be(o, pc[k][q]);
+                } else {
+                    // the symmetric tensor as 3 x 3, row by row
+                    static const int full[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+                    for (int k = 0; k < 9; k++) put_be(o, pc[full[k]][q]);
+                }
+            }
+        }
+        if (fwrite(o.data(), 1, o.size(), fp) != o.size()) rc = fail(RELAX_ERR_ARG, "writing %s failed", filename);
+    }
+    if (fclose(fp) != 0 && rc == RELAX_OK) rc = fail(RELAX_ERR_ARG, "writing %s failed", filename);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Fortran edit descriptors of RELAX's text output
+// ---------------------------------------------------------------------------
+// ESw.dEe: one digit before the point, d after, an exponent of e digits;
+// a field that does not fit is w asterisks
+std::string es(double v, int w, int d, int e)
+{
+    char buf[64];
+    snprintf(buf, sizeof buf, "%.*E", d, v);
+    std::string s(buf);
+    const size_t p = s.find('E');
+    if (p == std::string::npos) return std::string(w, '*');
+    std::string mant = s.substr(0, p);
+    const int ex = atoi(s.c_str() + p + 1);
+    const int ax = ex < 0 ? -ex : ex;
+    int lim = 1;
+    for (int k = 0; k < e; k++) lim *= 10;
+    if (ax >= lim) return std::string(w, '*');
+    char eb[16];
+    snprintf(eb, sizeof eb, "E%c%0*d", ex < 0 ? '-' : '+', e, ax);
+    std::string out = mant + eb;
+    if ((int)out.size() > w) return std::string(w, '*');
+    return std::string(w - out.size(), ' ') + out;
+}
+
+// Iw.m for a non-negative integer
+std::string iw(int v, int w, int m)
+{
+    char buf[32];
+    snprintf(buf, sizeof buf, "%0*d", m, v);
+    if (v < 0 || (int)strlen(buf) > w) return std::string(w, '*');
+    return std::string(w - strlen(buf), ' ') + buf;
+}
+
+int copy_out(const std::string &s, char *buf, size_t size)
+{
+    if (!buf || s.size() + 1 > size) return fail(RELAX_ERR_ARG, "buffer of %zu bytes too small", size);
+    memcpy(buf, s.c_str(), s.size() + 1);
+    return RELAX_OK;
+}
+
+// fix, src/elastic3d.f90:70-83: the nearest integer, halves rounded down
+int fix(double x)
+{
+    const double f = std::floor(x), c = std::ceil(x);
+    return (x - f) > 0.5 ? (int)c : (int)f;
+}
+
+// rotation, src/util.f90:153-166 (angle in degrees)
+void rotation(double &x, double &y, double rot)
+{
+    const double a = rot * 0.01745329251994329547437168059786927;
+    const double xx = x, yy = y;
+    x = +xx * std::cos(a) + yy * std::sin(a);
+    y = -xx * std::sin(a) + yy * std::cos(a);
+}
+
+std::string ned_row(double time, const double u[3], const relax_tensor &s)
+{
+    std::string r = es(time, 16, 8, 2);
+    for (int k = 0; k < 3; k++) r += es(u[k], 16, 8, 2);
+    const float c[6] = {s.s11, s.s12, s.s13, s.s22, s.s23, s.s33};
+    for (int k = 0; k < 6; k++) r += es((double)c[k], 16, 8, 2);
+    return r;
+}
+
+const char NED_HEADER[] = "#          t          u1          u2          u3         s11         s12         s13"
+                          "         s22         s23         s33";
+
+}  // namespace
+
+extern "C" int relax_write_grd(const float *z, int nx, int ny, double x0, double y0, double dx, double dy,
+                               const char *title, const char *filename)
+{
+    return write_grd(z, nx, ny, x0, y0, dx, dy, title, filename);
+}
+
+// exportgrd, src/export.f90:917-1057, for three unpadded (sx1, sx2) planes
+extern "C" int relax_write_grd3(const float *c1, const float *c2, const float *c3, int sx1, int sx2, double dx1,
+                                double dx2, double origx, double origy, const char *wdir, int index,
+                                int convention)
+{
+    static const char *const suffix[7][3] = {
+        {"north", "east", "up"}, {"relax-north", "relax-east", "relax-up"}, {"eqbf-north", "eqbf-east", "eqbf-up"},
+        {"s11", "s12", "s13"},   {"s22", "s23", "s33"},                     {"e11", "e12", "e13"},
+        {"e22", "e23", "e33"}};
+    if (!c1 || !c2 || !c3 || !wdir) return fail(RELAX_ERR_ARG, "null argument");
+    if (convention < 1 || convention > 7) return fail(RELAX_ERR_ARG, "convention %d outside 1..7", convention);
+    if (sx1 < 2 || sx2 < 2) return fail(RELAX_ERR_ARG, "grid %d x %d", sx1, sx2);
+    const size_t np = (size_t)sx1 * sx2;
+    std::vector<float> p(np);
+    const float *cs[3] = {c1, c2, c3};
+    const std::string digit = iw(index, 3, 3);
+    // x (east) from origy, y (north) from origx; pixel registration
+    const double xmin = origy - (sx2 / 2) * dx2, ymin = origx - (sx1 / 2) * dx1;
+    for (int k = 0; k < 3; k++) {
+        exportspatial(cs[k], sx1, sx2, p.data());
+        if (k == 2 && convention <= 3)
+            for (float &v : p) v = -v;   // positive up
+        const std::string title = digit + "-" + suffix[convention - 1][k];
+        const std::string file = std::string(wdir) + "/" + title + ".grd";
+        const int rc = write_grd(p.data(), sx2, sx1, xmin, ymin, dx2, dx1, title.c_str(), file.c_str());
+        if (rc != RELAX_OK) return rc;
+    }
+    return RELAX_OK;
+}
+
+// The map-view grids of a context's field: U at plane int(oz/dx3) as
+// NNN-north/east/up.grd (exportgrd, convention 1); SIG at plane fix(oz/dx3)
+// as NNN-s11..s33.grd and EPS (the transient strain) as NNN-e11..e33.grd
+// (exportstressgrd, src/export.f90:860-908, conventions 4/5 and 6/7).
+extern "C" int relax_export_grd(relax_ctx *ctx, int which, double oz, double origx, double origy, const char *wdir,
+                                int index)
+{
+    int sx[3];
+    double dx[3];
+    if (!ctx || !wdir) return fail(RELAX_ERR_ARG, "null argument");
+    int rc = relax_get_grid(ctx, sx, dx);
+    if (rc != RELAX_OK) return rc;
+    const size_t np = (size_t)sx[0] * sx[1];
+    if (which == RELAX_FIELD_U) {
+        std::vector<float> pl(3 * np);
+        rc = relax_get_plane(ctx, which, (int)(oz / dx[2]), pl.data(), pl.size() * sizeof(float));
+        if (rc != RELAX_OK) return rc;
+        return relax_write_grd3(pl.data(), pl.data() + np, pl.data() + 2 * np, sx[0], sx[1], dx[0], dx[1], origx,
+                                origy, wdir, index, 1);
+    }
+    if (which != RELAX_FIELD_SIG && which != RELAX_FIELD_EPS)
+        return fail(RELAX_ERR_ARG, "grids of field %d: U, SIG or EPS", which);
+    std::vector<float> pl(6 * np);
+    rc = relax_get_plane(ctx, which, fix(oz / dx[2]), pl.data(), pl.size() * sizeof(float));
+    if (rc != RELAX_OK) return rc;
+    const int conv = which == RELAX_FIELD_SIG ? 4 : 6;
+    const float *c = pl.data();
+    rc = relax_write_grd3(c, c + np, c + 2 * np, sx[0], sx[1], dx[0], dx[1], origx, origy, wdir, index, conv);
+    if (rc != RELAX_OK) return rc;
+    return relax_write_grd3(c + 3 * np, c + 4 * np, c + 5 * np, sx[0], sx[1], dx[0], dx[1], origx, origy, wdir, index,
+                            conv + 1);
+}
+
+// exportvtk_vectors_legacy / exportvtk_tensors_legacy, src/writevtk.c:72-225,
+// for host fields: ncomp = 3 (vector) or 6 (s11 s12 s13 s22 s23 s33)
+// component arrays of sx1 x sx2 x sx3 floats, x1 fastest.
+extern "C" int relax_write_vtk(const float *const *comp, int ncomp, int sx1, int sx2, int sx3, double dx1,
+                               double dx2, double dx3, int j1, int j2, int j3, const char *filename,
+                               const char *title, const char *name)
+{
+    if (!comp || (ncomp != 3 && ncomp != 6)) return fail(RELAX_ERR_ARG, "vtk: 3 or 6 components");
+    for (int k = 0; k < ncomp; k++)
+        if (!comp[k]) return fail(RELAX_ERR_ARG, "null component");
+    const size_t np = (size_t)sx1 * sx2;
+    return write_vtk(filename, title, name, ncomp, sx1, sx2, sx3, dx1, dx2, dx3, j1, j2, j3,
+                     [&](int k3, const float **pc) {
+                         for (int k = 0; k < ncomp; k++) pc[k] = comp[k] + (size_t)k3 * np;
+                         return RELAX_OK;
+                     });
+}
+
+// The same for a context's field (U or a tensor field), read plane by
+// plane; sx3 (<= sx3/2 of the grid) is the depth exported, as the
+// reference's sx3/4 for displacement and sx3/2 for stress.
+extern "C" int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int j2, int j3, const char *filename,
+                                const char *title, const char *name)
+{
+    int sx[3];
+    double dx[3];
+    if (!ctx) return fail(RELAX_ERR_ARG, "null context");
+    int rc = relax_get_grid(ctx, sx, dx);
+    if (rc != RELAX_OK) return rc;
+    if (sx3 < 1 || sx3 > sx[2] / 2) return fail(RELAX_ERR_ARG, "vtk depth %d outside [1, %d]", sx3, sx[2] / 2);
+    int ncomp;
+    switch (which) {
+    case RELAX_FIELD_U: ncomp = 3; break;
+    case RELAX_FIELD_SIG:
+    case RELAX_FIELD_TAU:
+    case RELAX_FIELD_MOMENT:
+    case RELAX_FIELD_EPS: ncomp = 6; break;
+    default: return fail(RELAX_ERR_ARG, "vtk of field %d: U or a tensor field", which);
+    }
+    const size_t np = (size_t)sx[0] * sx[1];
+    std::vector<float> pl(ncomp * np);
+    return write_vtk(filename, title, name, ncomp, sx[0], sx[1], sx3, dx[0], dx[1], dx[2], j1, j2, j3,
+                     [&](int k3, const float **pc) {
+                         const int r = relax_get_plane(ctx, which, k3, pl.data(), pl.size() * sizeof(float));
+                         for (int k = 0; k < ncomp; k++) pc[k] = pl.data() + k * np;
+                         return r;
+                     });
+}
+
+// shiftedindex, src/elastic3d.f90:4063-4101, 0-based; sx3 is the number of
+// planes (sx3/2 of the grid)
+extern "C" int relax_shifted_index(double x1, double x2, double x3, int sx1, int sx2, int sx3, double dx1,
+                                   double dx2, double dx3, int *i1, int *i2, int *i3)
+{
+    if (!i1 || !i2 || !i3) return fail(RELAX_ERR_ARG, "null argument");
+    if (x1 > (double)(sx1 / 2 - 1) * dx1 || x1 < -(double)(sx1 / 2) * dx1)
+        return fail(RELAX_ERR_ARG, "x1=%g outside the box", x1);
+    if (x2 > (double)(sx2 / 2 - 1) * dx2 || x2 < -(double)(sx2 / 2) * dx2)
+        return fail(RELAX_ERR_ARG, "x2=%g outside the box", x2);
+    if (x3 > (double)(sx3 - 1) * dx3 || x3 < 0) return fail(RELAX_ERR_ARG, "x3=%g outside the box", x3);
+    *i1 = (sx1 + fix(x1 / dx1)) % sx1;
+    *i2 = (sx2 + fix(x2 / dx2)) % sx2;
+    *i3 = fix(x3 / dx3);
+    return RELAX_OK;
+}
+
+// exportpoints, src/util.f90:59-170: for each observation point (x1, x2,
+// x3 in the computational frame) one line of wdir/<name>.ned, time,
+// displacement rotated back to the user frame and stress (a new file with
+// its header when isnew), and, when rot != 0, time and the unrotated
+// displacement in wdir/<name>.c.txt.
+extern "C" int relax_export_points(relax_ctx *ctx, int n, const double *x, const char *const *names, double time,
+                                   double rot, const char *wdir, int isnew)
+{
+    int sx[3];
+    double dx[3];
+    if (!ctx || n < 0 || (n > 0 && (!x || !names)) || !wdir) return fail(RELAX_ERR_ARG, "null argument");
+    if (n == 0) return RELAX_OK;
+    int rc = relax_get_grid(ctx, sx, dx);
+    if (rc != RELAX_OK) return rc;
+    std::vector<int> idx(3 * (size_t)n);
+    for (int k = 0; k < n; k++) {
+        rc = relax_shifted_index(x[3 * k], x[3 * k + 1], x[3 * k + 2], sx[0], sx[1], sx[2] / 2, dx[0], dx[1], dx[2],
+                                 &idx[3 * k], &idx[3 * k + 1], &idx[3 * k + 2]);
+        if (rc != RELAX_OK) return rc;
+    }
+    std::vector<double> u(3 * (size_t)n);
+    std::vector<relax_tensor> sig(n);
+    rc = relax_get_points(ctx, n, idx.data(), u.data(), sig.data());
+    if (rc != RELAX_OK) return rc;
+    for (int k = 0; k < n; k++) {
+        if (!names[k]) return fail(RELAX_ERR_ARG, "point %d has no name", k);
+        const std::string base = std::string(wdir) + "/" + names[k];
+        double v[3] = {u[3 * k], u[3 * k + 1], u[3 * k + 2]};
+        rotation(v[0], v[1], -rot);
+        FILE *fp = fopen((base + ".ned").c_str(), isnew ? "w" : "a");
+        if (!fp) return fail(RELAX_ERR_ARG, "could not open %s.ned for writing", base.c_str());
+        if (isnew) fprintf(fp, "%s\n", NED_HEADER);
+        fprintf(fp, "%s\n", ned_row(time, v, sig[k]).c_str());
+        if (fclose(fp) != 0) return fail(RELAX_ERR_ARG, "writing %s.ned failed", base.c_str());
+        if (rot != 0.0) {
+            fp = fopen((base + ".c.txt").c_str(), isnew ? "w" : "a");
+            if (!fp) return fail(RELAX_ERR_ARG, "could not open %s.c.txt for writing", base.c_str());
+            if (isnew) fprintf(fp, "#         t         u1         u2         u3\n");
+            std::string r = es(time, 11, 3, 2);
+            for (int j = 0; j < 3; j++) r += es(u[3 * k + j], 11, 3, 2);
+            fprintf(fp, "%s\n", r.c_str());
+            if (fclose(fp) != 0) return fail(RELAX_ERR_ARG, "writing %s.c.txt failed", base.c_str());
+        }
+    }
+    return RELAX_OK;
+}
+
+// The step log line, formats 1100-1103 of src/relax.f90:1102-1105: "*" after
+// the step number on output steps; the transient form adds the Maxwell times
+// of the linear and nonlinear transient mechanisms.
+extern "C" int relax_format_log(const relax_step_log *log, double interval, int transient, char *buf, size_t size)
+{
+    if (!log) return fail(RELAX_ERR_ARG, "null argument");
+    std::string s = iw(log->i, 3, 3) + (log->output ? "*" : " ");
+    s += es(log->dt, 9, 2, 2);
+    s += es(log->tm_ve, 9, 2, 2) + es(log->tm_pl, 9, 2, 2) + es(log->tm_as, 9, 2, 2);
+    if (transient) s += es(log->tm_tl, 9, 2, 2) + es(log->tm_tnl, 9, 2, 2);
+    s += es(log->t, 9, 2, 2) + "/" + es(interval, 7, 2, 1);
+    s += es(log->power, 9, 2, 2) + es(log->cei, 9, 2, 2);
+    return copy_out(s, buf, size);
+}
+
+// The column header, formats 0990/0991 of src/relax.f90:1100-1101
+extern "C" const char *relax_log_header(int transient)
+{
+    return transient ? " I  |   Dt   | tm(ve) | tm(pl) | tm(as) | tm(kl) | tm(kn) |     t/tmax     | power  |  C:E^i | "
+                     : " I  |   Dt   | tm(ve) | tm(pl) | tm(as) |     t/tmax     | power  |  C:E^i | ";
+}
+
+// one row of a .ned file (format 14ES16.8E2, src/util.f90:120)
+extern "C" int relax_format_ned(double time, const double *u, const relax_tensor *sig, char *buf, size_t size)
+{
+    if (!u || !sig) return fail(RELAX_ERR_ARG, "null argument");
+    return copy_out(ned_row(time, u, *sig), buf, size);
+}
+
+extern "C" const char *relax_ned_header(void) { return NED_HEADER; }
+
+// Fortran ESw.dEe of one value
+extern "C" int relax_es_format(double v, int w, int d, int e, char *buf, size_t size)
+{
+    if (w < 1 || w > 60 || d < 0 || d > 40 || e < 1 || e > 4) return fail(RELAX_ERR_ARG, "format");
+    return copy_out(es(v, w, d, e), buf, size);
+}

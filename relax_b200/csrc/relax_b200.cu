@@ -1361,6 +1361,7 @@ extern "C" int relax_coseismic(relax_ctx *c, int e, relax_step_log *log0)
         memset(log0, 0, sizeof *log0);
         log0->i = 0;
         log0->cei = c->hst->cei;
+        log0->output = 1;   // format 1101, src/relax.f90:469-472
     }
     return RELAX_OK;
 }
@@ -1413,11 +1414,14 @@ static int finish_step(relax_ctx *c, relax_step_log *log)
     c->m_valid = true;
     c->sig_valid = c->store_sig && !c->sig_mask;
     // isoutput, src/relax.f90:1364-1376
+    int output = 0;
     {
         const double odt = c->cfg.odt, etime = c->events[c->e].time;
         if ((0 == c->cfg.skip && fabs(c->t - c->oi * odt) < 1e-6 * odt) ||
-            (0 < c->cfg.skip && ((c->i - 1) % c->cfg.skip) == 0) || fabs(c->t - etime) < 1e-6)
+            (0 < c->cfg.skip && ((c->i - 1) % c->cfg.skip) == 0) || fabs(c->t - etime) < 1e-6) {
             c->oi++;
+            output = 1;
+        }
     }
     if (!c->fc.empty()) TRY(check_err(c));
     log->i = c->i;
@@ -1428,6 +1432,7 @@ static int finish_step(relax_ctx *c, relax_step_log *log)
     log->t = c->t;
     log->power = c->hst->power;
     log->cei = c->hst->cei;
+    log->output = output;
     return RELAX_OK;
 }
 
@@ -1564,6 +1569,17 @@ __global__ void k_scale(float *p, size_t n, float s)
     if (q < n) p[q] *= s;
 }
 
+static const float *tensor_field(relax_ctx *c, int which)
+{
+    switch (which) {
+    case RELAX_FIELD_SIG: return c->sig;
+    case RELAX_FIELD_TAU: return c->tau;
+    case RELAX_FIELD_MOMENT: return c->m;
+    case RELAX_FIELD_EPS: return c->eps;
+    default: return nullptr;
+    }
+}
+
 static int field_sig(relax_ctx *c)
 {
     const Grid &g = c->g;
@@ -1599,10 +1615,12 @@ extern "C" int relax_get_field(relax_ctx *c, int which, void *host, size_t bytes
     }
     case RELAX_FIELD_SIG:
     case RELAX_FIELD_TAU:
-    case RELAX_FIELD_MOMENT: {
+    case RELAX_FIELD_MOMENT:
+    case RELAX_FIELD_EPS: {
         if (bytes != g.nh * sizeof(relax_tensor)) return fail(RELAX_ERR_ARG, "field size %zu != %zu", bytes, g.nh * sizeof(relax_tensor));
+        if (which == RELAX_FIELD_EPS && !c->eps) return fail(RELAX_ERR_STATE, "no transient rheology");
         if (which == RELAX_FIELD_SIG) TRY(field_sig(c));
-        const float *src = which == RELAX_FIELD_SIG ? c->sig : which == RELAX_FIELD_TAU ? c->tau : c->m;
+        const float *src = tensor_field(c, which);
         TRY(dalloc(&tmp, 6 * g.nh));
         k_soa_to_aos<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(src, (relax_tensor *)tmp, g.nh);
         break;
@@ -1639,11 +1657,13 @@ extern "C" int relax_set_field(relax_ctx *c, int which, const void *host, size_t
     }
     case RELAX_FIELD_SIG:
     case RELAX_FIELD_TAU:
-    case RELAX_FIELD_MOMENT: {
+    case RELAX_FIELD_MOMENT:
+    case RELAX_FIELD_EPS: {
         if (bytes != g.nh * sizeof(relax_tensor)) return fail(RELAX_ERR_ARG, "field size mismatch");
+        if (which == RELAX_FIELD_EPS && !c->eps) return fail(RELAX_ERR_STATE, "no transient rheology");
         TRY(dalloc(&tmp, 6 * g.nh));
         CK(cudaMemcpyAsync(tmp, host, bytes, cudaMemcpyHostToDevice, c->st));
-        float *dst = which == RELAX_FIELD_SIG ? c->sig : which == RELAX_FIELD_TAU ? c->tau : c->m;
+        float *dst = const_cast<float *>(tensor_field(c, which));
         k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>((const relax_tensor *)tmp, dst, g.nh);
         break;
     }
@@ -1656,6 +1676,97 @@ extern "C" int relax_set_field(relax_ctx *c, int which, const void *host, size_t
     if (which == RELAX_FIELD_SIG) c->sig_valid = true;
     else c->m_valid = false, c->sig_valid = false;
     if (which == RELAX_FIELD_MOMENT) c->m_valid = true;
+    return RELAX_OK;
+}
+
+// One horizontal plane of a field, the slice cuexportspatial_ reads for
+// exportgrd (src/export.f90:952-955): components one after the other, each
+// sx1 x sx2 floats with x1 fastest and no padding.
+extern "C" int relax_get_plane(relax_ctx *c, int which, int i3, float *host, size_t bytes)
+{
+    if (!c || !host) return fail(RELAX_ERR_ARG, "null argument");
+    const Grid &g = c->g;
+    if (i3 < 0 || i3 >= g.sx3h) return fail(RELAX_ERR_ARG, "plane %d outside [0, %d)", i3, g.sx3h);
+    CK(cudaSetDevice(c->device));
+    const size_t np = (size_t)g.sx1 * g.sx2;
+    const float *src = nullptr;
+    int nc = 0;
+    switch (which) {
+    case RELAX_FIELD_U: src = c->u; nc = 3; break;
+    case RELAX_FIELD_GAMMA: src = c->gamma; nc = 1; break;
+    case RELAX_FIELD_SIG:
+    case RELAX_FIELD_TAU:
+    case RELAX_FIELD_MOMENT:
+    case RELAX_FIELD_EPS:
+        if (which == RELAX_FIELD_EPS && !c->eps) return fail(RELAX_ERR_STATE, "no transient rheology");
+        if (which == RELAX_FIELD_SIG) TRY(field_sig(c));
+        src = tensor_field(c, which);
+        nc = 6;
+        break;
+    default:
+        return fail(RELAX_ERR_ARG, "unknown field %d", which);
+    }
+    if (bytes != nc * np * sizeof(float)) return fail(RELAX_ERR_ARG, "plane size %zu != %zu", bytes, nc * np * sizeof(float));
+    for (int k = 0; k < nc; k++)
+        CK(cudaMemcpyAsync(host + k * np, src + k * g.nh + (size_t)i3 * np, np * sizeof(float),
+                           cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return RELAX_OK;
+}
+
+__global__ void k_gather_points(const float *u, const float *sig, size_t nh, const int *idx, int n, float *out)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const size_t q = (size_t)idx[p];
+    for (int k = 0; k < 3; k++) out[9 * p + k] = u[k * nh + q];
+    for (int k = 0; k < 6; k++) out[9 * p + 3 + k] = sig[k * nh + q];
+}
+
+// Displacement and stress at grid points, the read-back of cuexportpoints_
+// (src/util.f90:104-105) for n points at once.  index: n triples
+// (i1, i2, i3), 0-based; u: 3n doubles; sig: n tensors.
+extern "C" int relax_get_points(relax_ctx *c, int n, const int *index, double *u, relax_tensor *sig)
+{
+    if (!c || n < 0 || (n > 0 && (!index || !u || !sig))) return fail(RELAX_ERR_ARG, "null argument");
+    if (n == 0) return RELAX_OK;
+    const Grid &g = c->g;
+    std::vector<int> q(n);
+    for (int p = 0; p < n; p++) {
+        const int i1 = index[3 * p], i2 = index[3 * p + 1], i3 = index[3 * p + 2];
+        if (i1 < 0 || i1 >= g.sx1 || i2 < 0 || i2 >= g.sx2 || i3 < 0 || i3 >= g.sx3h)
+            return fail(RELAX_ERR_ARG, "point %d (%d, %d, %d) outside the grid", p, i1, i2, i3);
+        q[p] = i1 + g.sx1 * (i2 + g.sx2 * i3);
+    }
+    CK(cudaSetDevice(c->device));
+    TRY(field_sig(c));
+    float *buf = nullptr;
+    TRY(dalloc(&buf, 10 * (size_t)n));
+    int *didx = (int *)(buf + 9 * (size_t)n);
+    std::vector<float> out(9 * (size_t)n);
+    cudaError_t e = cudaMemcpyAsync(didx, q.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) {
+        k_gather_points<<<(n + 127) / 128, 128, 0, c->st>>>(c->u, c->sig, g.nh, didx, n, buf);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), buf, out.size() * sizeof(float), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(buf);
+    if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "point read-back: %s", cudaGetErrorString(e));
+    for (int p = 0; p < n; p++) {
+        const float *o = &out[9 * (size_t)p];
+        u[3 * p] = o[0]; u[3 * p + 1] = o[1]; u[3 * p + 2] = o[2];
+        sig[p].s11 = o[3]; sig[p].s12 = o[4]; sig[p].s13 = o[5];
+        sig[p].s22 = o[6]; sig[p].s23 = o[7]; sig[p].s33 = o[8];
+    }
+    return RELAX_OK;
+}
+
+extern "C" int relax_get_grid(relax_ctx *c, int *sx, double *dx)
+{
+    if (!c) return fail(RELAX_ERR_ARG, "null context");
+    if (sx) { sx[0] = c->g.sx1; sx[1] = c->g.sx2; sx[2] = c->g.sx3; }
+    if (dx) { dx[0] = c->g.dx1; dx[1] = c->g.dx2; dx[2] = c->g.dx3; }
     return RELAX_OK;
 }
 
