@@ -159,6 +159,8 @@ typedef struct relax_step_log {
 #define RELAX_FIELD_GAMMA   5   /* float (sx1+2, sx2, sx3/2)             */
 #define RELAX_FIELD_EPS     6   /* relax_tensor (sx1, sx2, sx3/2): the
                                    transient strain epsilonik            */
+#define RELAX_FIELD_V       7   /* planes only: the corrector's velocity  */
+#define RELAX_FIELD_UR      8   /* planes only: postseismic displacement  */
 
 /* ------------------------------------------------------------------ */
 /* host helpers (no device work)                                      */
@@ -229,10 +231,64 @@ int relax_get_grid(relax_ctx *ctx, int *sx, double *dx);
  * s11 s12 s13 s22 s23 s33), each sx1 x sx2 floats, x1 fastest, unpadded.
  * The read-back of cuexportspatial_ (src/cuelastic.cu:1629). */
 int relax_get_plane(relax_ctx *ctx, int which, int i3, float *host, size_t bytes);
+/* Keeps, from the next step on, the corrector's velocity field v
+ * (src/relax.f90:829) for planes i3 < vel_planes and the postseismic
+ * displacement sum Dt v (src/relax.f90:839-850) for planes i3 < ur_planes
+ * and for plane inter_i3 (-1: none), readable with relax_get_plane as
+ * RELAX_FIELD_V / RELAX_FIELD_UR.  Costs 12 bytes per kept point and step.
+ * Calling it again restarts the sums.  Not for batch members. */
+int relax_track_relaxation(relax_ctx *ctx, int vel_planes, int ur_planes,
+                           int inter_i3);
 /* Displacement and stress at n grid points given as 0-based (i1, i2, i3)
  * triples: cuexportpoints_ (src/cuelastic.cu:1652) for many points. */
 int relax_get_points(relax_ctx *ctx, int n, const int *index, double *u,
                      relax_tensor *sig);
+
+/* ------------------------------------------------------------------ */
+/* the input file (subroutine init, src/input.f90:43-1767)            */
+/*                                                                    */
+/* The text of a RELAX input file, in init's order and with its        */
+/* conventions (comment lines start with '#', Fortran list-directed   */
+/* records, wangconvention for faults, planes and weak zones, rotation */
+/* of points, dilatation sources and loads), is read into a           */
+/* relax_config ready for relax_create.  Errors (index misfits,       */
+/* negative rates, missing values) return RELAX_ERR_ARG with the line */
+/* number in relax_last_error.  Cuboid and tetrahedral eigenstrain    */
+/* sources are read and rejected (RELAX_ERR_UNSUPPORTED).             */
+/* ------------------------------------------------------------------ */
+typedef struct relax_input relax_input;
+
+#define RELAX_INPUT_TRANSIENT    1   /* --with-transient: transient sections  */
+#define RELAX_INPUT_EIGENSTRAIN  2   /* --with-eigenstrain: cuboid sections   */
+#define RELAX_INPUT_CURVILINEAR  4   /* --with-curvilinear: tetrahedra        */
+#define RELAX_INPUT_ECHO         8   /* print the values back as init does    */
+
+typedef struct relax_input_info {
+    const char *wdir;                /* output directory                      */
+    double x0, y0, rot, oz, ozs;     /* origin, rotation, observation depths  */
+    int npts;                        /* observation points: 3 * npts coords   */
+    const double *pts;               /* in the computational frame            */
+    const char *const *ptsname;      /* 4-character names                     */
+    int nop, nsop;                   /* observation planes, stress segments   */
+    int nwz[4];                      /* weak zones: linear, nonlinear, linear
+                                        and nonlinear transient              */
+    double minlength, minwidth;      /* smallest source dimensions            */
+} relax_input_info;
+
+int relax_input_parse(const char *text, int flags, relax_input **out);
+/* path NULL: standard input */
+int relax_input_read(const char *path, int flags, relax_input **out);
+void relax_input_free(relax_input *in);
+/* owned by the input; valid until relax_input_free */
+const relax_config *relax_input_config(const relax_input *in);
+int relax_input_get_info(const relax_input *in, relax_input_info *info);
+/* weak zones of mechanism 0..3 in the internal convention */
+int relax_input_weakzones(const relax_input *in, int mechanism,
+                          const relax_weakzone **zones, int *n);
+/* builddgammadot0 (src/viscoelastic3d.f90:320-435) of every mechanism with
+ * weak zones, evaluated on `device`; sets the *dgammadot0 fields of the
+ * configuration. */
+int relax_input_build_weakzones(relax_input *in, int device);
 
 /* ------------------------------------------------------------------ */
 /* output files (host code, fed from the device fields)               */
@@ -253,8 +309,9 @@ int relax_write_grd3(const float *c1, const float *c2, const float *c3,
                      double origy, const char *wdir, int index,
                      int convention);
 /* The grids of a context's field: RELAX_FIELD_U at plane int(oz/dx3)
- * (exportgrd, convention 1), RELAX_FIELD_SIG / RELAX_FIELD_EPS at plane
- * fix(oz/dx3) (exportstressgrd, src/export.f90:860-908: 4/5, 6/7). */
+ * (exportgrd, convention 1), RELAX_FIELD_UR there as NNN-relax-*.grd
+ * (convention 2), RELAX_FIELD_SIG / RELAX_FIELD_EPS at plane fix(oz/dx3)
+ * (exportstressgrd, src/export.f90:860-908: 4/5, 6/7). */
 int relax_export_grd(relax_ctx *ctx, int which, double oz, double origx,
                      double origy, const char *wdir, int index);
 /* exportvtk_vectors_legacy / exportvtk_tensors_legacy (src/writevtk.c:72,

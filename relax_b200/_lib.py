@@ -10,8 +10,8 @@ import os
 import re
 import subprocess
 
-from .config import (relax_config, relax_layer, relax_slippatch, relax_step_log, relax_tensor,
-                     relax_tensor_layer)
+from .config import (relax_config, relax_input_info, relax_layer, relax_slippatch, relax_step_log, relax_tensor,
+                     relax_tensor_layer, relax_weakzone)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "librelax_b200.so")
@@ -93,6 +93,14 @@ def load() -> C.CDLL:
         "relax_op_fft3": (I, [P, I, I, I, D, D, D, I, P]),
         "relax_op_tensoramplitude": (I, [P, I, I, I, D, D, D, C.POINTER(D), P]),
         "relax_get_grid": (I, [P, C.POINTER(I), C.POINTER(D)]),
+        "relax_track_relaxation": (I, [P, I, I, I]),
+        "relax_input_parse": (I, [C.c_char_p, I, C.POINTER(P)]),
+        "relax_input_read": (I, [C.c_char_p, I, C.POINTER(P)]),
+        "relax_input_free": (None, [P]),
+        "relax_input_config": (C.POINTER(relax_config), [P]),
+        "relax_input_get_info": (I, [P, C.POINTER(relax_input_info)]),
+        "relax_input_weakzones": (I, [P, I, C.POINTER(C.POINTER(relax_weakzone)), C.POINTER(I)]),
+        "relax_input_build_weakzones": (I, [P, I]),
         "relax_get_plane": (I, [P, I, I, P, S]),
         "relax_get_points": (I, [P, I, C.POINTER(I), C.POINTER(D), C.POINTER(relax_tensor)]),
         "relax_write_grd": (I, [FP, I, I, D, D, D, D, C.c_char_p, C.c_char_p]),

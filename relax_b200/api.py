@@ -19,10 +19,11 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from .config import TENSOR_DTYPE, Simulation, relax_slippatch, relax_step_log, relax_tensor
+from .config import (TENSOR_DTYPE, Simulation, relax_config, relax_input_info, relax_slippatch, relax_step_log,
+                     relax_tensor, relax_weakzone)
 
-FIELDS = {"u": 1, "sig": 2, "tau": 3, "moment": 4, "gamma": 5, "eps": 6}
-NCOMP = {"u": 3, "gamma": 1, "sig": 6, "tau": 6, "moment": 6, "eps": 6}
+FIELDS = {"u": 1, "sig": 2, "tau": 3, "moment": 4, "gamma": 5, "eps": 6, "v": 7, "ur": 8}
+NCOMP = {"u": 3, "gamma": 1, "sig": 6, "tau": 6, "moment": 6, "eps": 6, "v": 3, "ur": 3}
 
 
 def _path(p) -> bytes:
@@ -83,14 +84,85 @@ def shifted_index(x, sx, dx):
     return tuple(v.value for v in i)
 
 
+class Input:
+    """A RELAX input file read by the library (src/input.f90:43-1767).
+
+        inp = Input.parse(open("relax.inp").read(), transient=True)
+        with Relax.from_input(inp) as r:
+            ...
+    """
+
+    def __init__(self, handle):
+        self.lib = _lib.load()
+        self.h = handle
+
+    @classmethod
+    def parse(cls, text: str, transient: bool = False, eigenstrain: bool = False, curvilinear: bool = False,
+              echo: bool = False) -> "Input":
+        lib = _lib.load()
+        flags = (1 if transient else 0) | (2 if eigenstrain else 0) | (4 if curvilinear else 0) | \
+            (8 if echo else 0)
+        h = C.c_void_p()
+        _lib.check(lib.relax_input_parse(text.encode(), flags, C.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.relax_input_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def config(self) -> relax_config:
+        """The relax_config (owned by the input)."""
+        return self.lib.relax_input_config(self.h).contents
+
+    @property
+    def info(self) -> relax_input_info:
+        i = relax_input_info()
+        _lib.check(self.lib.relax_input_get_info(self.h, C.byref(i)))
+        return i
+
+    def weakzones(self, mechanism: int):
+        z = C.POINTER(relax_weakzone)()
+        n = C.c_int()
+        _lib.check(self.lib.relax_input_weakzones(self.h, mechanism, C.byref(z), C.byref(n)))
+        return [z[k] for k in range(n.value)]
+
+    def build_weakzones(self, device: int = 0):
+        _lib.check(self.lib.relax_input_build_weakzones(self.h, device))
+
+    def simulation(self) -> Simulation:
+        """The grid and scalar parameters as a Simulation (array shapes)."""
+        c = self.config
+        return Simulation(sx1=c.sx1, sx2=c.sx2, sx3=c.sx3, dx1=c.dx1, dx2=c.dx2, dx3=c.dx3, beta=c.beta,
+                          nyquist=c.nyquist, lambda_=c.lambda_, mu=c.mu, gam=c.gam, interval=c.interval,
+                          odt=c.odt, tscale=c.tscale)
+
+
 class Relax:
-    def __init__(self, sim: Simulation, device: int = 0):
+    def __init__(self, sim: Simulation, device: int = 0, config: Optional[relax_config] = None, keep=None):
         self.lib = _lib.load()
         self.sim = sim
-        self.cfg, self._keep = sim.to_c(_lib.structure_fn)
+        if config is None:
+            self.cfg, self._keep = sim.to_c(_lib.structure_fn)
+        else:
+            self.cfg, self._keep = config, keep
         h = C.c_void_p()
         _lib.check(self.lib.relax_create(C.byref(self.cfg), device, C.byref(h)))
         self.h = h
+
+    @classmethod
+    def from_input(cls, inp: Input, device: int = 0) -> "Relax":
+        """A context for an input file (weak-zone fields built on `device`)."""
+        if any(inp.info.nwz):
+            inp.build_weakzones(device)
+        return cls(inp.simulation(), device, config=inp.config, keep=inp)
 
     def close(self):
         if getattr(self, "h", None):
@@ -113,6 +185,7 @@ class Relax:
     def coseismic(self, e: int = 0) -> tuple:
         lg = relax_step_log()
         _lib.check(self.lib.relax_coseismic(self.h, e, C.byref(lg)))
+        self.last_log = lg
         return lg.as_tuple()
 
     def step(self, dt: Optional[float] = None) -> tuple:
@@ -173,6 +246,10 @@ class Relax:
         a = np.ascontiguousarray(a)
         _lib.check(self.lib.relax_set_field(self.h, FIELDS[name], a.ctypes.data_as(C.c_void_p),
                                             a.nbytes))
+
+    def track_relaxation(self, vel_planes: int = 0, ur_planes: int = 0, inter_i3: int = -1):
+        """Keep the corrector's velocity and the postseismic displacement (see the header)."""
+        _lib.check(self.lib.relax_track_relaxation(self.h, vel_planes, ur_planes, inter_i3))
 
     def plane(self, name: str, i3: int) -> np.ndarray:
         """Plane i3 of a field as (ncomp, sx2, sx1), unpadded."""

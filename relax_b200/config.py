@@ -91,6 +91,13 @@ class relax_config(C.Structure):
                 ("nltransientdgammadot0", C.POINTER(C.c_float))]
 
 
+class relax_input_info(C.Structure):
+    _fields_ = [("wdir", C.c_char_p)] + [(n, C.c_double) for n in ("x0", "y0", "rot", "oz", "ozs")] + \
+               [("npts", C.c_int), ("pts", C.POINTER(C.c_double)), ("ptsname", C.POINTER(C.c_char_p)),
+                ("nop", C.c_int), ("nsop", C.c_int), ("nwz", C.c_int * 4),
+                ("minlength", C.c_double), ("minwidth", C.c_double)]
+
+
 class relax_step_log(C.Structure):
     _fields_ = [("i", C.c_int), ("event", C.c_int)] + \
                [(n, C.c_double) for n in ("dt", "tm_ve", "tm_pl", "tm_as", "t", "power", "cei",
@@ -379,6 +386,72 @@ class Simulation:
                 cfg.inter.nt = len(self.inter.tensile)
                 cfg.inter.ts = C.cast(tarr, C.POINTER(relax_source))
         return cfg, keep
+
+    def to_input(self, wdir: str = "output", oz: float = 0.0, ozs: float = 0.0,
+                 points: Sequence[Tuple[str, float, float, float]] = ()) -> str:
+        """This deck as a RELAX input file (the order of src/input.f90:43-1767,
+        written with --with-transient sections when the deck has transient
+        interfaces).  Numbers are written with repr, so reading them back
+        gives the same doubles."""
+        r = repr
+        out = ["# grid dimension (sx1,sx2,sx3)", f"{self.sx1} {self.sx2} {self.sx3}",
+               "# sampling (dx1,dx2,dx3), smoothing (beta, nyquist)",
+               f"{r(self.dx1)} {r(self.dx2)} {r(self.dx3)} {r(self.beta)} {r(self.nyquist)}",
+               "# origin position and rotation", f"{r(self.x0)} {r(self.y0)} {r(self.rot)}",
+               "# observation depth (displacement and stress)", f"{r(oz)} {r(ozs)}",
+               "# output directory", wdir,
+               "# elastic parameters and gamma", f"{r(self.lambda_)} {r(self.mu)} {r(self.gam)}",
+               "# integration time, time step or (negative skip, scaling)",
+               f"{r(self.interval)} {r(self.odt)}" + (f" {r(self.tscale)}" if self.odt < 0 else ""),
+               "# number of observation planes", "0",
+               "# number of observation points", str(len(points))]
+        out += [f"{k + 1} {n} {r(x)} {r(y)} {r(z)}" for k, (n, x, y, z) in enumerate(points)]
+        out += ["# number of stress observation segments", "0", "# number of prestress interfaces", "0",
+                "# number of linear viscous interfaces", str(len(self.linear))]
+        out += [f"{k + 1} {r(d)} {r(g)} {r(c[0] if c else 0.0)}" for k, (d, g, *c) in enumerate(self.linear)]
+        if self.linear:
+            out += ["# number of linear weak zones", "0"]
+        out += ["# number of nonlinear viscous interfaces", str(len(self.nonlinear))]
+        out += [f"{k + 1} {r(d)} {r(g)} {r(n)} {r(c)}" for k, (d, g, n, c) in enumerate(self.nonlinear)]
+        if self.nonlinear:
+            out += ["# number of nonlinear weak zones", "0"]
+        if self.ltransient or self.nltransient:
+            out += ["# number of linear transient interfaces", str(len(self.ltransient))]
+            out += [f"{k + 1} {r(d)} {r(g)} {r(gk)}" for k, (d, g, gk) in enumerate(self.ltransient)]
+            if self.ltransient:
+                out += ["# number of transient weak zones", "0"]
+            out += ["# number of nonlinear transient interfaces", str(len(self.nltransient))]
+            out += [f"{k + 1} {r(d)} {r(g)} {r(n)} {r(gk)}" for k, (d, g, n, gk) in enumerate(self.nltransient)]
+            if self.nltransient:
+                out += ["# number of transient weak zones", "0"]
+        out += ["# number of fault creep interfaces", str(len(self.faultcreep))]
+        out += [f"{k + 1} {r(d)} {r(v)} {r(ab)} {r(f)} {r(c)}" for k, (d, v, ab, f, c) in enumerate(self.faultcreep)]
+        if self.faultcreep:
+            out += ["# number of afterslip planes", str(len(self.planes))]
+            out += [f"{k + 1} {r(p.x)} {r(p.y)} {r(p.z)} {r(p.length)} {r(p.width)} {r(p.strike)} {r(p.dip)} "
+                    f"{r(p.rake)}" for k, p in enumerate(self.planes)]
+        inter = self.inter or Event(0.0)
+        out += ["# number of interseismic strike-slip segments", str(len(inter.faults))]
+        out += [f"{k + 1} {r(f.slip)} {r(f.x)} {r(f.y)} {r(f.z)} {r(f.length)} {r(f.width)} {r(f.strike)} "
+                f"{r(f.dip)} {r(f.rake)}" for k, f in enumerate(inter.faults)]
+        out += ["# number of interseismic tensile segments", str(len(inter.tensile))]
+        out += [f"{k + 1} {r(t.opening)} {r(t.x)} {r(t.y)} {r(t.z)} {r(t.length)} {r(t.width)} {r(t.strike)} "
+                f"{r(t.dip)}" for k, t in enumerate(inter.tensile)]
+        out += ["# number of coseismic events", str(len(self.events))]
+        for e, ev in enumerate(self.events):
+            if e > 0:
+                out += ["# time of next event", r(ev.time)]
+            out += ["# number of shear dislocations", str(len(ev.faults))]
+            out += [f"{k + 1} {r(f.slip)} {r(f.x)} {r(f.y)} {r(f.z)} {r(f.length)} {r(f.width)} {r(f.strike)} "
+                    f"{r(f.dip)} {r(f.rake)}" + ("" if f.beta is None else f" {r(f.beta)}")
+                    for k, f in enumerate(ev.faults)]
+            out += ["# number of tensile cracks", str(len(ev.tensile))]
+            out += [f"{k + 1} {r(t.opening)} {r(t.x)} {r(t.y)} {r(t.z)} {r(t.length)} {r(t.width)} "
+                    f"{r(t.strike)} {r(t.dip)}" for k, t in enumerate(ev.tensile)]
+            out += ["# number of dilatation sources", str(len(ev.points))]
+            out += [f"{k + 1} {r(m.amplitude)} {r(m.x)} {r(m.y)} {r(m.z)}" for k, m in enumerate(ev.points)]
+            out += ["# number of surface traction", "0"]
+        return "\n".join(out) + "\n"
 
     # field sizes in the reference layout
     def vec_shape(self, full: bool = False):

@@ -370,15 +370,15 @@ extern "C" int relax_export_grd(relax_ctx *ctx, int which, double oz, double ori
     int rc = relax_get_grid(ctx, sx, dx);
     if (rc != RELAX_OK) return rc;
     const size_t np = (size_t)sx[0] * sx[1];
-    if (which == RELAX_FIELD_U) {
+    if (which == RELAX_FIELD_U || which == RELAX_FIELD_UR) {
         std::vector<float> pl(3 * np);
         rc = relax_get_plane(ctx, which, (int)(oz / dx[2]), pl.data(), pl.size() * sizeof(float));
         if (rc != RELAX_OK) return rc;
         return relax_write_grd3(pl.data(), pl.data() + np, pl.data() + 2 * np, sx[0], sx[1], dx[0], dx[1], origx,
-                                origy, wdir, index, 1);
+                                origy, wdir, index, which == RELAX_FIELD_U ? 1 : 2);
     }
     if (which != RELAX_FIELD_SIG && which != RELAX_FIELD_EPS)
-        return fail(RELAX_ERR_ARG, "grids of field %d: U, SIG or EPS", which);
+        return fail(RELAX_ERR_ARG, "grids of field %d: U, UR, SIG or EPS", which);
     std::vector<float> pl(6 * np);
     rc = relax_get_plane(ctx, which, fix(oz / dx[2]), pl.data(), pl.size() * sizeof(float));
     if (rc != RELAX_OK) return rc;
@@ -408,9 +408,9 @@ extern "C" int relax_write_vtk(const float *const *comp, int ncomp, int sx1, int
                      });
 }
 
-// The same for a context's field (U or a tensor field), read plane by
-// plane; sx3 (<= sx3/2 of the grid) is the depth exported, as the
-// reference's sx3/4 for displacement and sx3/2 for stress.
+// The same for a context's field (U, V, UR or a tensor field), read plane
+// by plane; sx3 (<= sx3/2 of the grid) is the depth exported, as the
+// reference's sx3/4 for displacement and sx3/2 for stress and velocity.
 extern "C" int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int j2, int j3, const char *filename,
                                 const char *title, const char *name)
 {
@@ -422,12 +422,14 @@ extern "C" int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int 
     if (sx3 < 1 || sx3 > sx[2] / 2) return fail(RELAX_ERR_ARG, "vtk depth %d outside [1, %d]", sx3, sx[2] / 2);
     int ncomp;
     switch (which) {
-    case RELAX_FIELD_U: ncomp = 3; break;
+    case RELAX_FIELD_U:
+    case RELAX_FIELD_V:
+    case RELAX_FIELD_UR: ncomp = 3; break;
     case RELAX_FIELD_SIG:
     case RELAX_FIELD_TAU:
     case RELAX_FIELD_MOMENT:
     case RELAX_FIELD_EPS: ncomp = 6; break;
-    default: return fail(RELAX_ERR_ARG, "vtk of field %d: U or a tensor field", which);
+    default: return fail(RELAX_ERR_ARG, "vtk of field %d: U, V, UR or a tensor field", which);
     }
     const size_t np = (size_t)sx[0] * sx[1];
     std::vector<float> pl(ncomp * np);

@@ -1702,6 +1702,8 @@ struct XiArgs {
     const StepState *st;     // coef = cmul * Dt (or cmul when st is null)
     float cmul, scale;
     const struct XiArgs *tab;   // batched launch: one entry per member (blockIdx.z / 3)
+    float *vout[3];          // optional copy of the transformed field (the
+    int vplanes;             // velocity v) for planes i3 < vplanes, pitches rp/pp
 };
 
 __global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
@@ -1732,6 +1734,7 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
         const float2 z = R[line * ls + nn];
         const size_t o = (size_t)i3 * a.pp + (size_t)i2 * a.rp + 2 * nn;
         float w0 = z.x * a.scale, w1 = z.y * a.scale;
+        if (a.vout[c] && i3 < a.vplanes) *reinterpret_cast<float2 *>(a.vout[c] + o) = make_float2(w0, w1);
         if (a.base[c]) {
             w0 = a.base[c][o] + coef * w0;
             w1 = a.base[c][o + 1] + coef * w1;
@@ -1823,6 +1826,7 @@ __global__ void __launch_bounds__(RW *N2) k_xinv_reg(const __grid_constant__ XiA
     const float coef = a.st ? (float)(a.cmul * a.st->Dt) : a.cmul;
     float *out = a.out[c];
     const float *bs = a.base[c];
+    float *vo = i3 < a.vplanes ? a.vout[c] : nullptr;
     constexpr int RV = SX1 / V, ITC = RW * RV / NT;
     static_assert((RW * RV) % NT == 0, "rows split evenly");
 #pragma unroll
@@ -1833,6 +1837,7 @@ __global__ void __launch_bounds__(RW *N2) k_xinv_reg(const __grid_constant__ XiA
         if (V == 4) {
             const float4 w4 = *reinterpret_cast<const float4 *>(row);
             float w[4] = {w4.x * a.scale, w4.y * a.scale, w4.z * a.scale, w4.w * a.scale};
+            if (vo) *reinterpret_cast<float4 *>(vo + o) = make_float4(w[0], w[1], w[2], w[3]);
             if (bs) {
                 const float4 b = __ldg(reinterpret_cast<const float4 *>(bs + o));
                 w[0] = b.x + coef * w[0]; w[1] = b.y + coef * w[1];
@@ -1842,6 +1847,7 @@ __global__ void __launch_bounds__(RW *N2) k_xinv_reg(const __grid_constant__ XiA
         } else {
             const float2 w2 = *reinterpret_cast<const float2 *>(row);
             float w0 = w2.x * a.scale, w1 = w2.y * a.scale;
+            if (vo) *reinterpret_cast<float2 *>(vo + o) = make_float2(w0, w1);
             if (bs) {
                 const float2 b = *reinterpret_cast<const float2 *>(bs + o);
                 w0 = b.x + coef * w0;
@@ -1849,6 +1855,24 @@ __global__ void __launch_bounds__(RW *N2) k_xinv_reg(const __grid_constant__ XiA
             }
             *reinterpret_cast<float2 *>(out + o) = make_float2(w0, w1);
         }
+    }
+}
+
+// postseismic displacement, src/relax.f90:839-850: ur += Dt v over the
+// planes i3 < nur and inter += Dt v in plane i3s (3 components each; v with
+// component stride vstride)
+__global__ void k_relax_accum(const float *v, size_t vstride, float *ur, int nur, float *inter, int i3s,
+                              size_t plane, const StepState *st)
+{
+    const float dt = (float)st->Dt;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t nu = (size_t)nur * plane;
+    if (q < 3 * nu) {
+        const size_t c = q / nu, r = q % nu;
+        ur[q] += dt * v[c * vstride + r];
+    } else if (inter && q - 3 * nu < 3 * plane) {
+        const size_t p = q - 3 * nu, c = p / plane, r = p % plane;
+        inter[p] += dt * v[c * vstride + (size_t)i3s * plane + r];
     }
 }
 

@@ -691,6 +691,11 @@ struct relax_ctx {
     double *amp_part = nullptr, *amp_alt = nullptr;
     int *err = nullptr;
     int nblk = 0, nfr = 0;
+    // optional outputs of the corrector: velocity v (planes < vel_planes),
+    // postseismic displacement sum Dt v (planes < ur_planes, and in urs
+    // plane inter_i3 alone)
+    float *vel = nullptr, *ur = nullptr, *urs = nullptr;
+    int vel_planes = 0, ur_planes = 0, inter_i3 = -1;
 
     // host time-loop state
     double t = 0.0;
@@ -707,7 +712,7 @@ static void free_ctx(relax_ctx *c)
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
     float *fs[] = {c->tau, c->m, c->sig, c->u, c->vp, c->gamma, c->work, c->twork, c->tload, c->spdev,
-                   c->dg0[0], c->dg0[1], c->tm_part, c->fr_part};
+                   c->dg0[0], c->dg0[1], c->tm_part, c->fr_part, c->vel, c->ur, c->urs};
     for (float *p : fs)
         if (p) cudaFree(p);
     if (c->visc[0]) cudaFree(c->visc[0]);
@@ -1515,7 +1520,19 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
         XfArgs xa = xf_div(c);
         xa.tload = loads ? c->tload : nullptr;
         XiArgs xi = xi_update(c, c->u, c->u, 1.0f, true);
+        if (c->vel) {
+            const size_t vs = (size_t)c->vel_planes * g.plane;
+            for (int k = 0; k < 3; k++) xi.vout[k] = c->vel + k * vs;
+            xi.vplanes = c->vel_planes;
+        }
         TRY(c->sp.green(xa, true, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st));
+    }
+    if (c->ur || c->urs) {
+        const size_t n = 3 * (size_t)c->ur_planes * g.plane + (c->urs ? 3 * g.plane : 0);
+        k_relax_accum<<<nblocks(n), RELAX_NTHREADS, 0, c->st>>>(c->vel, (size_t)c->vel_planes * g.plane, c->ur,
+                                                                c->ur_planes, c->urs, c->inter_i3, g.plane,
+                                                                c->dst);
+        CKL();
     }
     // tau += Dt m, sig, next predictor moment; tmin, power and cei reduced by
     // the kernel's last block.  When t + Dt reaches the next event (the test
@@ -1691,9 +1708,24 @@ extern "C" int relax_get_plane(relax_ctx *c, int which, int i3, float *host, siz
     const size_t np = (size_t)g.sx1 * g.sx2;
     const float *src = nullptr;
     int nc = 0;
+    size_t cs = g.nh, off = (size_t)i3 * np;    // component stride, plane offset
     switch (which) {
     case RELAX_FIELD_U: src = c->u; nc = 3; break;
     case RELAX_FIELD_GAMMA: src = c->gamma; nc = 1; break;
+    case RELAX_FIELD_V:
+        if (i3 >= c->vel_planes) return fail(RELAX_ERR_STATE, "velocity of plane %d not kept", i3);
+        src = c->vel; nc = 3; cs = (size_t)c->vel_planes * g.plane;
+        break;
+    case RELAX_FIELD_UR:
+        nc = 3;
+        if (i3 < c->ur_planes) {
+            src = c->ur; cs = (size_t)c->ur_planes * g.plane;
+        } else if (i3 == c->inter_i3) {
+            src = c->urs; cs = g.plane; off = 0;   // the slice buffer holds this plane alone
+        } else {
+            return fail(RELAX_ERR_STATE, "postseismic displacement of plane %d not kept", i3);
+        }
+        break;
     case RELAX_FIELD_SIG:
     case RELAX_FIELD_TAU:
     case RELAX_FIELD_MOMENT:
@@ -1708,7 +1740,7 @@ extern "C" int relax_get_plane(relax_ctx *c, int which, int i3, float *host, siz
     }
     if (bytes != nc * np * sizeof(float)) return fail(RELAX_ERR_ARG, "plane size %zu != %zu", bytes, nc * np * sizeof(float));
     for (int k = 0; k < nc; k++)
-        CK(cudaMemcpyAsync(host + k * np, src + k * g.nh + (size_t)i3 * np, np * sizeof(float),
+        CK(cudaMemcpyAsync(host + k * np, src + k * cs + off, np * sizeof(float),
                            cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return RELAX_OK;
@@ -1759,6 +1791,44 @@ extern "C" int relax_get_points(relax_ctx *c, int n, const int *index, double *u
         sig[p].s11 = o[3]; sig[p].s12 = o[4]; sig[p].s13 = o[5];
         sig[p].s22 = o[6]; sig[p].s23 = o[7]; sig[p].s33 = o[8];
     }
+    return RELAX_OK;
+}
+
+// Keeps the corrector's velocity field v (src/relax.f90:829, the v1..v3
+// of the output block :959-975) for planes i3 < vel_planes, and accumulates
+// the postseismic displacement sum Dt v over planes i3 < ur_planes (u1r..u3r,
+// :846-850) and in plane inter_i3 alone (inter1..inter3, :839-843; -1: off).
+// Every later step writes them; relax_get_plane reads them as RELAX_FIELD_V
+// and RELAX_FIELD_UR.
+extern "C" int relax_track_relaxation(relax_ctx *c, int vel_planes, int ur_planes, int inter_i3)
+{
+    if (!c) return fail(RELAX_ERR_ARG, "null context");
+    const Grid &g = c->g;
+    if (!c->own_dst) return fail(RELAX_ERR_UNSUPPORTED, "batch members do not track the relaxation");
+    if (vel_planes < 0 || vel_planes > g.sx3h || ur_planes < 0 || ur_planes > g.sx3h || inter_i3 < -1 ||
+        inter_i3 >= g.sx3h)
+        return fail(RELAX_ERR_ARG, "planes outside [0, %d]", g.sx3h);
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->st));
+    for (float **p : {&c->vel, &c->ur, &c->urs})
+        if (*p) { cudaFree(*p); *p = nullptr; }
+    const int nv = std::max(std::max(vel_planes, ur_planes), inter_i3 + 1);
+    c->vel_planes = nv;
+    c->ur_planes = ur_planes;
+    c->inter_i3 = inter_i3;
+    if (nv > 0) {
+        TRY(dalloc(&c->vel, 3 * (size_t)nv * g.plane));
+        CK(cudaMemsetAsync(c->vel, 0, 3 * (size_t)nv * g.plane * sizeof(float), c->st));
+    }
+    if (ur_planes > 0) {
+        TRY(dalloc(&c->ur, 3 * (size_t)ur_planes * g.plane));
+        CK(cudaMemsetAsync(c->ur, 0, 3 * (size_t)ur_planes * g.plane * sizeof(float), c->st));
+    }
+    if (inter_i3 >= 0) {
+        TRY(dalloc(&c->urs, 3 * g.plane));
+        CK(cudaMemsetAsync(c->urs, 0, 3 * g.plane * sizeof(float), c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
     return RELAX_OK;
 }
 
