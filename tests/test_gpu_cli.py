@@ -77,6 +77,7 @@ def test_cli_run_matches_the_api(tmp_path):
             if lg.i == 0:
                 break
             want.append(api.format_log(lg, sim.interval))
+            t_last = lg.t
             if lg.output:
                 last_oi = oi
                 oi += 1
@@ -84,7 +85,7 @@ def test_cli_run_matches_the_api(tmp_path):
         ur = rr.plane("ur", 0)
         v = rr.plane("v", 0)
         sig = rr.plane("sig", 2)
-        rr.export_points(np.ctypeslib.as_array(info.pts, (3 * info.npts,)), [n for n, *_ in pts], lg.t,
+        rr.export_points(np.ctypeslib.as_array(info.pts, (3 * info.npts,)), [n for n, *_ in pts], t_last,
                          api_dir, isnew=True)
     assert log_lines == want
     assert oi > 2
