@@ -135,6 +135,12 @@ typedef struct relax_config {
     const relax_layer *nltransientstruc;
     const float *ltransientdgammadot0;
     const float *nltransientdgammadot0;
+    /* origin and rotation of the input file (src/input.f90:238-241).  The
+     * sources of event 0 smaller than nyquist*min(dx) get the space-domain
+     * solution of Okada (1992) added to the coseismic displacement
+     * (dislocations_disp, src/relax.f90:355-360, :1298-1349), which the
+     * reference evaluates with the sources' input-file coordinates. */
+    double x0, y0, rot;
 } relax_config;
 
 /* One line of RELAX's step log (src/relax.f90:1027-1047, format 1100):
@@ -439,6 +445,19 @@ int relax_op_transienteigenstress(double mu, const relax_layer *structure, const
                                   const relax_tensor *epsilonik, int sx1, int sx2, int sx3h,
                                   relax_tensor *moment, relax_tensor *epsilonikdot,
                                   double *maxwelltime, const float *dgammadot0, void *stream);
+
+/* grnfct_okada, src/okada/green_space.f90:114-144: u += the displacement
+ * of n rectangular dislocations in the half-space (Okada, 1992) at the
+ * physical points, u1..u3 (sx1+2, sx2, sx3h) float on the device.  The
+ * sources are in the input-file convention: top-edge reference point
+ * (x = north, y = east, z = depth), strike, dip and rake in degrees, slip
+ * and opening (tensile cracks). */
+int relax_op_okada(const relax_source *sources, int n, double lambda, double mu,
+                   int sx1, int sx2, int sx3h, double dx1, double dx2,
+                   double dx3, float *u1, float *u2, float *u3, void *stream);
+/* The same at one receiver (north, east, depth >= 0), on the host. */
+int relax_okada_point(const relax_source *source, double lambda, double mu,
+                      double x1, double x2, double x3, double *disp);
 
 /* builddgammadot0, src/viscoelastic3d.f90:320-435: the fluidity
  * perturbation of `nz` weak zones (host array) at the physical points,

@@ -1463,6 +1463,199 @@ void orc_traction(double mu, const relax_event *e, int sx1, int sx2, double dx1,
 /* ------------------------------------------------------------------ */
 /* the time loop, src/relax.f90:555-890 + integrationstep :1420-1452    */
 /* ------------------------------------------------------------------ */
+/* ------------------------------------------------------------------ */
+/* Okada (1992), Bull. Seism. Soc. Am. 82(2), 1018-1040: displacement of a
+ * rectangular dislocation in a half-space, the space-domain solution RELAX
+ * adds for small coseismic sources (dislocations_disp, src/relax.f90:
+ * 1298-1349; okada / grnfct_okada, src/okada/green_space.f90:29-144, over
+ * the reference's DC3D, src/okada/dc3d.f).  Restated from the paper's
+ * Table 6: f^A, f^B, f^C per corner, Chinnery's alternating sum over the
+ * corners, the real source (d = c + z) and its image (d = c - z).  FP64.
+ * ------------------------------------------------------------------ */
+typedef struct {
+    double xi, et, q, r, yt, dt, th, lx, le, x11, y11, x32, y32;
+} okc;
+
+static void okada_c(double xi, double et, double q, double sd, double cd, int kx, int ke, okc *c)
+{
+    if (fabs(xi) < 1e-6) xi = 0;
+    if (fabs(et) < 1e-6) et = 0;
+    if (fabs(q) < 1e-6) q = 0;
+    c->xi = xi; c->et = et; c->q = q;
+    c->r = sqrt(xi * xi + et * et + q * q);
+    c->yt = et * cd + q * sd;
+    c->dt = et * sd - q * cd;
+    c->th = q == 0 ? 0 : atan(xi * et / (q * c->r));
+    if (kx) { c->lx = -log(c->r - xi); c->x11 = 0; c->x32 = 0; }
+    else {
+        c->lx = log(c->r + xi);
+        c->x11 = 1 / (c->r * (c->r + xi));
+        c->x32 = (2 * c->r + xi) / (c->r * c->r * c->r * (c->r + xi) * (c->r + xi));
+    }
+    if (ke) { c->le = -log(c->r - et); c->y11 = 0; c->y32 = 0; }
+    else {
+        c->le = log(c->r + et);
+        c->y11 = 1 / (c->r * (c->r + et));
+        c->y32 = (2 * c->r + et) / (c->r * c->r * c->r * (c->r + et) * (c->r + et));
+    }
+}
+
+/* f^A, f^B, f^C of Table 6 for the dislocation (u1, u2, u3) */
+static void okada_f(const okc *c, double z, double al, double sd, double cd, const double U[3], int part,
+                    double f[3])
+{
+    const double a1 = (1 - al) / 2, a2 = al / 2, a3 = (1 - al) / al, a4 = 1 - al;
+    const double xi = c->xi, et = c->et, q = c->q, R = c->r, yt = c->yt, dt = c->dt, th = c->th;
+    f[0] = f[1] = f[2] = 0;
+    if (part == 0) {
+        f[0] = U[0] * (th / 2 + a2 * xi * q * c->y11) + U[1] * (a2 * q / R) +
+               U[2] * (-a1 * c->le - a2 * q * q * c->y11);
+        f[1] = U[0] * (a2 * q / R) + U[1] * (th / 2 + a2 * et * q * c->x11) +
+               U[2] * (-a1 * c->lx - a2 * q * q * c->x11);
+        f[2] = U[0] * (a1 * c->le - a2 * q * q * c->y11) + U[1] * (a1 * c->lx - a2 * q * q * c->x11) +
+               U[2] * (th / 2 - a2 * q * (et * c->x11 + xi * c->y11));
+    } else if (part == 1) {
+        const double Rd = R + dt;
+        double I3, I4;
+        if (cd != 0) {
+            const double X = sqrt(xi * xi + q * q);
+            I4 = xi == 0 ? 0
+                         : sd / cd * xi / Rd +
+                               2 / (cd * cd) * atan((et * (X + q * cd) + X * (R + X) * sd) / (xi * (R + X) * cd));
+            I3 = yt / (cd * Rd) - (c->le - sd * log(Rd)) / (cd * cd);
+        } else {
+            I3 = 0.5 * (et / Rd + yt * q / (Rd * Rd) - c->le);
+            I4 = 0.5 * xi * yt / (Rd * Rd);
+        }
+        const double I1 = -xi / Rd * cd - I4 * sd, I2 = log(Rd) + I3 * sd;
+        f[0] = U[0] * (-xi * q * c->y11 - th - a3 * I1 * sd) + U[1] * (-q / R + a3 * I3 * sd * cd) +
+               U[2] * (q * q * c->y11 - a3 * I3 * sd * sd);
+        f[1] = U[0] * (-q / R + a3 * yt / Rd * sd) + U[1] * (-et * q * c->x11 - th - a3 * xi / Rd * sd * cd) +
+               U[2] * (q * q * c->x11 + a3 * xi / Rd * sd * sd);
+        f[2] = U[0] * (q * q * c->y11 - a3 * I2 * sd) + U[1] * (q * q * c->x11 + a3 * I4 * sd * cd) +
+               U[2] * (q * (et * c->x11 + xi * c->y11) - th - a3 * I4 * sd * sd);
+    } else {
+        const double cb = dt + z, R3 = R * R * R, h = q * cd - z;
+        const double Z32 = sd / R3 - h * c->y32;
+        f[0] = U[0] * (a4 * xi * c->y11 * cd - al * xi * q * Z32) +
+               U[1] * (a4 * cd / R - q * c->y11 * sd - al * cb * q / R3) +
+               U[2] * (-a4 * (sd / R + q * c->y11 * cd) - al * (z * c->y11 - q * q * Z32));
+        f[1] = U[0] * (a4 * (cd / R + 2 * q * c->y11 * sd) - al * cb * q / R3) +
+               U[1] * (a4 * yt * c->x11 - al * cb * et * q * c->x32) +
+               U[2] * (a4 * 2 * xi * c->y11 * sd + dt * c->x11 - al * cb * (c->x11 - q * q * c->x32));
+        f[2] = U[0] * (a4 * q * c->y11 * cd - al * (cb * et / R3 - z * c->y11 + xi * xi * Z32)) +
+               U[1] * (-dt * c->x11 - xi * c->y11 * sd - al * cb * (c->x11 - q * q * c->x32)) +
+               U[2] * (a4 * (yt * c->x11 + xi * c->y11 * cd) + al * q * (cb * et * c->x32 + xi * Z32));
+    }
+}
+
+/* displacement at (x, y, z <= 0) in the fault frame; 0, or 1 on a fault edge */
+static int okada_dc(double al, double x, double y, double z, double c0, double dipd, double L, double W,
+                    const double U[3], double u[3])
+{
+    double sd = sin(dipd * 0.01745329251994329547437168059786927);
+    double cd = cos(dipd * 0.01745329251994329547437168059786927);
+    if (fabs(cd) < 1e-6) { cd = 0; sd = sd > 0 ? 1 : -1; }
+    double xi[2] = {x, x - L};
+    for (int i = 0; i < 2; i++) if (fabs(xi[i]) < 1e-6) xi[i] = 0;
+    u[0] = u[1] = u[2] = 0;
+    for (int img = 0; img < 2; img++) {
+        const double d = img ? c0 - z : c0 + z;
+        const double p = y * cd + d * sd;
+        double q = y * sd - d * cd;
+        double et[2] = {p + W, p};
+        if (fabs(q) < 1e-6) q = 0;
+        for (int i = 0; i < 2; i++) if (fabs(et[i]) < 1e-6) et[i] = 0;
+        if (q == 0 && ((xi[0] * xi[1] <= 0 && et[0] * et[1] == 0) || (et[0] * et[1] <= 0 && xi[0] * xi[1] == 0))) {
+            u[0] = u[1] = u[2] = 0;
+            return 1;
+        }
+        int kx[2] = {0, 0}, ke[2] = {0, 0};
+        if (xi[0] < 0 && sqrt(xi[1] * xi[1] + et[0] * et[0] + q * q) + xi[1] < 1e-6) kx[0] = 1;
+        if (xi[0] < 0 && sqrt(xi[1] * xi[1] + et[1] * et[1] + q * q) + xi[1] < 1e-6) kx[1] = 1;
+        if (et[0] < 0 && sqrt(xi[0] * xi[0] + et[1] * et[1] + q * q) + et[1] < 1e-6) ke[0] = 1;
+        if (et[0] < 0 && sqrt(xi[1] * xi[1] + et[1] * et[1] + q * q) + et[1] < 1e-6) ke[1] = 1;
+        for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+                okc c;
+                okada_c(xi[i], et[j], q, sd, cd, kx[j], ke[i], &c);
+                if (c.r == 0) continue;
+                double w[3], fa[3];
+                okada_f(&c, z, al, sd, cd, U, 0, fa);
+                if (!img) {
+                    w[0] = -fa[0];
+                    w[1] = -fa[1] * cd + fa[2] * sd;
+                    w[2] = -fa[1] * sd - fa[2] * cd;
+                } else {
+                    double fb[3], fc[3];
+                    okada_f(&c, z, al, sd, cd, U, 1, fb);
+                    okada_f(&c, z, al, sd, cd, U, 2, fc);
+                    w[0] = fa[0] + fb[0] + z * fc[0];
+                    w[1] = (fa[1] + fb[1] + z * fc[1]) * cd - (fa[2] + fb[2] + z * fc[2]) * sd;
+                    w[2] = (fa[1] + fb[1] - z * fc[1]) * sd + (fa[2] + fb[2] - z * fc[2]) * cd;
+                }
+                const double sg = (i + j) % 2 ? -1.0 : 1.0;
+                for (int k = 0; k < 3; k++) u[k] += sg * w[k] / (2 * M_PI);
+            }
+    }
+    return 0;
+}
+
+/* okada, src/okada/green_space.f90:29-105: source in the input convention
+ * (north, east, depth of the top edge; degrees), receiver (north, east,
+ * depth); displacement with x3 down */
+void orc_okada(double lambda, double mu, double slip, double opening, double x1, double x2, double x3, double width,
+               double length, double strike, double dip, double rake, double xr, double yr, double zr, double *d)
+{
+    const double rad = 0.01745329251994329547437168059786927;
+    const double cs = cos(strike * rad), ss = sin(strike * rad);
+    const double U[3] = {slip * cos(rake * rad), slip * sin(rake * rad), opening};
+    double u[3];
+    if (okada_dc((lambda + mu) / (lambda + 2 * mu), (xr - x1) * cs + (yr - x2) * ss, (xr - x1) * ss - (yr - x2) * cs,
+                 -zr, x3, dip, length, width, U, u)) {
+        d[0] = d[1] = d[2] = 0;
+        return;
+    }
+    d[0] = u[0] * cs + u[1] * ss;
+    d[1] = u[0] * ss - u[1] * cs;
+    d[2] = -u[2];
+}
+
+/* grnfct_okada, src/okada/green_space.f90:114-144, into the padded v */
+static void grnfct_okada(double lambda, double mu, double slip, double opening, double x, double y, double z,
+                         double width, double length, double strike, double dip, double rake, int sx1, int sx2,
+                         int sx3h, double dx1, double dx2, double dx3, real *u1, real *u2, real *u3)
+{
+#pragma omp parallel for schedule(static)
+    for (int i3 = 0; i3 < sx3h; i3++)
+        for (int i2 = 0; i2 < sx2; i2++)
+            for (int i1 = 0; i1 < sx1; i1++) {
+                const double x1 = (i1 < sx1 / 2 ? i1 : i1 - sx1) * dx1, x2 = (i2 < sx2 / 2 ? i2 : i2 - sx2) * dx2;
+                double d[3];
+                orc_okada(lambda, mu, slip, opening, x, y, z, width, length, strike, dip, rake, x1, x2, i3 * dx3, d);
+                const size_t o = (size_t)i1 + (size_t)(sx1 + 2) * (i2 + (size_t)sx2 * i3);
+                u1[o] += (real)d[0];
+                u2[o] += (real)d[1];
+                u3[o] += (real)d[2];
+            }
+}
+
+/* the input-file form of a configured source: wangconvention and the
+ * rotation (src/input.f90:1780-1822) undone */
+static void input_form(const relax_config *c, const relax_source *s, double *x, double *y, double *z,
+                       double *strike, double *dip, double *rake)
+{
+    const double rad = 0.01745329251994329547437168059786927;
+    const double st = s->strike - c->rot * rad, a = -c->rot * rad;
+    const double xx = s->x * cos(a) + s->y * sin(a), yy = -s->x * sin(a) + s->y * cos(a);
+    *x = xx + c->x0 + s->length / 2 * sin(st) - s->width / 2 * sin(s->dip) * cos(st);
+    *y = yy + c->y0 + s->length / 2 * cos(st) + s->width / 2 * sin(s->dip) * sin(st);
+    *z = s->z - s->width / 2 * cos(s->dip);
+    *strike = -90 - st / rad;
+    *dip = 90 - s->dip / rad;
+    *rake = s->rake / rad;
+}
+
 typedef struct orc_state {
     relax_config cfg;
     int sx1, sx2, sx3, sx3h;
@@ -1659,6 +1852,21 @@ int orc_coseismic(orc_state *S, relax_step_log *log)
     const relax_event *ev = &c->events[0];
     if (ev->nt || ev->ns || ev->nm || ev->nl) {
         if ((err = green(S))) return err;
+        /* dislocations_disp: the sources smaller than the Nyquist length
+         * (src/relax.f90:355-360, :1320-1347) */
+        double mind = c->dx1 < c->dx2 ? c->dx1 : c->dx2;
+        if (c->dx3 < mind) mind = c->dx3;
+        const double small = c->nyquist * mind;
+        for (int i = 0; i < ev->ns + ev->nt; i++) {
+            const int tens = i >= ev->ns;
+            const relax_source *s = tens ? &ev->ts[i - ev->ns] : &ev->s[i];
+            if (!(small >= s->length || small >= s->width)) continue;
+            double x, y, z, strike, dip, rake;
+            input_form(c, s, &x, &y, &z, &strike, &dip, &rake);
+            grnfct_okada(c->lambda, c->mu, tens ? 0.0 : -s->slip, tens ? s->opening : 0.0, x, y, z, s->width,
+                         s->length, strike, dip, tens ? 0.0 : rake, S->sx1, S->sx2, S->sx3h, c->dx1, c->dx2, c->dx3,
+                         S->v[0], S->v[1], S->v[2]);
+        }
     }
     for (int k = 0; k < 3; k++) memcpy(S->u[k], S->v[k], sizeof(real) * S->nu);
     orc_tensorfieldadd(S->sig, S->tau, S->nt, 1, 0, 1, -1);

@@ -10,8 +10,8 @@ import os
 import re
 import subprocess
 
-from .config import (relax_config, relax_input_info, relax_layer, relax_slippatch, relax_step_log, relax_tensor,
-                     relax_tensor_layer, relax_weakzone)
+from .config import (relax_config, relax_input_info, relax_layer, relax_slippatch, relax_source, relax_step_log,
+                     relax_tensor, relax_tensor_layer, relax_weakzone)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "librelax_b200.so")
@@ -93,6 +93,8 @@ def load() -> C.CDLL:
         "relax_op_fft3": (I, [P, I, I, I, D, D, D, I, P]),
         "relax_op_tensoramplitude": (I, [P, I, I, I, D, D, D, C.POINTER(D), P]),
         "relax_get_grid": (I, [P, C.POINTER(I), C.POINTER(D)]),
+        "relax_op_okada": (I, [P, I, D, D, I, I, I, D, D, D, P, P, P, P]),
+        "relax_okada_point": (I, [C.POINTER(relax_source), D, D, D, D, D, C.POINTER(D)]),
         "relax_track_relaxation": (I, [P, I, I, I]),
         "relax_input_parse": (I, [C.c_char_p, I, C.POINTER(P)]),
         "relax_input_read": (I, [C.c_char_p, I, C.POINTER(P)]),

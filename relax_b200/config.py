@@ -88,7 +88,8 @@ class relax_config(C.Structure):
                 ("ltransientstruc", C.POINTER(relax_layer)),
                 ("nltransientstruc", C.POINTER(relax_layer)),
                 ("ltransientdgammadot0", C.POINTER(C.c_float)),
-                ("nltransientdgammadot0", C.POINTER(C.c_float))]
+                ("nltransientdgammadot0", C.POINTER(C.c_float)),
+                ("x0", C.c_double), ("y0", C.c_double), ("rot", C.c_double)]
 
 
 class relax_input_info(C.Structure):
@@ -292,6 +293,7 @@ class Simulation:
         cfg.interval, cfg.tscale = self.interval, self.tscale
         cfg.odt = self.odt
         cfg.skip = self.skip
+        cfg.x0, cfg.y0, cfg.rot = self.x0, self.y0, self.rot
         lin, non, fc = self.layer_lists()
         lt, nlt = self.transient_lists()
         for name, lst in (("linearstruc", lin), ("nonlinearstruc", non),

@@ -906,6 +906,7 @@ int finish(relax_input &in)
     c.inter = relax_event{};
     c.inter.ns = (int)in.is.size(); c.inter.s = in.is.empty() ? nullptr : in.is.data();
     c.inter.nt = (int)in.its.size(); c.inter.ts = in.its.empty() ? nullptr : in.its.data();
+    c.x0 = in.x0; c.y0 = in.y0; c.rot = in.rot;
     c.lineardgammadot0 = c.nonlineardgammadot0 = nullptr;
     c.ltransientdgammadot0 = c.nltransientdgammadot0 = nullptr;
     in.ptsname_c.clear();

@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "okada.cuh"
 
 using namespace relax;
 
@@ -1126,6 +1127,89 @@ static int event_sources(relax_ctx *c, const EventCopy &ev, bool *any, bool *ful
     return RELAX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// space-domain solution of the small coseismic sources (dislocations_disp,
+// src/relax.f90:1298-1349; grnfct_okada, src/okada/green_space.f90:114-144)
+// ---------------------------------------------------------------------------
+// one thread per physical grid point, all sources in turn; u in rows of
+// pitch rp and planes of pitch pp
+__global__ void k_okada(Grid g, const relax_source *src, int n, double lambda, double mu, float *u1, float *u2,
+                        float *u3, size_t rp, size_t pp)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1);
+    const size_t r = q / g.sx1;
+    const int i2 = (int)(r % g.sx2), i3 = (int)(r / g.sx2);
+    // shiftedcoordinates, src/elastic3d.f90:4027-4048
+    const double x1 = (double)(i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (double)(i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = (double)i3 * g.dx3;
+    const size_t o = (size_t)i3 * pp + (size_t)i2 * rp + i1;
+    float a0 = u1[o], a1 = u2[o], a2 = u3[o];
+    for (int k = 0; k < n; k++) {
+        const relax_source &s = src[k];
+        double d[3];
+        okada_relax(lambda, mu, s.slip, s.opening, s.x, s.y, s.z, s.width, s.length, s.strike, s.dip, s.rake, x1,
+                    x2, x3, d);
+        a0 += (float)d[0];
+        a1 += (float)d[1];
+        a2 += (float)d[2];
+    }
+    u1[o] = a0;
+    u2[o] = a1;
+    u3[o] = a2;
+}
+
+// A source of the configuration (after wangconvention and the rotation,
+// src/input.f90:1780-1822) back in the input-file convention that the
+// space-domain solution is evaluated in.
+static relax_source input_convention(const relax_source &s, const relax_config &cfg, bool tensile)
+{
+    const double deg = 0.01745329251994329547437168059786927;
+    const double strike = s.strike - cfg.rot * deg, dip = s.dip;
+    const double a = -cfg.rot * deg;
+    const double xx = +s.x * cos(a) + s.y * sin(a), yy = -s.x * sin(a) + s.y * cos(a);
+    relax_source o{};
+    o.x = xx + cfg.x0 + s.length / 2.0 * sin(strike) - s.width / 2.0 * sin(dip) * cos(strike);
+    o.y = yy + cfg.y0 + s.length / 2.0 * cos(strike) + s.width / 2.0 * sin(dip) * sin(strike);
+    o.z = s.z - s.width / 2.0 * cos(dip);
+    o.width = s.width;
+    o.length = s.length;
+    o.strike = -90.0 - strike / deg;
+    o.dip = 90.0 - dip / deg;
+    o.rake = tensile ? 0.0 : s.rake / deg;
+    o.slip = tensile ? 0.0 : -s.slip;
+    o.opening = tensile ? s.opening : 0.0;
+    return o;
+}
+
+// u += the space-domain solution of event 0's sources no longer than
+// nyquist * min(dx) along strike or dip (src/relax.f90:1320-1347)
+static int event_okada(relax_ctx *c, const EventCopy &ev)
+{
+    const Grid &g = c->g;
+    const double small = c->cfg.nyquist * std::min(std::min(g.dx1, g.dx2), g.dx3);
+    std::vector<relax_source> h;
+    for (const auto &s : ev.s)
+        if (small >= s.length || small >= s.width) h.push_back(input_convention(s, c->cfg, false));
+    for (const auto &s : ev.ts)
+        if (small >= s.length || small >= s.width) h.push_back(input_convention(s, c->cfg, true));
+    if (h.empty()) return RELAX_OK;
+    relax_source *d = nullptr;
+    TRY(dalloc(&d, h.size()));
+    cudaError_t e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(relax_source), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) {
+        k_okada<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(g, d, (int)h.size(), c->cfg.lambda, c->cfg.mu, c->u,
+                                                             c->u + g.nh, c->u + 2 * g.nh, g.sx1, g.plane);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "okada: %s", cudaGetErrorString(e));
+    return RELAX_OK;
+}
+
 // the coseismic Green's function of c->work (the whole box when `full`,
 // else its physical half), u += the displacement
 static int event_green(relax_ctx *c, bool loads, bool full)
@@ -1356,6 +1440,7 @@ extern "C" int relax_coseismic(relax_ctx *c, int e, relax_step_log *log0)
     TRY(event_sources(c, c->events[e], &any, &full));
     TRY(upload_loads(c, c->events[e], c->t, 0.0, false, &loads));
     if (any) TRY(event_green(c, loads, full));
+    if (e == 0) TRY(event_okada(c, c->events[0]));
     TRY(tail_init(c));
     CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -2043,6 +2128,36 @@ extern "C" int relax_op_dgammadot0(const relax_weakzone *zones, int nz, int sx1,
     if (nz > 0) CK(cudaMemcpyAsync(zd, zones, nz * sizeof(relax_weakzone), cudaMemcpyHostToDevice, st));
     k_dgammadot0<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(g, zd, nz, beta, out);
     CKL();
+    return RELAX_OK;
+}
+
+extern "C" int relax_op_okada(const relax_source *sources, int n, double lambda, double mu, int sx1, int sx2,
+                              int sx3h, double dx1, double dx2, double dx3, float *u1, float *u2, float *u3,
+                              void *stream)
+{
+    if (n < 0 || (n > 0 && !sources) || !u1 || !u2 || !u3) return fail(RELAX_ERR_ARG, "null argument");
+    if (sx1 < 2 || sx2 < 2 || sx3h < 1) return fail(RELAX_ERR_ARG, "grid");
+    if (n == 0) return RELAX_OK;
+    Grid g{};
+    g.sx1 = sx1; g.sx2 = sx2; g.sx3 = 2 * sx3h; g.sx3h = sx3h; g.dx1 = dx1; g.dx2 = dx2; g.dx3 = dx3;
+    g.plane = (size_t)sx1 * sx2; g.nh = g.plane * sx3h;
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch sc(st);
+    relax_source *d = nullptr;
+    TRY(sc.get(&d, (size_t)n));
+    CK(cudaMemcpyAsync(d, sources, n * sizeof(relax_source), cudaMemcpyHostToDevice, st));
+    const size_t rp = (size_t)sx1 + 2;
+    k_okada<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(g, d, n, lambda, mu, u1, u2, u3, rp, rp * sx2);
+    CKL();
+    return RELAX_OK;
+}
+
+extern "C" int relax_okada_point(const relax_source *s, double lambda, double mu, double x1, double x2, double x3,
+                                 double *disp)
+{
+    if (!s || !disp) return fail(RELAX_ERR_ARG, "null argument");
+    okada_relax(lambda, mu, s->slip, s->opening, s->x, s->y, s->z, s->width, s->length, s->strike, s->dip, s->rake,
+                x1, x2, x3, disp);
     return RELAX_OK;
 }
 

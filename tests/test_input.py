@@ -32,7 +32,7 @@ def _layers_eq(a, b, nz, what):
 
 def compare(got, want, nz):
     for f in ("sx1", "sx2", "sx3", "dx1", "dx2", "dx3", "beta", "nyquist", "lambda_", "mu", "gam", "interval",
-              "odt", "skip", "np", "ne"):
+              "odt", "skip", "np", "ne", "x0", "y0", "rot"):
         assert getattr(got, f) == getattr(want, f), f
     if want.skip:
         assert got.tscale == want.tscale
