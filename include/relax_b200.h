@@ -355,6 +355,16 @@ const char *relax_ned_header(void);
 /* Fortran ESw.dEe of one value. */
 int relax_es_format(double v, int w, int d, int e, char *buf, size_t size);
 
+/* Checkpoint (no counterpart in the reference, which cannot restart a
+ * run): relax_checkpoint_save writes the state a step reads -- u, tau,
+ * moment, sig, gamma, the transient strain, the afterslip patches, the
+ * tracked relaxation fields, time, counters and the step state -- to a raw
+ * file with a checksum; relax_checkpoint_load restores it into a context
+ * created from the same configuration (and the same
+ * relax_track_relaxation), which then continues bit for bit. */
+int relax_checkpoint_save(relax_ctx *ctx, const char *path);
+int relax_checkpoint_load(relax_ctx *ctx, const char *path);
+
 /* Waits for the context's stream. */
 int relax_synchronize(relax_ctx *ctx);
 

@@ -93,6 +93,8 @@ def load() -> C.CDLL:
         "relax_op_fft3": (I, [P, I, I, I, D, D, D, I, P]),
         "relax_op_tensoramplitude": (I, [P, I, I, I, D, D, D, C.POINTER(D), P]),
         "relax_get_grid": (I, [P, C.POINTER(I), C.POINTER(D)]),
+        "relax_checkpoint_save": (I, [P, C.c_char_p]),
+        "relax_checkpoint_load": (I, [P, C.c_char_p]),
         "relax_op_okada": (I, [P, I, D, D, I, I, I, D, D, D, P, P, P, P]),
         "relax_okada_point": (I, [C.POINTER(relax_source), D, D, D, D, D, C.POINTER(D)]),
         "relax_track_relaxation": (I, [P, I, I, I]),

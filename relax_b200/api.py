@@ -247,6 +247,14 @@ class Relax:
         _lib.check(self.lib.relax_set_field(self.h, FIELDS[name], a.ctypes.data_as(C.c_void_p),
                                             a.nbytes))
 
+    def save(self, path):
+        """Checkpoint of the state between steps (relax_checkpoint_save)."""
+        _lib.check(self.lib.relax_checkpoint_save(self.h, _path(path)))
+
+    def load(self, path):
+        """Restores a checkpoint written by a context of the same configuration."""
+        _lib.check(self.lib.relax_checkpoint_load(self.h, _path(path)))
+
     def track_relaxation(self, vel_planes: int = 0, ur_planes: int = 0, inter_i3: int = -1):
         """Keep the corrector's velocity and the postseismic displacement (see the header)."""
         _lib.check(self.lib.relax_track_relaxation(self.h, vel_planes, ur_planes, inter_i3))

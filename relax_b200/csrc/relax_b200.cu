@@ -1937,6 +1937,161 @@ extern "C" int relax_get_patches(relax_ctx *c, int k, relax_slippatch *host, siz
 }
 
 // ---------------------------------------------------------------------------
+// checkpoint: the state a step reads, to a raw file and back
+// ---------------------------------------------------------------------------
+namespace ckpt {
+
+const char MAGIC[8] = {'R', 'L', 'X', 'C', 'K', 'P', 'T', '1'};
+
+struct Header {
+    char magic[8];
+    int sx1, sx2, sx3, npatch;
+    int has_eps, vel_planes, ur_planes, inter_i3;
+    double t;
+    int i, e, oi, cos_done, m_valid, sig_valid;
+    StepState st;
+    unsigned long long payload_bytes, checksum;
+};
+
+struct Block {
+    void *d;
+    size_t bytes;
+};
+
+// FNV-1a over the payload, in the order written
+inline void fnv(unsigned long long &h, const unsigned char *p, size_t n)
+{
+    for (size_t k = 0; k < n; k++) {
+        h ^= p[k];
+        h *= 1099511628211ull;
+    }
+}
+
+std::vector<Block> blocks(relax_ctx *c, int npatch)
+{
+    const Grid &g = c->g;
+    std::vector<Block> b = {{c->u, 3 * g.nh * sizeof(float)},   {c->tau, 6 * g.nh * sizeof(float)},
+                            {c->m, 6 * g.nh * sizeof(float)},   {c->sig, 6 * g.nh * sizeof(float)},
+                            {c->gamma, g.nh * sizeof(float)}};
+    if (c->eps) b.push_back({c->eps, 6 * g.nh * sizeof(float)});
+    if (c->epsdot) b.push_back({c->epsdot, 6 * g.nh * sizeof(float)});
+    if (npatch > 0) b.push_back({c->patch, (size_t)npatch * sizeof(relax_slippatch)});
+    if (c->vel) b.push_back({c->vel, 3 * (size_t)c->vel_planes * g.plane * sizeof(float)});
+    if (c->ur) b.push_back({c->ur, 3 * (size_t)c->ur_planes * g.plane * sizeof(float)});
+    if (c->urs) b.push_back({c->urs, 3 * g.plane * sizeof(float)});
+    return b;
+}
+
+int npatch(const relax_ctx *c)
+{
+    int n = 0;
+    for (const auto &p : c->planes) n += std::max(0, p.px2) * std::max(0, p.px3);
+    return n;
+}
+
+}  // namespace ckpt
+
+// Writes the state of a context between steps (displacement, stress,
+// moment, prestress, afterslip history, transient strain, slip patches,
+// the tracked relaxation fields, time, counters and the step state) to a
+// raw file.  RELAX has no restart (its output files cannot restart a run);
+// a context created from the same configuration and given the file with
+// relax_checkpoint_load continues bit for bit.
+extern "C" int relax_checkpoint_save(relax_ctx *c, const char *path)
+{
+    if (!c || !path) return fail(RELAX_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->device));
+    if (c->cos_done && !c->m_valid) TRY(tail_init(c));
+    CK(cudaMemcpyAsync(c->hst, c->dst, sizeof(StepState), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    ckpt::Header h{};
+    memcpy(h.magic, ckpt::MAGIC, 8);
+    h.sx1 = c->g.sx1; h.sx2 = c->g.sx2; h.sx3 = c->g.sx3;
+    h.npatch = ckpt::npatch(c);
+    h.has_eps = c->eps ? 1 : 0;
+    h.vel_planes = c->vel ? c->vel_planes : 0;
+    h.ur_planes = c->ur ? c->ur_planes : 0;
+    h.inter_i3 = c->urs ? c->inter_i3 : -1;
+    h.t = c->t; h.i = c->i; h.e = c->e; h.oi = c->oi;
+    h.cos_done = c->cos_done; h.m_valid = c->m_valid; h.sig_valid = c->sig_valid;
+    h.st = *c->hst;
+    const std::vector<ckpt::Block> bl = ckpt::blocks(c, h.npatch);
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return fail(RELAX_ERR_ARG, "cannot open %s for writing", path);
+    // header first (rewritten with the checksum at the end)
+    bool ok = fwrite(&h, sizeof h, 1, fp) == 1;
+    unsigned long long sum = 1469598103934665603ull, total = 0;
+    std::vector<unsigned char> buf;
+    for (const auto &b : bl) {
+        if (!ok) break;
+        buf.resize(b.bytes);
+        if (cudaMemcpy(buf.data(), b.d, b.bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            fclose(fp);
+            return fail(RELAX_ERR_CUDA, "checkpoint: device copy failed");
+        }
+        ckpt::fnv(sum, buf.data(), b.bytes);
+        total += b.bytes;
+        ok = fwrite(buf.data(), 1, b.bytes, fp) == b.bytes;
+    }
+    h.payload_bytes = total;
+    h.checksum = sum;
+    if (ok) ok = fseek(fp, 0, SEEK_SET) == 0 && fwrite(&h, sizeof h, 1, fp) == 1;
+    if (fclose(fp) != 0) ok = false;
+    if (!ok) return fail(RELAX_ERR_ARG, "writing %s failed", path);
+    return RELAX_OK;
+}
+
+// Restores a checkpoint into a context created from the same configuration
+// (grid, mechanisms, afterslip planes) and with the same tracking of the
+// relaxation fields.  The file's checksum is verified before the state is
+// replaced.
+extern "C" int relax_checkpoint_load(relax_ctx *c, const char *path)
+{
+    if (!c || !path) return fail(RELAX_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->device));
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return fail(RELAX_ERR_ARG, "cannot open %s", path);
+    ckpt::Header h{};
+    if (fread(&h, sizeof h, 1, fp) != 1 || memcmp(h.magic, ckpt::MAGIC, 8) != 0) {
+        fclose(fp);
+        return fail(RELAX_ERR_ARG, "%s is not a checkpoint", path);
+    }
+    const int npatch = ckpt::npatch(c);
+    if (h.sx1 != c->g.sx1 || h.sx2 != c->g.sx2 || h.sx3 != c->g.sx3 || h.npatch != npatch ||
+        h.has_eps != (c->eps ? 1 : 0) || h.vel_planes != (c->vel ? c->vel_planes : 0) ||
+        h.ur_planes != (c->ur ? c->ur_planes : 0) || h.inter_i3 != (c->urs ? c->inter_i3 : -1)) {
+        fclose(fp);
+        return fail(RELAX_ERR_STATE, "checkpoint %s does not match this context (grid %dx%dx%d, %d patches)", path,
+                    h.sx1, h.sx2, h.sx3, h.npatch);
+    }
+    const std::vector<ckpt::Block> bl = ckpt::blocks(c, npatch);
+    std::vector<std::vector<unsigned char>> data(bl.size());
+    unsigned long long sum = 1469598103934665603ull, total = 0;
+    bool ok = true;
+    for (size_t k = 0; k < bl.size() && ok; k++) {
+        data[k].resize(bl[k].bytes);
+        ok = fread(data[k].data(), 1, bl[k].bytes, fp) == bl[k].bytes;
+        if (ok) ckpt::fnv(sum, data[k].data(), bl[k].bytes);
+        total += bl[k].bytes;
+    }
+    unsigned char extra;
+    if (ok && fread(&extra, 1, 1, fp) == 1) ok = false;
+    fclose(fp);
+    if (!ok || total != h.payload_bytes || sum != h.checksum)
+        return fail(RELAX_ERR_ARG, "checkpoint %s is truncated or corrupt", path);
+    CK(cudaStreamSynchronize(c->st));
+    for (size_t k = 0; k < bl.size(); k++)
+        CK(cudaMemcpy(bl[k].d, data[k].data(), bl[k].bytes, cudaMemcpyHostToDevice));
+    *c->hst = h.st;
+    CK(cudaMemcpy(c->dst, c->hst, sizeof(StepState), cudaMemcpyHostToDevice));
+    c->t = h.t; c->i = h.i; c->e = h.e; c->oi = h.oi;
+    c->cos_done = h.cos_done != 0;
+    c->m_valid = h.m_valid != 0;
+    c->sig_valid = h.sig_valid != 0;
+    return RELAX_OK;
+}
+
+// ---------------------------------------------------------------------------
 // stateless operators on device buffers in the reference layout
 // ---------------------------------------------------------------------------
 struct Scratch {
