@@ -157,6 +157,41 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const 
         else if (i3 == g.sx3h - 1) { rzm = idx - g.plane; rzp = idx; kz = a.k3b; }
         else { rzm = idx - g.plane; rzp = idx + g.plane; kz = a.k3; }
 
+        // END: tau += Dt m first, with every load of tau and m issued before
+        // the stores of tau (which could alias them), so that the kernel waits
+        // for memory once here and once for the strain source below
+        float tn[6][4];
+        if (MODE == MODE_END) {
+            const float dt = (float)a.st->Dt;
+            float4 tv[6], mv[6];
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                tv[c] = ldc4(a.tau + c * nh + idx);
+                mv[c] = ldc4(a.m + c * nh + idx);
+            }
+            constexpr float wn[6] = {1.f, 2.f, 2.f, 1.f, 2.f, 1.f};
+            float qm[4], qt[4];
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const float m4[4] = {mv[c].x, mv[c].y, mv[c].z, mv[c].w};
+                const float t4[4] = {tv[c].x, tv[c].y, tv[c].z, tv[c].w};
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    tn[c][j] = t4[j] + dt * m4[j];
+                    qm[j] = c == 0 ? m4[j] * m4[j] : qm[j] + wn[c] * m4[j] * m4[j];
+                    qt[j] = c == 0 ? tn[c][j] * tn[c][j] : qt[j] + wn[c] * tn[c][j] * tn[c][j];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 6; c++)
+                st4(a.tau + c * nh + idx, make_float4(tn[c][0], tn[c][1], tn[c][2], tn[c][3]));
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                amp_m += (double)sqrtf(qm[j] * 0.5f);
+                amp_t += (double)sqrtf(qt[j] * 0.5f);
+            }
+        }
+
         // Hooke's law (src/elastic3d.f90:129-142) on the strain of w at 4
         // points; h = C:E is added to the base stress below
         float h[6][4];
@@ -231,27 +266,10 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const 
 #pragma unroll
             for (int j = 0; j < 4; j++) amp_t += (double)sqrtf(qt[j] * 0.5f);
         } else if (MODE == MODE_END) {
-            const float dt = (float)a.st->Dt;
-            float qm[4], qt[4];
 #pragma unroll
-            for (int c = 0; c < 6; c++) {
-                const float4 t = ldc4(a.tau + c * nh + idx);
-                const float4 m = ldc4(a.m + c * nh + idx);
-                const float mv[4] = {m.x, m.y, m.z, m.w};
-                const float tn[4] = {t.x + dt * m.x, t.y + dt * m.y, t.z + dt * m.z, t.w + dt * m.w};
-                st4(a.tau + c * nh + idx, make_float4(tn[0], tn[1], tn[2], tn[3]));
+            for (int c = 0; c < 6; c++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    qm[j] = c == 0 ? mv[j] * mv[j] : qm[j] + wnorm[c] * mv[j] * mv[j];
-                    qt[j] = c == 0 ? tn[j] * tn[j] : qt[j] + wnorm[c] * tn[j] * tn[j];
-                    s[c][j] = -tn[j] + h[c][j];
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                amp_m += (double)sqrtf(qm[j] * 0.5f);
-                amp_t += (double)sqrtf(qt[j] * 0.5f);
-            }
+                for (int j = 0; j < 4; j++) s[c][j] = -tn[c][j] + h[c][j];
         } else {  // MODE_CORR
             const float c1 = -(float)(a.st->Dt / 2);
 #pragma unroll
