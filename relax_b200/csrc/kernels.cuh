@@ -1129,7 +1129,7 @@ __global__ void __launch_bounds__(RW *N2, (RW * N2 <= 128) ? 8 : 4) k_xfwd_reg(c
             if (i3 == 0) { zp = g.plane; zm = 0; kz = a.k3b; }
             else if (i3 == g.sx3h - 1) { zp = pl; zm = pl - g.plane; kz = a.k3b; }
             else { zp = pl + g.plane; zm = pl - g.plane; kz = a.k3; }
-#pragma unroll 2
+#pragma unroll 4
             for (int it = 0; it < ITS; it++) {
                 const int q = threadIdx.x + NT * it, rr = q / R4, x = 4 * (q % R4);
                 const int row = blockIdx.x * RW + rr;
