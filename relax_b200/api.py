@@ -230,17 +230,28 @@ class Relax:
         return n.value
 
     # -- fields --------------------------------------------------------------
-    def field(self, name: str) -> np.ndarray:
+    def field_shape(self, name: str):
+        """(shape, dtype) of a field in the reference layout."""
         s = self.sim
         if name == "u":
-            a = np.zeros(s.vec_shape(), np.float32)
-        elif name == "gamma":
-            a = np.zeros(s.vec_shape()[1:], np.float32)
-        else:
-            a = np.zeros(s.tensor_shape(), TENSOR_DTYPE)
-        _lib.check(self.lib.relax_get_field(self.h, FIELDS[name], a.ctypes.data_as(C.c_void_p),
-                                            a.nbytes))
-        return a
+            return s.vec_shape(), np.dtype(np.float32)
+        if name == "gamma":
+            return s.vec_shape()[1:], np.dtype(np.float32)
+        return s.tensor_shape(), TENSOR_DTYPE
+
+    def field(self, name: str) -> np.ndarray:
+        shape, dt = self.field_shape(name)
+        return self.field_into(name, np.zeros(shape, dt))
+
+    def field_into(self, name: str, out) -> np.ndarray:
+        """Reads a field into a caller's buffer (a numpy array, or any object
+        with the array interface and the field's size, page-locked or not)."""
+        a = np.asarray(out)
+        shape, dt = self.field_shape(name)
+        if a.nbytes != int(np.prod(shape)) * dt.itemsize or not a.flags.c_contiguous:
+            raise ValueError(f"field {name}: need a contiguous buffer of {int(np.prod(shape)) * dt.itemsize} bytes")
+        _lib.check(self.lib.relax_get_field(self.h, FIELDS[name], a.ctypes.data_as(C.c_void_p), a.nbytes))
+        return out
 
     def set_field(self, name: str, a: np.ndarray):
         a = np.ascontiguousarray(a)

@@ -752,6 +752,15 @@ static int dalloc(T **p, size_t n)
 
 static int build_bands(relax_ctx *c);
 
+// dst[c][i] = v[c][depth of i] for the 6 components of a tensor field
+__global__ void k_fill_depth(float *dst, const float *v, int nz, size_t plane, size_t nh)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 6 * nh) return;
+    const size_t cc = q / nh, i3 = (q % nh) / plane;
+    dst[q] = v[cc * nz + i3];
+}
+
 static int create(const relax_config *cfg, int device, relax_ctx *c)
 {
     c->device = device;
@@ -814,16 +823,26 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     c->sp.prof = &c->prof;
 
     // tau = -prestress (src/relax.f90:287-297)
-    {
-        std::vector<float> h(6 * nh, 0.f);
-        if (!c->pre.empty())
-            for (int i3 = 0; i3 < nz; i3++) {
-                const relax_tensor &t = c->pre[i3].t;
-                const float v[6] = {-t.s11, -t.s12, -t.s13, -t.s22, -t.s23, -t.s33};
-                for (int cc = 0; cc < 6; cc++)
-                    std::fill(h.begin() + cc * nh + (size_t)i3 * g.plane, h.begin() + cc * nh + (size_t)(i3 + 1) * g.plane, v[cc]);
-            }
-        CK(cudaMemcpy(c->tau, h.data(), 6 * nh * sizeof(float), cudaMemcpyHostToDevice));
+    // tau = -prestress(depth) (src/relax.f90:290-296), filled on the device
+    if (c->pre.empty()) {
+        CK(cudaMemsetAsync(c->tau, 0, 6 * nh * sizeof(float), c->st));
+    } else {
+        std::vector<float> h(6 * (size_t)nz);
+        for (int i3 = 0; i3 < nz; i3++) {
+            const relax_tensor &t = c->pre[i3].t;
+            const float v[6] = {-t.s11, -t.s12, -t.s13, -t.s22, -t.s23, -t.s33};
+            for (int cc = 0; cc < 6; cc++) h[(size_t)cc * nz + i3] = v[cc];
+        }
+        float *d = nullptr;
+        TRY(dalloc(&d, h.size()));
+        cudaError_t e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, c->st);
+        if (e == cudaSuccess) {
+            k_fill_depth<<<nblocks(6 * nh), RELAX_NTHREADS, 0, c->st>>>(c->tau, d, nz, g.plane, nh);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+        cudaFree(d);
+        if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "prestress: %s", cudaGetErrorString(e));
     }
     // rheology tables
     std::vector<float> spdev;
@@ -1707,7 +1726,7 @@ extern "C" int relax_get_field(relax_ctx *c, int which, void *host, size_t bytes
     case RELAX_FIELD_GAMMA: {
         const int nc = which == RELAX_FIELD_U ? 3 : 1;
         if (bytes != nc * nvec * sizeof(float)) return fail(RELAX_ERR_ARG, "field size %zu != %zu", bytes, nc * nvec * sizeof(float));
-        TRY(dalloc(&tmp, nc * nvec));
+        tmp = c->work;   // free between steps; holds 6 nh >= 3 nvec floats
         const float *src = which == RELAX_FIELD_U ? c->u : c->gamma;
         for (int k = 0; k < nc; k++) {
             k_pad<<<nblocks(nvec), RELAX_NTHREADS, 0, c->st>>>(src + k * g.nh, tmp + k * nvec, g.sx1,
@@ -1723,7 +1742,7 @@ extern "C" int relax_get_field(relax_ctx *c, int which, void *host, size_t bytes
         if (which == RELAX_FIELD_EPS && !c->eps) return fail(RELAX_ERR_STATE, "no transient rheology");
         if (which == RELAX_FIELD_SIG) TRY(field_sig(c));
         const float *src = tensor_field(c, which);
-        TRY(dalloc(&tmp, 6 * g.nh));
+        tmp = c->work;
         k_soa_to_aos<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(src, (relax_tensor *)tmp, g.nh);
         break;
     }
@@ -1731,9 +1750,10 @@ extern "C" int relax_get_field(relax_ctx *c, int which, void *host, size_t bytes
         return fail(RELAX_ERR_ARG, "unknown field %d", which);
     }
     CKL();
+    // one copy: a DMA straight into page-locked host memory, else the
+    // driver's staged copy of pageable memory
     CK(cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    cudaFree(tmp);
     return RELAX_OK;
 }
 
