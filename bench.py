@@ -283,17 +283,22 @@ def run_gpu(args, rank, world, local_rank):
     u = torch.empty(ushape[0] * ushape[1] * ushape[2] * ushape[3], dtype=torch.float32,
                     pin_memory=True).numpy().reshape(ushape)
     tau = torch.empty(sim.npoints // 2 * 6, dtype=torch.float32, pin_memory=True).numpy()
-    barrier()
-    t0 = time.perf_counter()
-    r2 = Relax(sim, device=local_rank)
-    r2.coseismic()
-    for _ in range(args.steps):
-        r2.step()
-    r2.field_into("u", u)
-    r2.field_into("tau", tau)
-    r2.close()
-    torch.cuda.synchronize()
-    e2e_s = allmax(time.perf_counter() - t0)
+    # five passes, the median reported (set-up times vary with the state of
+    # the device memory allocator)
+    passes = []
+    for _ in range(5):
+        barrier()
+        t0 = time.perf_counter()
+        r2 = Relax(sim, device=local_rank)
+        r2.coseismic()
+        for _ in range(args.steps):
+            r2.step()
+        r2.field_into("u", u)
+        r2.field_into("tau", tau)
+        r2.close()
+        torch.cuda.synchronize()
+        passes.append(allmax(time.perf_counter() - t0))
+    e2e_s = statistics.median(passes)
     nz = sim.sx3h
     # H2D: the deck's per-depth structures and the twiddle tables (the
     # prestress is filled on the device from its per-depth values)
@@ -301,7 +306,9 @@ def run_gpu(args, rank, world, local_rank):
     d2h = 120 + (u.nbytes + tau.nbytes) / args.steps
     e2e = {"value": world * sim.npoints * args.steps / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-           "timing": "host wall clock around create + coseismic + K steps + field readback"}
+           "timing": "host wall clock around create + coseismic + K steps + field readback, "
+                     "median of 5 passes",
+           "passes_s": [round(x, 4) for x in passes]}
 
     if rank != 0:
         return 0

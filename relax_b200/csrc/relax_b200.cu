@@ -1287,6 +1287,75 @@ static FrictionArgs plane_args(relax_ctx *c, const relax_plane &p)
 }
 
 // band point lists of every plane, once per context
+// Band compaction on the device, in the order of the plane's box: the points
+// whose impulse is defined (>= 0) go to consecutive slots.
+__global__ void k_band_count(const double *imp, size_t n, unsigned *cnt)
+{
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = __syncthreads_count(t < n && imp[t] >= 0.0);
+    if (threadIdx.x == 0) cnt[blockIdx.x] = (unsigned)v;
+}
+
+// exclusive scan of the per-block counts, one block; total in cnt[nb]
+__global__ void k_band_scan(unsigned *cnt, int nb)
+{
+    __shared__ unsigned carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const unsigned v = i < nb ? cnt[i] : 0u;
+        // inclusive warp scan, then across warps
+        unsigned x = v;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        __shared__ unsigned ws[32];
+        if (lane == 31) ws[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            unsigned s = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0u;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            ws[lane] = s;
+        }
+        __syncthreads();
+        const unsigned incl = x + (w ? ws[w - 1] : 0u) + carry;
+        if (i < nb) cnt[i] = incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) cnt[nb] = carry;
+}
+
+__global__ void k_band_write(FrictionArgs a, const double *imp, const unsigned *off, unsigned *idx, double *out)
+{
+    const Grid &g = a.g;
+    const size_t n = (size_t)a.n1 * a.n2 * a.n3;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = t < n && imp[t] >= 0.0;
+    const unsigned ball = __ballot_sync(0xffffffffu, in);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __shared__ unsigned wc[32];
+    if (lane == 0) wc[w] = __popc(ball);
+    __syncthreads();
+    unsigned before = 0;
+    for (int k = 0; k < w; k++) before += wc[k];
+    if (!in) return;
+    const unsigned slot = off[blockIdx.x] + before + __popc(ball & ((1u << lane) - 1u));
+    const int j1 = a.j1lo + (int)(t % a.n1);
+    const int j2 = a.j2lo + (int)((t / a.n1) % a.n2);
+    const int i3 = a.i3lo + (int)(t / ((size_t)a.n1 * a.n2));
+    const int i1 = (j1 + g.sx1) % g.sx1, i2 = (j2 + g.sx2) % g.sx2;
+    idx[slot] = (unsigned)(((size_t)i3 * g.sx2 + i2) * g.sx1 + i1);
+    out[slot] = imp[t];
+}
+
 static int build_bands(relax_ctx *c)
 {
     const Grid &g = c->g;
@@ -1297,31 +1366,35 @@ static int build_bands(relax_ctx *c)
         c->band_n.push_back(0);
         if (!plane_box(g, a, &a.j1lo, &a.n1, &a.j2lo, &a.n2, &a.i3lo, &a.n3)) continue;
         const size_t n = (size_t)a.n1 * a.n2 * a.n3;
+        const int nb = (int)nblocks(n);
         double *dimp = nullptr;
+        unsigned *cnt = nullptr;
         TRY(dalloc(&dimp, n));
-        k_friction_mark<<<nblocks(n), RELAX_NTHREADS, 0, c->st>>>(a, dimp);
-        std::vector<double> h(n);
-        cudaError_t e = cudaMemcpyAsync(h.data(), dimp, n * sizeof(double), cudaMemcpyDeviceToHost, c->st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
-        cudaFree(dimp);
-        if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "band of plane %zu: %s", k, cudaGetErrorString(e));
-        std::vector<unsigned> idx;
-        std::vector<double> imp;
-        for (size_t t = 0; t < n; t++) {
-            if (!(h[t] >= 0.0)) continue;
-            const int j1 = a.j1lo + (int)(t % a.n1);
-            const int j2 = a.j2lo + (int)((t / a.n1) % a.n2);
-            const int i3 = a.i3lo + (int)(t / ((size_t)a.n1 * a.n2));
-            const int i1 = (j1 + g.sx1) % g.sx1, i2 = (j2 + g.sx2) % g.sx2;
-            idx.push_back((unsigned)(((size_t)i3 * g.sx2 + i2) * g.sx1 + i1));
-            imp.push_back(h[t]);
+        if (dalloc(&cnt, (size_t)nb + 1) != RELAX_OK) {
+            cudaFree(dimp);
+            return RELAX_ERR_NOMEM;
         }
-        c->band_n[k] = (int)idx.size();
-        if (idx.empty()) continue;
-        TRY(dalloc(&c->band_idx[k], idx.size()));
-        TRY(dalloc(&c->band_imp[k], imp.size()));
-        CK(cudaMemcpy(c->band_idx[k], idx.data(), idx.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(c->band_imp[k], imp.data(), imp.size() * sizeof(double), cudaMemcpyHostToDevice));
+        unsigned total = 0;
+        k_friction_mark<<<nb, RELAX_NTHREADS, 0, c->st>>>(a, dimp);
+        k_band_count<<<nb, RELAX_NTHREADS, 0, c->st>>>(dimp, n, cnt);
+        k_band_scan<<<1, 1024, 0, c->st>>>(cnt, nb);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&total, cnt + nb, sizeof total, cudaMemcpyDeviceToHost, c->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+        if (e == cudaSuccess && total > 0) {
+            if (dalloc(&c->band_idx[k], total) != RELAX_OK || dalloc(&c->band_imp[k], total) != RELAX_OK) {
+                cudaFree(dimp);
+                cudaFree(cnt);
+                return RELAX_ERR_NOMEM;
+            }
+            k_band_write<<<nb, RELAX_NTHREADS, 0, c->st>>>(a, dimp, cnt, c->band_idx[k], c->band_imp[k]);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+        }
+        cudaFree(dimp);
+        cudaFree(cnt);
+        if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "band of plane %zu: %s", k, cudaGetErrorString(e));
+        c->band_n[k] = (int)total;
     }
     if (c->planes.empty()) return RELAX_OK;
     TRY(dalloc(&c->sig_mask, g.nh / 4));
