@@ -1971,6 +1971,18 @@ __global__ void k_dt(StepState *st, DtPolicy pol, DtIn in, const float *tm_part,
     dt_body(st, pol, in, tm_part, ntm, fr_part, nfr);
 }
 
+// the same with the policy and the step's inputs in device memory, written
+// by the host before each step (the form a captured step graph launches)
+struct DtParams {
+    DtPolicy pol;
+    DtIn in;
+};
+
+__global__ void k_dt_dev(StepState *st, const DtParams *p, const float *fr_part, int nfr)
+{
+    dt_body(st, p->pol, p->in, nullptr, 0, fr_part, nfr);
+}
+
 // one block per member of a batch
 struct DtArgs {
     StepState *st;

@@ -697,6 +697,13 @@ struct relax_ctx {
     // plane inter_i3 alone)
     float *vel = nullptr, *ur = nullptr, *urs = nullptr;
     int vel_planes = 0, ur_planes = 0, inter_i3 = -1;
+    // the step's time-step inputs (pinned host copy, device copy) and the
+    // captured graph of a step's kernels (steps without surface loads)
+    DtParams *dtp_h = nullptr, *dtp_d = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    long long glaunches = 0;
+    bool graph_off = false;
+    int plain_steps = 0;
 
     // host time-loop state
     double t = 0.0;
@@ -732,6 +739,9 @@ static void free_ctx(relax_ctx *c)
     if (c->ticket) cudaFree(c->ticket);
     if (c->dst && c->own_dst) cudaFree(c->dst);
     if (c->hst) cudaFreeHost(c->hst);
+    if (c->dtp_h) cudaFreeHost(c->dtp_h);
+    if (c->dtp_d) cudaFree(c->dtp_d);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->amp_part) cudaFree(c->amp_part);
     if (c->amp_alt) cudaFree(c->amp_alt);
     c->sp.release();
@@ -925,6 +935,8 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     TRY(dalloc(&c->dst, 1));
     CK(cudaMemset(c->dst, 0, sizeof(StepState)));
     CK(cudaMallocHost(&c->hst, sizeof(StepState)));
+    CK(cudaMallocHost(&c->dtp_h, sizeof(DtParams)));
+    TRY(dalloc(&c->dtp_d, 1));
     memset(c->hst, 0, sizeof(StepState));
     c->err = &c->dst->error;   // read back with the step state
     TRY(dalloc(&c->ticket, 1));
@@ -1618,27 +1630,19 @@ static int finish_step(relax_ctx *c, relax_step_log *log)
     return RELAX_OK;
 }
 
-static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
+// The kernels of one RK2 step, after the step's time-step inputs are in
+// c->dtp_d.  Without surface loads on the current event the sequence does
+// not depend on the host between its launches, and do_step captures it once
+// in a CUDA graph and replays it.
+static int step_kernels(relax_ctx *c)
 {
     const Grid &g = c->g;
-    const double STEP_MAX = 1e7;
-    (void)STEP_MAX;
-    if (!c->cos_done) TRY(relax_coseismic(c, 0, nullptr));
-    if (!c->m_valid) TRY(tail_init(c));
-    memset(log, 0, sizeof *log);
-    if (c->t >= c->cfg.interval) return RELAX_OK;
-
     // ---- predictor -------------------------------------------------------
     int nfr = 0;
     if (!c->fc.empty()) TRY(friction_planes(c, true, &nfr));
-    DtIn din{};
-    din.t = c->t;
-    din.dt_override = dt_override ? *dt_override : 0.0;
-    din.oi = c->oi;
-    din.use_override = dt_override ? 1 : 0;
-    // the Maxwell-time minima come reduced from the last INIT/END stress pass
-    TIMED(&c->prof, ST_DT, c->st,
-          (k_dt<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, policy(c), din, nullptr, 0, c->fr_part, nfr)));
+    // the Maxwell-time minima come reduced from the last INIT/END stress
+    // pass; the policy and the step's inputs are in c->dtp_d
+    TIMED(&c->prof, ST_DT, c->st, (k_dt_dev<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->dtp_d, c->fr_part, nfr)));
     // The kernels take Dt from the device state.  The host needs it before
     // the end of the step only for surface loads (evaluated on the host at
     // t + Dt); otherwise the step runs with one synchronisation, at its end.
@@ -1716,6 +1720,69 @@ static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
     // of src/relax.f90:859, made by k_dt) the kernel does nothing and
     // finish_step runs the event branch instead.
     TRY(launch_stress<MODE_END>(c, stress_args(c, c->u)));
+    return RELAX_OK;
+}
+
+static void drop_graph(relax_ctx *c)
+{
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+}
+
+// captures step_kernels into c->gexec; on any failure the context steps
+// without a graph from then on
+static int capture_step(relax_ctx *c)
+{
+    cudaGraph_t graph = nullptr;
+    const long long l0 = c->prof.launches;
+    if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaGetLastError();
+        c->graph_off = true;
+        return RELAX_OK;
+    }
+    const int rc = step_kernels(c);
+    const cudaError_t e = cudaStreamEndCapture(c->st, &graph);
+    c->glaunches = c->prof.launches - l0;
+    c->prof.launches = l0;
+    if (rc != RELAX_OK || e != cudaSuccess || !graph ||
+        cudaGraphInstantiate(&c->gexec, graph, 0) != cudaSuccess) {
+        cudaGetLastError();
+        if (graph) cudaGraphDestroy(graph);
+        c->gexec = nullptr;
+        c->graph_off = true;
+        return rc;
+    }
+    cudaGraphDestroy(graph);
+    return RELAX_OK;
+}
+
+static int do_step(relax_ctx *c, const double *dt_override, relax_step_log *log)
+{
+    if (!c->cos_done) TRY(relax_coseismic(c, 0, nullptr));
+    if (!c->m_valid) TRY(tail_init(c));
+    memset(log, 0, sizeof *log);
+    if (c->t >= c->cfg.interval) return RELAX_OK;
+    // the step's time-step inputs; the pinned copy is free again once the
+    // previous step's state came back
+    c->dtp_h->pol = policy(c);
+    c->dtp_h->in = DtIn{};
+    c->dtp_h->in.t = c->t;
+    c->dtp_h->in.dt_override = dt_override ? *dt_override : 0.0;
+    c->dtp_h->in.oi = c->oi;
+    c->dtp_h->in.use_override = dt_override ? 1 : 0;
+    CK(cudaMemcpyAsync(c->dtp_d, c->dtp_h, sizeof(DtParams), cudaMemcpyHostToDevice, c->st));
+    // a graph replays the step where the host has no part in it: no surface
+    // loads, no per-launch profiling, after one plain step (which sizes the
+    // friction partials)
+    const bool graphable = c->events[c->e].l.empty() && !c->prof.on && !c->graph_off && c->plain_steps > 0;
+    if (graphable && !c->gexec) TRY(capture_step(c));
+    if (graphable && c->gexec) {
+        CK(cudaGraphLaunch(c->gexec, c->st));
+        c->prof.launches += c->glaunches;
+    } else {
+        TRY(step_kernels(c));
+        c->plain_steps++;
+    }
     TRY(pull_state(c));
     return finish_step(c, log);
 }
@@ -1988,6 +2055,7 @@ extern "C" int relax_track_relaxation(relax_ctx *c, int vel_planes, int ur_plane
         return fail(RELAX_ERR_ARG, "planes outside [0, %d]", g.sx3h);
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->st));
+    drop_graph(c);   // the corrector's epilogue arguments change
     for (float **p : {&c->vel, &c->ur, &c->urs})
         if (*p) { cudaFree(*p); *p = nullptr; }
     const int nv = std::max(std::max(vel_planes, ur_planes), inter_i3 + 1);
