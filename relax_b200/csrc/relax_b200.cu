@@ -2763,6 +2763,12 @@ struct relax_batch {
     DtArgs *hdt = nullptr;         // pinned: this step's k_dt inputs
     std::vector<int> nfr;          // friction partial slots per member
     long long launches = 0;
+    // the captured graph of a batched step's kernels (dropped when the
+    // argument tables are rebuilt)
+    cudaGraphExec_t gexec = nullptr;
+    long long glaunches = 0;
+    bool graph_off = false;
+    int plain_steps = 0;
 };
 
 static void free_batch(relax_batch *b)
@@ -2773,6 +2779,7 @@ static void free_batch(relax_batch *b)
     if (b->dst) cudaFree(b->dst);
     if (b->hst) cudaFreeHost(b->hst);
     if (b->hdt) cudaFreeHost(b->hdt);
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
 }
@@ -2872,6 +2879,8 @@ static T *carve(unsigned char *base, size_t *off, size_t n)
 // rebuilt after an event or a change of plane geometry
 static int build_tables(relax_batch *b)
 {
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);   // its arguments live in the old tables
+    b->gexec = nullptr;
     const int n = (int)b->m.size();
     relax_ctx *c0 = b->m[0];
     const Grid &g = c0->g;
@@ -2997,50 +3006,16 @@ static int batch_green(relax_batch *b, const XiArgs &xi0)
 // One RK2 step of every member (the steps of src/relax.f90:555-890 as in
 // relax_step).  Members whose time reached the interval take Dt = 0 on the
 // device and report i = 0.
-extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
+// the kernels of a batched step, after the members' time-step inputs are in
+// the k_dt table
+static int batch_kernels(relax_batch *b)
 {
-    if (!b || !logs) return fail(RELAX_ERR_ARG, "null argument");
-    CK(cudaSetDevice(b->device));
     const int n = (int)b->m.size();
-    std::vector<char> live(n, 0);
-    int nlive = 0;
-    for (int k = 0; k < n; k++) {
-        relax_ctx *c = b->m[k];
-        if (!c->cos_done) TRY(relax_coseismic(c, 0, nullptr));
-        memset(&logs[k], 0, sizeof(relax_step_log));
-        live[k] = c->t < c->cfg.interval;
-        nlive += live[k];
-    }
-    if (!nlive) return RELAX_OK;
-    if (!b->batched || n == 1) {
-        // no batched instantiation for this grid: the members in turn
-        for (int k = 0; k < n; k++)
-            if (live[k]) TRY(do_step(b->m[k], nullptr, &logs[k]));
-        return RELAX_OK;
-    }
-    if (!b->tables_valid) TRY(build_tables(b));
-    // the members' own streams carry their set-up and event work
-    for (auto *c : b->m) CK(cudaStreamSynchronize(c->st));
     BatchTables &t = b->tab;
     relax_ctx *c0 = b->m[0];
     const Grid &g = c0->g;
     const size_t np = c0->planes.size();
     cudaStream_t st = b->st;
-    // ---- predictor
-    for (int k = 0; k < n; k++) {
-        relax_ctx *c = b->m[k];
-        DtArgs &d = b->hdt[k];
-        d.st = c->dst;
-        d.pol = policy(c);
-        d.in = DtIn{};
-        d.in.t = c->t;
-        d.in.oi = c->oi;
-        d.in.use_override = live[k] ? 0 : 1;   // finished members: Dt = 0
-        d.in.dt_override = 0.0;
-        d.fr_part = c->fr_part;
-        d.nfr = c->fc.empty() ? 0 : b->nfr[k];
-    }
-    CK(cudaMemcpyAsync(t.dt, b->hdt, n * sizeof(DtArgs), cudaMemcpyHostToDevice, st));
     if (!c0->fc.empty())
         for (size_t q = 0; q < np; q++)
             if (t.frblk[q] > 0) {
@@ -3095,6 +3070,77 @@ extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
     else k_stress<MODE_END, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.end0);
     b->launches++;
     CKL();
+    return RELAX_OK;
+}
+
+extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
+{
+    if (!b || !logs) return fail(RELAX_ERR_ARG, "null argument");
+    CK(cudaSetDevice(b->device));
+    const int n = (int)b->m.size();
+    std::vector<char> live(n, 0);
+    int nlive = 0;
+    for (int k = 0; k < n; k++) {
+        relax_ctx *c = b->m[k];
+        if (!c->cos_done) TRY(relax_coseismic(c, 0, nullptr));
+        memset(&logs[k], 0, sizeof(relax_step_log));
+        live[k] = c->t < c->cfg.interval;
+        nlive += live[k];
+    }
+    if (!nlive) return RELAX_OK;
+    if (!b->batched || n == 1) {
+        // no batched instantiation for this grid: the members in turn
+        for (int k = 0; k < n; k++)
+            if (live[k]) TRY(do_step(b->m[k], nullptr, &logs[k]));
+        return RELAX_OK;
+    }
+    if (!b->tables_valid) TRY(build_tables(b));
+    // the members' own streams carry their set-up and event work
+    for (auto *c : b->m) CK(cudaStreamSynchronize(c->st));
+    BatchTables &t = b->tab;
+    cudaStream_t st = b->st;
+    // ---- predictor
+    for (int k = 0; k < n; k++) {
+        relax_ctx *c = b->m[k];
+        DtArgs &d = b->hdt[k];
+        d.st = c->dst;
+        d.pol = policy(c);
+        d.in = DtIn{};
+        d.in.t = c->t;
+        d.in.oi = c->oi;
+        d.in.use_override = live[k] ? 0 : 1;   // finished members: Dt = 0
+        d.in.dt_override = 0.0;
+        d.fr_part = c->fr_part;
+        d.nfr = c->fc.empty() ? 0 : b->nfr[k];
+    }
+    CK(cudaMemcpyAsync(t.dt, b->hdt, n * sizeof(DtArgs), cudaMemcpyHostToDevice, st));
+    // the kernels, replayed from a captured graph after one plain step
+    if (!b->graph_off && b->plain_steps > 0 && !b->gexec) {
+        cudaGraph_t graph = nullptr;
+        const long long l0 = b->launches;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+            const int rc = batch_kernels(b);
+            const cudaError_t e = cudaStreamEndCapture(st, &graph);
+            b->glaunches = b->launches - l0;
+            if (rc != RELAX_OK || e != cudaSuccess || !graph ||
+                cudaGraphInstantiate(&b->gexec, graph, 0) != cudaSuccess) {
+                b->gexec = nullptr;
+                b->graph_off = true;
+            }
+            if (graph) cudaGraphDestroy(graph);
+        } else {
+            b->graph_off = true;
+        }
+        cudaGetLastError();
+        b->launches = l0;
+    }
+    if (b->gexec) {
+        CK(cudaGraphLaunch(b->gexec, st));
+        b->launches += b->glaunches;
+    } else {
+        TRY(batch_kernels(b));
+        b->plain_steps++;
+    }
     CK(cudaMemcpyAsync(b->hst, b->dst, n * sizeof(StepState), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     // ---- host part of each member's step end
