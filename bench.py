@@ -354,7 +354,15 @@ def run_ensemble(args):
     from relax_b200.config import ensemble_uneven
 
     torch.cuda.set_device(0)
-    sims = ensemble_uneven(seed=4, n=64)
+    if args.ensemble == "c5":
+        from relax_b200.config import ensemble_thrust_afterslip
+        sims = ensemble_thrust_afterslip(seed=5, n=16)
+        workload_name = ("16 thrust instances on 256^2x128 (dx 0.5 km, gravity), 5 km slip patches "
+                         "2(1+N(0,0.2)), two afterslip planes, n=3 below 35 km")
+    else:
+        sims = ensemble_uneven(seed=4, n=64)
+        workload_name = ("uneven ensemble of 64 members, grids {64^3, 128^2x64, 128^3, 192^2x96}, "
+                         "power-law n U[1,3.5], prefactor 10^U[-1,1], lid U[15,40] km, one fault each")
     groups = collections.OrderedDict()
     for s in sims:
         groups.setdefault((s.sx1, s.sx2, s.sx3), []).append(s)
@@ -406,8 +414,7 @@ def run_ensemble(args):
         "metric": "ensemble solves/s (100 RK2 steps per member)", "value": solves / t_batch,
         "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": W, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "uneven ensemble of 64 members, grids {64^3, 128^2x64, 128^3, 192^2x96}, "
-                               "power-law n U[1,3.5], prefactor 10^U[-1,1], lid U[15,40] km, one fault each",
+        "config": {"workload": workload_name,
                    "members": {f"{a}x{b}x{c}": len(g) for (a, b, c), g in groups.items()},
                    "grid_points_total": npts, "parallelism": "one batch per grid shape",
                    "timing": "host wall clock around K steps of every member, after W warm-up steps"},
@@ -432,8 +439,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--ensemble", action="store_true",
-                    help="the batched 64-member ensemble against a loop of plain solves (1 GPU)")
+    ap.add_argument("--ensemble", nargs="?", const="c4", choices=["c4", "c5"], default=None,
+                    help="a batched ensemble against a loop of plain solves (1 GPU): c4, the 64 uneven "
+                         "members (default), or c5, 16 thrust instances with afterslip")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

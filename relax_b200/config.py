@@ -566,6 +566,40 @@ def ensemble_uneven(seed: int = 4, n: int = 64) -> List[Simulation]:
     return sims
 
 
+def ensemble_thrust_afterslip(seed: int = 5, n: int = 16, sx: int = 256, sz: int = 128,
+                              dx: float = 0.5) -> List[Simulation]:
+    """Ensemble of `n` thrust instances on one 256^2 x 128 box (dx = 0.5 km,
+    gravity 8.3e-4): a 20-degree thrust 80 km x 40 km made of 5 km patches
+    (16 x 8) with slip 2 (1 + N(0, 0.2)) each, two rate-strengthening
+    afterslip planes (one down-dip of the rupture, one shallow in front of
+    it), power law n = 3
+    below 35 km with a fluidity prefactor drawn per member (10^U[-0.5, 0.5]).
+    Skip mode, Dt = tm/10."""
+    rng = np.random.default_rng(seed)
+    sd, cd = math.sin(math.radians(20.0)), math.cos(math.radians(20.0))
+    top, width, length, patch = 1.0, 40.0, 80.0, 5.0
+    sims = []
+    for k in range(n):
+        faults = []
+        for i in range(int(length / patch)):
+            for j in range(int(width / patch)):
+                slip = float(2.0 * (1.0 + rng.normal(0.0, 0.2)))
+                faults.append(Fault(slip, -length / 2 + i * patch, j * patch * cd, top + j * patch * sd, patch,
+                                    patch, 0.0, 20.0, 90.0))
+        bottom = top + width * sd
+        planes = [Plane(x=-25.0, y=width * cd, z=bottom, length=50.0, width=20.0, strike=0.0, dip=20.0,
+                        rake=90.0),
+                  Plane(x=-25.0, y=-12.0 * cd, z=top + 0.5, length=50.0, width=10.0, strike=0.0, dip=20.0,
+                        rake=90.0)]
+        g0 = float(10.0 ** rng.uniform(-0.5, 0.5))
+        sims.append(Simulation(
+            sx1=sx, sx2=sx, sx3=sz, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0, lambda_=1.0, mu=1.0,
+            gam=8.3e-4, interval=1.0e6, odt=-1, tscale=1.0, nonlinear=[(35.0, g0, 3.0, 0.0)],
+            faultcreep=[(0.0, 1.0, 0.1, 0.0, 0.0)], planes=planes, events=[Event(0.0, faults)],
+            name=f"thrust-afterslip-{k}"))
+    return sims
+
+
 def reference_output2() -> Simulation:
     """The input echoed in examples/tutorials/output2.param:8-62 (power-law
     n=3 relaxation after a strike-slip fault, 256^3)."""
