@@ -226,6 +226,9 @@ int relax_run(relax_ctx *ctx, int max_steps, const double *dt_schedule,
  * RELAX_FIELD_*); `bytes` must equal the field size. */
 int relax_get_field(relax_ctx *ctx, int which, void *host, size_t bytes);
 int relax_set_field(relax_ctx *ctx, int which, const void *host, size_t bytes);
+/* Number of afterslip planes, and the patch grid (px2 x px3) of plane k. */
+int relax_num_planes(relax_ctx *ctx, int *np);
+int relax_get_plane_shape(relax_ctx *ctx, int k, int *px2, int *px3);
 /* Afterslip patch state of plane k (px2*px3 entries, j2 fastest). */
 int relax_get_patches(relax_ctx *ctx, int k, relax_slippatch *host, size_t n);
 /* Current time, step counter, event index. */
@@ -331,6 +334,13 @@ int relax_write_vtk(const float *const *comp, int ncomp, int sx1, int sx2,
 int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int j2,
                      int j3, const char *filename, const char *title,
                      const char *name);
+/* exportcreep_asc / exportcreep_grd (src/export.f90:563-767): the patches
+ * of every afterslip plane as wdir/NNN.sKKKKK.creep.dat (every third patch,
+ * RELAX_CREEP_TXT) and as GMT grids of slip and slip rate (RELAX_CREEP_GRD). */
+#define RELAX_CREEP_TXT 1
+#define RELAX_CREEP_GRD 2
+int relax_export_creep(relax_ctx *ctx, const char *wdir, int index,
+                       int formats);
 /* shiftedindex, src/elastic3d.f90:4063-4101, 0-based indices; sx3 is the
  * number of x3-planes held (sx3/2 of the grid). */
 int relax_shifted_index(double x1, double x2, double x3, int sx1, int sx2,

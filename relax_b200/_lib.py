@@ -67,6 +67,8 @@ def load() -> C.CDLL:
         "relax_get_field": (I, [P, I, P, S]),
         "relax_set_field": (I, [P, I, P, S]),
         "relax_get_patches": (I, [P, I, C.POINTER(relax_slippatch), S]),
+        "relax_num_planes": (I, [P, C.POINTER(I)]),
+        "relax_get_plane_shape": (I, [P, I, C.POINTER(I), C.POINTER(I)]),
         "relax_get_time": (I, [P, C.POINTER(D), C.POINTER(I), C.POINTER(I)]),
         "relax_synchronize": (I, [P]),
         "relax_profile": (I, [P, I]),
@@ -113,6 +115,7 @@ def load() -> C.CDLL:
         "relax_write_vtk": (I, [C.POINTER(FP), I, I, I, I, D, D, D, I, I, I, C.c_char_p, C.c_char_p,
                                 C.c_char_p]),
         "relax_export_vtk": (I, [P, I, I, I, I, I, C.c_char_p, C.c_char_p, C.c_char_p]),
+        "relax_export_creep": (I, [P, C.c_char_p, I, I]),
         "relax_shifted_index": (I, [D, D, D, I, I, I, D, D, D, C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
         "relax_export_points": (I, [P, I, C.POINTER(D), C.POINTER(C.c_char_p), D, D, C.c_char_p, I]),
         "relax_format_log": (I, [C.POINTER(relax_step_log), D, I, C.c_char_p, S]),

@@ -298,6 +298,12 @@ class Relax:
         _lib.check(self.lib.relax_export_vtk(self.h, FIELDS[name], sx3, *strides, _path(filename), title.encode(),
                                              vname.encode()))
 
+    def export_creep(self, wdir, index: int, txt: bool = True, grd: bool = True):
+        """exportcreep_asc / exportcreep_grd: the afterslip planes' patches as
+        NNN.sKKKKK.creep.dat and NNN.sKKKKK.{slip,vel}*.grd files in wdir."""
+        formats = (1 if txt else 0) | (2 if grd else 0)
+        _lib.check(self.lib.relax_export_creep(self.h, _path(wdir), index, formats))
+
     def export_points(self, xyz, names: Sequence[str], time: float, wdir, isnew: bool, rot: float = 0.0):
         """exportpoints: one .ned line per observation point (x1, x2, x3 in the computational frame)."""
         x = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)

@@ -441,6 +441,71 @@ extern "C" int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int 
                      });
 }
 
+// The afterslip planes' patches (src/export.f90:563-767): with
+// RELAX_CREEP_TXT wdir/NNN.sKKKKK.creep.dat (every third patch along both
+// directions, one patch per line, 18ES11.3E2; exportcreep_asc), with
+// RELAX_CREEP_GRD the grids NNN.sKKKKK.slip-dip/slip-strike/slip.grd and
+// NNN.sKKKKK.vel-strike/vel-dip/vel.grd (exportcreep_grd, which writes the
+// dip-slip rate into vel-strike and the strike-slip rate into vel-dip; kept).
+extern "C" int relax_export_creep(relax_ctx *ctx, const char *wdir, int index, int formats)
+{
+    int np = 0, sx[3];
+    double dx[3];
+    if (!ctx || !wdir) return fail(RELAX_ERR_ARG, "null argument");
+    int rc = relax_num_planes(ctx, &np);
+    if (rc == RELAX_OK) rc = relax_get_grid(ctx, sx, dx);
+    if (rc != RELAX_OK) return rc;
+    const std::string digit = iw(index, 3, 3);
+    for (int k = 0; k < np; k++) {
+        int n1 = 0, n2 = 0;
+        if ((rc = relax_get_plane_shape(ctx, k, &n1, &n2)) != RELAX_OK) return rc;
+        if (n1 <= 0 || n2 <= 0) continue;
+        std::vector<relax_slippatch> p((size_t)n1 * n2);
+        if ((rc = relax_get_patches(ctx, k, p.data(), p.size())) != RELAX_OK) return rc;
+        const std::string stem = std::string(wdir) + "/" + digit + ".s" + iw(k + 1, 5, 5);
+        if (formats & RELAX_CREEP_TXT) {
+            FILE *fp = fopen((stem + ".creep.dat").c_str(), "w");
+            if (!fp) return fail(RELAX_ERR_ARG, "could not open %s.creep.dat", stem.c_str());
+            fprintf(fp, "#        x1         x2         x3          yr        yz       slip strike-slip  dip-slip"
+                        "   velocity     ss vel     ds vel       taus      sig11      sig12      sig13      sig22"
+                        "      sig23      sig33\n");
+            for (int i2 = 0; i2 < n2; i2 += 3)
+                for (int i1 = 0; i1 < n1; i1 += 3) {
+                    const relax_slippatch &q = p[(size_t)i1 + (size_t)n1 * i2];
+                    const double v[18] = {q.x1, q.x2, q.x3, q.lx, q.lz, q.slip, q.ss, q.ds, q.v, q.vss, q.vds,
+                                          q.taus, q.sig.s11, q.sig.s12, q.sig.s13, q.sig.s22, q.sig.s23, q.sig.s33};
+                    std::string line;
+                    for (double x : v) line += es(x, 11, 3, 2);
+                    fprintf(fp, "%s\n", line.c_str());
+                }
+            if (fclose(fp) != 0) return fail(RELAX_ERR_ARG, "writing %s.creep.dat failed", stem.c_str());
+        }
+        if (formats & RELAX_CREEP_GRD) {
+            if (n1 < 2 || n2 < 2) continue;   // a grid needs two nodes each way
+            double xmin = p[0].lx, zmax = p[0].lz;
+            for (const auto &q : p) {
+                xmin = std::fmin(xmin, q.lx);
+                zmax = std::fmax(zmax, q.lz);
+            }
+            std::vector<float> z((size_t)n1 * n2);
+            auto grid = [&](double relax_slippatch::*f, const char *name) {
+                for (int i2 = 0; i2 < n2; i2++)
+                    for (int i1 = 0; i1 < n1; i1++)
+                        z[(size_t)(n1 - 1 - i1) + (size_t)n1 * i2] = (float)(p[(size_t)i1 + (size_t)n1 * i2].*f);
+                return write_grd(z.data(), n1, n2, xmin, -zmax, dx[1], dx[2], "monitor field",
+                                 (stem + name).c_str());
+            };
+            if ((rc = grid(&relax_slippatch::ds, ".slip-dip.grd")) != RELAX_OK) return rc;
+            if ((rc = grid(&relax_slippatch::ss, ".slip-strike.grd")) != RELAX_OK) return rc;
+            if ((rc = grid(&relax_slippatch::slip, ".slip.grd")) != RELAX_OK) return rc;
+            if ((rc = grid(&relax_slippatch::vds, ".vel-strike.grd")) != RELAX_OK) return rc;
+            if ((rc = grid(&relax_slippatch::vss, ".vel-dip.grd")) != RELAX_OK) return rc;
+            if ((rc = grid(&relax_slippatch::v, ".vel.grd")) != RELAX_OK) return rc;
+        }
+    }
+    return RELAX_OK;
+}
+
 // shiftedindex, src/elastic3d.f90:4063-4101, 0-based; sx3 is the number of
 // planes (sx3/2 of the grid)
 extern "C" int relax_shifted_index(double x1, double x2, double x3, int sx1, int sx2, int sx3, double dx1,

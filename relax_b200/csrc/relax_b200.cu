@@ -2086,6 +2086,22 @@ extern "C" int relax_get_grid(relax_ctx *c, int *sx, double *dx)
     return RELAX_OK;
 }
 
+extern "C" int relax_get_plane_shape(relax_ctx *c, int k, int *px2, int *px3)
+{
+    if (!c) return fail(RELAX_ERR_ARG, "null context");
+    if (k < 0 || k >= (int)c->planes.size()) return fail(RELAX_ERR_ARG, "plane %d out of range", k);
+    if (px2) *px2 = std::max(0, c->planes[k].px2);
+    if (px3) *px3 = std::max(0, c->planes[k].px3);
+    return RELAX_OK;
+}
+
+extern "C" int relax_num_planes(relax_ctx *c, int *np)
+{
+    if (!c || !np) return fail(RELAX_ERR_ARG, "null argument");
+    *np = (int)c->planes.size();
+    return RELAX_OK;
+}
+
 extern "C" int relax_get_patches(relax_ctx *c, int k, relax_slippatch *host, size_t n)
 {
     if (!c || !host) return fail(RELAX_ERR_ARG, "null argument");

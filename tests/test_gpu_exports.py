@@ -12,7 +12,7 @@ from scipy.io import netcdf_file
 from relax_b200 import api
 from relax_b200.api import Relax
 
-from cases import linear_small, transient_small
+from cases import linear_small, powerlaw_small, transient_small
 
 pytestmark = pytest.mark.gpu
 
@@ -162,3 +162,42 @@ def test_transient_strain_grids(tmp_path):
         for n in eps.dtype.names:
             e = "e" + n[1:]
             np.testing.assert_array_equal(_grd(tmp_path / f"001-{e}.grd"), np.fft.fftshift(eps[n][0].T))
+
+
+def test_creep_exports(tmp_path):
+    """exportcreep_asc / exportcreep_grd (src/export.f90:563-767) of an
+    afterslip plane: every third patch per line in ES11.3E2, and the
+    strike-reversed grids of slip and slip rate (the reference's vel-strike
+    grid holds the dip-slip rate, vel-dip the strike-slip rate)."""
+    sim = powerlaw_small(sx=64, sz=32)
+    with Relax(sim) as r:
+        r.coseismic()
+        for _ in range(3):
+            r.step()
+        r.export_creep(tmp_path, 4)
+        p = np.ctypeslib.as_array(r.patches(0)).copy()
+        n1, n2 = r.cfg.planes[0].px2, r.cfg.planes[0].px3
+    assert n1 >= 6 and n2 >= 4 and np.abs(p["v"]).max() > 0
+    p = p.reshape(n2, n1)
+    names = ("x1", "x2", "x3", "lx", "lz", "slip", "ss", "ds", "v", "vss", "vds", "taus")
+    lines = (tmp_path / "004.s00001.creep.dat").read_text().splitlines()
+    assert lines[0].split() == ["#", "x1", "x2", "x3", "yr", "yz", "slip", "strike-slip", "dip-slip", "velocity",
+                                "ss", "vel", "ds", "vel", "taus", "sig11", "sig12", "sig13", "sig22", "sig23",
+                                "sig33"]
+    want = []
+    for i2 in range(0, n2, 3):
+        for i1 in range(0, n1, 3):
+            q = p[i2, i1]
+            vals = [q[n] for n in names] + [q["sig"][n] for n in ("s11", "s12", "s13", "s22", "s23", "s33")]
+            want.append("".join(api.es_format(float(v), 11, 3, 2) for v in vals))
+    assert lines[1:] == want
+    for f, name in (("ds", "slip-dip"), ("ss", "slip-strike"), ("slip", "slip"), ("vds", "vel-strike"),
+                    ("vss", "vel-dip"), ("v", "vel")):
+        with netcdf_file(tmp_path / f"004.s00001.{name}.grd", "r", mmap=False) as g:
+            z = g.variables["z"][:].copy()
+            x = g.variables["x"][:].copy()
+            y = g.variables["y"][:].copy()
+        np.testing.assert_array_equal(z, p[f][:, ::-1].astype(np.float32))
+        assert x[0] == p["lx"].min() and y[0] == -p["lz"].max()
+        np.testing.assert_allclose(np.diff(x), sim.dx2)
+        np.testing.assert_allclose(np.diff(y), sim.dx3)
