@@ -94,6 +94,20 @@ typedef struct relax_weakzone {
     relax_tensor e;
 } relax_weakzone;
 
+/* An observation plane (the geometry of PLANE_STRUCT, src/types.f90:92-97)
+ * in the internal convention: centre after wangconvention and the rotation,
+ * strike and dip in radians (src/input.f90:321-356). */
+typedef struct relax_obsplane {
+    double x, y, z, length, width, strike, dip;
+} relax_obsplane;
+
+/* SEGMENT_STRUCT, src/types.f90:58-62 without sig0 (the stress at the
+ * coseismic step, kept by the caller): a stress observation segment in the
+ * internal convention (src/input.f90:399-451). */
+typedef struct relax_segment {
+    double x, y, z, length, width, strike, dip, friction;
+} relax_segment;
+
 /* EVENT_STRUC, src/types.f90:99-106 (shear, tensile, point and load
  * sources; cuboid/tetrahedron eigenstrain sources are not supported). */
 typedef struct relax_event {
@@ -252,6 +266,21 @@ int relax_track_relaxation(relax_ctx *ctx, int vel_planes, int ur_planes,
  * triples: cuexportpoints_ (src/cuelastic.cu:1652) for many points. */
 int relax_get_points(relax_ctx *ctx, int n, const int *index, double *u,
                      relax_tensor *sig);
+/* monitorstressfield / monitorfield (src/elastic3d.f90:3404-3762): the
+ * stress (RELAX_FIELD_SIG, into patch.sig) or the scalar RELAX_FIELD_GAMMA
+ * (into patch.slip) sampled with the sinc-weighted 5x5x5 window on the
+ * (px2+1) x (px3+1) points of plane `op` (tapered by beta), px2 + 1 fastest;
+ * x1..x3 the point, lx / lz its along-strike / down-dip coordinates; points
+ * outside the box read zero.  *px2, *px3 are set; `out` may be NULL to size
+ * the grid, else it holds n >= (px2+1)(px3+1) patches. */
+int relax_monitor_plane(relax_ctx *ctx, int which, const relax_obsplane *op,
+                        double beta, relax_slippatch *out, size_t n,
+                        int *px2, int *px3);
+/* The stress at the centres of n stress observation segments (the nearest
+ * grid node, shiftedindex with the full sx3 as in src/export.f90:1364-1394);
+ * a centre below the stored half of the grid is an error. */
+int relax_segment_stress(relax_ctx *ctx, int n, const relax_segment *sop,
+                         relax_tensor *sig);
 
 /* ------------------------------------------------------------------ */
 /* the input file (subroutine init, src/input.f90:43-1767)            */
@@ -292,6 +321,11 @@ void relax_input_free(relax_input *in);
 const relax_config *relax_input_config(const relax_input *in);
 int relax_input_get_info(const relax_input *in, relax_input_info *info);
 /* weak zones of mechanism 0..3 in the internal convention */
+/* observation planes and stress observation segments of the input */
+int relax_input_obsplanes(const relax_input *in, const relax_obsplane **op,
+                          int *n);
+int relax_input_segments(const relax_input *in, const relax_segment **sop,
+                         int *n);
 int relax_input_weakzones(const relax_input *in, int mechanism,
                           const relax_weakzone **zones, int *n);
 /* builddgammadot0 (src/viscoelastic3d.f90:320-435) of every mechanism with
@@ -341,6 +375,34 @@ int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int j2,
 #define RELAX_CREEP_GRD 2
 int relax_export_creep(relax_ctx *ctx, const char *wdir, int index,
                        int formats);
+/* exportplanestress (src/export.f90:308-397): the stress on observation
+ * plane k sampled by relax_monitor_plane, as the grids
+ * wdir/NNN.opKKK-s11.grd ... -s33.grd; exporteigenstrain (:423-512) with
+ * which = RELAX_FIELD_GAMMA: wdir/NNN.sKKKKK.estrain.grd.  x0, y0: origin
+ * added to the sample points. */
+int relax_export_plane_stress(relax_ctx *ctx, int which, int nop,
+                              const relax_obsplane *op, double x0, double y0,
+                              const char *wdir, int index);
+/* The stress observation segments (src/export.f90:1403-2005), from the
+ * stress at their centres (sig; NULL: zero) less sig0 when sig0 is given
+ * (convention 1 of the reference):
+ *   RELAX_SEG_GMT      exportgmt_rfaults_stress, one "> -Z" polygon each;
+ *   RELAX_SEG_TRACTION exportgmt_rfaults_traction, position, shear traction
+ *                      and normal vector;
+ *   RELAX_SEG_VTP      exportvtk_rfaults_stress, VTK PolyData XML.
+ * `filename` is the file written. */
+#define RELAX_SEG_GMT 1
+#define RELAX_SEG_TRACTION 2
+#define RELAX_SEG_VTP 3
+int relax_write_segments(int kind, int n, const relax_segment *sop,
+                         const relax_tensor *sig, const relax_tensor *sig0,
+                         const char *filename);
+/* exportcoulombstress (src/export.f90:1893-2005): one line of time, stress
+ * and shear, normal and Coulomb stress per segment appended to
+ * wdir/cfaults-sigma-KKKK.txt (a new file with its header when isnew). */
+int relax_write_coulomb(int n, const relax_segment *sop,
+                        const relax_tensor *sig, double time,
+                        const char *wdir, int isnew);
 /* shiftedindex, src/elastic3d.f90:4063-4101, 0-based indices; sx3 is the
  * number of x3-planes held (sx3/2 of the grid). */
 int relax_shifted_index(double x1, double x2, double x3, int sx1, int sx2,
@@ -362,7 +424,7 @@ const char *relax_log_header(int transient);
 int relax_format_ned(double time, const double *u, const relax_tensor *sig,
                      char *buf, size_t size);
 const char *relax_ned_header(void);
-/* Fortran ESw.dEe of one value. */
+/* Fortran ESw.dEe of one value; e = 0 gives ESw.d. */
 int relax_es_format(double v, int w, int d, int e, char *buf, size_t size);
 
 /* Checkpoint (no counterpart in the reference, which cannot restart a

@@ -56,6 +56,8 @@ def load(precision: int = 32) -> C.CDLL:
         "orc_source": (None, [D, D, D, D, D, D, D, D, D, D, D, I, I, I, D, D, D, P, P, P, P, P, P]),
         "orc_momentdensityshear": (None, [D, D, D, D, D, D, D, D, D, D, D, I, I, I, D, D, D, P]),
         "orc_okada": (None, [D] * 15 + [C.POINTER(D)]),
+        "orc_monitor_plane": (None, [P, I, I, I, I, D, D, D, D, D, D, D, D, D, D, D, C.POINTER(I), C.POINTER(I),
+                                     P]),
         "orc_state_create": (P, [P]),
         "orc_state_free": (None, [P]),
         "orc_coseismic": (I, [P, P]),

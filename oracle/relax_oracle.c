@@ -1601,6 +1601,100 @@ static int okada_dc(double al, double x, double y, double z, double c0, double d
     return 0;
 }
 
+/* monitorstressfield / monitorfield, src/elastic3d.f90:3404-3762: the field f
+ * (nc = 6 tensor components or nc = 1 scalar, each sx1 x sx2 x sx3 floats,
+ * x1 fastest; sx3 the stored half) sampled on the (px2+1) x (px3+1) points of
+ * a plane (L along dip, W along strike, as the reference names them); out:
+ * 5 + nc doubles per point (x1, x2, x3, yr, zr, values) or NULL to size. */
+static double orc_sinc(double x)
+{
+    const double pi = 3.141592653589793115997963468544185161;
+    return x != 0 ? sin(pi * x) / (pi * x) : 1.0;
+}
+
+void orc_monitor_plane(const float *f, int nc, int sx1, int sx2, int sx3, double dx1, double dx2, double dx3,
+                       double x, double y, double z, double L, double W, double strike, double dip, double beta,
+                       int *px2_out, int *px3_out, double *out)
+{
+    const double cstrike = cos(strike), sstrike = sin(strike), cdip = cos(dip), sdip = sin(dip);
+    const double Wp = W * (1.0 + 2.0 * beta), Lp = L * (1.0 + 2.0 * beta);
+    const int px3 = orc_fix(Lp / dx3), px2 = orc_fix(Wp / dx2);
+    const size_t nh = (size_t)sx1 * sx2 * sx3;
+    *px2_out = px2;
+    *px3_out = px3;
+    if (!out) return;
+    for (int j3 = 1; j3 <= px3 + 1; j3++)
+        for (int j2 = 1; j2 <= px2 + 1; j2++) {
+            /* ref2local */
+            const double xa = cstrike * x - sstrike * y;
+            const double xr = cdip * xa - sdip * z;
+            double yr = sstrike * x + cstrike * y;
+            double zr = sdip * xa + cdip * z;
+            yr = (double)((float)yr + (float)(((double)j2 - (double)px2 / 2.0 - 1.0) * dx2));
+            zr = (double)((float)zr + (float)(((double)j3 - (double)px3 / 2.0 - 1.0) * dx3));
+            /* local2ref */
+            const double x2p = cdip * xr + sdip * zr;
+            const double x1 = cstrike * x2p + sstrike * yr;
+            const double x2 = -sstrike * x2p + cstrike * yr;
+            const double x3 = -sdip * xr + cdip * zr;
+            double *o = out + (size_t)(5 + nc) * ((size_t)(j2 - 1) + (size_t)(px2 + 1) * (j3 - 1));
+            o[0] = x1; o[1] = x2; o[2] = x3; o[3] = yr; o[4] = zr;
+            float lsig[6] = {0, 0, 0, 0, 0, 0};
+            double value = 0;
+            if (!(x1 > (double)(sx1 / 2 - 1) * dx1 || x1 < -(double)(sx1 / 2) * dx1 ||
+                  x2 > (double)(sx2 / 2 - 1) * dx2 || x2 < -(double)(sx2 / 2) * dx2 ||
+                  x3 > (double)(sx3 - 1) * dx3 || x3 < 0)) {
+                /* sampletensor / sample */
+                const int i = (sx1 + orc_fix(x1 / dx1)) % sx1 + 1;
+                const int j = (sx2 + orc_fix(x2 / dx2)) % sx2 + 1;
+                const int k = orc_fix(x3 / dx3) + 1;
+                const double xs = (double)(i <= sx1 / 2 ? i - 1 : i - sx1 - 1) * dx1;
+                const double ys = (double)(j <= sx2 / 2 ? j - 1 : j - sx2 - 1) * dx2;
+                const double zs = (double)(k <= sx3 ? k - 1 : k - 2 * sx3 - 1) * dx3;
+                const double EPS = (double)1e-2f;
+                if (fabs(xs - x1) < EPS * dx1 && fabs(ys - x2) < EPS * dx2 && fabs(zs - x3) < EPS * dx3) {
+                    const size_t c = (size_t)(i - 1) + (size_t)sx1 * ((size_t)(j - 1) + (size_t)sx2 * (k - 1));
+                    if (nc == 1) value = f[c];
+                    else for (int m = 0; m < 6; m++) lsig[m] = f[m * nh + c];
+                } else {
+                    double sum = 0;
+                    for (int l3 = -2; l3 <= 2; l3++) {
+                        if (k + l3 <= 0 || k + l3 > sx3) continue;
+                        const int i3p = l3 >= 0 ? (k - 1 + l3) % sx3 + 1 : (sx3 + k - 1 + l3) % sx3 + 1;
+                        for (int l2 = -2; l2 <= 2; l2++) {
+                            const int i2p = l2 >= 0 ? (j - 1 + l2) % sx2 + 1 : (sx2 + j - 1 + l2) % sx2 + 1;
+                            for (int l1 = -2; l1 <= 2; l1++) {
+                                const int i1p = l1 >= 0 ? (i - 1 + l1) % sx1 + 1 : (sx1 + i - 1 + l1) % sx1 + 1;
+                                const double weight = orc_sinc(((xs + l1 * dx1) - x1) / dx1) * dx1 *
+                                                      orc_sinc(((ys + l2 * dx2) - x2) / dx2) * dx2 *
+                                                      orc_sinc(((zs + l3 * dx3) - x3) / dx3) * dx3;
+                                const size_t c = (size_t)(i1p - 1) +
+                                                 (size_t)sx1 * ((size_t)(i2p - 1) + (size_t)sx2 * (i3p - 1));
+                                if (nc == 1) {
+                                    value = value + weight * f[c];
+                                } else {
+                                    const float w = (float)weight;
+                                    for (int m = 0; m < 6; m++) lsig[m] = lsig[m] + w * f[m * nh + c];
+                                }
+                                sum = sum + weight;
+                            }
+                        }
+                    }
+                    if (sum > (double)1e-6f) {
+                        if (nc == 1) {
+                            value = value / sum;
+                        } else {
+                            const float r = (float)(1.0 / sum);
+                            for (int m = 0; m < 6; m++) lsig[m] = r * lsig[m];
+                        }
+                    }
+                }
+            }
+            if (nc == 1) o[5] = value;
+            else for (int m = 0; m < 6; m++) o[5 + m] = lsig[m];
+        }
+}
+
 /* okada, src/okada/green_space.f90:29-105: source in the input convention
  * (north, east, depth of the top edge; degrees), receiver (north, east,
  * depth); displacement with x3 down */

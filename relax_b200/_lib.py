@@ -10,8 +10,8 @@ import os
 import re
 import subprocess
 
-from .config import (relax_config, relax_input_info, relax_layer, relax_slippatch, relax_source, relax_step_log,
-                     relax_tensor, relax_tensor_layer, relax_weakzone)
+from .config import (relax_config, relax_input_info, relax_layer, relax_obsplane, relax_segment, relax_slippatch,
+                     relax_source, relax_step_log, relax_tensor, relax_tensor_layer, relax_weakzone)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "librelax_b200.so")
@@ -106,6 +106,15 @@ def load() -> C.CDLL:
         "relax_input_config": (C.POINTER(relax_config), [P]),
         "relax_input_get_info": (I, [P, C.POINTER(relax_input_info)]),
         "relax_input_weakzones": (I, [P, I, C.POINTER(C.POINTER(relax_weakzone)), C.POINTER(I)]),
+        "relax_input_obsplanes": (I, [P, C.POINTER(C.POINTER(relax_obsplane)), C.POINTER(I)]),
+        "relax_input_segments": (I, [P, C.POINTER(C.POINTER(relax_segment)), C.POINTER(I)]),
+        "relax_monitor_plane": (I, [P, I, C.POINTER(relax_obsplane), D, C.POINTER(relax_slippatch), S,
+                                    C.POINTER(I), C.POINTER(I)]),
+        "relax_segment_stress": (I, [P, I, C.POINTER(relax_segment), C.POINTER(relax_tensor)]),
+        "relax_export_plane_stress": (I, [P, I, I, C.POINTER(relax_obsplane), D, D, C.c_char_p, I]),
+        "relax_write_segments": (I, [I, I, C.POINTER(relax_segment), C.POINTER(relax_tensor),
+                                     C.POINTER(relax_tensor), C.c_char_p]),
+        "relax_write_coulomb": (I, [I, C.POINTER(relax_segment), C.POINTER(relax_tensor), D, C.c_char_p, I]),
         "relax_input_build_weakzones": (I, [P, I]),
         "relax_get_plane": (I, [P, I, I, P, S]),
         "relax_get_points": (I, [P, I, C.POINTER(I), C.POINTER(D), C.POINTER(relax_tensor)]),

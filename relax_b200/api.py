@@ -19,8 +19,8 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from .config import (TENSOR_DTYPE, Simulation, relax_config, relax_input_info, relax_slippatch, relax_step_log,
-                     relax_tensor, relax_weakzone)
+from .config import (TENSOR_DTYPE, Simulation, relax_config, relax_input_info, relax_obsplane, relax_segment,
+                     relax_slippatch, relax_step_log, relax_tensor, relax_weakzone)
 
 FIELDS = {"u": 1, "sig": 2, "tau": 3, "moment": 4, "gamma": 5, "eps": 6, "v": 7, "ur": 8}
 NCOMP = {"u": 3, "gamma": 1, "sig": 6, "tau": 6, "moment": 6, "eps": 6, "v": 3, "ur": 3}
@@ -47,6 +47,28 @@ def es_format(v: float, w: int, d: int, e: int) -> str:
     buf = C.create_string_buffer(128)
     _lib.check(_lib.load().relax_es_format(v, w, d, e, buf, 128))
     return buf.value.decode()
+
+
+SEGMENT_EXPORTS = {"gmt": 1, "traction": 2, "vtp": 3}
+
+
+def write_segments(kind: str, segments: Sequence[relax_segment], filename, sig=None, sig0=None):
+    """exportgmt_rfaults_stress ("gmt"), exportgmt_rfaults_traction
+    ("traction") or exportvtk_rfaults_stress ("vtp") of the segments, from
+    the stress at their centres (None: zero) less sig0 when given."""
+    n = len(segments)
+    sop = (relax_segment * n)(*segments)
+    s = (relax_tensor * n)(*sig) if sig is not None else None
+    s0 = (relax_tensor * n)(*sig0) if sig0 is not None else None
+    _lib.check(_lib.load().relax_write_segments(SEGMENT_EXPORTS[kind], n, sop, s, s0, _path(filename)))
+
+
+def write_coulomb(segments: Sequence[relax_segment], sig, time: float, wdir, isnew: bool):
+    """exportcoulombstress: a line per segment in wdir/cfaults-sigma-KKKK.txt."""
+    n = len(segments)
+    sop = (relax_segment * n)(*segments)
+    s = (relax_tensor * n)(*sig)
+    _lib.check(_lib.load().relax_write_coulomb(n, sop, s, time, _path(wdir), 1 if isnew else 0))
 
 
 def write_grd(z: np.ndarray, x0: float, y0: float, dx: float, dy: float, title: str, filename):
@@ -132,6 +154,20 @@ class Input:
         z = C.POINTER(relax_weakzone)()
         n = C.c_int()
         _lib.check(self.lib.relax_input_weakzones(self.h, mechanism, C.byref(z), C.byref(n)))
+        return [z[k] for k in range(n.value)]
+
+    def obsplanes(self):
+        """Observation planes (internal convention, radians)."""
+        z = C.POINTER(relax_obsplane)()
+        n = C.c_int()
+        _lib.check(self.lib.relax_input_obsplanes(self.h, C.byref(z), C.byref(n)))
+        return [z[k] for k in range(n.value)]
+
+    def segments(self):
+        """Stress observation segments (internal convention, radians)."""
+        z = C.POINTER(relax_segment)()
+        n = C.c_int()
+        _lib.check(self.lib.relax_input_segments(self.h, C.byref(z), C.byref(n)))
         return [z[k] for k in range(n.value)]
 
     def build_weakzones(self, device: int = 0):
@@ -303,6 +339,34 @@ class Relax:
         NNN.sKKKKK.creep.dat and NNN.sKKKKK.{slip,vel}*.grd files in wdir."""
         formats = (1 if txt else 0) | (2 if grd else 0)
         _lib.check(self.lib.relax_export_creep(self.h, _path(wdir), index, formats))
+
+    def monitor_plane(self, op, name: str = "sig", beta: float = 0.0):
+        """monitorstressfield / monitorfield: the stress (patch.sig) or gamma
+        (patch.slip) sampled on an observation plane; an array of
+        (px3+1, px2+1) patches."""
+        px2, px3 = C.c_int(), C.c_int()
+        _lib.check(self.lib.relax_monitor_plane(self.h, FIELDS[name], C.byref(op), beta, None, 0, C.byref(px2),
+                                                C.byref(px3)))
+        n = (px2.value + 1) * (px3.value + 1)
+        arr = (relax_slippatch * n)()
+        _lib.check(self.lib.relax_monitor_plane(self.h, FIELDS[name], C.byref(op), beta, arr, n, C.byref(px2),
+                                                C.byref(px3)))
+        return np.ctypeslib.as_array(arr).copy().reshape(px3.value + 1, px2.value + 1)
+
+    def segment_stress(self, segments: Sequence[relax_segment]):
+        """The stress at the segment centres (nearest grid node)."""
+        n = len(segments)
+        sop = (relax_segment * n)(*segments)
+        sig = (relax_tensor * n)()
+        _lib.check(self.lib.relax_segment_stress(self.h, n, sop, sig))
+        return sig
+
+    def export_plane_stress(self, planes: Sequence[relax_obsplane], wdir, index: int, origx: float = 0.0,
+                            origy: float = 0.0, name: str = "sig"):
+        """exportplanestress (name "sig") / exporteigenstrain (name "gamma")."""
+        n = len(planes)
+        op = (relax_obsplane * n)(*planes)
+        _lib.check(self.lib.relax_export_plane_stress(self.h, FIELDS[name], n, op, origx, origy, _path(wdir), index))
 
     def export_points(self, xyz, names: Sequence[str], time: float, wdir, isnew: bool, rot: float = 0.0):
         """exportpoints: one .ned line per observation point (x1, x2, x3 in the computational frame)."""

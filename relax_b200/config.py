@@ -56,6 +56,14 @@ class relax_slippatch(C.Structure):
                  "taus")] + [("sig", relax_tensor)]
 
 
+class relax_obsplane(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("x", "y", "z", "length", "width", "strike", "dip")]
+
+
+class relax_segment(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("x", "y", "z", "length", "width", "strike", "dip", "friction")]
+
+
 class relax_weakzone(C.Structure):
     _fields_ = [(n, C.c_double) for n in
                 ("dgammadot0", "x", "y", "z", "width", "length", "thickness", "strike", "dip")] + \
@@ -390,11 +398,14 @@ class Simulation:
         return cfg, keep
 
     def to_input(self, wdir: str = "output", oz: float = 0.0, ozs: float = 0.0,
-                 points: Sequence[Tuple[str, float, float, float]] = ()) -> str:
+                 points: Sequence[Tuple[str, float, float, float]] = (),
+                 obsplanes: Sequence[Tuple[float, ...]] = (), segments: Sequence[Tuple[float, ...]] = ()) -> str:
         """This deck as a RELAX input file (the order of src/input.f90:43-1767,
         written with --with-transient sections when the deck has transient
         interfaces).  Numbers are written with repr, so reading them back
-        gives the same doubles."""
+        gives the same doubles.  obsplanes: (x1, x2, x3, length, width,
+        strike, dip) and segments: (x1, x2, x3, length, width, strike, dip,
+        friction), in the input file's convention (degrees)."""
         r = repr
         out = ["# grid dimension (sx1,sx2,sx3)", f"{self.sx1} {self.sx2} {self.sx3}",
                "# sampling (dx1,dx2,dx3), smoothing (beta, nyquist)",
@@ -405,10 +416,13 @@ class Simulation:
                "# elastic parameters and gamma", f"{r(self.lambda_)} {r(self.mu)} {r(self.gam)}",
                "# integration time, time step or (negative skip, scaling)",
                f"{r(self.interval)} {r(self.odt)}" + (f" {r(self.tscale)}" if self.odt < 0 else ""),
-               "# number of observation planes", "0",
-               "# number of observation points", str(len(points))]
+               "# number of observation planes", str(len(obsplanes))]
+        out += [f"{k + 1} " + " ".join(r(float(v)) for v in p) for k, p in enumerate(obsplanes)]
+        out += ["# number of observation points", str(len(points))]
         out += [f"{k + 1} {n} {r(x)} {r(y)} {r(z)}" for k, (n, x, y, z) in enumerate(points)]
-        out += ["# number of stress observation segments", "0", "# number of prestress interfaces", "0",
+        out += ["# number of stress observation segments", str(len(segments))]
+        out += [f"{k + 1} " + " ".join(r(float(v)) for v in g) for k, g in enumerate(segments)]
+        out += ["# number of prestress interfaces", "0",
                 "# number of linear viscous interfaces", str(len(self.linear))]
         out += [f"{k + 1} {r(d)} {r(g)} {r(c[0] if c else 0.0)}" for k, (d, g, *c) in enumerate(self.linear)]
         if self.linear:

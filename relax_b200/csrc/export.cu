@@ -7,6 +7,8 @@
 //   * VTK legacy binary files of a vector or a tensor field,
 //     src/writevtk.c:72-141 and the tensor variant that follows it;
 //   * the .ned time series at observation points, src/util.f90:83-124;
+//   * the afterslip planes, the observation planes and the stress
+//     observation segments, src/export.f90:308-849, :1364-2005;
 //   * the step log line, formats 1100-1103 of src/relax.f90:1102-1105.
 //
 // The netCDF classic format is written directly (big-endian header and
@@ -20,7 +22,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/relax_b200.h"
@@ -254,7 +258,8 @@ int write_vtk(const char *filename, const char *title, const char *name, int nco
 // Fortran edit descriptors of RELAX's text output
 // ---------------------------------------------------------------------------
 // ESw.dEe: one digit before the point, d after, an exponent of e digits;
-// a field that does not fit is w asterisks
+// a field that does not fit is w asterisks.  e = 0 is ESw.d: E and two
+// digits up to 99, a sign and three digits (no E) up to 999.
 std::string es(double v, int w, int d, int e)
 {
     char buf[64];
@@ -265,11 +270,14 @@ std::string es(double v, int w, int d, int e)
     std::string mant = s.substr(0, p);
     const int ex = atoi(s.c_str() + p + 1);
     const int ax = ex < 0 ? -ex : ex;
+    if (e < 0 || e > 4) return std::string(w, '*');
     int lim = 1;
-    for (int k = 0; k < e; k++) lim *= 10;
+    for (int k = 0; k < (e > 0 ? e : 3); k++) lim *= 10;
     if (ax >= lim) return std::string(w, '*');
     char eb[16];
-    snprintf(eb, sizeof eb, "E%c%0*d", ex < 0 ? '-' : '+', e, ax);
+    if (e > 0) snprintf(eb, sizeof eb, "E%c%0*d", ex < 0 ? '-' : '+', e, ax);
+    else if (ax <= 99) snprintf(eb, sizeof eb, "E%c%02d", ex < 0 ? '-' : '+', ax);
+    else snprintf(eb, sizeof eb, "%c%03d", ex < 0 ? '-' : '+', ax);
     std::string out = mant + eb;
     if ((int)out.size() > w) return std::string(w, '*');
     return std::string(w - out.size(), ' ') + out;
@@ -506,6 +514,207 @@ extern "C" int relax_export_creep(relax_ctx *ctx, const char *wdir, int index, i
     return RELAX_OK;
 }
 
+// exportplanestress / exporteigenstrain, src/export.f90:308-512
+extern "C" int relax_export_plane_stress(relax_ctx *ctx, int which, int nop, const relax_obsplane *op, double x0,
+                                         double y0, const char *wdir, int index)
+{
+    int sx[3];
+    double dx[3];
+    if (!ctx || !wdir || nop < 0 || (nop > 0 && !op)) return fail(RELAX_ERR_ARG, "null argument");
+    if (which != RELAX_FIELD_SIG && which != RELAX_FIELD_GAMMA)
+        return fail(RELAX_ERR_ARG, "plane exports sample the stress or gamma, not field %d", which);
+    int rc = relax_get_grid(ctx, sx, dx);
+    if (rc != RELAX_OK) return rc;
+    const std::string digit = iw(index, 3, 3);
+    for (int k = 0; k < nop; k++) {
+        int px2 = 0, px3 = 0;
+        if ((rc = relax_monitor_plane(ctx, which, &op[k], 0.0, nullptr, 0, &px2, &px3)) != RELAX_OK) return rc;
+        const int n1 = px2 + 1, n2 = px3 + 1;
+        std::vector<relax_slippatch> p((size_t)n1 * n2);
+        if ((rc = relax_monitor_plane(ctx, which, &op[k], 0.0, p.data(), p.size(), &px2, &px3)) != RELAX_OK)
+            return rc;
+        double xmin = p[0].lx, zmax = p[0].lz;
+        for (auto &q : p) {
+            q.x1 += x0;
+            q.x2 += y0;
+            xmin = std::fmin(xmin, q.lx);
+            zmax = std::fmax(zmax, q.lz);
+        }
+        std::vector<float> z((size_t)n1 * n2);
+        auto grid = [&](auto value, const std::string &file, const char *title) {
+            for (int i2 = 0; i2 < n2; i2++)
+                for (int i1 = 0; i1 < n1; i1++)
+                    z[(size_t)(n1 - 1 - i1) + (size_t)n1 * i2] = value(p[(size_t)i1 + (size_t)n1 * i2]);
+            return write_grd(z.data(), n1, n2, xmin, -zmax, dx[1], dx[2], title, file.c_str());
+        };
+        if (which == RELAX_FIELD_GAMMA) {
+            rc = grid([](const relax_slippatch &q) { return (float)q.slip; },
+                      std::string(wdir) + "/" + digit + ".s" + iw(k + 1, 5, 5) + ".estrain.grd", "monitor field");
+            if (rc != RELAX_OK) return rc;
+            continue;
+        }
+        const std::string stem = std::string(wdir) + "/" + digit + ".op" + iw(k + 1, 3, 3) + "-s";
+        float relax_tensor::*c[6] = {&relax_tensor::s11, &relax_tensor::s12, &relax_tensor::s13,
+                                     &relax_tensor::s22, &relax_tensor::s23, &relax_tensor::s33};
+        const char *suffix[6] = {"11", "12", "13", "22", "23", "33"};
+        for (int m = 0; m < 6; m++) {
+            rc = grid([&](const relax_slippatch &q) { return q.sig.*c[m]; }, stem + suffix[m] + ".grd",
+                      "monitor tensor field");
+            if (rc != RELAX_OK) return rc;
+        }
+    }
+    return RELAX_OK;
+}
+
+namespace {
+
+// The orientation and stress resolution of a segment, src/export.f90:1580-1622
+struct SegStress {
+    double n[3], s[3], d[3], t[3], ts[3];
+    double taun, taus, taustrike, taudip, taucoulomb;
+    relax_tensor sig;
+};
+
+SegStress resolve(const relax_segment &g, const relax_tensor *sig, const relax_tensor *sig0)
+{
+    SegStress r{};
+    r.sig = sig ? *sig : relax_tensor{0, 0, 0, 0, 0, 0};
+    if (sig && sig0) {
+        r.sig.s11 = r.sig.s11 - sig0->s11;
+        r.sig.s12 = r.sig.s12 - sig0->s12;
+        r.sig.s13 = r.sig.s13 - sig0->s13;
+        r.sig.s22 = r.sig.s22 - sig0->s22;
+        r.sig.s23 = r.sig.s23 - sig0->s23;
+        r.sig.s33 = r.sig.s33 - sig0->s33;
+    }
+    const double cs = std::cos(g.strike), ss = std::sin(g.strike), cd = std::cos(g.dip), sd = std::sin(g.dip);
+    r.n[0] = cd * cs;   r.n[1] = -cd * ss; r.n[2] = -sd;
+    r.s[0] = ss;        r.s[1] = cs;       r.s[2] = 0.0;
+    r.d[0] = -cs * sd;  r.d[1] = ss * sd;  r.d[2] = -cd;
+    const relax_tensor &t = r.sig;
+    const double *n = r.n;
+    r.t[0] = (double)t.s11 * n[0] + (double)t.s12 * n[1] + (double)t.s13 * n[2];
+    r.t[1] = (double)t.s12 * n[0] + (double)t.s22 * n[1] + (double)t.s23 * n[2];
+    r.t[2] = (double)t.s13 * n[0] + (double)t.s23 * n[1] + (double)t.s33 * n[2];
+    r.taun = r.t[0] * n[0] + r.t[1] * n[1] + r.t[2] * n[2];
+    for (int k = 0; k < 3; k++) r.ts[k] = r.t[k] - r.taun * n[k];
+    r.taus = std::sqrt(r.ts[0] * r.ts[0] + r.ts[1] * r.ts[1] + r.ts[2] * r.ts[2]);
+    r.taustrike = r.ts[0] * r.s[0] + r.ts[1] * r.s[1] + r.ts[2] * r.s[2];
+    r.taudip = r.ts[0] * r.d[0] + r.ts[1] * r.d[1] + r.ts[2] * r.d[2];
+    r.taucoulomb = r.taus + g.friction * r.taun;
+    return r;
+}
+
+std::string row(std::initializer_list<double> v, int w, int d, int e)
+{
+    std::string out;
+    for (double x : v) out += es(x, w, d, e);
+    return out;
+}
+
+// the XML lines of exportvtk_rfaults_stress, src/export.f90:1777-1863
+void vtp_array(FILE *fp, const char *type, const char *name, int ncomp, const char *extra)
+{
+    fprintf(fp, "        <DataArray type=\"%s\" Name=\"%s\"", type, name);
+    if (ncomp > 0) fprintf(fp, " NumberOfComponents=\"%d\"", ncomp);
+    fprintf(fp, " format=\"ascii\"%s>\n", extra);
+}
+
+}  // namespace
+
+extern "C" int relax_write_segments(int kind, int n, const relax_segment *sop, const relax_tensor *sig,
+                                    const relax_tensor *sig0, const char *filename)
+{
+    if (!filename || n < 0 || (n > 0 && !sop)) return fail(RELAX_ERR_ARG, "null argument");
+    if (kind < RELAX_SEG_GMT || kind > RELAX_SEG_VTP) return fail(RELAX_ERR_ARG, "unknown segment export %d", kind);
+    if (n == 0) return RELAX_OK;   // no file, as the reference
+    FILE *fp = fopen(filename, "w");
+    if (!fp) return fail(RELAX_ERR_ARG, "could not open %s for export", filename);
+    if (kind == RELAX_SEG_TRACTION)
+        fprintf(fp, "# position east, north, up, traction e, n, u, normal vector e, n, u\n");
+    if (kind == RELAX_SEG_VTP) {
+        fprintf(fp, "<?xml version=\"1.0\"?>\n<VTKFile type=\"PolyData\" version=\"0.1\">\n  <PolyData>\n");
+    }
+    for (int k = 0; k < n; k++) {
+        const relax_segment &g = sop[k];
+        const SegStress r = resolve(g, sig ? &sig[k] : nullptr, sig0 ? &sig0[k] : nullptr);
+        const double x1 = g.x, x2 = g.y, x3 = g.z, W = g.width, L = g.length;
+        const double *s = r.s, *d = r.d;
+        if (kind == RELAX_SEG_GMT) {
+            fprintf(fp, "> -Z%s\n", row({r.taus, r.taun, r.taucoulomb, r.taustrike, r.taudip}, 11, 2, 0).c_str());
+            fprintf(fp, "%s\n", row({x2 - d[1] * W / 2 - s[1] * L / 2, x1 - d[0] * W / 2 - s[0] * L / 2}, 11, 2, 0).c_str());
+            fprintf(fp, "%s\n", row({x2 - d[1] * W / 2 + s[1] * L / 2, x1 - d[0] * W / 2 + s[0] * L / 2}, 11, 2, 0).c_str());
+            fprintf(fp, "%s\n", row({x2 + d[1] * W / 2 + s[1] * L / 2, x1 + d[0] * W / 2 + s[0] * L / 2}, 11, 2, 0).c_str());
+            fprintf(fp, "%s\n", row({x2 + d[1] * W / 2 - s[1] * L / 2, x1 + d[0] * W / 2 - s[0] * L / 2}, 11, 2, 0).c_str());
+        } else if (kind == RELAX_SEG_TRACTION) {
+            fprintf(fp, "%s\n", row({x2, x1, -x3, r.ts[1], r.ts[0], -r.ts[2], r.n[1], r.n[0], -r.n[2]}, 11, 2, 0).c_str());
+        } else {
+            fprintf(fp, "    <Piece NumberOfPoints=\"4\" NumberOfPolys=\"1\">\n      <Points>\n");
+            vtp_array(fp, "Float32", "Fault Patch", 3, "");
+            fprintf(fp, "%s\n", row({x1 - d[0] * W / 2 - s[0] * L / 2, x2 - d[1] * W / 2 - s[1] * L / 2,
+                                      x3 - d[2] * W / 2 - s[2] * L / 2, x1 - d[0] * W / 2 + s[0] * L / 2,
+                                      x2 - d[1] * W / 2 + s[1] * L / 2, x3 - d[2] * W / 2 + s[2] * L / 2,
+                                      x1 + d[0] * W / 2 + s[0] * L / 2, x2 + d[1] * W / 2 + s[1] * L / 2,
+                                      x3 + d[2] * W / 2 + s[2] * L / 2, x1 + d[0] * W / 2 - s[0] * L / 2,
+                                      x2 + d[1] * W / 2 - s[1] * L / 2, x3 + d[2] * W / 2 - s[2] * L / 2},
+                                     11, 2, 0).c_str());
+            fprintf(fp, "        </DataArray>\n      </Points>\n      <Polys>\n");
+            vtp_array(fp, "Int32", "connectivity", 0, " RangeMin=\"0\" RangeMax=\"3\"");
+            fprintf(fp, "0 1 2 3\n        </DataArray>\n");
+            vtp_array(fp, "Int32", "offsets", 0, " RangeMin=\"4\" RangeMax=\"4\"");
+            fprintf(fp, "          4\n        </DataArray>\n      </Polys>\n");
+            fprintf(fp, "      <CellData Normals=\"stress\">\n");
+            vtp_array(fp, "Float32", "stress tensor", 6, "");
+            fprintf(fp, "%s\n        </DataArray>\n",
+                    row({r.sig.s11, r.sig.s12, r.sig.s13, r.sig.s22, r.sig.s23, r.sig.s33}, 11, 2, 0).c_str());
+            vtp_array(fp, "Float32", "traction vector", 3, "");
+            fprintf(fp, "%s\n        </DataArray>\n", row({r.t[0], r.t[1], r.t[2]}, 11, 2, 0).c_str());
+            vtp_array(fp, "Float32", "shear traction vector", 3, "");
+            for (int m = 0; m < 3; m++) fprintf(fp, "%s\n", es(r.ts[m], 11, 2, 0).c_str());
+            fprintf(fp, "        </DataArray>\n");
+            const std::pair<const char *, double> scalars[5] = {{"shear stress", r.taus},
+                                                                {"normal stress", r.taun},
+                                                                {"Coulomb stress", r.taucoulomb},
+                                                                {"stress in strike direction", r.taustrike},
+                                                                {"stress in dip direction", r.taudip}};
+            for (const auto &sc : scalars) {
+                vtp_array(fp, "Float32", sc.first, 1, "");
+                fprintf(fp, "%s\n        </DataArray>\n", es(sc.second, 11, 2, 0).c_str());
+            }
+            fprintf(fp, "      </CellData>\n    </Piece>\n");
+        }
+    }
+    if (kind == RELAX_SEG_VTP) fprintf(fp, "  </PolyData>\n</VTKFile>\n");
+    if (fclose(fp) != 0) return fail(RELAX_ERR_ARG, "writing %s failed", filename);
+    return RELAX_OK;
+}
+
+// exportcoulombstress, src/export.f90:1893-2005
+extern "C" int relax_write_coulomb(int n, const relax_segment *sop, const relax_tensor *sig, double time,
+                                   const char *wdir, int isnew)
+{
+    if (!wdir || n < 0 || (n > 0 && (!sop || !sig))) return fail(RELAX_ERR_ARG, "null argument");
+    for (int k = 0; k < n; k++) {
+        const std::string file = std::string(wdir) + "/cfaults-sigma-" + iw(k + 1, 4, 4) + ".txt";
+        FILE *fp = fopen(file.c_str(), isnew ? "w" : "a");
+        if (!fp) return fail(RELAX_ERR_ARG, "could not open %s for writing", file.c_str());
+        const relax_segment &g = sop[k];
+        if (isnew) {
+            fprintf(fp, "# center position (north, east, down): %s\n", row({g.x, g.y, g.z}, 9, 2, 0).c_str());
+            fprintf(fp, "#         t        s11        s12        s13        s22        s23        s33       taus"
+                        "       taud        tau       taun    Coulomb\n");
+        }
+        const SegStress r = resolve(g, &sig[k], nullptr);
+        fprintf(fp, "%s\n",
+                row({time, r.sig.s11, r.sig.s12, r.sig.s13, r.sig.s22, r.sig.s23, r.sig.s33, r.taustrike, r.taudip,
+                     r.taus, r.taun, r.taucoulomb},
+                    11, 3, 2)
+                    .c_str());
+        if (fclose(fp) != 0) return fail(RELAX_ERR_ARG, "writing %s failed", file.c_str());
+    }
+    return RELAX_OK;
+}
+
 // shiftedindex, src/elastic3d.f90:4063-4101, 0-based; sx3 is the number of
 // planes (sx3/2 of the grid)
 extern "C" int relax_shifted_index(double x1, double x2, double x3, int sx1, int sx2, int sx3, double dx1,
@@ -604,6 +813,6 @@ extern "C" const char *relax_ned_header(void) { return NED_HEADER; }
 // Fortran ESw.dEe of one value
 extern "C" int relax_es_format(double v, int w, int d, int e, char *buf, size_t size)
 {
-    if (w < 1 || w > 60 || d < 0 || d > 40 || e < 1 || e > 4) return fail(RELAX_ERR_ARG, "format");
+    if (w < 1 || w > 60 || d < 0 || d > 40 || e < 0 || e > 4) return fail(RELAX_ERR_ARG, "format");
     return copy_out(es(v, w, d, e), buf, size);
 }

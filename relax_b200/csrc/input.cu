@@ -29,13 +29,8 @@ namespace {
 
 const double DEG2RAD = 0.01745329251994329547437168059786927;
 
-struct ObsPlane {
-    double x, y, z, length, width, strike, dip;
-};
-
-struct Segment {
-    double x, y, z, length, width, strike, dip, friction;
-};
+typedef relax_obsplane ObsPlane;
+typedef relax_segment Segment;
 
 // ---------------------------------------------------------------------------
 // Fortran edit descriptors used by the echo
@@ -971,6 +966,22 @@ extern "C" int relax_input_get_info(const relax_input *in, relax_input_info *inf
     for (int m = 0; m < 4; m++) info->nwz[m] = (int)in->wz[m].size();
     info->minlength = in->minlength;
     info->minwidth = in->minwidth;
+    return RELAX_OK;
+}
+
+extern "C" int relax_input_obsplanes(const relax_input *in, const relax_obsplane **op, int *n)
+{
+    if (!in || !op || !n) return relax_noalloc_fail(RELAX_ERR_ARG, "null argument");
+    *n = (int)in->op.size();
+    *op = in->op.empty() ? nullptr : in->op.data();
+    return RELAX_OK;
+}
+
+extern "C" int relax_input_segments(const relax_input *in, const relax_segment **sop, int *n)
+{
+    if (!in || !sop || !n) return relax_noalloc_fail(RELAX_ERR_ARG, "null argument");
+    *n = (int)in->sop.size();
+    *sop = in->sop.empty() ? nullptr : in->sop.data();
     return RELAX_OK;
 }
 

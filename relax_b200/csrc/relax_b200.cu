@@ -2039,6 +2039,188 @@ extern "C" int relax_get_points(relax_ctx *c, int n, const int *index, double *u
     return RELAX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// observation planes: monitorstressfield / monitorfield,
+// src/elastic3d.f90:3404-3762
+// ---------------------------------------------------------------------------
+struct MonitorGeom {
+    double x, y, z, cs, ss, cd, sd;   // plane centre, cos / sin of strike and dip
+    int px2, px3;
+};
+
+// fix, src/elastic3d.f90:70-83: the nearest integer, halves rounded down
+__device__ __forceinline__ int fix_d(double v)
+{
+    const double f = floor(v), c = ceil(v);
+    return (int)(__dsub_rn(v, f) > 0.5 ? c : f);
+}
+
+// sinc, src/elastic3d.f90:498-506 (pi in double precision)
+__device__ __forceinline__ double sinc_d(double x)
+{
+    const double pi = 3.141592653589793115997963468544185161;
+    return x != 0.0 ? sin(__dmul_rn(pi, x)) / __dmul_rn(pi, x) : 1.0;
+}
+
+// One thread per sample point j2 + (px2 + 1) j3 of the plane.  NC = 6
+// samples the stress (sampletensor: a single-precision weighted sum, then
+// the single-precision factor 1/sum), NC = 1 the scalar field (sample:
+// double-precision sum).  The arithmetic keeps the reference's order and
+// precisions, with no contraction into fused multiply-adds.  out: 5 + NC
+// doubles per point -- x1, x2, x3, yr, zr and the sampled values.
+template <int NC>
+__global__ void k_monitor_plane(Grid g, const float *f, MonitorGeom p, double *out)
+{
+    const int n2 = p.px2 + 1;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n2 * (p.px3 + 1)) return;
+    const int j2 = q % n2 + 1, j3 = q / n2 + 1;
+    // ref2local
+    const double xa = __dsub_rn(__dmul_rn(p.cs, p.x), __dmul_rn(p.ss, p.y));
+    const double xr = __dsub_rn(__dmul_rn(p.cd, xa), __dmul_rn(p.sd, p.z));
+    double yr = __dadd_rn(__dmul_rn(p.ss, p.x), __dmul_rn(p.cs, p.y));
+    double zr = __dadd_rn(__dmul_rn(p.sd, xa), __dmul_rn(p.cd, p.z));
+    // single-precision offsets along strike and down dip
+    yr = (double)__fadd_rn((float)yr, (float)(((double)j2 - (double)p.px2 / 2.0 - 1.0) * g.dx2));
+    zr = (double)__fadd_rn((float)zr, (float)(((double)j3 - (double)p.px3 / 2.0 - 1.0) * g.dx3));
+    // local2ref
+    const double x2p = __dadd_rn(__dmul_rn(p.cd, xr), __dmul_rn(p.sd, zr));
+    const double x1 = __dadd_rn(__dmul_rn(p.cs, x2p), __dmul_rn(p.ss, yr));
+    const double x2 = __dadd_rn(-__dmul_rn(p.ss, x2p), __dmul_rn(p.cs, yr));
+    const double x3 = __dadd_rn(-__dmul_rn(p.sd, xr), __dmul_rn(p.cd, zr));
+    double *o = out + (size_t)q * (5 + NC);
+    o[0] = x1; o[1] = x2; o[2] = x3; o[3] = yr; o[4] = zr;
+    float acc[NC];
+    for (int m = 0; m < NC; m++) acc[m] = 0.f;
+    double value = 0.0;
+    const int sx1 = g.sx1, sx2 = g.sx2, sx3 = g.sx3h;
+    const double dx1 = g.dx1, dx2 = g.dx2, dx3 = g.dx3;
+    const bool inside = !(x1 > (double)(sx1 / 2 - 1) * dx1 || x1 < -(double)(sx1 / 2) * dx1 ||
+                          x2 > (double)(sx2 / 2 - 1) * dx2 || x2 < -(double)(sx2 / 2) * dx2 ||
+                          x3 > (double)(sx3 - 1) * dx3 || x3 < 0.0);
+    if (inside) {
+        // shiftedindex (1-based) and shiftedcoordinates of the closest node
+        const int i = (sx1 + fix_d(x1 / dx1)) % sx1 + 1;
+        const int j = (sx2 + fix_d(x2 / dx2)) % sx2 + 1;
+        const int k = fix_d(x3 / dx3) + 1;
+        const double x = (double)(i <= sx1 / 2 ? i - 1 : i - sx1 - 1) * dx1;
+        const double y = (double)(j <= sx2 / 2 ? j - 1 : j - sx2 - 1) * dx2;
+        const double z = (double)(k <= sx3 ? k - 1 : k - 2 * sx3 - 1) * dx3;
+        const double eps = (double)1e-2f;   // a single-precision literal in the reference
+        const size_t nh = g.nh;
+        if (fabs(x - x1) < eps * dx1 && fabs(y - x2) < eps * dx2 && fabs(z - x3) < eps * dx3) {
+            const size_t c = (size_t)(i - 1) + (size_t)sx1 * ((size_t)(j - 1) + (size_t)sx2 * (k - 1));
+            if (NC == 1) value = (double)f[c];
+            else for (int m = 0; m < NC; m++) acc[m] = f[m * nh + c];
+        } else {
+            double sum = 0.0;
+            for (int l3 = -2; l3 <= 2; l3++) {
+                if (k + l3 <= 0 || k + l3 > sx3) continue;
+                const int i3p = k + l3;
+                const double w3 = sinc_d(__dsub_rn(__dadd_rn(z, __dmul_rn((double)l3, dx3)), x3) / dx3);
+                for (int l2 = -2; l2 <= 2; l2++) {
+                    const int i2p = (sx2 + j - 1 + l2) % sx2 + 1;
+                    const double w2 = sinc_d(__dsub_rn(__dadd_rn(y, __dmul_rn((double)l2, dx2)), x2) / dx2);
+                    for (int l1 = -2; l1 <= 2; l1++) {
+                        const int i1p = (sx1 + i - 1 + l1) % sx1 + 1;
+                        const double w1 = sinc_d(__dsub_rn(__dadd_rn(x, __dmul_rn((double)l1, dx1)), x1) / dx1);
+                        // sinc(.)*dx1*sinc(.)*dx2*sinc(.)*dx3, left to right
+                        double w = __dmul_rn(w1, dx1);
+                        w = __dmul_rn(w, w2);
+                        w = __dmul_rn(w, dx2);
+                        w = __dmul_rn(w, w3);
+                        w = __dmul_rn(w, dx3);
+                        const size_t c = (size_t)(i1p - 1) + (size_t)sx1 * ((size_t)(i2p - 1) + (size_t)sx2 * (i3p - 1));
+                        if (NC == 1) {
+                            value = __dadd_rn(value, __dmul_rn(w, (double)f[c]));
+                        } else {
+                            const float wf = (float)w;
+                            for (int m = 0; m < NC; m++) acc[m] = __fadd_rn(acc[m], __fmul_rn(wf, f[m * nh + c]));
+                        }
+                        sum = __dadd_rn(sum, w);
+                    }
+                }
+            }
+            if (sum > (double)1e-6f) {
+                if (NC == 1) {
+                    value = value / sum;
+                } else {
+                    const float r = (float)(1.0 / sum);
+                    for (int m = 0; m < NC; m++) acc[m] = __fmul_rn(r, acc[m]);
+                }
+            }
+        }
+    }
+    if (NC == 1) o[5] = value;
+    else for (int m = 0; m < NC; m++) o[5 + m] = (double)acc[m];
+}
+
+extern "C" int relax_monitor_plane(relax_ctx *c, int which, const relax_obsplane *op, double beta,
+                                   relax_slippatch *out, size_t n, int *px2, int *px3)
+{
+    if (!c || !op) return fail(RELAX_ERR_ARG, "null argument");
+    if (which != RELAX_FIELD_SIG && which != RELAX_FIELD_GAMMA)
+        return fail(RELAX_ERR_ARG, "planes sample the stress or gamma, not field %d", which);
+    const Grid &g = c->g;
+    // called as monitorstressfield(x, y, z, width, length, ...): its L is the
+    // plane's width (down dip), its W the length (along strike)
+    const double Wp = op->length * (1.0 + 2.0 * beta), Lp = op->width * (1.0 + 2.0 * beta);
+    const int p2 = fixr(Wp / g.dx2), p3 = fixr(Lp / g.dx3);
+    if (p2 < 0 || p3 < 0 || p2 > (1 << 15) || p3 > (1 << 15))
+        return fail(RELAX_ERR_ARG, "observation plane of %d x %d samples", p2 + 1, p3 + 1);
+    if (px2) *px2 = p2;
+    if (px3) *px3 = p3;
+    if (!out) return RELAX_OK;
+    const size_t np = (size_t)(p2 + 1) * (p3 + 1);
+    if (n < np) return fail(RELAX_ERR_ARG, "%zu patches for a plane of %zu samples", n, np);
+    const int nc = which == RELAX_FIELD_SIG ? 6 : 1;
+    CK(cudaSetDevice(c->device));
+    if (which == RELAX_FIELD_SIG) TRY(field_sig(c));
+    double *buf = nullptr;
+    TRY(dalloc(&buf, (5 + nc) * np));
+    const MonitorGeom geo{op->x, op->y, op->z, cos(op->strike), sin(op->strike), cos(op->dip), sin(op->dip), p2, p3};
+    const unsigned nb = (unsigned)((np + 127) / 128);
+    if (nc == 6) k_monitor_plane<6><<<nb, 128, 0, c->st>>>(g, c->sig, geo, buf);
+    else k_monitor_plane<1><<<nb, 128, 0, c->st>>>(g, c->gamma, geo, buf);
+    cudaError_t e = cudaGetLastError();
+    std::vector<double> h((5 + nc) * np);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), buf, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(buf);
+    if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "plane sampling: %s", cudaGetErrorString(e));
+    for (size_t q = 0; q < np; q++) {
+        const double *v = &h[(5 + nc) * q];
+        relax_slippatch &s = out[q];
+        memset(&s, 0, sizeof s);
+        s.x1 = v[0]; s.x2 = v[1]; s.x3 = v[2]; s.lx = v[3]; s.lz = v[4];
+        if (nc == 1) {
+            s.slip = v[5];
+        } else {
+            s.sig.s11 = (float)v[5]; s.sig.s12 = (float)v[6]; s.sig.s13 = (float)v[7];
+            s.sig.s22 = (float)v[8]; s.sig.s23 = (float)v[9]; s.sig.s33 = (float)v[10];
+        }
+    }
+    return RELAX_OK;
+}
+
+extern "C" int relax_segment_stress(relax_ctx *c, int n, const relax_segment *sop, relax_tensor *sig)
+{
+    if (!c || n < 0 || (n > 0 && (!sop || !sig))) return fail(RELAX_ERR_ARG, "null argument");
+    if (n == 0) return RELAX_OK;
+    const Grid &g = c->g;
+    std::vector<int> idx(3 * (size_t)n);
+    for (int k = 0; k < n; k++) {
+        // shiftedindex with the full sx3, as the segment exports call it
+        TRY(relax_shifted_index(sop[k].x, sop[k].y, sop[k].z, g.sx1, g.sx2, 2 * g.sx3h, g.dx1, g.dx2, g.dx3,
+                                &idx[3 * k], &idx[3 * k + 1], &idx[3 * k + 2]));
+        if (idx[3 * k + 2] >= g.sx3h)
+            return fail(RELAX_ERR_ARG, "segment %d at depth %g lies below the stored half of the grid", k + 1,
+                        sop[k].z);
+    }
+    std::vector<double> u(3 * (size_t)n);
+    return relax_get_points(c, n, idx.data(), u.data(), sig);
+}
+
 // Keeps the corrector's velocity field v (src/relax.f90:829, the v1..v3
 // of the output block :959-975) for planes i3 < vel_planes, and accumulates
 // the postseismic displacement sum Dt v over planes i3 < ur_planes (u1r..u3r,

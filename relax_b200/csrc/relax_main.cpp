@@ -2,8 +2,9 @@
 // options of src/input.f90:64-185) on the B200 library: reads the input
 // file (an argument or standard input), runs the coseismic solve of the
 // first event and the relaxation loop on one GPU, writes the point time
-// series every step and the map-view grids, VTK fields and the time report
-// on output steps, and prints the step log.
+// series every step and the map-view grids, VTK fields, afterslip planes,
+// observation planes, stress segments and the time report on output steps,
+// and prints the step log.
 //
 // GPU: RELAX_DEVICE (default 0).
 #include <getopt.h>
@@ -12,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/relax_b200.h"
 
@@ -90,6 +92,14 @@ void exportoptsdat(const relax_input_info &info)
         fprintf(fp, "%s%s%s %s\n", a[0], a[1], a[2], info.ptsname[k]);
     }
     fclose(fp);
+}
+
+// wdir/<stem>-NNNN<ext>, the names of the segment exports
+std::string name4(const std::string &wdir, const char *stem, int i, const char *ext)
+{
+    char b[96];
+    snprintf(b, sizeof b, "/%s-%04d%s", stem, i, ext);
+    return wdir + b;
 }
 
 std::string name3(const std::string &wdir, const char *stem, int i, int digits)
@@ -197,6 +207,44 @@ int main(int argc, char **argv)
     int e = 1, oi = 1;
     relax_step_log log{};
 
+    // observation planes and stress observation segments (src/relax.f90:
+    // 330-333, 425-466 after the coseismic step; 939-942, 993-1025 at output
+    // steps); sig0 is the segments' stress after the coseismic step
+    // (export_rfaults_stress_init, src/export.f90:1364-1394)
+    const relax_obsplane *op = nullptr;
+    const relax_segment *sop = nullptr;
+    int nop = 0, nsop = 0;
+    relax_input_obsplanes(in, &op, &nop);
+    relax_input_segments(in, &sop, &nsop);
+    std::vector<relax_tensor> sig0(nsop), sigs(nsop);
+    auto planes_and_segments = [&](int index, double t, bool first) -> int {
+        int r = RELAX_OK;
+        if (o.eigenstrain && nop > 0)
+            r = relax_export_plane_stress(ctx, RELAX_FIELD_GAMMA, nop, op, info.x0, info.y0, wdir.c_str(), index);
+        if (r == RELAX_OK && nop > 0)
+            r = relax_export_plane_stress(ctx, RELAX_FIELD_SIG, nop, op, info.x0, info.y0, wdir.c_str(), index);
+        if (r != RELAX_OK || nsop == 0) return r;
+        if ((r = relax_segment_stress(ctx, nsop, sop, sigs.data())) != RELAX_OK) return r;
+        if (first) sig0 = sigs;
+        const relax_tensor *s = sigs.data(), *ds = first ? nullptr : sigs.data(), *s0 = first ? nullptr : sig0.data();
+        r = relax_write_segments(RELAX_SEG_VTP, nsop, sop, s, nullptr,
+                                 name4(wdir, "rfaults-sigma", index, ".vtp").c_str());
+        if (r == RELAX_OK)
+            r = relax_write_segments(RELAX_SEG_VTP, nsop, sop, ds, s0,
+                                     name4(wdir, "rfaults-dsigma", index, ".vtp").c_str());
+        if (r == RELAX_OK)
+            r = relax_write_segments(RELAX_SEG_GMT, nsop, sop, s, nullptr,
+                                     name4(wdir, "rfaults-sigma", index, ".xy").c_str());
+        if (r == RELAX_OK && first)
+            r = relax_write_segments(RELAX_SEG_TRACTION, nsop, sop, s, nullptr,
+                                     name4(wdir, "rfaults-traction", index, ".dat").c_str());
+        if (r == RELAX_OK)
+            r = relax_write_segments(RELAX_SEG_GMT, nsop, sop, ds, s0,
+                                     name4(wdir, "rfaults-dsigma", index, ".xy").c_str());
+        if (r == RELAX_OK) r = relax_write_coulomb(nsop, sop, s, t, wdir.c_str(), first ? 1 : 0);
+        return r;
+    };
+
     auto exports = [&](int index, double t, bool first) -> int {
         int r = RELAX_OK;
         // the afterslip planes, at output steps only (src/relax.f90:910-918)
@@ -245,6 +293,7 @@ int main(int argc, char **argv)
             r = check(relax_export_vtk(ctx, RELAX_FIELD_SIG, sx3h, 4, 4, 8, name3(wdir, "sigma", index, 4).c_str(),
                                        "stress tensor field", "stress"),
                       "vtk");
+        if (r == RELAX_OK) r = check(planes_and_segments(index, t, first), "observation planes and segments");
         if (r == RELAX_OK) r = reporttime(wdir, first ? 0 : 1, t);
         return r;
     };

@@ -92,3 +92,19 @@ def sources_small(sx=64, sz=32, interseismic=False):
         s.inter = Event(0.0, [Fault(0.1, -15.0, 10.0, 8.0, 10.0, 4.0, 0.0, 30.0, 90.0)],
                         tensile=[Tensile(0.05, 10.0, 10.0, 6.0, 1.0, 5.0, 0.0, 90.0)])
     return s
+
+
+def oracle_monitor_plane(lib, field, sx, dx, op, beta=0.0):
+    """The oracle's monitorstressfield / monitorfield on field (6 or 1
+    components of sx3h x sx2 x sx1 floats); returns an array of
+    (px3 + 1, px2 + 1, 5 + nc) doubles: x1, x2, x3, yr, zr and the values."""
+    import ctypes as C
+    f = np.ascontiguousarray(field, np.float32)
+    nc = 1 if f.ndim == 3 else f.shape[0]
+    px2, px3 = C.c_int(), C.c_int()
+    args = [nc, sx[0], sx[1], sx[2], dx[0], dx[1], dx[2], op.x, op.y, op.z, op.width, op.length, op.strike, op.dip,
+            beta, C.byref(px2), C.byref(px3)]
+    lib.orc_monitor_plane(f.ctypes.data, *args, None)
+    out = np.zeros((px3.value + 1, px2.value + 1, 5 + nc))
+    lib.orc_monitor_plane(f.ctypes.data, *args, out.ctypes.data)
+    return out

@@ -147,6 +147,12 @@ def test_vtk_legacy(tmp_path, ncomp, strides):
     (1234.5, 9, 2, 2, " 1.23E+03"),
     (-0.000123, 9, 2, 2, "-1.23E-04"),
     (0.0, 9, 2, 2, " 0.00E+00"),
+    (1234.5, 11, 2, 0, "   1.23E+03"),
+    (-4.5e-7, 11, 2, 0, "  -4.50E-07"),
+    (1.0e150, 11, 2, 0, "   1.00+150"),
+    (-2.5e-120, 11, 2, 0, "  -2.50-120"),
+    (1.0e300, 11, 2, 0, "   1.00+300"),
+    (-1.0e300, 8, 2, 0, "********"),
     (9.996, 9, 2, 2, " 1.00E+01"),
     (1e100, 9, 2, 2, "*********"),
     (100.0, 7, 2, 1, "1.00E+2"),

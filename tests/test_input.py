@@ -202,3 +202,20 @@ def test_echo_formats(capfd):
     assert "# output every 001 steps, dt scaled by 5.00E+0" in out
     assert "001  6.00E+00  1.00E+00  0.00E+00" in out
     assert "0001  1.00E+0 -1.00E+1  0.00E+0  0.00E+0 2.00E+1 6.00E+0    0.0  90.0    0.0" in out
+
+
+def test_observation_planes_and_segments_in_internal_convention():
+    from relax_b200.config import wang_convention
+    sim = linear_small(sx=32, sz=16)
+    sim.x0, sim.y0, sim.rot = 2.0, -1.0, 15.0
+    planes = [(1.0, 2.0, 0.5, 8.0, 6.0, 30.0, 60.0), (-3.0, 4.0, 1.0, 5.0, 5.0, -20.0, 90.0)]
+    segs = [(0.5, -1.5, 2.0, 4.0, 3.0, 10.0, 45.0, 0.6)]
+    inp = Input.parse(sim.to_input(obsplanes=planes, segments=segs))
+    assert (inp.info.nop, inp.info.nsop) == (2, 1)
+    for got, (x, y, z, L, W, s, d) in zip(inp.obsplanes(), planes):
+        _, wx, wy, wz, ws, wd, _ = wang_convention(0.0, x, y, z, L, W, s, d, 0.0, 2.0, -1.0, 15.0)
+        assert (got.x, got.y, got.z, got.length, got.width, got.strike, got.dip) == (wx, wy, wz, L, W, ws, wd)
+    (g,) = inp.segments()
+    x, y, z, L, W, s, d, fr = segs[0]
+    _, wx, wy, wz, ws, wd, _ = wang_convention(0.0, x, y, z, L, W, s, d, 0.0, 2.0, -1.0, 15.0)
+    assert (g.x, g.y, g.z, g.length, g.width, g.strike, g.dip, g.friction) == (wx, wy, wz, L, W, ws, wd, fr)
