@@ -110,9 +110,10 @@ def test_batch_without_batched_passes_steps_members_in_turn():
         _same(outs[k], _alone(s, 3))
 
 
-@pytest.mark.parametrize("sx,sz", [(64, 64), (192, 96)])
+@pytest.mark.parametrize("sx,sz", [(64, 64), (192, 96), (64, 128)])
 def test_batch_ensemble_shapes(sx, sz):
-    """the grid shapes of the uneven ensemble that need the 8 x 4 and 24 x 4 / 24 x 8 passes"""
+    """the grid shapes of the uneven ensemble that need the 8 x 4 and 24 x 4 / 24 x 8 passes, and
+    the 128-deep z pass"""
     base = powerlaw_small(sx=sx, sz=sz, dx=1.0, afterslip=False)
     sims = [_variant(base, k) for k in range(2)]
     outs, launches = _batched(sims, 2)

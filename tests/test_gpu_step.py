@@ -24,8 +24,10 @@ def compare(gpu, ref, tol):
         errs[k] = rel_l2(tensor_array(gpu[k]), tensor_array(ref[k]))
     if np.abs(ref["gamma"]).max() > 0:
         errs["gamma"] = rel_l2(gpu["gamma"][..., :-2], ref["gamma"][..., :-2])
+    # gamma accumulates gammadot ~ tau^n: for n = 3 it triples the stress
+    # error, so it gets three times the fields' bound
     for k, v in errs.items():
-        assert v <= tol, (k, v, errs)
+        assert v <= (3 * tol if k == "gamma" else tol), (k, v, errs)
     return errs
 
 
@@ -48,12 +50,20 @@ def check_logs(glogs, rlogs, tol):
         assert g[0] == o[0]
         for c in (1, 5, 6, 7):       # Dt, t, power, C:E^i
             assert abs(g[c] - o[c]) <= tol * max(abs(o[c]), 1e-30), (g, o, c)
-        for c in (2, 3, 4):          # Maxwell times (minima over the grid)
-            assert abs(g[c] - o[c]) <= 1e-5 * abs(o[c]), (g, o, c)
+        # Maxwell times (minima over the grid): tm ~ stress^(1 - n) doubles a
+        # field's relative error for n = 3, hence 2e-5 against the fields' 1e-5
+        for c in (2, 3, 4):
+            assert abs(g[c] - o[c]) <= 2e-5 * abs(o[c]), (g, o, c)
+
+
+def powerlaw_deep():
+    """sx3 = 128: the z pass with 16 threads per column."""
+    return powerlaw_small(sx=32, sz=128)
 
 
 @pytest.mark.parametrize("builder,nsteps", [(linear_small, 1), (linear_small, 5),
-                                            (powerlaw_small, 1), (powerlaw_small, 6)])
+                                            (powerlaw_small, 1), (powerlaw_small, 6),
+                                            (powerlaw_deep, 1), (powerlaw_deep, 4)])
 def test_run_matches_fp32_oracle(oracle32, oracle64, builder, nsteps):
     sim = builder()
     glogs, gf, gp = gpu_run(sim, nsteps)
@@ -63,9 +73,10 @@ def test_run_matches_fp32_oracle(oracle32, oracle64, builder, nsteps):
     tol = 1e-5 if nsteps == 1 else 1e-4
     check_logs(glogs, rlogs, 10 * tol)
     compare(gf, rf, tol)
-    # adaptive Dt of the oracle itself agrees with the GPU's
+    # adaptive Dt of the oracle itself agrees with the GPU's (Dt = tm/10: the
+    # Maxwell-time bound)
     alogs, _ = oracle32.run(sim, 1, fields=False)
-    assert abs(alogs[1][1] - glogs[1][1]) <= 1e-5 * alogs[1][1]
+    assert abs(alogs[1][1] - glogs[1][1]) <= 2e-5 * alogs[1][1]
     # error against the FP64 oracle of the same method
     dlogs, df = oracle64.run(sim, nsteps, dt_schedule=dts)
     compare(gf, df, tol)
