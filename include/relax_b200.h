@@ -368,11 +368,14 @@ int relax_write_vtk(const float *const *comp, int ncomp, int sx1, int sx2,
 int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int j2,
                      int j3, const char *filename, const char *title,
                      const char *name);
-/* exportcreep_asc / exportcreep_grd (src/export.f90:563-767): the patches
- * of every afterslip plane as wdir/NNN.sKKKKK.creep.dat (every third patch,
- * RELAX_CREEP_TXT) and as GMT grids of slip and slip rate (RELAX_CREEP_GRD). */
+/* exportcreep_asc / exportcreep_grd / exportcreep_vtk (src/export.f90:
+ * 563-849): the patches of every afterslip plane as wdir/NNN.sKKKKK.creep.dat
+ * (every third patch, RELAX_CREEP_TXT), as GMT grids of slip and slip rate
+ * (RELAX_CREEP_GRD) and as VTK polydata wdir/creep-KKKKKs-NNN.vtk
+ * (RELAX_CREEP_VTK). */
 #define RELAX_CREEP_TXT 1
 #define RELAX_CREEP_GRD 2
+#define RELAX_CREEP_VTK 4
 int relax_export_creep(relax_ctx *ctx, const char *wdir, int index,
                        int formats);
 /* exportplanestress (src/export.f90:308-397): the stress on observation

@@ -334,10 +334,11 @@ class Relax:
         _lib.check(self.lib.relax_export_vtk(self.h, FIELDS[name], sx3, *strides, _path(filename), title.encode(),
                                              vname.encode()))
 
-    def export_creep(self, wdir, index: int, txt: bool = True, grd: bool = True):
-        """exportcreep_asc / exportcreep_grd: the afterslip planes' patches as
-        NNN.sKKKKK.creep.dat and NNN.sKKKKK.{slip,vel}*.grd files in wdir."""
-        formats = (1 if txt else 0) | (2 if grd else 0)
+    def export_creep(self, wdir, index: int, txt: bool = True, grd: bool = True, vtk: bool = False):
+        """exportcreep_asc / exportcreep_grd / exportcreep_vtk: the afterslip
+        planes' patches as NNN.sKKKKK.creep.dat, NNN.sKKKKK.{slip,vel}*.grd and
+        creep-KKKKKs-NNN.vtk files in wdir."""
+        formats = (1 if txt else 0) | (2 if grd else 0) | (4 if vtk else 0)
         _lib.check(self.lib.relax_export_creep(self.h, _path(wdir), index, formats))
 
     def monitor_plane(self, op, name: str = "sig", beta: float = 0.0):

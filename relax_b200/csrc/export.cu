@@ -22,6 +22,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <initializer_list>
 #include <string>
 #include <utility>
@@ -454,7 +455,8 @@ extern "C" int relax_export_vtk(relax_ctx *ctx, int which, int sx3, int j1, int 
 // directions, one patch per line, 18ES11.3E2; exportcreep_asc), with
 // RELAX_CREEP_GRD the grids NNN.sKKKKK.slip-dip/slip-strike/slip.grd and
 // NNN.sKKKKK.vel-strike/vel-dip/vel.grd (exportcreep_grd, which writes the
-// dip-slip rate into vel-strike and the strike-slip rate into vel-dip; kept).
+// dip-slip rate into vel-strike and the strike-slip rate into vel-dip; kept),
+// with RELAX_CREEP_VTK wdir/creep-KKKKKs-NNN.vtk (exportcreep_vtk).
 extern "C" int relax_export_creep(relax_ctx *ctx, const char *wdir, int index, int formats)
 {
     int np = 0, sx[3];
@@ -487,6 +489,38 @@ extern "C" int relax_export_creep(relax_ctx *ctx, const char *wdir, int index, i
                     fprintf(fp, "%s\n", line.c_str());
                 }
             if (fclose(fp) != 0) return fail(RELAX_ERR_ARG, "writing %s.creep.dat failed", stem.c_str());
+        }
+        if (formats & RELAX_CREEP_VTK) {
+            // exportcreep_vtk, src/export.f90:776-849: the patch centres as
+            // points, two triangles per cell, the slip and rate fields
+            char name[64];
+            snprintf(name, sizeof name, "/creep-%05ds-%s.vtk", k + 1, digit.c_str());
+            const std::string file = std::string(wdir) + name;
+            FILE *fp = fopen(file.c_str(), "w");
+            if (!fp) return fail(RELAX_ERR_ARG, "could not open %s", file.c_str());
+            fprintf(fp, "# vtk DataFile Version 3.0\nafterslip\nASCII\nDATASET POLYDATA\nPOINTS %d float\n", n1 * n2);
+            for (const auto &q : p) fprintf(fp, "%s\n", (es(q.x1, 11, 3, 2) + es(q.x2, 11, 3, 2) + es(q.x3, 11, 3, 2)).c_str());
+            const int ncell = (n1 - 1) * (n2 - 1);
+            fprintf(fp, "\nPOLYGONS %d %d\n", std::max(0, ncell) * 2, std::max(0, ncell) * 2 * 4);
+            for (int i2 = 1; i2 <= n2 - 1; i2++)
+                for (int i1 = 1; i1 <= n1 - 1; i1++) {
+                    const int a0 = (i2 - 1) * n1 + i1 - 1;
+                    fprintf(fp, "3 %d %d %d\n", a0, a0 + 1, i2 * n1 + i1);
+                    fprintf(fp, "3 %d %d %d\n", a0, i2 * n1 + i1 - 1, i2 * n1 + i1);
+                }
+            fprintf(fp, "\nPOINT_DATA %d\n", n1 * n2);
+            // list-directed output in the reference (the layout is the
+            // compiler's); here one value per line, 17 significant digits
+            const std::pair<const char *, double relax_slippatch::*> fields[7] = {
+                {"afterslip", &relax_slippatch::slip},   {"strike_slip", &relax_slippatch::ss},
+                {"dip-slip", &relax_slippatch::ds},      {"velocity", &relax_slippatch::v},
+                {"velocity_strike_slip", &relax_slippatch::vss}, {"velocity_dip_slip", &relax_slippatch::vds},
+                {"shear_stress", &relax_slippatch::taus}};
+            for (const auto &f : fields) {
+                fprintf(fp, "SCALARS %s float\nLOOKUP_TABLE default\n", f.first);
+                for (const auto &q : p) fprintf(fp, " %.17G\n", q.*(f.second));
+            }
+            if (fclose(fp) != 0) return fail(RELAX_ERR_ARG, "writing %s failed", file.c_str());
         }
         if (formats & RELAX_CREEP_GRD) {
             if (n1 < 2 || n2 < 2) continue;   // a grid needs two nodes each way

@@ -248,7 +248,7 @@ int main(int argc, char **argv)
     auto exports = [&](int index, double t, bool first) -> int {
         int r = RELAX_OK;
         // the afterslip planes, at output steps only (src/relax.f90:910-918)
-        const int creep = (o.txt ? RELAX_CREEP_TXT : 0) | (o.grd ? RELAX_CREEP_GRD : 0);
+        const int creep = (o.txt ? RELAX_CREEP_TXT : 0) | (o.grd ? RELAX_CREEP_GRD : 0) | (o.vtk ? RELAX_CREEP_VTK : 0);
         if (!first && creep)
             r = check(relax_export_creep(ctx, wdir.c_str(), index, creep), "afterslip planes");
         if (!first && transient && o.grd && r == RELAX_OK)

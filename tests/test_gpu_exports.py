@@ -174,7 +174,7 @@ def test_creep_exports(tmp_path):
         r.coseismic()
         for _ in range(3):
             r.step()
-        r.export_creep(tmp_path, 4)
+        r.export_creep(tmp_path, 4, vtk=True)
         p = np.ctypeslib.as_array(r.patches(0)).copy()
         n1, n2 = r.cfg.planes[0].px2, r.cfg.planes[0].px3
     assert n1 >= 6 and n2 >= 4 and np.abs(p["v"]).max() > 0
@@ -201,3 +201,28 @@ def test_creep_exports(tmp_path):
         assert x[0] == p["lx"].min() and y[0] == -p["lz"].max()
         np.testing.assert_allclose(np.diff(x), sim.dx2)
         np.testing.assert_allclose(np.diff(y), sim.dx3)
+    # exportcreep_vtk: points, two triangles per cell, seven scalar fields
+    flat = p.reshape(-1)
+    text = (tmp_path / "creep-00001s-004.vtk").read_text().splitlines()
+    assert text[:5] == ["# vtk DataFile Version 3.0", "afterslip", "ASCII", "DATASET POLYDATA",
+                        f"POINTS {n1 * n2} float"]
+    pts = text[5:5 + n1 * n2]
+    assert pts == ["".join(api.es_format(float(q[f]), 11, 3, 2) for f in ("x1", "x2", "x3")) for q in flat]
+    k = 5 + n1 * n2
+    ncell = (n1 - 1) * (n2 - 1)
+    assert text[k] == "" and text[k + 1] == f"POLYGONS {2 * ncell} {8 * ncell}"
+    tri = [list(map(int, l.split()))[1:] for l in text[k + 2:k + 2 + 2 * ncell]]
+    assert tri[0] == [0, 1, n1 + 1] and tri[1] == [0, n1, n1 + 1]
+    a0 = (n2 - 2) * n1 + n1 - 2
+    assert tri[-2] == [a0, a0 + 1, (n2 - 1) * n1 + n1 - 1]
+    assert tri[-1] == [a0, (n2 - 1) * n1 + n1 - 2, (n2 - 1) * n1 + n1 - 1]
+    k += 2 + 2 * ncell
+    assert text[k] == "" and text[k + 1] == f"POINT_DATA {n1 * n2}"
+    k += 2
+    for name, f in (("afterslip", "slip"), ("strike_slip", "ss"), ("dip-slip", "ds"), ("velocity", "v"),
+                    ("velocity_strike_slip", "vss"), ("velocity_dip_slip", "vds"), ("shear_stress", "taus")):
+        assert text[k:k + 2] == [f"SCALARS {name} float", "LOOKUP_TABLE default"]
+        vals = np.array([float(v) for v in text[k + 2:k + 2 + n1 * n2]])
+        np.testing.assert_array_equal(vals, flat[f])
+        k += 2 + n1 * n2
+    assert k == len(text)
