@@ -433,7 +433,7 @@ struct Spectral {
     // Green's function: forward (x pass from `xa`), y, z spectral, y inverse,
     // x inverse with the epilogue in `xi`.
     int green(XfArgs xa, bool div, int nin, int nout, XiArgs xi, double lambda, double mu, double gam,
-              cudaStream_t st)
+              cudaStream_t st, cudaEvent_t join_before_xinv = nullptr)
     {
         xa = xargs(xa, nin);
         dim3 gx(g.sx2 / rows, nin + 1);
@@ -481,6 +481,7 @@ struct Spectral {
                   (k_ypass<+1><<<dim3((g.K1 + twy - 1) / twy, nout, 3), RELAX_NTHREADS, smy, st>>>(yb)));
         }
         xi = xiargs(xi);
+        if (join_before_xinv) CK(cudaStreamWaitEvent(st, join_before_xinv, 0));
         bool xr = false;
         if (use_reg) {
             TIMED(prof, ST_XINV, st, (xr = xinv_reg(xi, nout, st, &re)));
@@ -686,6 +687,12 @@ struct relax_ctx {
     // stress kernels store sig only there
     unsigned char *sig_mask = nullptr;
     unsigned *ticket = nullptr;                 // last-block counter of the stress kernels
+    // a side stream for the step's two kernels off the critical path: the
+    // time-step choice runs beside the predictor's FFT passes (joined before
+    // the x-inverse pass, the first to read Dt) and the patch monitor beside
+    // the corrector's (joined before the END pass, which rewrites sig)
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_dt = nullptr, ev_fork2 = nullptr, ev_mon = nullptr;
     StepState *dst = nullptr, *hst = nullptr;   // device state, pinned host mirror
     bool own_dst = true;                         // false: dst lives in a batch's array
     float *tm_part = nullptr, *fr_part = nullptr;
@@ -745,6 +752,9 @@ static void free_ctx(relax_ctx *c)
     if (c->amp_part) cudaFree(c->amp_part);
     if (c->amp_alt) cudaFree(c->amp_alt);
     c->sp.release();
+    for (cudaEvent_t e : {c->ev_fork, c->ev_dt, c->ev_fork2, c->ev_mon})
+        if (e) cudaEventDestroy(e);
+    if (c->st2) cudaStreamDestroy(c->st2);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }
@@ -776,6 +786,9 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&c->ev_fork, &c->ev_dt, &c->ev_fork2, &c->ev_mon})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     TRY(make_grid(c->g, cfg->sx1, cfg->sx2, cfg->sx3, cfg->dx1, cfg->dx2, cfg->dx3));
     const Grid &g = c->g;
     const int nz = g.sx3h;
@@ -1496,14 +1509,15 @@ static int friction_planes(relax_ctx *c, bool want_tm, int *nblk_out)
     return RELAX_OK;
 }
 
-static int monitor_planes(relax_ctx *c, bool with_dt)
+static int monitor_planes(relax_ctx *c, bool with_dt, cudaStream_t st = nullptr)
 {
+    if (!st) st = c->st;
     for (size_t k = 0; k < c->planes.size(); k++) {
         const relax_plane &p = c->planes[k];
         const int n = std::max(0, p.px2) * std::max(0, p.px3);
         if (n == 0) continue;
         MonitorArgs a = monitor_args(c, k, with_dt);
-        TIMED(&c->prof, ST_MONITOR, c->st, (k_monitor<<<nblocks(n, 128), 128, 0, c->st>>>(a)));
+        TIMED(&c->prof, ST_MONITOR, st, (k_monitor<<<nblocks(n, 128), 128, 0, st>>>(a)));
     }
     return RELAX_OK;
 }
@@ -1641,8 +1655,13 @@ static int step_kernels(relax_ctx *c)
     int nfr = 0;
     if (!c->fc.empty()) TRY(friction_planes(c, true, &nfr));
     // the Maxwell-time minima come reduced from the last INIT/END stress
-    // pass; the policy and the step's inputs are in c->dtp_d
-    TIMED(&c->prof, ST_DT, c->st, (k_dt_dev<<<1, RELAX_NTHREADS, 0, c->st>>>(c->dst, c->dtp_d, c->fr_part, nfr)));
+    // pass; the policy and the step's inputs are in c->dtp_d.  The choice
+    // runs on the side stream: nothing before the predictor's x-inverse pass
+    // reads Dt (surface loads join at once, below).
+    CK(cudaEventRecord(c->ev_fork, c->st));
+    CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+    TIMED(&c->prof, ST_DT, c->st2, (k_dt_dev<<<1, RELAX_NTHREADS, 0, c->st2>>>(c->dst, c->dtp_d, c->fr_part, nfr)));
+    CK(cudaEventRecord(c->ev_dt, c->st2));
     // The kernels take Dt from the device state.  The host needs it before
     // the end of the step only for surface loads (evaluated on the host at
     // t + Dt); otherwise the step runs with one synchronisation, at its end.
@@ -1651,6 +1670,7 @@ static int step_kernels(relax_ctx *c)
     const EventCopy &ev = c->events[c->e];
     double Dt = 0.0;
     if (!ev.l.empty()) {
+        CK(cudaStreamWaitEvent(c->st, c->ev_dt, 0));
         TRY(pull_state(c));
         Dt = c->hst->Dt;
         if (!(c->hst->dt_raw > 0.0) || !std::isfinite(c->hst->dt_raw))
@@ -1663,14 +1683,20 @@ static int step_kernels(relax_ctx *c)
         XfArgs xa = xf_div(c);
         xa.tload = loads ? c->tload : nullptr;
         XiArgs xi = xi_update(c, c->vp, c->u, 0.5f, true);
-        TRY(c->sp.green(xa, true, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st));
+        TRY(c->sp.green(xa, true, g.sx3h, g.sx3h, xi, c->cfg.lambda, c->cfg.mu, c->cfg.gam, c->st, c->ev_dt));
     }
     // ---- corrector -------------------------------------------------------
+    bool mon_forked = false;
     TRY(launch_stress<MODE_CORR>(c, stress_args(c, c->vp)));
     if (!c->fc.empty()) {
         int unused = 0;
         TRY(friction_planes(c, false, &unused));
-        TRY(monitor_planes(c, true));
+        // the patches read sig and Dt only; joined before the END pass
+        CK(cudaEventRecord(c->ev_fork2, c->st));
+        CK(cudaStreamWaitEvent(c->st2, c->ev_fork2, 0));
+        TRY(monitor_planes(c, true, c->st2));
+        CK(cudaEventRecord(c->ev_mon, c->st2));
+        mon_forked = true;
     }
     if (!c->inter.s.empty()) {
         for (const auto &s : c->inter.s) {
@@ -1719,6 +1745,7 @@ static int step_kernels(relax_ctx *c)
     // the kernel's last block.  When t + Dt reaches the next event (the test
     // of src/relax.f90:859, made by k_dt) the kernel does nothing and
     // finish_step runs the event branch instead.
+    if (mon_forked) CK(cudaStreamWaitEvent(c->st, c->ev_mon, 0));
     TRY(launch_stress<MODE_END>(c, stress_args(c, c->u)));
     return RELAX_OK;
 }
