@@ -400,6 +400,31 @@ int relax_export_plane_stress(relax_ctx *ctx, int which, int nop,
 int relax_write_segments(int kind, int n, const relax_segment *sop,
                          const relax_tensor *sig, const relax_tensor *sig0,
                          const char *filename);
+/* The geometry files of the input reader (VTK PolyData XML and GMT .xy):
+ * exportvtk_grid (src/export.f90:1068-1127), the box of the grid;
+ * exportvtk_rectangle (:2014-2093), a rectangle of centre x, length L along
+ * strike, width W down dip (radians); exportxy_brick (:2101-2153) and
+ * exportvtk_allbricks (:2295-2599), weak zones; exportvtk_rfaults
+ * (RELAX_FAULTS_VTP, :1216-1354) and exportxy_rfaults (RELAX_FAULTS_XY,
+ * :1139-1206, origin x0, y0 added), the sources of an event. */
+#define RELAX_FAULTS_VTP 1
+#define RELAX_FAULTS_XY 2
+int relax_write_vtk_grid(int sx1, int sx2, int sx3, double dx1, double dx2,
+                         double dx3, const char *filename);
+int relax_write_vtk_rectangle(double x1, double x2, double x3, double L,
+                              double W, double strike, double dip,
+                              const char *filename);
+int relax_write_xy_brick(const relax_weakzone *zone, const char *filename);
+int relax_write_vtk_bricks(int n, const relax_weakzone *zones,
+                           const char *filename);
+int relax_write_faults(int kind, int n, const relax_source *src, double x0,
+                       double y0, const char *filename);
+/* All the geometry files that the input reader (init, src/input.f90:
+ * 296-1452) writes into the input's output directory: with vtk the .vtp
+ * files (grid, viscous and transient interfaces, weak zones, afterslip
+ * planes, each event's faults), always the GMT .xy files (weak zones, each
+ * event's faults). */
+int relax_input_export_geometry(const relax_input *in, int vtk);
 /* exportcoulombstress (src/export.f90:1893-2005): one line of time, stress
  * and shear, normal and Coulomb stress per segment appended to
  * wdir/cfaults-sigma-KKKK.txt (a new file with its header when isnew). */

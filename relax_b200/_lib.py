@@ -106,6 +106,12 @@ def load() -> C.CDLL:
         "relax_input_config": (C.POINTER(relax_config), [P]),
         "relax_input_get_info": (I, [P, C.POINTER(relax_input_info)]),
         "relax_input_weakzones": (I, [P, I, C.POINTER(C.POINTER(relax_weakzone)), C.POINTER(I)]),
+        "relax_input_export_geometry": (I, [P, I]),
+        "relax_write_vtk_grid": (I, [I, I, I, D, D, D, C.c_char_p]),
+        "relax_write_vtk_rectangle": (I, [D, D, D, D, D, D, D, C.c_char_p]),
+        "relax_write_xy_brick": (I, [C.POINTER(relax_weakzone), C.c_char_p]),
+        "relax_write_vtk_bricks": (I, [I, C.POINTER(relax_weakzone), C.c_char_p]),
+        "relax_write_faults": (I, [I, I, C.POINTER(relax_source), D, D, C.c_char_p]),
         "relax_input_obsplanes": (I, [P, C.POINTER(C.POINTER(relax_obsplane)), C.POINTER(I)]),
         "relax_input_segments": (I, [P, C.POINTER(C.POINTER(relax_segment)), C.POINTER(I)]),
         "relax_monitor_plane": (I, [P, I, C.POINTER(relax_obsplane), D, C.POINTER(relax_slippatch), S,

@@ -156,6 +156,11 @@ class Input:
         _lib.check(self.lib.relax_input_weakzones(self.h, mechanism, C.byref(z), C.byref(n)))
         return [z[k] for k in range(n.value)]
 
+    def export_geometry(self, vtk: bool = True):
+        """The geometry files that the reference's input reader writes into
+        the output directory (grid, interfaces, weak zones, planes, faults)."""
+        _lib.check(self.lib.relax_input_export_geometry(self.h, 1 if vtk else 0))
+
     def obsplanes(self):
         """Observation planes (internal convention, radians)."""
         z = C.POINTER(relax_obsplane)()

@@ -723,6 +723,226 @@ extern "C" int relax_write_segments(int kind, int n, const relax_segment *sop, c
     return RELAX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// geometry files of the input reader (src/export.f90:1068-1206, 1216-1354,
+// 2014-2153, 2295-2599)
+// ---------------------------------------------------------------------------
+namespace {
+
+const char *const XML_HEAD = "<?xml version=\"1.0\"?>\n<VTKFile type=\"PolyData\" version=\"0.1\">\n  <PolyData>\n";
+const char *const XML_TAIL = "  </PolyData>\n</VTKFile>\n";
+
+// strike, dip and normal unit vectors of the rectangle writers (dip vector
+// pointing down dip: d = (cs sd, -ss sd, cd))
+struct Frame {
+    double s[3], d[3], n[3];
+    Frame(double strike, double dip)
+    {
+        const double cs = std::cos(strike), ss = std::sin(strike), cd = std::cos(dip), sd = std::sin(dip);
+        s[0] = ss; s[1] = cs; s[2] = 0.0;
+        d[0] = cs * sd; d[1] = -ss * sd; d[2] = cd;
+        n[0] = cd * cs; n[1] = -cd * ss; n[2] = -sd;
+    }
+};
+
+// corner (sd, ss, sn = +-1) of a brick of centre x, half-extents W/2 down
+// dip, L/2 along strike, T/2 along the normal
+void corner(const Frame &f, const double *x, double L, double W, double T, int sd, int ss, int sn, double *out)
+{
+    for (int k = 0; k < 3; k++) {
+        out[k] = x[k] + sd * f.d[k] * W / 2 + ss * f.s[k] * L / 2;
+        if (sn) out[k] = out[k] + sn * f.n[k] * T / 2.0;   // rectangles (sn = 0) have no normal term
+    }
+}
+
+std::string row_es(const std::vector<double> &v, int w, int d, int e)
+{
+    std::string out;
+    for (double x : v) out += es(x, w, d, e);
+    return out;
+}
+
+void vtp_polys(FILE *fp, const char *conn, int rmax, const char *offsets, int omin, int omax)
+{
+    fprintf(fp, "      <Polys>\n        <DataArray type=\"Int32\" Name=\"connectivity\" format=\"ascii\" "
+                "RangeMin=\"0\" RangeMax=\"%d\">\n%s\n        </DataArray>\n", rmax, conn);
+    fprintf(fp, "        <DataArray type=\"Int32\" Name=\"offsets\" format=\"ascii\" RangeMin=\"%d\" "
+                "RangeMax=\"%d\">\n%s\n        </DataArray>\n      </Polys>\n", omin, omax, offsets);
+}
+
+void vtp_points(FILE *fp, int npts, int npolys, const char *name, const std::string &coords)
+{
+    fprintf(fp, "    <Piece NumberOfPoints=\"%d\" NumberOfPolys=\"%d\">\n      <Points>\n", npts, npolys);
+    fprintf(fp, "        <DataArray type=\"Float32\" Name=\"%s\" NumberOfComponents=\"3\" format=\"ascii\">\n"
+                "%s\n        </DataArray>\n      </Points>\n", name, coords.c_str());
+}
+
+int closed(FILE *fp, const char *filename)
+{
+    if (fclose(fp) != 0) return fail(RELAX_ERR_ARG, "writing %s failed", filename);
+    return RELAX_OK;
+}
+
+}  // namespace
+
+// exportvtk_grid, src/export.f90:1068-1127
+extern "C" int relax_write_vtk_grid(int sx1, int sx2, int sx3, double dx1, double dx2, double dx3,
+                                    const char *filename)
+{
+    if (!filename) return fail(RELAX_ERR_ARG, "null argument");
+    FILE *fp = fopen(filename, "w");
+    if (!fp) return fail(RELAX_ERR_ARG, "could not open %s for export", filename);
+    const double a = sx1 * dx1 / 2, b = sx2 * dx2 / 2, c = sx3 * dx3 / 2;
+    fputs(XML_HEAD, fp);
+    vtp_points(fp, 8, 6, "Computational Grid",
+               row_es({-a, -b, c, a, -b, c, a, b, c, -a, b, c, -a, -b, 0.0, a, -b, 0.0, a, b, 0.0, -a, b, 0.0}, 9, 2,
+                      1));
+    vtp_polys(fp, "0 1 2 3 4 5 6 7 2 3 7 6 0 3 7 4 0 1 5 4 1 2 6 5", 7, "          4 8 12 16 20 24", 4, 24);
+    fprintf(fp, "    </Piece>\n");
+    fputs(XML_TAIL, fp);
+    return closed(fp, filename);
+}
+
+// exportvtk_rectangle, src/export.f90:2014-2093
+extern "C" int relax_write_vtk_rectangle(double x1, double x2, double x3, double L, double W, double strike,
+                                         double dip, const char *filename)
+{
+    if (!filename) return fail(RELAX_ERR_ARG, "null argument");
+    FILE *fp = fopen(filename, "w");
+    if (!fp) return fail(RELAX_ERR_ARG, "could not open %s for export in ExportVTK_Rectangle", filename);
+    const Frame f(strike, dip);
+    const double x[3] = {x1, x2, x3};
+    std::vector<double> v;
+    const int sgn[4][2] = {{-1, -1}, {-1, 1}, {1, 1}, {1, -1}};
+    for (const auto &q : sgn) {
+        double c[3];
+        corner(f, x, L, W, 0.0, q[0], q[1], 0, c);
+        v.insert(v.end(), c, c + 3);
+    }
+    fputs(XML_HEAD, fp);
+    vtp_points(fp, 4, 1, "Fault Patch", row_es(v, 11, 2, 0));
+    vtp_polys(fp, "0 1 2 3", 3, "          4", 4, 4);
+    fprintf(fp, "    </Piece>\n");
+    fputs(XML_TAIL, fp);
+    return closed(fp, filename);
+}
+
+// exportxy_brick, src/export.f90:2101-2153: the faces below and above the
+// zone's mid-plane as two closed GMT polygons (east, north, depth)
+extern "C" int relax_write_xy_brick(const relax_weakzone *z, const char *filename)
+{
+    if (!z || !filename) return fail(RELAX_ERR_ARG, "null argument");
+    FILE *fp = fopen(filename, "w");
+    if (!fp) return fail(RELAX_ERR_ARG, "could not open %s for export in ExportXY_Brick", filename);
+    const Frame f(z->strike, z->dip);
+    const double x[3] = {z->x, z->y, z->z};
+    const int loop[5][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}, {-1, -1}};   // (strike, normal) signs
+    for (int sd = -1; sd <= 1; sd += 2) {
+        fprintf(fp, ">\n");
+        for (const auto &q : loop) {
+            double c[3];
+            corner(f, x, z->length, z->width, z->thickness, sd, q[0], q[1], c);
+            fprintf(fp, "%s\n", row_es({c[1], c[0], c[2]}, 11, 2, 0).c_str());
+        }
+    }
+    return closed(fp, filename);
+}
+
+// exportvtk_allbricks, src/export.f90:2295-2599: two pieces per zone (three
+// faces each) with the zone's strain
+extern "C" int relax_write_vtk_bricks(int n, const relax_weakzone *z, const char *filename)
+{
+    if (!filename || n < 0 || (n > 0 && !z)) return fail(RELAX_ERR_ARG, "null argument");
+    FILE *fp = fopen(filename, "w");
+    if (!fp) return fail(RELAX_ERR_ARG, "could not open %s for export in ExportVTK_Brick", filename);
+    fputs(XML_HEAD, fp);
+    // the eight corners in the reference's order: (dip, strike, normal) signs
+    const int order[8][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1},
+                             {1, -1, 1},   {-1, -1, 1}, {-1, 1, 1}, {1, 1, 1}};
+    for (int i = 0; i < n; i++) {
+        const relax_weakzone &w = z[i];
+        const Frame f(w.strike, w.dip);
+        const double x[3] = {w.x, w.y, w.z};
+        std::vector<double> v;
+        for (const auto &o : order) {
+            double c[3];
+            corner(f, x, w.length, w.width, w.thickness, o[0], o[1], o[2], c);
+            v.insert(v.end(), c, c + 3);
+        }
+        const relax_tensor &e = w.e;
+        const double ekk = (double)(e.s11 + e.s22 + e.s33);
+        const double dev = std::sqrt((e.s11 - ekk / 3) * (e.s11 - ekk / 3) + (e.s22 - ekk / 3) * (e.s22 - ekk / 3) +
+                                     (e.s33 - ekk / 3) * (e.s33 - ekk / 3) + (double)(2 * e.s12 * e.s12) +
+                                     (double)(2 * e.s13 * e.s13) + (double)(2 * e.s23 * e.s23));
+        const std::pair<const char *, double> cells[8] = {{"isotropic strain", ekk}, {"deviatoric strain", dev},
+                                                          {"e11", e.s11}, {"e12", e.s12}, {"e13", e.s13},
+                                                          {"e22", e.s22}, {"e23", e.s23}, {"e33", e.s33}};
+        const char *conn[2] = {"7 4 5 6 7 4 3 2 7 2 1 6", "0 1 2 3 0 5 4 3 0 1 6 5"};
+        const int rmax[2] = {6, 7};
+        for (int piece = 0; piece < 2; piece++) {
+            vtp_points(fp, 8, 1, "Weak Zone", row_es(v, 11, 2, 0));
+            vtp_polys(fp, conn[piece], rmax[piece], "          12", 12, 12);
+            fprintf(fp, "      <CellData Normals=\"slip\">\n");
+            for (const auto &cell : cells) {
+                vtp_array(fp, "Float32", cell.first, 1, "");
+                fprintf(fp, "%s\n        </DataArray>\n", es(cell.second, 11, 2, 0).c_str());
+            }
+            fprintf(fp, "      </CellData>\n    </Piece>\n");
+        }
+    }
+    fputs(XML_TAIL, fp);
+    return closed(fp, filename);
+}
+
+// exportvtk_rfaults (kind RELAX_FAULTS_VTP, src/export.f90:1216-1354) and
+// exportxy_rfaults (kind RELAX_FAULTS_XY, :1139-1206) of n sources in the
+// internal convention; the GMT file adds the origin x0, y0
+extern "C" int relax_write_faults(int kind, int n, const relax_source *src, double x0, double y0,
+                                  const char *filename)
+{
+    if (!filename || n < 0 || (n > 0 && !src)) return fail(RELAX_ERR_ARG, "null argument");
+    if (kind != RELAX_FAULTS_VTP && kind != RELAX_FAULTS_XY) return fail(RELAX_ERR_ARG, "unknown fault export %d", kind);
+    FILE *fp = fopen(filename, "w");
+    if (!fp) return fail(RELAX_ERR_ARG, "could not open %s for export", filename);
+    if (kind == RELAX_FAULTS_VTP) fputs(XML_HEAD, fp);
+    else fprintf(fp, "> # east, north\n");
+    const int sgn[4][2] = {{-1, -1}, {-1, 1}, {1, 1}, {1, -1}};
+    for (int k = 0; k < n; k++) {
+        const relax_source &q = src[k];
+        const Frame f(q.strike, q.dip);
+        if (kind == RELAX_FAULTS_XY) {
+            const double x[3] = {q.x + x0, q.y + y0, q.z};
+            fprintf(fp, "> -Z%s\n", es(std::fabs(q.slip), 11, 2, 0).c_str());
+            for (const auto &c4 : sgn) {
+                double c[3];
+                corner(f, x, q.length, q.width, 0.0, c4[0], c4[1], 0, c);
+                fprintf(fp, "%s\n", row_es({c[1], c[0]}, 11, 2, 0).c_str());
+            }
+            continue;
+        }
+        const double x[3] = {q.x, q.y, q.z};
+        std::vector<double> v;
+        for (const auto &c4 : sgn) {
+            double c[3];
+            corner(f, x, q.length, q.width, 0.0, c4[0], c4[1], 0, c);
+            v.insert(v.end(), c, c + 3);
+        }
+        vtp_points(fp, 4, 1, "Fault Patch", row_es(v, 11, 2, 0));
+        vtp_polys(fp, "0 1 2 3", 3, "          4", 4, 4);
+        fprintf(fp, "      <CellData Normals=\"slip\">\n");
+        const double cr = std::cos(q.rake), sr = std::sin(q.rake);
+        vtp_array(fp, "Float32", "slip", 3, "");
+        fprintf(fp, "%s\n        </DataArray>\n",
+                row_es({(f.s[0] * cr + f.d[0] * sr) * q.slip, (f.s[1] * cr + f.d[1] * sr) * q.slip,
+                        (f.s[2] * cr + f.d[2] * sr) * q.slip}, 11, 2, 0).c_str());
+        vtp_array(fp, "Float32", "opening", 3, "");
+        fprintf(fp, "%s\n        </DataArray>\n      </CellData>\n    </Piece>\n",
+                row_es({f.n[0] * q.opening, f.n[1] * q.opening, f.n[2] * q.opening}, 11, 2, 0).c_str());
+    }
+    if (kind == RELAX_FAULTS_VTP) fputs(XML_TAIL, fp);
+    return closed(fp, filename);
+}
+
 // exportcoulombstress, src/export.f90:1893-2005
 extern "C" int relax_write_coulomb(int n, const relax_segment *sop, const relax_tensor *sig, double time,
                                    const char *wdir, int isnew)

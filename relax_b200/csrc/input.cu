@@ -969,6 +969,72 @@ extern "C" int relax_input_get_info(const relax_input *in, relax_input_info *inf
     return RELAX_OK;
 }
 
+// The geometry files of init (src/input.f90:296-1452), in the order init
+// writes them.  The reference's own names are kept, including two of its
+// quirks: the linear transient weak zones go to weakzone-nl-KKK.xy and
+// weakzones-nonlinear.vtp (the nonlinear zones' names), and rdykes-EEE.*
+// hold the event's shear sources (exportvtk_rfaults / exportxy_rfaults read
+// the shear list).  The linear transient .vtp takes that mechanism's own
+// zone count, where the reference passes the nonlinear count.
+extern "C" int relax_input_export_geometry(const relax_input *in, int vtk)
+{
+    if (!in) return relax_noalloc_fail(RELAX_ERR_ARG, "null input");
+    const relax_config &c = in->cfg;
+    const std::string w = in->wdir;
+    auto name = [&](const char *stem, int k, int digits, const char *ext) {
+        char b[96];
+        snprintf(b, sizeof b, "/%s%0*d%s", stem, digits, k, ext);
+        return w + b;
+    };
+    int rc = RELAX_OK;
+    if (vtk) rc = relax_write_vtk_grid(c.sx1, c.sx2, c.sx3, c.dx1, c.dx2, c.dx3, (w + "/cgrid.vtp").c_str());
+    // viscous and transient interfaces (a horizontal rectangle over the box)
+    // and their weak zones
+    struct Mech {
+        int layer, zones;
+        const char *lname, *xyname, *vtpname;
+    };
+    const Mech mech[4] = {{0, 0, "linearlayer-", "weakzone-", "/weakzones-linear.vtp"},
+                          {1, 1, "nonlinearlayer-", "weakzone-nl-", "/weakzones-nonlinear.vtp"},
+                          {2, 2, "ltransientlayer-", "weakzone-nl-", "/weakzones-nonlinear.vtp"},
+                          {3, 3, "nltransientlayer-", "weakzone-nltr-", "/weakzones-nonlinear-transient.vtp"}};
+    for (int m = 0; m < 4 && rc == RELAX_OK; m++) {
+        if (m >= 2 && !(in->flags & RELAX_INPUT_TRANSIENT)) break;
+        const auto &layers = in->layers[mech[m].layer];
+        for (size_t k = 0; k < layers.size() && vtk && rc == RELAX_OK; k++)
+            rc = relax_write_vtk_rectangle(0.0, 0.0, layers[k].z, (double)c.sx2 * c.dx2, (double)c.sx1 * c.dx1, 0.0,
+                                           1.5708, name(mech[m].lname, (int)k + 1, 3, ".vtp").c_str());
+        const auto &zones = in->wz[mech[m].zones];
+        if (layers.empty() || zones.empty()) continue;
+        for (size_t k = 0; k < zones.size() && rc == RELAX_OK; k++)
+            rc = relax_write_xy_brick(&zones[k], name(mech[m].xyname, (int)k + 1, 3, ".xy").c_str());
+        if (vtk && rc == RELAX_OK)
+            rc = relax_write_vtk_bricks((int)zones.size(), zones.data(), (w + mech[m].vtpname).c_str());
+    }
+    // afterslip planes
+    for (size_t k = 0; k < in->planes.size() && vtk && rc == RELAX_OK; k++) {
+        const relax_plane &p = in->planes[k];
+        rc = relax_write_vtk_rectangle(p.x, p.y, p.z, p.length, p.width, p.strike, p.dip,
+                                       name("aplane-", (int)k + 1, 4, ".vtp").c_str());
+    }
+    // each event's shear faults and tensile dykes
+    for (size_t e = 0; e < in->es.size() && rc == RELAX_OK; e++) {
+        const auto &s = in->es[e];
+        const relax_source *sp = s.empty() ? nullptr : s.data();
+        const char *stems[2] = {"rfaults-", "rdykes-"};
+        const bool has[2] = {!s.empty(), !in->ets[e].empty()};
+        for (int q = 0; q < 2 && rc == RELAX_OK; q++) {
+            if (!has[q]) continue;
+            if (vtk) rc = relax_write_faults(RELAX_FAULTS_VTP, (int)s.size(), sp, 0.0, 0.0,
+                                             name(stems[q], (int)e + 1, 3, ".vtp").c_str());
+            if (rc == RELAX_OK)
+                rc = relax_write_faults(RELAX_FAULTS_XY, (int)s.size(), sp, in->x0, in->y0,
+                                        name(stems[q], (int)e + 1, 3, ".xy").c_str());
+        }
+    }
+    return rc;
+}
+
 extern "C" int relax_input_obsplanes(const relax_input *in, const relax_obsplane **op, int *n)
 {
     if (!in || !op || !n) return relax_noalloc_fail(RELAX_ERR_ARG, "null argument");

@@ -183,8 +183,11 @@ int main(int argc, char **argv)
         fclose(fp);
     }
     exportoptsdat(info);
-    if (info.nop > 0 || info.nsop > 0)
-        printf("# observation planes and stress segments are read; their stress files are not written\n");
+    // the geometry files of init (grid, interfaces, weak zones, planes, faults)
+    if (check(relax_input_export_geometry(in, o.vtk ? 1 : 0), "geometry files") != RELAX_OK) {
+        relax_input_free(in);
+        return 1;
+    }
     if (o.dryrun) {
         printf("dry run: abort calculation\n");
         relax_input_free(in);
