@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -64,6 +65,63 @@ extern "C" __attribute__((visibility("hidden"))) int relax_noalloc_fail(int code
             return fail(RELAX_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__,          \
                         cudaGetErrorString(e_));                                          \
     } while (0)
+
+// Device memory of the contexts and batches comes from a memory pool of the
+// library's own per device (not the device's default pool, which other code
+// in the process may tune), which keeps freed memory for the next context:
+// creating and destroying a context costs no cudaMalloc / cudaFree once the
+// pool is warm.  Allocations and frees are ordered on the legacy default
+// stream and made synchronous for the caller (allocations wait for the
+// allocation, frees happen only after the owner's streams were synchronized),
+// so the buffers behave like cudaMalloc'd ones on every stream.
+static cudaMemPool_t dpool(int device)
+{
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)pools.size() <= device) pools.resize(device + 1, nullptr);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+        uint64_t keep = UINT64_MAX;   // no release to the device between contexts
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
+template <typename T>
+static int dalloc(T **p, size_t n)
+{
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    cudaMemPool_t pool = e == cudaSuccess ? dpool(device) : nullptr;
+    if (pool) {
+        e = cudaMallocFromPoolAsync((void **)p, bytes, pool, 0);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    } else {
+        e = cudaMalloc((void **)p, bytes);
+    }
+    if (e != cudaSuccess) return fail(RELAX_ERR_NOMEM, "device allocation of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    return RELAX_OK;
+}
+
+// frees a dalloc'd buffer once the device is idle (as cudaFree would wait),
+// back into the pool
+static void dfree(void *p)
+{
+    if (!p) return;
+    int device = 0;
+    cudaGetDevice(&device);
+    cudaDeviceSynchronize();
+    if (dpool(device)) cudaFreeAsync(p, 0);
+    else cudaFree(p);
+}
 
 #define TRY(call)                  \
     do {                               \
@@ -367,14 +425,14 @@ struct Spectral {
             }
             o += ns[i];
         }
-        CK(cudaMalloc(&tw, tot * sizeof(float2)));
+        TRY(dalloc(&tw, tot));
         CK(cudaMemcpyAsync(tw, h.data(), tot * sizeof(float2), cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st));
         pm.tw = tw + off[0];
         tw1 = tw + off[1];
         py.tw = tw + off[2];
         pz.tw = tw + off[3];
-        CK(cudaMalloc(&S, 3 * (size_t)(g.sx3 + 1) * g.sx2 * g.K1 * sizeof(float2)));
+        TRY(dalloc(&S, 3 * (size_t)(g.sx3 + 1) * g.sx2 * g.K1));
         // tile choices
         rows = 1;
         while (rows * 2 <= std::max(1, 1024 / g.M) && g.sx2 % (rows * 2) == 0) rows *= 2;
@@ -398,8 +456,8 @@ struct Spectral {
 
     void release()
     {
-        if (S) cudaFree(S);
-        if (tw) cudaFree(tw);
+        if (S) dfree(S);
+        if (tw) dfree(tw);
         S = nullptr;
         tw = nullptr;
     }
@@ -726,31 +784,32 @@ static void free_ctx(relax_ctx *c)
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->st2) cudaStreamSynchronize(c->st2);
     float *fs[] = {c->tau, c->m, c->sig, c->u, c->vp, c->gamma, c->work, c->twork, c->tload, c->spdev,
                    c->dg0[0], c->dg0[1], c->tm_part, c->fr_part, c->vel, c->ur, c->urs};
     for (float *p : fs)
-        if (p) cudaFree(p);
-    if (c->visc[0]) cudaFree(c->visc[0]);
-    if (c->visc[1]) cudaFree(c->visc[1]);
-    if (c->fcd) cudaFree(c->fcd);
-    if (c->patch) cudaFree(c->patch);
-    for (auto p : c->band_idx) if (p) cudaFree(p);
-    for (auto p : c->band_imp) if (p) cudaFree(p);
-    if (c->sig_mask) cudaFree(c->sig_mask);
+        if (p) dfree(p);
+    if (c->visc[0]) dfree(c->visc[0]);
+    if (c->visc[1]) dfree(c->visc[1]);
+    if (c->fcd) dfree(c->fcd);
+    if (c->patch) dfree(c->patch);
+    for (auto p : c->band_idx) if (p) dfree(p);
+    for (auto p : c->band_imp) if (p) dfree(p);
+    if (c->sig_mask) dfree(c->sig_mask);
     for (int k = 0; k < 2; k++) {
-        if (c->tvisc[k]) cudaFree(c->tvisc[k]);
-        if (c->tdg0[k]) cudaFree(c->tdg0[k]);
+        if (c->tvisc[k]) dfree(c->tvisc[k]);
+        if (c->tdg0[k]) dfree(c->tdg0[k]);
     }
-    if (c->eps) cudaFree(c->eps);
-    if (c->epsdot) cudaFree(c->epsdot);
-    if (c->ticket) cudaFree(c->ticket);
-    if (c->dst && c->own_dst) cudaFree(c->dst);
+    if (c->eps) dfree(c->eps);
+    if (c->epsdot) dfree(c->epsdot);
+    if (c->ticket) dfree(c->ticket);
+    if (c->dst && c->own_dst) dfree(c->dst);
     if (c->hst) cudaFreeHost(c->hst);
     if (c->dtp_h) cudaFreeHost(c->dtp_h);
-    if (c->dtp_d) cudaFree(c->dtp_d);
+    if (c->dtp_d) dfree(c->dtp_d);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    if (c->amp_part) cudaFree(c->amp_part);
-    if (c->amp_alt) cudaFree(c->amp_alt);
+    if (c->amp_part) dfree(c->amp_part);
+    if (c->amp_alt) dfree(c->amp_alt);
     c->sp.release();
     for (cudaEvent_t e : {c->ev_fork, c->ev_dt, c->ev_fork2, c->ev_mon})
         if (e) cudaEventDestroy(e);
@@ -762,13 +821,6 @@ static void free_ctx(relax_ctx *c)
 extern "C" const char *relax_version(void) { return "relax_b200 1.0 (sm_100a)"; }
 extern "C" const char *relax_last_error(void) { return g_err.c_str(); }
 
-template <typename T>
-static int dalloc(T **p, size_t n)
-{
-    cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
-    if (e != cudaSuccess) return fail(RELAX_ERR_NOMEM, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
-    return RELAX_OK;
-}
 
 static int build_bands(relax_ctx *c);
 
@@ -864,7 +916,7 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
-        cudaFree(d);
+        dfree(d);
         if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "prestress: %s", cudaGetErrorString(e));
     }
     // rheology tables
@@ -1249,7 +1301,7 @@ static int event_okada(relax_ctx *c, const EventCopy &ev)
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
-    cudaFree(d);
+    dfree(d);
     if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "okada: %s", cudaGetErrorString(e));
     return RELAX_OK;
 }
@@ -1396,7 +1448,7 @@ static int build_bands(relax_ctx *c)
         unsigned *cnt = nullptr;
         TRY(dalloc(&dimp, n));
         if (dalloc(&cnt, (size_t)nb + 1) != RELAX_OK) {
-            cudaFree(dimp);
+            dfree(dimp);
             return RELAX_ERR_NOMEM;
         }
         unsigned total = 0;
@@ -1408,16 +1460,16 @@ static int build_bands(relax_ctx *c)
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
         if (e == cudaSuccess && total > 0) {
             if (dalloc(&c->band_idx[k], total) != RELAX_OK || dalloc(&c->band_imp[k], total) != RELAX_OK) {
-                cudaFree(dimp);
-                cudaFree(cnt);
+                dfree(dimp);
+                dfree(cnt);
                 return RELAX_ERR_NOMEM;
             }
             k_band_write<<<nb, RELAX_NTHREADS, 0, c->st>>>(a, dimp, cnt, c->band_idx[k], c->band_imp[k]);
             e = cudaGetLastError();
             if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
         }
-        cudaFree(dimp);
-        cudaFree(cnt);
+        dfree(dimp);
+        dfree(cnt);
         if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "band of plane %zu: %s", k, cudaGetErrorString(e));
         c->band_n[k] = (int)total;
     }
@@ -1483,7 +1535,7 @@ static int friction_slots(relax_ctx *c, int *total)
         CK(cudaStreamSynchronize(c->st));
         float *np = nullptr;
         TRY(dalloc(&np, (size_t)blk));
-        if (c->fr_part) cudaFree(c->fr_part);
+        if (c->fr_part) dfree(c->fr_part);
         c->fr_part = np;
         c->nfr = blk;
     }
@@ -1961,7 +2013,7 @@ extern "C" int relax_set_field(relax_ctx *c, int which, const void *host, size_t
     }
     CKL();
     CK(cudaStreamSynchronize(c->st));
-    cudaFree(tmp);
+    dfree(tmp);
     if (which == RELAX_FIELD_SIG) c->sig_valid = true;
     else c->m_valid = false, c->sig_valid = false;
     if (which == RELAX_FIELD_MOMENT) c->m_valid = true;
@@ -2055,7 +2107,7 @@ extern "C" int relax_get_points(relax_ctx *c, int n, const int *index, double *u
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), buf, out.size() * sizeof(float), cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
-    cudaFree(buf);
+    dfree(buf);
     if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "point read-back: %s", cudaGetErrorString(e));
     for (int p = 0; p < n; p++) {
         const float *o = &out[9 * (size_t)p];
@@ -2213,7 +2265,7 @@ extern "C" int relax_monitor_plane(relax_ctx *c, int which, const relax_obsplane
     std::vector<double> h((5 + nc) * np);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), buf, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
-    cudaFree(buf);
+    dfree(buf);
     if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "plane sampling: %s", cudaGetErrorString(e));
     for (size_t q = 0; q < np; q++) {
         const double *v = &h[(5 + nc) * q];
@@ -2266,7 +2318,7 @@ extern "C" int relax_track_relaxation(relax_ctx *c, int vel_planes, int ur_plane
     CK(cudaStreamSynchronize(c->st));
     drop_graph(c);   // the corrector's epilogue arguments change
     for (float **p : {&c->vel, &c->ur, &c->urs})
-        if (*p) { cudaFree(*p); *p = nullptr; }
+        if (*p) { dfree(*p); *p = nullptr; }
     const int nv = std::max(std::max(vel_planes, ur_planes), inter_i3 + 1);
     c->vel_planes = nv;
     c->ur_planes = ur_planes;
@@ -3000,8 +3052,8 @@ static void free_batch(relax_batch *b)
 {
     if (!b) return;
     for (auto *c : b->m) free_ctx(c);
-    if (b->tab.dev) cudaFree(b->tab.dev);
-    if (b->dst) cudaFree(b->dst);
+    if (b->tab.dev) dfree(b->tab.dev);
+    if (b->dst) dfree(b->dst);
     if (b->hst) cudaFreeHost(b->hst);
     if (b->hdt) cudaFreeHost(b->hdt);
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
@@ -3050,7 +3102,7 @@ extern "C" int relax_batch_create(const relax_config *members, int n, int device
         return bail(fail(RELAX_ERR_NOMEM, "batch state"));
     for (int k = 0; k < n; k++) {
         relax_ctx *c = b->m[k];
-        cudaFree(c->dst);
+        dfree(c->dst);
         c->dst = b->dst + k;
         c->own_dst = false;
         c->err = &c->dst->error;
@@ -3167,7 +3219,7 @@ static int build_tables(relax_batch *b)
         t.dt = carve<DtArgs>(base, &off, n);
     };
     layout(nul);
-    if (t.dev) cudaFree(t.dev);
+    if (t.dev) dfree(t.dev);
     t.dev = nullptr;
     TRY(dalloc(&t.dev, off));
     layout(t.dev);
