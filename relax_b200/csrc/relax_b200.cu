@@ -111,6 +111,45 @@ static int dalloc(T **p, size_t n)
     return RELAX_OK;
 }
 
+// Small page-locked host blocks of a context (its step state and time-step
+// inputs) from one page-locked slab per process, so that creating a context
+// makes no cudaMallocHost call; larger requests, or a full slab, fall back to
+// cudaMallocHost.
+namespace hpin {
+constexpr size_t kBlock = 1024, kBlocks = 512;
+std::mutex mu;
+char *slab = nullptr;
+std::vector<int> free_list;
+
+int alloc(void **p, size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!slab && cudaMallocHost((void **)&slab, kBlock * kBlocks) == cudaSuccess)
+            for (int k = (int)kBlocks - 1; k >= 0; k--) free_list.push_back(k);
+        if (slab && bytes <= kBlock && !free_list.empty()) {
+            *p = slab + kBlock * (size_t)free_list.back();
+            free_list.pop_back();
+            memset(*p, 0, kBlock);
+            return RELAX_OK;
+        }
+    }
+    CK(cudaMallocHost(p, bytes));
+    return RELAX_OK;
+}
+
+void release(void *p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (slab && (char *)p >= slab && (char *)p < slab + kBlock * kBlocks) {
+        free_list.push_back((int)(((char *)p - slab) / kBlock));
+        return;
+    }
+    cudaFreeHost(p);
+}
+}  // namespace hpin
+
 // frees a dalloc'd buffer once the device is idle (as cudaFree would wait),
 // back into the pool
 static void dfree(void *p)
@@ -804,8 +843,8 @@ static void free_ctx(relax_ctx *c)
     if (c->epsdot) dfree(c->epsdot);
     if (c->ticket) dfree(c->ticket);
     if (c->dst && c->own_dst) dfree(c->dst);
-    if (c->hst) cudaFreeHost(c->hst);
-    if (c->dtp_h) cudaFreeHost(c->dtp_h);
+    hpin::release(c->hst);
+    hpin::release(c->dtp_h);
     if (c->dtp_d) dfree(c->dtp_d);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->amp_part) dfree(c->amp_part);
@@ -999,8 +1038,8 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     TRY(dalloc(&c->fr_part, 1));
     TRY(dalloc(&c->dst, 1));
     CK(cudaMemset(c->dst, 0, sizeof(StepState)));
-    CK(cudaMallocHost(&c->hst, sizeof(StepState)));
-    CK(cudaMallocHost(&c->dtp_h, sizeof(DtParams)));
+    TRY(hpin::alloc((void **)&c->hst, sizeof(StepState)));
+    TRY(hpin::alloc((void **)&c->dtp_h, sizeof(DtParams)));
     TRY(dalloc(&c->dtp_d, 1));
     memset(c->hst, 0, sizeof(StepState));
     c->err = &c->dst->error;   // read back with the step state
