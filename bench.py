@@ -99,7 +99,8 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------
-# algorithmic bytes per launch of each kernel (FP32 fields)
+# algorithmic bytes per launch of each kernel: every operand of the stage
+# streamed once in FP32
 # --------------------------------------------------------------------------
 def kernel_bytes(sim):
     sx1, sx2, sx3 = sim.sx1, sim.sx2, sim.sx3
@@ -166,6 +167,47 @@ def cpu_sample(sim, nsteps: int):
     finally:
         o.lib.orc_state_free(st)
     return sim.npoints * nsteps / dt, o.threads(), dt
+
+
+def rel_l2(a, b):
+    import numpy as np
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def accuracy_vs_fp64(sim, nsteps: int, device: int):
+    """The checker half of the CPU leg (untimed): the workload stepped
+    nsteps times on the GPU through the public API from a fresh context,
+    and the FP64 oracle (every field in double precision, the same method)
+    replaying the GPU's Dt sequence; relative L2 of each field after the
+    run (u over the physical half-space without the two pad columns)."""
+    import numpy as np
+    from oracle.oracle import Oracle
+    from relax_b200.api import Relax
+    t0 = time.perf_counter()
+    with Relax(sim, device=device) as r:
+        logs = [r.coseismic()]
+        for _ in range(nsteps):
+            logs.append(r.step())
+        g = {k: r.field(k) for k in ("u", "sig", "tau", "gamma")}
+    dts = [lg[1] for lg in logs[1:]]
+    rlogs, ref = Oracle(64).run(sim, nsteps, dt_schedule=dts)
+
+    def tens(t):
+        return np.stack([t[n].astype(np.float64) for n in t.dtype.names], axis=-1)
+
+    err = {"u": rel_l2(g["u"][..., :-2], ref["u"][..., :-2]),
+           "sig": rel_l2(tens(g["sig"]), tens(ref["sig"])),
+           "tau": rel_l2(tens(g["tau"]), tens(ref["tau"])),
+           "gamma": rel_l2(g["gamma"][..., :-2], ref["gamma"][..., :-2])}
+    logdev = {name: max(abs(a[c] - b[c]) / abs(b[c]) for a, b in zip(logs[1:], rlogs[1:]) if b[c] != 0)
+              for name, c in (("power", 6), ("cei", 7))}
+    return {"vs": "FP64 oracle (oracle/relax_oracle.c built with every field in double precision), "
+                  "replaying the GPU's Dt sequence",
+            "steps": nsteps, "rel_l2": err, "bound": 1e-4, "within_bound": max(err.values()) <= 1e-4,
+            "log_rel_dev": logdev, "seconds": round(time.perf_counter() - t0, 1)}
 
 
 def run_reference(args, rank, world):
@@ -313,12 +355,14 @@ def run_gpu(args, rank, world, local_rank):
     if rank != 0:
         return 0
     cpu = None
+    accuracy = None
     if world == 1 and not args.no_cpu:
         rate, cores, dt = cpu_sample(sim, 2)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "2 RK2 steps of the same workload on the host cores (after the "
                          "coseismic solve and one untimed step), FP32 oracle restating the "
                          "reference CPU path"}
+        accuracy = accuracy_vs_fp64(sim, args.steps, local_rank)
     b_alg = 536.0 * sim.npoints
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -339,6 +383,7 @@ def run_gpu(args, rank, world, local_rank):
         "clocks": clocks,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "accuracy": accuracy,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -213,8 +213,17 @@ const char *relax_last_error(void);     /* thread-local message        */
  * configuration is deep-copied.  Replaces cuinflags_/cuinit_
  * (src/cuelastic.cu:736, :476). */
 int relax_create(const relax_config *cfg, int device, relax_ctx **out);
-/* Replaces cudeinit_ (src/cuelastic.cu:1344). */
+/* Replaces cudeinit_ (src/cuelastic.cu:1344).  The context's device
+ * memory goes back to the library's own memory pool on that device, which
+ * keeps it for the next context (creating a context then allocates nothing
+ * from the device); relax_release_cached_memory returns it to the device. */
 int relax_destroy(relax_ctx *ctx);
+/* Returns the device memory that the library's pool on `device` holds but
+ * no live context, batch or operator uses (cudaMemPoolTrimTo after a device
+ * synchronisation).  Call it after destroying contexts when other code of
+ * the process needs the memory.  No counterpart in the reference, whose
+ * cudeinit_ frees with cudaFree. */
+int relax_release_cached_memory(int device);
 
 /* Stream the context's work is ordered on (cudaStream_t as void*). */
 int relax_get_stream(relax_ctx *ctx, void **stream);
@@ -608,7 +617,11 @@ int relax_op_green(float *c1, float *c2, float *c3, float *t1, float *t2,
  * RELAX_ERR_ARG.  The first call on each device looks the array up
  * (cudaGetSymbolAddress) and sets kernel attributes: make that first call
  * before any stream capture.  All calls share the array; calls that overlap
- * on the GPU race on it, so order them on one stream. */
+ * on the GPU race on it, so order them on one stream.  Grid rules: sx1 >= 16
+ * and a multiple of 4, even sx3 >= 4, sx2 >= 2, FFT lengths sx1/2, sx2, sx3
+ * products of 2 and 3.  relax_op_green asks in addition what a context
+ * needs (sx2 <= 4 or >= 15, sx3/2 >= 15, for the stencils of the step), so
+ * this entry point also takes smaller grids. */
 int relax_op_green_noalloc(float *c1, float *c2, float *c3, float *t1,
                            float *t2, float *t3, int sx1, int sx2, int sx3,
                            double dx1, double dx2, double dx3, double lambda,

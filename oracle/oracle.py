@@ -170,9 +170,11 @@ class Oracle:
 
     # -- the time loop ------------------------------------------------------
     def run(self, sim: Simulation, nsteps: int, dt_schedule: Optional[Sequence[float]] = None,
-            fields: bool = True):
-        """Coseismic solve + nsteps RK2 steps.  Returns (logs, fields dict)."""
-        cfg, keep = sim.to_c(self.structure_fn)
+            fields: bool = True, config=None):
+        """Coseismic solve + nsteps RK2 steps.  Returns (logs, fields dict).
+        config: a relax_config to run instead of sim.to_c (e.g. one read
+        from an input file; sim then only gives the array shapes)."""
+        cfg, keep = (config, None) if config is not None else sim.to_c(self.structure_fn)
         st = self.lib.orc_state_create(C.byref(cfg))
         if not st:
             raise MemoryError("oracle state allocation failed")

@@ -60,6 +60,7 @@ def load() -> C.CDLL:
         "relax_tensor_structure": (I, [P, I, D, I, P]),
         "relax_create": (I, [C.POINTER(relax_config), I, C.POINTER(P)]),
         "relax_destroy": (I, [P]),
+        "relax_release_cached_memory": (I, [I]),
         "relax_get_stream": (I, [P, C.POINTER(P)]),
         "relax_coseismic": (I, [P, I, C.POINTER(relax_step_log)]),
         "relax_step": (I, [P, C.POINTER(D), C.POINTER(relax_step_log)]),

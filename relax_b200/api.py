@@ -186,6 +186,12 @@ class Input:
                           odt=c.odt, tscale=c.tscale)
 
 
+def release_cached_memory(device: int = 0):
+    """Returns the device memory that the library keeps pooled after
+    destroyed contexts, batches and operators (relax_release_cached_memory)."""
+    _lib.check(_lib.load().relax_release_cached_memory(device))
+
+
 class Relax:
     def __init__(self, sim: Simulation, device: int = 0, config: Optional[relax_config] = None, keep=None):
         self.lib = _lib.load()

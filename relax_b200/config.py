@@ -214,11 +214,28 @@ class Point:
 
 
 @dataclass
+class Load:
+    """A surface load (src/input.f90:1676-1735): traction t3 (force per
+    surface, positive down) on a tapered L x W rectangle centred at (x, y);
+    period T > 0 gives t3 sin(2 pi t / T + phase), T = 0 a step t3 H(t)
+    (src/elastic3d.f90:2517-2590).  beta None takes the deck's smoothing."""
+    x: float
+    y: float
+    length: float
+    width: float
+    t3: float
+    period: float = 0.0
+    phase: float = 0.0
+    beta: Optional[float] = None
+
+
+@dataclass
 class Event:
     time: float
     faults: List[Fault] = field(default_factory=list)
     tensile: List[Tensile] = field(default_factory=list)
     points: List[Point] = field(default_factory=list)
+    loads: List[Load] = field(default_factory=list)
 
 
 @dataclass
@@ -366,6 +383,19 @@ class Simulation:
                 keep.append(marr)
                 earr[e].nm = len(ev.points)
                 earr[e].m = C.cast(marr, C.POINTER(relax_source))
+            if ev.loads:
+                larr = (relax_source * len(ev.loads))()
+                for k, ld in enumerate(ev.loads):
+                    # rotation only (src/input.f90:1733)
+                    a = self.rot * DEG2RAD
+                    x = ld.x * math.cos(a) + ld.y * math.sin(a)
+                    y = -ld.x * math.sin(a) + ld.y * math.cos(a)
+                    larr[k] = relax_source(slip=ld.t3, x=x, y=y, length=ld.length, width=ld.width,
+                                           period=ld.period, phase=ld.phase,
+                                           beta=self.beta if ld.beta is None else ld.beta)
+                keep.append(larr)
+                earr[e].nl = len(ev.loads)
+                earr[e].l = C.cast(larr, C.POINTER(relax_source))
         keep.append(earr)
         cfg.ne = len(self.events)
         cfg.events = C.cast(earr, C.POINTER(relax_event))
@@ -466,7 +496,10 @@ class Simulation:
                     f"{r(t.strike)} {r(t.dip)}" for k, t in enumerate(ev.tensile)]
             out += ["# number of dilatation sources", str(len(ev.points))]
             out += [f"{k + 1} {r(m.amplitude)} {r(m.x)} {r(m.y)} {r(m.z)}" for k, m in enumerate(ev.points)]
-            out += ["# number of surface traction", "0"]
+            out += ["# number of surface loads", str(len(ev.loads))]
+            out += [f"{k + 1} {r(ld.x)} {r(ld.y)} {r(ld.length)} {r(ld.width)} {r(ld.t3)} {r(ld.period)} "
+                    f"{r(ld.phase)}" + ("" if ld.beta is None else f" {r(ld.beta)}")
+                    for k, ld in enumerate(ev.loads)]
         return "\n".join(out) + "\n"
 
     # field sizes in the reference layout
@@ -526,25 +559,30 @@ def powerlaw_thrust(sx: int = 256, sz: int = 128, dx: float = 0.5, steps: int = 
 
 
 def random_faults(seed: int, sx: int = 512, sz: int = 256, dx: float = 0.4, nfaults: int = 3,
-                  lid: float = 25.0, n: float = 3.5, gam: float = 8.3e-4) -> Simulation:
-    """Large instance with gravity: faults drawn from `seed` (lengths U[20,100],
-    dip U[30,90], slip lognormal median 1 sigma 0.5, width L/2), power-law
-    n below an elastic lid."""
+                  lid: float = 25.0, n: float = 3.5, gam: float = 8.3e-4, sx2: Optional[int] = None,
+                  lmax: float = 100.0) -> Simulation:
+    """Large instance with gravity: faults drawn from `seed` (lengths
+    U[20, lmax] km, dip U[30,90], slip lognormal median 1 sigma 0.5, width
+    L/2, centres inside the middle 60 % of the box), power-law n below an
+    elastic lid.  sx2 (default sx) narrows the box along x2 for reduced
+    parity cases."""
     rng = np.random.default_rng(seed)
-    half = 0.3 * sx * dx
+    sx2 = sx if sx2 is None else sx2
+    half1 = 0.3 * sx * dx
+    half2 = 0.3 * sx2 * dx
     faults = []
     for _ in range(nfaults):
-        L = float(rng.uniform(20, 100))
+        L = float(rng.uniform(20, lmax))
         dip = float(rng.uniform(30, 90))
         slip = float(np.exp(rng.normal(0.0, 0.5)))
-        faults.append(Fault(slip, float(rng.uniform(-half, half - L)),
-                            float(rng.uniform(-half, half)), float(rng.uniform(0, 5)), L, L / 2,
+        faults.append(Fault(slip, float(rng.uniform(-half1, half1 - L)),
+                            float(rng.uniform(-half2, half2)), float(rng.uniform(0, 5)), L, L / 2,
                             float(rng.uniform(0, 360)), dip, float(rng.uniform(-180, 180))))
     return Simulation(
-        sx1=sx, sx2=sx, sx3=sz, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0, lambda_=1.0,
+        sx1=sx, sx2=sx2, sx3=sz, dx1=dx, dx2=dx, dx3=dx, beta=0.2, nyquist=2.0, lambda_=1.0,
         mu=1.0, gam=gam, interval=1.0e6, odt=-1, tscale=1.0,
         nonlinear=[(lid, 1.0, n, 0.0)], events=[Event(0.0, faults)],
-        name=f"random-faults-{sx}x{sx}x{sz}-seed{seed}")
+        name=f"random-faults-{sx}x{sx2}x{sz}-seed{seed}")
 
 
 ENSEMBLE_SHAPES = ((64, 64, 64), (128, 128, 64), (128, 128, 128), (192, 192, 96))

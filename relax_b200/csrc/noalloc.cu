@@ -1,10 +1,10 @@
 // noalloc.cu -- the Green's function operator without any allocation.
 //
-// relax_op_green (relax_b200.cu) allocates its spectrum buffer and twiddle
-// tables with cudaMalloc on every call.  Some callers cannot do that: a host
-// that hands all device memory to its own pool allocator (and forbids other
-// cudaMalloc/cudaFree calls, which also synchronise the device), or code
-// running where allocation is not allowed at all.  relax_op_green_noalloc
+// relax_op_green (relax_b200.cu) takes its spectrum buffer and twiddle
+// tables from the library's own device memory pool on every call.  Some
+// callers cannot allow that: a host that hands all device memory to its own
+// pool allocator (and forbids other allocations, which also synchronise the
+// device), or code running where allocation is not allowed at all.  relax_op_green_noalloc
 // does the same transform with its scratch in a fixed device array defined
 // in this file, so the only memory it touches is the caller's buffers and
 // that array.

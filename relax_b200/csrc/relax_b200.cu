@@ -74,22 +74,35 @@ extern "C" __attribute__((visibility("hidden"))) int relax_noalloc_fail(int code
 // stream and made synchronous for the caller (allocations wait for the
 // allocation, frees happen only after the owner's streams were synchronized),
 // so the buffers behave like cudaMalloc'd ones on every stream.
+// The pool keeps freed memory until relax_release_cached_memory trims it.
+// Whether a device has a pool is decided once, at its first allocation: if
+// the pool cannot be created the device takes plain cudaMalloc / cudaFree
+// from then on, so that every buffer is freed the way it was allocated.
 static cudaMemPool_t dpool(int device)
 {
     static std::mutex mu;
+    static std::vector<int> state;             // 0 undecided, 1 pool, -1 plain
     static std::vector<cudaMemPool_t> pools;
     std::lock_guard<std::mutex> lock(mu);
-    if ((int)pools.size() <= device) pools.resize(device + 1, nullptr);
-    if (!pools[device]) {
+    if ((int)pools.size() <= device) {
+        pools.resize(device + 1, nullptr);
+        state.resize(device + 1, 0);
+    }
+    if (state[device] == 0) {
         cudaMemPoolProps props{};
         props.allocType = cudaMemAllocationTypePinned;
         props.location.type = cudaMemLocationTypeDevice;
         props.location.id = device;
         cudaMemPool_t pool = nullptr;
-        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
-        uint64_t keep = UINT64_MAX;   // no release to the device between contexts
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-        pools[device] = pool;
+        if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;   // no release to the device between contexts
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            pools[device] = pool;
+            state[device] = 1;
+        } else {
+            cudaGetLastError();
+            state[device] = -1;
+        }
     }
     return pools[device];
 }
@@ -151,15 +164,33 @@ void release(void *p)
 }  // namespace hpin
 
 // frees a dalloc'd buffer once the device is idle (as cudaFree would wait),
-// back into the pool
-static void dfree(void *p)
+// back into the pool; `idle`: the caller has synchronized the device already
+static void dfree(void *p, bool idle = false)
 {
     if (!p) return;
     int device = 0;
     cudaGetDevice(&device);
-    cudaDeviceSynchronize();
+    if (!idle) cudaDeviceSynchronize();
     if (dpool(device)) cudaFreeAsync(p, 0);
     else cudaFree(p);
+}
+
+extern "C" int relax_release_cached_memory(int device)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return fail(RELAX_ERR_ARG, "relax_release_cached_memory: no device %d", device);
+    }
+    int cur = 0;
+    CK(cudaGetDevice(&cur));
+    CK(cudaSetDevice(device));
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaMemPool_t pool = dpool(device);
+    if (e == cudaSuccess && pool) e = cudaMemPoolTrimTo(pool, 0);
+    cudaSetDevice(cur);
+    if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "relax_release_cached_memory: %s", cudaGetErrorString(e));
+    return RELAX_OK;
 }
 
 #define TRY(call)                  \
@@ -493,10 +524,10 @@ struct Spectral {
         return RELAX_OK;
     }
 
-    void release()
+    void release(bool idle = false)
     {
-        if (S) dfree(S);
-        if (tw) dfree(tw);
+        if (S) dfree(S, idle);
+        if (tw) dfree(tw, idle);
         S = nullptr;
         tw = nullptr;
     }
@@ -822,34 +853,35 @@ static void free_ctx(relax_ctx *c)
 {
     if (!c) return;
     cudaSetDevice(c->device);
-    if (c->st) cudaStreamSynchronize(c->st);
-    if (c->st2) cudaStreamSynchronize(c->st2);
+    // one wait for the device, then every buffer goes back to the pool
+    cudaDeviceSynchronize();
+    const bool idle = true;
     float *fs[] = {c->tau, c->m, c->sig, c->u, c->vp, c->gamma, c->work, c->twork, c->tload, c->spdev,
                    c->dg0[0], c->dg0[1], c->tm_part, c->fr_part, c->vel, c->ur, c->urs};
     for (float *p : fs)
-        if (p) dfree(p);
-    if (c->visc[0]) dfree(c->visc[0]);
-    if (c->visc[1]) dfree(c->visc[1]);
-    if (c->fcd) dfree(c->fcd);
-    if (c->patch) dfree(c->patch);
-    for (auto p : c->band_idx) if (p) dfree(p);
-    for (auto p : c->band_imp) if (p) dfree(p);
-    if (c->sig_mask) dfree(c->sig_mask);
+        if (p) dfree(p, idle);
+    if (c->visc[0]) dfree(c->visc[0], idle);
+    if (c->visc[1]) dfree(c->visc[1], idle);
+    if (c->fcd) dfree(c->fcd, idle);
+    if (c->patch) dfree(c->patch, idle);
+    for (auto p : c->band_idx) if (p) dfree(p, idle);
+    for (auto p : c->band_imp) if (p) dfree(p, idle);
+    if (c->sig_mask) dfree(c->sig_mask, idle);
     for (int k = 0; k < 2; k++) {
-        if (c->tvisc[k]) dfree(c->tvisc[k]);
-        if (c->tdg0[k]) dfree(c->tdg0[k]);
+        if (c->tvisc[k]) dfree(c->tvisc[k], idle);
+        if (c->tdg0[k]) dfree(c->tdg0[k], idle);
     }
-    if (c->eps) dfree(c->eps);
-    if (c->epsdot) dfree(c->epsdot);
-    if (c->ticket) dfree(c->ticket);
-    if (c->dst && c->own_dst) dfree(c->dst);
+    if (c->eps) dfree(c->eps, idle);
+    if (c->epsdot) dfree(c->epsdot, idle);
+    if (c->ticket) dfree(c->ticket, idle);
+    if (c->dst && c->own_dst) dfree(c->dst, idle);
     hpin::release(c->hst);
     hpin::release(c->dtp_h);
-    if (c->dtp_d) dfree(c->dtp_d);
+    if (c->dtp_d) dfree(c->dtp_d, idle);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    if (c->amp_part) dfree(c->amp_part);
-    if (c->amp_alt) dfree(c->amp_alt);
-    c->sp.release();
+    if (c->amp_part) dfree(c->amp_part, idle);
+    if (c->amp_alt) dfree(c->amp_alt, idle);
+    c->sp.release(idle);
     for (cudaEvent_t e : {c->ev_fork, c->ev_dt, c->ev_fork2, c->ev_mon})
         if (e) cudaEventDestroy(e);
     if (c->st2) cudaStreamDestroy(c->st2);
@@ -3091,8 +3123,9 @@ static void free_batch(relax_batch *b)
 {
     if (!b) return;
     for (auto *c : b->m) free_ctx(c);
-    if (b->tab.dev) dfree(b->tab.dev);
-    if (b->dst) dfree(b->dst);
+    cudaDeviceSynchronize();
+    if (b->tab.dev) dfree(b->tab.dev, true);
+    if (b->dst) dfree(b->dst, true);
     if (b->hst) cudaFreeHost(b->hst);
     if (b->hdt) cudaFreeHost(b->hdt);
     if (b->gexec) cudaGraphExecDestroy(b->gexec);

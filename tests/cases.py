@@ -108,3 +108,22 @@ def oracle_monitor_plane(lib, field, sx, dx, op, beta=0.0):
     out = np.zeros((px3.value + 1, px2.value + 1, 5 + nc))
     lib.orc_monitor_plane(f.ctypes.data, *args, out.ctypes.data)
     return out
+
+
+def loads_small(periodic=True, second_event=True, sx=64, sz=32):
+    """Linear Maxwell below 6 km with surface loads (src/elastic3d.f90:2517-2590):
+    a step load t3 H(t) with the coseismic fault, optionally a periodic load
+    t3 sin(2 pi t / T + phase) whose rate enters every step (the predictor's
+    rate with the reference's Dt/2e8, src/relax.f90:685, the corrector's
+    with Dt, :806), and a second event at t = 1.0 carrying its own loads."""
+    from relax_b200.config import Load
+    s = linear_small(sx, sz, steps=8)
+    s.name = "loads-small"
+    s.tscale = 3.0           # Dt = 0.3: steps land on 0.3, 0.6, 0.9, then 1.0
+    s.events[0].loads = [Load(4.0, -3.0, 12.0, 8.0, 0.3)]
+    if periodic:
+        s.events[0].loads.append(Load(-6.0, 5.0, 10.0, 10.0, 0.2, period=2.0, phase=0.3, beta=0.3))
+    if second_event:
+        s.events.append(Event(1.0, [Fault(0.5, -5.0, 8.0, 0.0, 10.0, 5.0, 30.0, 60.0, 45.0)],
+                              loads=[Load(2.0, 2.0, 8.0, 6.0, -0.25, period=1.5, phase=-0.4)]))
+    return s

@@ -13,7 +13,7 @@ from relax_b200 import _lib
 from relax_b200.api import Input
 from relax_b200.config import Event, Fault, Plane, Point, Tensile, relax_layer, relax_source
 
-from cases import linear_small, powerlaw_small, sources_small, transient_small, two_events
+from cases import linear_small, loads_small, powerlaw_small, sources_small, transient_small, two_events
 
 
 def _src_eq(a, b, what):
@@ -65,6 +65,12 @@ def _rotated(sim):
     return s
 
 
+def _loads_rotated():
+    s = loads_small()
+    s.x0, s.y0, s.rot = -1.5, 2.0, 23.0
+    return s
+
+
 CASES = {
     "linear": lambda: linear_small(),
     "powerlaw-afterslip": lambda: powerlaw_small(),
@@ -72,6 +78,8 @@ CASES = {
     "transient": lambda: transient_small(linear=True, nonlinear=True, viscous=True),
     "sources-interseismic": lambda: sources_small(interseismic=True),
     "rotated-origin": lambda: _rotated(None),
+    "surface-loads": lambda: loads_small(),
+    "surface-loads-rotated": lambda: _loads_rotated(),
 }
 
 

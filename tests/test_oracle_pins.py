@@ -5,7 +5,8 @@ its captured run logs are the golden vectors: tests/golden/reference_logs.json
 holds the per-step log lines of examples/tutorials/output2.param (power-law
 n=3 after a strike-slip fault) and output3.param (afterslip on a frictional
 plane), 3 significant figures, extracted by tests/golden/make_reference_logs.py.
-The oracle replays the echoed input decks at their full 256^3 size.
+The oracle replays the echoed input decks at their full 256^3 size, read
+by the library's input reader from tests/golden/reference_output{2,3}.input.
 
 Tolerance: one unit in the 3rd printed digit, or 0.3 % -- the logs were
 written by an older MKL build, and the Maxwell time tm(pl) of output2 step 1
@@ -18,7 +19,7 @@ import os
 
 import pytest
 
-from relax_b200.config import reference_output2, reference_output3
+from test_reference_decks import read_deck
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_logs.json")
 
@@ -31,13 +32,13 @@ def _close(ours, ref):
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("name,builder", [("output2", reference_output2),
-                                          ("output3", reference_output3)])
-def test_oracle_reproduces_reference_log(oracle32, name, builder):
+@pytest.mark.parametrize("name", ["output2", "output3"])
+def test_oracle_reproduces_reference_log(oracle32, name):
     with open(GOLDEN) as f:
         ref = json.load(f)[name]
     nsteps = 2
-    logs, _ = oracle32.run(builder(), nsteps, fields=False)
+    inp = read_deck(name)
+    logs, _ = oracle32.run(inp.simulation(), nsteps, fields=False, config=inp.config)
     assert len(logs) == nsteps + 1
     for ours, theirs in zip(logs, ref[: nsteps + 1]):
         assert ours[0] == theirs[0]

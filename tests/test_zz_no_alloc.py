@@ -41,7 +41,9 @@ def _rel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
 
 
-@pytest.mark.parametrize("sx1,sx2,sx3", [(64, 48, 32), (32, 32, 32)])
+# 128 x 128 x 64 needs 13 MB of the 16 MiB scratch (the twiddle tables sit
+# near the end of the array) and takes the register passes in relax_op_green
+@pytest.mark.parametrize("sx1,sx2,sx3", [(64, 48, 32), (32, 32, 32), (128, 128, 64)])
 def test_noalloc_green_matches_allocating_green_twice(sx1, sx2, sx3):
     lib = _lib.load()
     for call, (seed, gam) in enumerate(((1, 8.3e-4), (2, 0.0))):
@@ -61,3 +63,31 @@ def test_noalloc_green_rejects_grids_beyond_its_scratch():
                                     sx1, sx2, sx3, 1.0, 1.0, 1.0, 1.0, 1.0, 0.0, None)
     assert rc == 1
     assert b"scratch" in lib.relax_last_error()
+
+
+def test_noalloc_green_rejects_a_grid_just_over_its_scratch():
+    """48 x 384 x 72 needs 16 MiB + 46 KB; 48 x 384 x 64 fits."""
+    lib = _lib.load()
+    for sx3, want in ((72, 1), (64, 0)):
+        sx1, sx2 = 48, 384
+        c = torch.zeros((3, sx3, sx2, sx1 + 2), device="cuda")
+        t = torch.zeros((3, sx2, sx1 + 2), device="cuda")
+        rc = lib.relax_op_green_noalloc(*[C.c_void_p(c[k].data_ptr()) for k in range(3)],
+                                        *[C.c_void_p(t[k].data_ptr()) for k in range(3)],
+                                        sx1, sx2, sx3, 1.0, 1.0, 1.0, 1.0, 1.0, 0.0, None)
+        torch.cuda.synchronize()
+        assert rc == want, (sx3, rc, lib.relax_last_error())
+
+
+def test_noalloc_green_small_grid_matches_oracle(oracle32):
+    """A grid that only this entry point takes (sx2 = 8, sx3/2 = 8: the
+    context's stencil rules do not apply to the Green's function alone),
+    against the oracle's greenfunctioncowling."""
+    lib = _lib.load()
+    sx1, sx2, sx3 = 32, 8, 16
+    c, t = _inputs(5, sx1, sx2, sx3)
+    cr, tr = c.copy(), t.copy()
+    oracle32.green(cr, tr, sx1, sx2, sx3, (0.5, 0.4, 0.25), 1.0, 1.0, 8.3e-4)
+    for call in range(2):
+        got = _green(lib.relax_op_green_noalloc, c, t, sx1, sx2, sx3, 8.3e-4)
+        assert _rel(got, cr[..., :sx1]) < 1e-5, (call, _rel(got, cr[..., :sx1]))
