@@ -177,37 +177,51 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
 
 
-def accuracy_vs_fp64(sim, nsteps: int, device: int):
+def accuracy_vs_fp64(sim, nsteps: int, device: int, mixed: bool):
     """The checker half of the CPU leg (untimed): the workload stepped
-    nsteps times on the GPU through the public API from a fresh context,
-    and the FP64 oracle (every field in double precision, the same method)
-    replaying the GPU's Dt sequence; relative L2 of each field after the
-    run (u over the physical half-space without the two pad columns)."""
+    nsteps times on the GPU through the public API from a fresh context in
+    the plain FP32 form (adaptive Dt) and, when `mixed`, in the
+    mixed-precision form with the plain run's Dt sequence prescribed; the
+    FP64 oracle (every field in double precision, the same method) replays
+    that Dt sequence.  Relative L2 of each field after the run (u over the
+    physical half-space without the two pad columns)."""
     import numpy as np
     from oracle.oracle import Oracle
     from relax_b200.api import Relax
     t0 = time.perf_counter()
-    with Relax(sim, device=device) as r:
-        logs = [r.coseismic()]
-        for _ in range(nsteps):
-            logs.append(r.step())
-        g = {k: r.field(k) for k in ("u", "sig", "tau", "gamma")}
+
+    def gpu(mode, dts=None):
+        with Relax(sim, device=device) as r:
+            if mode == "mixed":
+                r.set_precision("mixed")
+            logs = [r.coseismic()]
+            for k in range(nsteps):
+                logs.append(r.step(None if dts is None else dts[k]))
+            return logs, {k: r.field(k) for k in ("u", "sig", "tau", "gamma")}
+
+    logs, g = gpu("fp32")
     dts = [lg[1] for lg in logs[1:]]
+    runs = {"fp32": (logs, g)}
+    if mixed:
+        runs["mixed"] = gpu("mixed", dts)
     rlogs, ref = Oracle(64).run(sim, nsteps, dt_schedule=dts)
 
     def tens(t):
         return np.stack([t[n].astype(np.float64) for n in t.dtype.names], axis=-1)
 
-    err = {"u": rel_l2(g["u"][..., :-2], ref["u"][..., :-2]),
-           "sig": rel_l2(tens(g["sig"]), tens(ref["sig"])),
-           "tau": rel_l2(tens(g["tau"]), tens(ref["tau"])),
-           "gamma": rel_l2(g["gamma"][..., :-2], ref["gamma"][..., :-2])}
-    logdev = {name: max(abs(a[c] - b[c]) / abs(b[c]) for a, b in zip(logs[1:], rlogs[1:]) if b[c] != 0)
-              for name, c in (("power", 6), ("cei", 7))}
-    return {"vs": "FP64 oracle (oracle/relax_oracle.c built with every field in double precision), "
-                  "replaying the GPU's Dt sequence",
-            "steps": nsteps, "rel_l2": err, "bound": 1e-4, "within_bound": max(err.values()) <= 1e-4,
-            "log_rel_dev": logdev, "seconds": round(time.perf_counter() - t0, 1)}
+    out = {"vs": "FP64 oracle (oracle/relax_oracle.c built with every field in double precision), "
+                 "replaying the plain run's Dt sequence",
+           "steps": nsteps, "bound": 1e-4}
+    for name, (lg, f) in runs.items():
+        err = {"u": rel_l2(f["u"][..., :-2], ref["u"][..., :-2]),
+               "sig": rel_l2(tens(f["sig"]), tens(ref["sig"])),
+               "tau": rel_l2(tens(f["tau"]), tens(ref["tau"])),
+               "gamma": rel_l2(f["gamma"][..., :-2], ref["gamma"][..., :-2])}
+        logdev = {q: max(abs(a[c] - b[c]) / abs(b[c]) for a, b in zip(lg[1:], rlogs[1:]) if b[c] != 0)
+                  for q, c in (("power", 6), ("cei", 7))}
+        out[name] = {"rel_l2": err, "within_bound": max(err.values()) <= 1e-4, "log_rel_dev": logdev}
+    out["seconds"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def run_reference(args, rank, world):
@@ -264,44 +278,54 @@ def run_gpu(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    r = Relax(sim, device=local_rank)
-    r.coseismic()
-    for _ in range(args.warmup):
-        r.step()
-    sptr = r.lib.relax_get_stream
     import ctypes as C
-    s = C.c_void_p()
-    sptr(r.h, C.byref(s))
-    stream = torch.cuda.ExternalStream(s.value)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
 
-    clk = ClockSampler(local_rank)
-    clk.start()
-    time.sleep(0.3)
-    barrier()
-    n0 = r.launch_count()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        lg = r.step()
-        if lg[0] == 0:
-            raise RuntimeError("simulation ended inside the timed region")
-    ev1.record(stream)
-    barrier()
-    launches = r.launch_count() - n0
-    ms = ev0.elapsed_time(ev1)
-    clocks = clk.stop()
-    ms = allmax(ms)
+    def timed_form(mode, wsim=sim, steps=None, warmup=None):
+        """W warm-up steps, then K steps timed with CUDA events on the
+        context's stream (barrier + synchronize on both sides), then a
+        profiled pass of per-kernel durations."""
+        steps = args.steps if steps is None else steps
+        warmup = args.warmup if warmup is None else warmup
+        r = Relax(wsim, device=local_rank)
+        if mode == "mixed":
+            r.set_precision("mixed")
+        r.coseismic()
+        for _ in range(warmup):
+            r.step()
+        s = C.c_void_p()
+        r.lib.relax_get_stream(r.h, C.byref(s))
+        stream = torch.cuda.ExternalStream(s.value)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        clk = ClockSampler(local_rank)
+        clk.start()
+        time.sleep(0.3)
+        barrier()
+        n0 = r.launch_count()
+        ev0.record(stream)
+        for _ in range(steps):
+            lg = r.step()
+            if lg[0] == 0:
+                raise RuntimeError("simulation ended inside the timed region")
+        ev1.record(stream)
+        barrier()
+        launches = r.launch_count() - n0
+        ms = ev0.elapsed_time(ev1)
+        clocks = clk.stop()
+        ms = allmax(ms)
+        # per-kernel durations (CUDA events around each launch, separate pass)
+        r.profile(True)
+        nprof = max(3, min(steps, 10))
+        for _ in range(nprof):
+            r.step()
+        prof = r.profile_read()
+        r.profile(False)
+        r.close()
+        return ms, launches, clocks, prof, nprof
+
+    ms, launches, clocks, prof, nprof = timed_form("fp32")
     ms_step = ms / args.steps
     value = world * sim.npoints * args.steps / (ms / 1e3)
-
-    # per-kernel durations (CUDA events around each launch, separate pass)
-    r.profile(True)
-    nprof = max(3, min(args.steps, 10))
-    for _ in range(nprof):
-        r.step()
-    prof = r.profile_read()
-    r.profile(False)
     algo = kernel_bytes(sim)
     kernels = {}
     for name, (tot, n) in prof.items():
@@ -315,7 +339,52 @@ def run_gpu(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     ach = kernels[dom]["gbs"]
     traffic = traffic_from_profiles().get(dom)
-    r.close()
+
+    # the large single instance (512^2 x 256 box, gravity, three seeded
+    # faults, n = 3.5 below a 25 km lid): a few steps, plain form
+    large = None
+    if not args.no_large:
+        from relax_b200.config import random_faults
+        lsim = random_faults(1)
+        lsteps = 5
+        lms, llaunches, lclocks, lprof, lnprof = timed_form("fp32", lsim, lsteps, 3)
+        lstep = lms / lsteps
+        lb = 536.0 * lsim.npoints
+        lalgo = kernel_bytes(lsim)
+        lk = {}
+        for name, (tot, n) in lprof.items():
+            d = {"ms_per_launch": tot / n, "launches": n}
+            if name in lalgo:
+                d["gbs"] = lalgo[name] / (tot / n / 1e3) / 1e9
+            lk[name] = d
+        large = {"workload": f"random faults seed 1, box {lsim.sx1}x{lsim.sx2}x{lsim.sx3}, dx={lsim.dx1} km, "
+                             "gravity 8.3e-4, n=3.5 below 25 km, adaptive dt",
+                 "grid_points": lsim.npoints, "steps": lsteps, "warmup": 3,
+                 "value": world * lsim.npoints * lsteps / (lms / 1e3), "unit": UNIT, "ms_per_step": lstep,
+                 "step_roofline": {"alg_bytes_per_step": lb, "achieved_gbs": lb / (lstep / 1e3) / 1e9,
+                                   "frac": lb / (lstep / 1e3) / 1e9 / peaks()[0]},
+                 "kernels": lk, "gpu_launches": llaunches, "clocks": lclocks}
+
+    # the mixed-precision form beside the plain one (x3 transform's DFT-64
+    # sub-transforms on the tensor cores), same workload, same timing
+    mixed = None
+    if sim.sx3 == 128:
+        mms, mlaunches, mclocks, mprof, mnprof = timed_form("mixed")
+        mvalue = world * sim.npoints * args.steps / (mms / 1e3)
+        mk = {}
+        for name, (tot, n) in mprof.items():
+            d = {"ms_total": tot, "launches": n, "ms_per_launch": tot / n}
+            if name in algo:
+                d["alg_bytes"] = algo[name]
+                d["gbs"] = algo[name] / (tot / n / 1e3) / 1e9
+            mk[name] = d
+        mixed = {"value": mvalue, "unit": UNIT, "ms_per_step": mms / args.steps,
+                 "speedup_vs_plain": mvalue / value, "gpu_launches": mlaunches, "clocks": mclocks,
+                 "kernel_ms_per_step": sum(v[0] for v in mprof.values()) / mnprof,
+                 "k_zspec": mk.get("k_zspec"),
+                 "form": "x3 transform as two interleaved length-64 DFTs per column, each a tcgen05 "
+                         "BF16 product with hi/lo split operands (3 products) and FP32 accumulation; "
+                         "everything else as the plain form"}
 
     # end to end through the public API with host buffers: create (H2D of the
     # deck, structures and prestress), coseismic solve, K steps each reading
@@ -354,6 +423,11 @@ def run_gpu(args, rank, world, local_rank):
 
     if rank != 0:
         return 0
+    # the two ensembles, a few steps each, on rank 0's GPU
+    ens = {}
+    if world == 1 and not args.no_ensemble:
+        for which in ("c4", "c5"):
+            ens[which] = ensemble_figure(which, 5, 3, local_rank)
     cpu = None
     accuracy = None
     if world == 1 and not args.no_cpu:
@@ -362,7 +436,7 @@ def run_gpu(args, rank, world, local_rank):
                "sample": "2 RK2 steps of the same workload on the host cores (after the "
                          "coseismic solve and one untimed step), FP32 oracle restating the "
                          "reference CPU path"}
-        accuracy = accuracy_vs_fp64(sim, args.steps, local_rank)
+        accuracy = accuracy_vs_fp64(sim, args.steps, local_rank, mixed is not None)
     b_alg = 536.0 * sim.npoints
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -384,6 +458,10 @@ def run_gpu(args, rank, world, local_rank):
         "e2e": e2e,
         "cpu_baseline": cpu,
         "accuracy": accuracy,
+        "mixed": mixed,
+        "large_instance": large,
+        "ensemble_c4": ens.get("c4"),
+        "ensemble_c5": ens.get("c5"),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -392,14 +470,18 @@ def run_gpu(args, rank, world, local_rank):
 # --------------------------------------------------------------------------
 # the batched ensemble (64 members, uneven grids), against a loop of plain solves
 # --------------------------------------------------------------------------
-def run_ensemble(args):
+def ensemble_figure(which: str, K: int, W: int, device: int = 0):
+    """K ensemble steps (after W warm-up steps) of every member through
+    relax_ensemble (one batch per grid shape, each on its own stream, one
+    host synchronisation per step) against the same members solved one
+    after the other through relax_step; host wall clock around the K steps,
+    the device synchronised on both sides."""
     import collections
     import torch
-    from relax_b200.api import Batch, Relax
+    from relax_b200.api import Ensemble, Relax
     from relax_b200.config import ensemble_uneven
 
-    torch.cuda.set_device(0)
-    if args.ensemble == "c5":
+    if which == "c5":
         from relax_b200.config import ensemble_thrust_afterslip
         sims = ensemble_thrust_afterslip(seed=5, n=16)
         workload_name = ("16 thrust instances on 256^2x128 (dx 0.5 km, gravity), 5 km slip patches "
@@ -408,39 +490,28 @@ def run_ensemble(args):
         sims = ensemble_uneven(seed=4, n=64)
         workload_name = ("uneven ensemble of 64 members, grids {64^3, 128^2x64, 128^3, 192^2x96}, "
                          "power-law n U[1,3.5], prefactor 10^U[-1,1], lid U[15,40] km, one fault each")
-    groups = collections.OrderedDict()
-    for s in sims:
-        groups.setdefault((s.sx1, s.sx2, s.sx3), []).append(s)
+    shapes = collections.Counter((s.sx1, s.sx2, s.sx3) for s in sims)
     npts = sum(s.npoints for s in sims)
-    K, W = args.steps, args.warmup
 
-    # batched: one batch per grid shape, every batch stepped once per step
-    batches = [Batch(g) for g in groups.values()]
-    for b in batches:
-        b.coseismic()
-    for _ in range(W):
-        for b in batches:
-            b.step()
-    n0 = sum(b.launch_count() for b in batches)
-    per_batch = [0.0] * len(batches)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(K):
-        for j, b in enumerate(batches):
-            tb = time.perf_counter()
-            b.step()             # ends with the batch's host synchronisation
-            per_batch[j] += time.perf_counter() - tb
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    launches = sum(b.launch_count() for b in batches) - n0
-    for b in batches:
-        b.close()
+    with Ensemble(sims, device) as e:
+        e.coseismic()
+        for _ in range(W):
+            e.step()
+        n0 = e.launch_count()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            e.step()             # ends with the ensemble's host synchronisation
+        torch.cuda.synchronize()
+        t_batch = time.perf_counter() - t0
+        launches = e.launch_count() - n0
+        groups = e.groups()
 
     # the loop of plain solves: each member alone through relax_step
     t_loop = 0.0
     per_shape_loop = collections.Counter()
     for s in sims:
-        with Relax(s) as r:
+        with Relax(s, device) as r:
             r.coseismic()
             for _ in range(W):
                 r.step()
@@ -455,24 +526,32 @@ def run_ensemble(args):
 
     steps_per_solve = 100
     solves = len(sims) * K / steps_per_solve
-    line = {
+    return {
         "metric": "ensemble solves/s (100 RK2 steps per member)", "value": solves / t_batch,
-        "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": W, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name,
-                   "members": {f"{a}x{b}x{c}": len(g) for (a, b, c), g in groups.items()},
-                   "grid_points_total": npts, "parallelism": "one batch per grid shape",
-                   "timing": "host wall clock around K steps of every member, after W warm-up steps"},
+        "unit": "solves/s", "steps": K, "warmup": W, "higher_is_better": True,
+        "workload": workload_name, "members": {f"{a}x{b}x{c}": n for (a, b, c), n in shapes.items()},
+        "groups": groups, "grid_points_total": npts,
+        "timing": "host wall clock around K ensemble steps (one host synchronisation each), after W warm-up steps",
         "grid_pt_steps_per_s": npts * K / t_batch,
         "loop_of_plain_solves": {"value": solves / t_loop, "unit": "solves/s",
-                                 "grid_pt_steps_per_s": npts * K / t_loop},
+                                 "grid_pt_steps_per_s": npts * K / t_loop,
+                                 "ms_per_step_by_shape": {f"{a}x{b}x{c}": 1e3 * v / K
+                                                          for (a, b, c), v in per_shape_loop.items()}},
         "speedup_vs_loop": t_loop / t_batch,
-        "per_shape": {f"{a}x{b}x{c}": {"members": len(g), "batch_ms_per_step": 1e3 * per_batch[j] / K,
-                                       "loop_ms_per_step": 1e3 * per_shape_loop[(a, b, c)] / K,
-                                       "speedup": per_shape_loop[(a, b, c)] / per_batch[j]}
-                      for j, ((a, b, c), g) in enumerate(groups.items())},
         "gpu_launches": launches,
     }
+
+
+def run_ensemble(args):
+    import torch
+    torch.cuda.set_device(0)
+    fig = ensemble_figure(args.ensemble, args.steps, args.warmup)
+    line = {"metric": fig["metric"], "value": fig["value"], "unit": fig["unit"], "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": fig["workload"], "members": fig["members"], "parallelism": "one batch per shape",
+                       "timing": fig["timing"]},
+            "ensemble": fig, "gpu_launches": fig["gpu_launches"]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -484,6 +563,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-large", action="store_true", help="skip the 512^2 x 256 single-instance figure")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble figures of the default line")
     ap.add_argument("--ensemble", nargs="?", const="c4", choices=["c4", "c5"], default=None,
                     help="a batched ensemble against a loop of plain solves (1 GPU): c4, the 64 uneven "
                          "members (default), or c5, 16 thrust instances with afterslip")

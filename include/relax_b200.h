@@ -225,6 +225,18 @@ int relax_destroy(relax_ctx *ctx);
  * cudeinit_ frees with cudaFree. */
 int relax_release_cached_memory(int device);
 
+/* Precision of the time step's Green's functions.  RELAX_PRECISION_FP32
+ * (the default) runs every FFT butterfly in FP32 as the reference does
+ * (fft3, src/fourier.f90:177-201).  RELAX_PRECISION_MIXED runs the x3
+ * transform's length-64 DFT sub-transforms as tensor-core products
+ * (tcgen05, split BF16 hi/lo operands, FP32 accumulation; elastic response,
+ * surface traction and Cerruti correction unchanged); boxes 128 deep only
+ * (RELAX_ERR_UNSUPPORTED otherwise).  A mode of this library with no
+ * counterpart in the reference. */
+#define RELAX_PRECISION_FP32  0
+#define RELAX_PRECISION_MIXED 1
+int relax_set_precision(relax_ctx *ctx, int mode);
+
 /* Stream the context's work is ordered on (cudaStream_t as void*). */
 int relax_get_stream(relax_ctx *ctx, void **stream);
 
@@ -517,6 +529,26 @@ int relax_batch_step(relax_batch *batch, relax_step_log *logs);
 int relax_batch_launch_count(relax_batch *batch, long long *n);
 int relax_batch_get_stream(relax_batch *batch, void **stream);
 
+/* An ensemble of members with uneven grids (no reference counterpart).
+ * The members are grouped by shape (grid, spacing, elastic constants,
+ * number of afterslip planes) into batches, each with its own stream;
+ * relax_ensemble_step queues every group's step (one launch per stage per
+ * group, replayed from a captured graph) and then waits once per group, so
+ * that groups of different shapes run concurrently and the ensemble step
+ * costs one host synchronisation.  Members keep their order: logs[k] and
+ * relax_ensemble_member(k) are member k of `members`.  Members stepped in
+ * an ensemble equal the same decks stepped alone, bit for bit. */
+typedef struct relax_ensemble relax_ensemble;
+
+int relax_ensemble_create(const relax_config *members, int n, int device, relax_ensemble **ensemble);
+int relax_ensemble_destroy(relax_ensemble *ensemble);
+/* n: members, ngroups: shape groups (either may be NULL) */
+int relax_ensemble_size(relax_ensemble *ensemble, int *n, int *ngroups);
+int relax_ensemble_member(relax_ensemble *ensemble, int k, relax_ctx **member);
+int relax_ensemble_coseismic(relax_ensemble *ensemble, relax_step_log *logs);
+int relax_ensemble_step(relax_ensemble *ensemble, relax_step_log *logs);
+int relax_ensemble_launch_count(relax_ensemble *ensemble, long long *n);
+
 /* ------------------------------------------------------------------ */
 /* stateless operators on device buffers (reference layout)           */
 /*                                                                    */
@@ -606,6 +638,25 @@ int relax_op_green(float *c1, float *c2, float *c3, float *t1, float *t2,
                    float *t3, int sx1, int sx2, int sx3, double dx1,
                    double dx2, double dx3, double lambda, double mu,
                    double gam, void *stream);
+
+/* greenfunctioncowling in the mixed-precision form of
+ * RELAX_PRECISION_MIXED, on a 128-deep box (sx3 = 128), pruned as in the
+ * time step (src/relax.f90:681): the body force's lower half (layers
+ * sx3/2 .. sx3-1) must be zero, and only the upper sx3/2 layers of
+ * c1..c3 receive the displacement (the lower half is left as it was).
+ * Replaces calfftnelasic_ (src/cugreen.cu:1453) in that setting. */
+int relax_op_green_mixed(float *c1, float *c2, float *c3, float *t1,
+                         float *t2, float *t3, int sx1, int sx2, int sx3,
+                         double dx1, double dx2, double dx3, double lambda,
+                         double mu, double gam, void *stream);
+
+/* The tensor-core DFT of relax_op_green_mixed on its own: `in` holds 128
+ * vectors of 64 complex values (interleaved FP32 pairs, 128 x 64 x 2
+ * floats), `out` receives their forward (inverse = 0, sign -1) or inverse
+ * (inverse = 1, sign +1, unnormalised) DFT, each 64 x 2 floats.  For tests
+ * of the split-precision product; synchronous.  No counterpart in the
+ * reference (its FFT is FFTW / cuFFT). */
+int relax_op_dft64_tc(const float *in, float *out, int inverse, void *stream);
 
 /* greenfunctioncowling like relax_op_green, for callers that cannot
  * allocate device memory (a host whose pool allocator owns the device, or

@@ -61,6 +61,9 @@ def load() -> C.CDLL:
         "relax_create": (I, [C.POINTER(relax_config), I, C.POINTER(P)]),
         "relax_destroy": (I, [P]),
         "relax_release_cached_memory": (I, [I]),
+        "relax_set_precision": (I, [P, I]),
+        "relax_op_green_mixed": (I, [P, P, P, P, P, P, I, I, I, D, D, D, D, D, D, P]),
+        "relax_op_dft64_tc": (I, [P, P, I, P]),
         "relax_get_stream": (I, [P, C.POINTER(P)]),
         "relax_coseismic": (I, [P, I, C.POINTER(relax_step_log)]),
         "relax_step": (I, [P, C.POINTER(D), C.POINTER(relax_step_log)]),
@@ -84,6 +87,13 @@ def load() -> C.CDLL:
         "relax_batch_step": (I, [P, C.POINTER(relax_step_log)]),
         "relax_batch_launch_count": (I, [P, C.POINTER(C.c_longlong)]),
         "relax_batch_get_stream": (I, [P, C.POINTER(P)]),
+        "relax_ensemble_create": (I, [C.POINTER(relax_config), I, I, C.POINTER(P)]),
+        "relax_ensemble_destroy": (I, [P]),
+        "relax_ensemble_size": (I, [P, C.POINTER(I), C.POINTER(I)]),
+        "relax_ensemble_member": (I, [P, I, C.POINTER(P)]),
+        "relax_ensemble_coseismic": (I, [P, C.POINTER(relax_step_log)]),
+        "relax_ensemble_step": (I, [P, C.POINTER(relax_step_log)]),
+        "relax_ensemble_launch_count": (I, [P, C.POINTER(C.c_longlong)]),
         "relax_op_stressupdate": (I, [P, P, P, D, D, D, D, D, I, I, I, P, P]),
         "relax_op_bodyforce": (I, [P, D, D, D, I, I, I, P, P, P, P, P, P, P]),
         "relax_op_viscouseigenstress": (I, [D, P, P, P, I, I, I, P, C.POINTER(D), P, P, P]),

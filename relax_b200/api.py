@@ -252,6 +252,11 @@ class Relax:
         _lib.check(self.lib.relax_run(self.h, nsteps, sched, logs, C.byref(n)))
         return [logs[k].as_tuple() for k in range(n.value + 1)]
 
+    def set_precision(self, mode: str):
+        """"fp32" (default) or "mixed": the x3 transform's length-64 DFTs on
+        the tensor cores (split BF16, FP32 accumulation), 128-deep boxes."""
+        _lib.check(self.lib.relax_set_precision(self.h, {"fp32": 0, "mixed": 1}[mode]))
+
     def synchronize(self):
         _lib.check(self.lib.relax_synchronize(self.h))
 
@@ -481,3 +486,61 @@ class Batch:
         s = C.c_void_p()
         _lib.check(self.lib.relax_batch_get_stream(self.h, C.byref(s)))
         return s.value
+
+
+class Ensemble(Batch):
+    """Members with uneven grids, grouped by shape into batches that run
+    concurrently; one host synchronisation per ensemble step.
+
+        with Ensemble(ensemble_uneven(seed=4)) as e:
+            e.coseismic()
+            for _ in range(100):
+                logs = e.step()
+    """
+
+    def __init__(self, sims: Sequence[Simulation], device: int = 0):
+        self.lib = _lib.load()
+        self.sims = list(sims)
+        cfgs, self._keep = [], []
+        for s in self.sims:
+            cfg, keep = s.to_c(_lib.structure_fn)
+            cfgs.append(cfg)
+            self._keep.append(keep)
+        self._cfgs = (type(cfgs[0]) * len(cfgs))(*cfgs)
+        h = C.c_void_p()
+        _lib.check(self.lib.relax_ensemble_create(self._cfgs, len(cfgs), device, C.byref(h)))
+        self.h = h
+        self.n = len(cfgs)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.relax_ensemble_destroy(self.h)
+            self.h = None
+
+    def groups(self) -> int:
+        g = C.c_int()
+        _lib.check(self.lib.relax_ensemble_size(self.h, None, C.byref(g)))
+        return g.value
+
+    def coseismic(self) -> List[tuple]:
+        logs = (relax_step_log * self.n)()
+        _lib.check(self.lib.relax_ensemble_coseismic(self.h, logs))
+        return [logs[k].as_tuple() for k in range(self.n)]
+
+    def step(self) -> List[tuple]:
+        logs = (relax_step_log * self.n)()
+        _lib.check(self.lib.relax_ensemble_step(self.h, logs))
+        return [logs[k].as_tuple() for k in range(self.n)]
+
+    def member(self, k: int) -> Relax:
+        h = C.c_void_p()
+        _lib.check(self.lib.relax_ensemble_member(self.h, k, C.byref(h)))
+        return _Member(self.lib, self.sims[k], self._cfgs[k], h)
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        _lib.check(self.lib.relax_ensemble_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def stream(self) -> int:
+        raise NotImplementedError("an ensemble runs one stream per shape group")

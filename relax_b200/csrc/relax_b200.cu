@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "okada.cuh"
+#include "zspec_tc.cuh"
 
 using namespace relax;
 
@@ -461,9 +462,28 @@ static bool reg_shape(const Grid &g)
            (g.sx3 == 64 || g.sx3 == 96 || g.sx3 == 128 || g.sx3 == 256);
 }
 
+// the x3 pass with its DFT-64 sub-transforms on the tensor cores: 128-deep
+// boxes, pruned transform (the time step's Green's functions)
+static bool zspec_tc_ok(const ZArgs &za) { return za.g.sx3 == 128 && za.nin == 64 && za.nout == 64; }
+
+static cudaError_t launch_zspec_tc(const ZArgs &za, int nsm, int *err, cudaStream_t st)
+{
+    ZtcArgs t{};
+    t.z = za;
+    t.ncol = za.g.sx2 * za.g.K1;
+    t.ntiles = (t.ncol + ZT_COLS - 1) / ZT_COLS;
+    t.err = err;
+    set_smem(k_zspec_tc, ZT_SMEM);
+    k_zspec_tc<<<std::min(t.ntiles, std::max(1, nsm)), ZT_THREADS, ZT_SMEM, st>>>(t);
+    return cudaGetLastError();
+}
+
 struct Spectral {
     Prof *prof = nullptr;
     bool use_reg = true;   // register-resident y/z passes where instantiated
+    int mixed = 0;         // 1: the x3 pass on the tensor cores where zspec_tc_ok
+    int *tc_err = nullptr; // device flag of k_zspec_tc (the context's error word)
+    int nsm = 0;           // SMs of the device (persistent x3 pass)
     bool yreg = false;
     Grid g{};
     float2 *S = nullptr;
@@ -476,6 +496,11 @@ struct Spectral {
     int init(const Grid &gg, cudaStream_t st)
     {
         g = gg;
+        {
+            int dev = 0;
+            CK(cudaGetDevice(&dev));
+            CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        }
         int nr;
         if (!factor(g.M, pm.r, &pm.nr) || !factor(g.sx2, py.r, &py.nr) || !factor(g.sx3, pz.r, &pz.nr))
             return fail(RELAX_ERR_UNSUPPORTED, "FFT sizes must be products of 2 and 3 (sx1/2=%d sx2=%d sx3=%d)",
@@ -588,7 +613,12 @@ struct Spectral {
         }
         ZArgs za = zargs(nin, nout, lambda, mu, gam, twz);
         bool zr = false;
-        if (use_reg) {
+        if (mixed && tc_err && zspec_tc_ok(za)) {
+            TIMED(prof, ST_ZSPEC, st, (re = launch_zspec_tc(za, nsm, tc_err, st)));
+            if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_zspec_tc: %s", cudaGetErrorString(re));
+            zr = true;
+        }
+        if (use_reg && !zr) {
             TIMED(prof, ST_ZSPEC, st, (zr = zspec_reg(za, dim3((g.sx2 * g.K1 + kCW - 1) / kCW), st, &re)));
             if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_zspec_reg: %s", cudaGetErrorString(re));
         }
@@ -1650,6 +1680,8 @@ static int check_err(relax_ctx *c)
 {
     if (c->hst->error & (1 << RELAX_ERR_FRICTION))
         return fail(RELAX_ERR_FRICTION, "wrong value of (a-b)sigma: tau/((a-b)sigma) > 20");
+    if (c->hst->error & (1 << RELAX_ERR_CUDA))
+        return fail(RELAX_ERR_CUDA, "tensor-core x3 pass: a wait on the tensor cores timed out");
     return RELAX_OK;
 }
 
@@ -2377,6 +2409,21 @@ extern "C" int relax_segment_stress(relax_ctx *c, int n, const relax_segment *so
 // :846-850) and in plane inter_i3 alone (inter1..inter3, :839-843; -1: off).
 // Every later step writes them; relax_get_plane reads them as RELAX_FIELD_V
 // and RELAX_FIELD_UR.
+extern "C" int relax_set_precision(relax_ctx *c, int mode)
+{
+    if (!c) return fail(RELAX_ERR_ARG, "null context");
+    if (mode != RELAX_PRECISION_FP32 && mode != RELAX_PRECISION_MIXED)
+        return fail(RELAX_ERR_ARG, "precision mode %d", mode);
+    if (mode == RELAX_PRECISION_MIXED && c->g.sx3 != 128)
+        return fail(RELAX_ERR_UNSUPPORTED, "the mixed-precision x3 pass needs a 128-deep box (sx3 = %d)", c->g.sx3);
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->st));
+    c->sp.mixed = mode;
+    c->sp.tc_err = c->err;
+    drop_graph(c);
+    return RELAX_OK;
+}
+
 extern "C" int relax_track_relaxation(relax_ctx *c, int vel_planes, int ur_planes, int inter_i3)
 {
     if (!c) return fail(RELAX_ERR_ARG, "null context");
@@ -2905,6 +2952,64 @@ extern "C" int relax_op_green(float *c1, float *c2, float *c3, float *t1, float 
     return rc;
 }
 
+extern "C" int relax_op_green_mixed(float *c1, float *c2, float *c3, float *t1, float *t2, float *t3, int sx1,
+                                    int sx2, int sx3, double dx1, double dx2, double dx3, double lambda,
+                                    double mu, double gam, void *stream)
+{
+    Grid g;
+    TRY(make_grid(g, sx1, sx2, sx3, dx1, dx2, dx3));
+    if (sx3 != 128) return fail(RELAX_ERR_UNSUPPORTED, "relax_op_green_mixed: the box must be 128 deep (sx3 = %d)", sx3);
+    cudaStream_t st = (cudaStream_t)stream;
+    Spectral sp;
+    int *err = nullptr;
+    int rc = sp.init(g, st);
+    if (rc == RELAX_OK) rc = dalloc(&err, 1);
+    if (rc != RELAX_OK) {
+        sp.release();
+        dfree(err);
+        return rc;
+    }
+    cudaMemsetAsync(err, 0, sizeof(int), st);
+    sp.mixed = 1;
+    sp.tc_err = err;
+    XfArgs xa{};
+    float *cs[3] = {c1, c2, c3}, *ts[3] = {t1, t2, t3};
+    for (int k = 0; k < 3; k++) { xa.in[k] = cs[k]; xa.tin[k] = ts[k]; }
+    xa.rp = sx1 + 2; xa.pp = (size_t)(sx1 + 2) * sx2; xa.trp = sx1 + 2;
+    XiArgs xi{};
+    for (int k = 0; k < 3; k++) { xi.out[k] = cs[k]; xi.base[k] = nullptr; }
+    xi.rp = sx1 + 2; xi.pp = (size_t)(sx1 + 2) * sx2; xi.st = nullptr; xi.cmul = 1.f;
+    rc = sp.green(xa, false, sx3 / 2, sx3 / 2, xi, lambda, mu, gam, st);
+    int herr = 0;
+    if (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        if (rc == RELAX_OK) rc = fail(RELAX_ERR_CUDA, "relax_op_green_mixed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    if (rc == RELAX_OK && herr) rc = fail(RELAX_ERR_CUDA, "tensor-core x3 pass: a wait on the tensor cores timed out");
+    sp.release();
+    dfree(err);
+    return rc;
+}
+
+extern "C" int relax_op_dft64_tc(const float *in, float *out, int inverse, void *stream)
+{
+    if (!in || !out) return fail(RELAX_ERR_ARG, "null buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    int *err = nullptr;
+    TRY(dalloc(&err, 1));
+    cudaMemsetAsync(err, 0, sizeof(int), st);
+    set_smem(k_dft64_tc, DP_SMEM);
+    k_dft64_tc<<<1, 128, DP_SMEM, st>>>((const float2 *)in, (float2 *)out, inverse ? 1 : 0, err);
+    cudaError_t e = cudaGetLastError();
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    dfree(err);
+    if (e != cudaSuccess) return fail(RELAX_ERR_CUDA, "relax_op_dft64_tc: %s", cudaGetErrorString(e));
+    if (herr) return fail(RELAX_ERR_CUDA, "relax_op_dft64_tc: a wait on the tensor cores timed out");
+    return RELAX_OK;
+}
+
 __global__ void k_amp_aos(const relax_tensor *t, size_t n, double *part)
 {
     __shared__ double shd[32];
@@ -3422,12 +3527,17 @@ static int batch_kernels(relax_batch *b)
     return RELAX_OK;
 }
 
-extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
+// The launch half of a batch step: every member's time-step inputs, the
+// step's kernels (a captured graph after one plain step) and the read-back
+// of the members' states, all queued on the batch's stream.  *queued is
+// false when the members were stepped in turn (no batched instantiation)
+// or none is live; batch_step_finish then has nothing to collect.
+static int batch_step_begin(relax_batch *b, relax_step_log *logs, std::vector<char> &live, bool *queued)
 {
-    if (!b || !logs) return fail(RELAX_ERR_ARG, "null argument");
+    *queued = false;
     CK(cudaSetDevice(b->device));
     const int n = (int)b->m.size();
-    std::vector<char> live(n, 0);
+    live.assign(n, 0);
     int nlive = 0;
     for (int k = 0; k < n; k++) {
         relax_ctx *c = b->m[k];
@@ -3491,15 +3601,150 @@ extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
         b->plain_steps++;
     }
     CK(cudaMemcpyAsync(b->hst, b->dst, n * sizeof(StepState), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    // ---- host part of each member's step end
-    for (int k = 0; k < n; k++) {
+    *queued = true;
+    return RELAX_OK;
+}
+
+// The host half: waits for the batch's stream and runs each live member's
+// step end (counters, event branch, log).
+static int batch_step_finish(relax_batch *b, relax_step_log *logs, const std::vector<char> &live)
+{
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->st));
+    for (int k = 0; k < (int)b->m.size(); k++) {
         if (!live[k]) continue;
         relax_ctx *c = b->m[k];
         *c->hst = b->hst[k];
         const int e0 = c->e;
         TRY(finish_step(c, &logs[k]));
         if (c->e != e0) b->tables_valid = false;   // the event branch ran on the member's stream
+    }
+    return RELAX_OK;
+}
+
+extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
+{
+    if (!b || !logs) return fail(RELAX_ERR_ARG, "null argument");
+    std::vector<char> live;
+    bool queued = false;
+    TRY(batch_step_begin(b, logs, live, &queued));
+    if (queued) TRY(batch_step_finish(b, logs, live));
+    return RELAX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ensembles of uneven grids: one batch per grid shape, each on its own
+// stream, stepped together with one host synchronisation per step
+// ---------------------------------------------------------------------------
+struct relax_ensemble {
+    std::vector<relax_batch *> groups;
+    std::vector<std::vector<int>> index;   // member numbers of each group
+    std::vector<std::pair<int, int>> where;   // group and slot of each member
+    std::vector<std::vector<relax_step_log>> glog;
+    int device = 0;
+};
+
+static void free_ensemble(relax_ensemble *e)
+{
+    if (!e) return;
+    for (auto *b : e->groups) free_batch(b);
+    delete e;
+}
+
+extern "C" int relax_ensemble_create(const relax_config *members, int n, int device, relax_ensemble **out)
+{
+    if (!members || !out || n < 1) return fail(RELAX_ERR_ARG, "null argument or empty ensemble");
+    *out = nullptr;
+    relax_ensemble *e = new relax_ensemble();
+    e->device = device;
+    e->where.resize(n);
+    for (int k = 0; k < n; k++) {
+        int gidx = -1;
+        for (size_t q = 0; q < e->index.size(); q++)
+            if (same_shape(members[e->index[q][0]], members[k])) { gidx = (int)q; break; }
+        if (gidx < 0) {
+            gidx = (int)e->index.size();
+            e->index.emplace_back();
+        }
+        e->where[k] = {gidx, (int)e->index[gidx].size()};
+        e->index[gidx].push_back(k);
+    }
+    for (auto &idx : e->index) {
+        std::vector<relax_config> cfgs;
+        for (int k : idx) cfgs.push_back(members[k]);
+        relax_batch *b = nullptr;
+        const int rc = relax_batch_create(cfgs.data(), (int)cfgs.size(), device, &b);
+        if (rc != RELAX_OK) {
+            free_ensemble(e);
+            return rc;
+        }
+        e->groups.push_back(b);
+        e->glog.emplace_back(idx.size());
+    }
+    *out = e;
+    return RELAX_OK;
+}
+
+extern "C" int relax_ensemble_destroy(relax_ensemble *e)
+{
+    free_ensemble(e);
+    return RELAX_OK;
+}
+
+extern "C" int relax_ensemble_size(relax_ensemble *e, int *n, int *ngroups)
+{
+    if (!e) return fail(RELAX_ERR_ARG, "null ensemble");
+    if (n) *n = (int)e->where.size();
+    if (ngroups) *ngroups = (int)e->groups.size();
+    return RELAX_OK;
+}
+
+extern "C" int relax_ensemble_member(relax_ensemble *e, int k, relax_ctx **c)
+{
+    if (!e || !c) return fail(RELAX_ERR_ARG, "null argument");
+    if (k < 0 || k >= (int)e->where.size()) return fail(RELAX_ERR_ARG, "member %d out of range", k);
+    *c = e->groups[e->where[k].first]->m[e->where[k].second];
+    return RELAX_OK;
+}
+
+extern "C" int relax_ensemble_coseismic(relax_ensemble *e, relax_step_log *logs)
+{
+    if (!e) return fail(RELAX_ERR_ARG, "null ensemble");
+    for (size_t q = 0; q < e->groups.size(); q++) {
+        TRY(relax_batch_coseismic(e->groups[q], e->glog[q].data()));
+        if (logs)
+            for (size_t j = 0; j < e->index[q].size(); j++) logs[e->index[q][j]] = e->glog[q][j];
+    }
+    return RELAX_OK;
+}
+
+extern "C" int relax_ensemble_step(relax_ensemble *e, relax_step_log *logs)
+{
+    if (!e || !logs) return fail(RELAX_ERR_ARG, "null argument");
+    const size_t ng = e->groups.size();
+    std::vector<std::vector<char>> live(ng);
+    std::vector<char> queued(ng, 0);
+    // every group's step queued on its own stream, then one wait per group
+    for (size_t q = 0; q < ng; q++) {
+        bool qd = false;
+        TRY(batch_step_begin(e->groups[q], e->glog[q].data(), live[q], &qd));
+        queued[q] = qd;
+    }
+    for (size_t q = 0; q < ng; q++)
+        if (queued[q]) TRY(batch_step_finish(e->groups[q], e->glog[q].data(), live[q]));
+    for (size_t q = 0; q < ng; q++)
+        for (size_t j = 0; j < e->index[q].size(); j++) logs[e->index[q][j]] = e->glog[q][j];
+    return RELAX_OK;
+}
+
+extern "C" int relax_ensemble_launch_count(relax_ensemble *e, long long *n)
+{
+    if (!e || !n) return fail(RELAX_ERR_ARG, "null argument");
+    *n = 0;
+    for (auto *b : e->groups) {
+        long long m = 0;
+        TRY(relax_batch_launch_count(b, &m));
+        *n += m;
     }
     return RELAX_OK;
 }

@@ -129,3 +129,29 @@ def test_batch_rejects_mismatched_members():
     with pytest.raises(_lib.RelaxError) as e:
         Batch([a, b])
     assert e.value.code == 1
+
+
+def test_ensemble_of_uneven_grids_matches_members_alone():
+    """relax_ensemble_*: members of three shapes (two batched groups and a
+    grid stepped in turn), interleaved in the member list, each equal to
+    its deck stepped alone; one host synchronisation per ensemble step."""
+    from relax_b200.api import Ensemble
+    a = powerlaw_small(sx=64, sz=64, dx=1.0, afterslip=False)
+    b = powerlaw_small(sx=128, sz=64, dx=1.0)
+    c = linear_small(sx=96, sz=64, steps=3)
+    sims = [_variant(a, 0), _variant(b, 0), _variant(c, 0), _variant(a, 1), _variant(b, 1)]
+    with Ensemble(sims) as e:
+        assert e.groups() == 3
+        logs = [[l] for l in e.coseismic()]
+        for _ in range(3):
+            for k, l in enumerate(e.step()):
+                logs[k].append(l)
+        outs = []
+        for k in range(len(sims)):
+            m = e.member(k)
+            o = {"logs": logs[k], "u": m.field("u"), "tau": m.field("tau"), "gamma": m.field("gamma")}
+            if sims[k].planes:
+                o["patches"] = np.array([(p.slip, p.v, p.taus) for p in m.patches(0)])
+            outs.append(o)
+    for k, s in enumerate(sims):
+        _same(outs[k], _alone(s, 3))
