@@ -108,8 +108,18 @@ typedef struct relax_segment {
     double x, y, z, length, width, strike, dip, friction;
 } relax_segment;
 
-/* EVENT_STRUC, src/types.f90:99-106 (shear, tensile, point and load
- * sources; cuboid/tetrahedron eigenstrain sources are not supported). */
+/* TETRAHEDRON_STRUCT, src/types.f90:70-74: an eigenstrain e in the
+ * tetrahedron of four vertices of the event's vertex list (1-based). */
+typedef struct relax_tetrahedron {
+    relax_tensor e;
+    int i1, i2, i3, i4;
+} relax_tetrahedron;
+
+/* EVENT_STRUC, src/types.f90:99-106: shear, tensile, point and load
+ * sources, and (input flag --with-eigenstrain, src/input.f90:1496-1660)
+ * cuboid eigenstrain sources (WEAK_STRUCT: e and the geometry after
+ * wangconvention; dgammadot0 unused) and, with --with-curvilinear,
+ * tetrahedral ones over a vertex list (3 doubles per vertex). */
 typedef struct relax_event {
     double time;
     int ns, nt, nm, nl;
@@ -117,6 +127,10 @@ typedef struct relax_event {
     const relax_source *ts;   /* tensile cracks                        */
     const relax_source *m;    /* dilatation point sources              */
     const relax_source *l;    /* surface loads                         */
+    int nc, ntet, nvert;      /* cuboids, tetrahedra, vertices         */
+    const relax_weakzone *c;  /* cuboid eigenstrain sources            */
+    const relax_tetrahedron *tet;
+    const double *vert;       /* x1, x2, x3 of each vertex             */
 } relax_event;
 
 /* The part of SIMULATION_STRUCT (src/types.f90:118-266) that the time

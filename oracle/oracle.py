@@ -56,6 +56,10 @@ def load(precision: int = 32) -> C.CDLL:
         "orc_source": (None, [D, D, D, D, D, D, D, D, D, D, D, I, I, I, D, D, D, P, P, P, P, P, P]),
         "orc_momentdensityshear": (None, [D, D, D, D, D, D, D, D, D, D, D, I, I, I, D, D, D, P]),
         "orc_okada": (None, [D] * 15 + [C.POINTER(D)]),
+        "orc_cuboidsource": (None, [D, D, P] + [D] * 9 + [I, I, I, D, D, D, P, P, P]),
+        "orc_momentdensitycuboid": (None, [D, D, P] + [D] * 9 + [I, I, I, D, D, D, P]),
+        "orc_tetrahedronsource": (None, [D, D, P, P, P, P, P, I, I, I, D, D, D, P, P, P]),
+        "orc_momentdensitytetrahedron": (None, [D, D, P, P, P, P, P, I, I, I, D, D, D, P]),
         "orc_monitor_plane": (None, [P, I, I, I, I, D, D, D, D, D, D, D, D, D, D, D, C.POINTER(I), C.POINTER(I),
                                      P]),
         "orc_state_create": (P, [P]),
@@ -158,6 +162,24 @@ class Oracle:
             plane.rake, beta, ptr(sig), mu, C.cast(structure, C.c_void_p), sx1, sx2, sx3h, *dx,
             ptr(moment), None if tm is None else C.byref(tm))
         return rc, (tm.value if tm is not None else None)
+
+    # eigenstrain sources: e a relax_tensor, geometry in the internal convention
+    def cuboidsource(self, lam, mu, e, geo, beta, sx, dx, f):
+        """geo = (x, y, z, L, W, T, strike, dip) as dislocations passes them"""
+        self.lib.orc_cuboidsource(lam, mu, C.byref(e), *geo, beta, *sx, *dx, ptr(f[0]), ptr(f[1]), ptr(f[2]))
+
+    def momentdensitycuboid(self, mu, lam, e, geo, beta, sx1, sx2, sx3h, dx, sig):
+        self.lib.orc_momentdensitycuboid(mu, lam, C.byref(e), *geo, beta, sx1, sx2, sx3h, *dx, ptr(sig))
+
+    def tetrahedronsource(self, lam, mu, e, verts, sx, dx, f):
+        v = [np.ascontiguousarray(x, np.float64) for x in verts]
+        self.lib.orc_tetrahedronsource(lam, mu, C.byref(e), *[ptr(x) for x in v], *sx, *dx, ptr(f[0]), ptr(f[1]),
+                                       ptr(f[2]))
+
+    def momentdensitytetrahedron(self, mu, lam, e, verts, sx1, sx2, sx3h, dx, sig):
+        v = [np.ascontiguousarray(x, np.float64) for x in verts]
+        self.lib.orc_momentdensitytetrahedron(mu, lam, C.byref(e), *[ptr(x) for x in v], sx1, sx2, sx3h, *dx,
+                                              ptr(sig))
 
     def green(self, c, t, sx1, sx2, sx3, dx, lam, mu, gam):
         rc = self.lib.orc_greenfunctioncowling(ptr(c[0]), ptr(c[1]), ptr(c[2]), ptr(t[0]),

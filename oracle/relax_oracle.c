@@ -1775,8 +1775,258 @@ static void integrationstep(double tm, double *Dt, double t, int oi, double odt,
     }
 }
 
-/* dislocations without eigenstress, src/relax.f90:1116-1289 (shear
- * sources only) */
+/* ------------------------------------------------------------------ */
+/* eigenstrain sources (--with-eigenstrain, --with-curvilinear)        */
+/* ------------------------------------------------------------------ */
+
+/* gaussi, src/elastic3d.f90:513-518 */
+static double gaussi(double x, double sigma) { return (1.0 + erf(x / sqrt(2.0) / sigma)) / 2.0; }
+
+/* cuboidSource, src/elastic3d.f90:1680-1884: body force of an eigenstrain
+ * e in a cuboid (L, W, T as passed by dislocations: L = width, W = length,
+ * src/relax.f90:1157-1166), physical layers of the (sx1+2, sx2, sx3) box.
+ * The surface-traction loop of the source computes a moment it does not
+ * store (its additions are commented out there) and is left out. */
+void orc_cuboidsource(double lambda, double mu, const relax_tensor *e, double x, double y, double z, double L,
+                      double W, double T, double strike, double dip, double beta, int sx1, int sx2, int sx3,
+                      double dx1, double dx2, double dx3, real *f1, real *f2, real *f3)
+{
+    const double ekk = (double)((real)e->s11 + (real)e->s22 + (real)e->s33);
+    const double e11 = e->s11, e12 = e->s12, e13 = e->s13, e22 = e->s22, e23 = e->s23, e33 = e->s33;
+    const double cstrike = cos(strike), sstrike = sin(strike), cdip = cos(dip), sdip = sin(dip);
+    const double Wp = W * (1.0 + 2.0 * beta) / 2.0, Lp = L * (1.0 + 2.0 * beta) / 2.0,
+                 Tp = T * (1.0 + 2.0 * beta) / 2.0;
+    double mx = Wp > Lp ? Wp : Lp;
+    if (Tp > mx) mx = Tp;
+    const double r2 = (double)sqrtf(2.0f) * mx;              /* SQRT(2.) is default-real */
+    const double x2r0 = cstrike * x - sstrike * y;
+    const double xr = cdip * x2r0 - sdip * z, yr = sstrike * x + cstrike * y, zr = sdip * x2r0 + cdip * z;
+    const int sx1p = sx1 + 2;
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3 / 2; i3++) {
+        const double x3 = (double)(i3 - 1) * dx3;
+        if (fabs(x3 - z) > r2) continue;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                double x1, x2, dum;
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &dum);
+                if (fabs(x1 - x) > r2 || fabs(x2 - y) > r2 || fabs(x3 - z) > r2) continue;
+                const double x2r = cstrike * x1 - sstrike * x2;
+                const double x1s = cdip * x2r - sdip * x3, x1i = cdip * x2r + sdip * x3;
+                const double x2s = sstrike * x1 + cstrike * x2;
+                const double x3s = sdip * x2r + cdip * x3, x3i = -sdip * x2r + cdip * x3;
+                double temp1 = omega((x1s - xr) / T, beta), temp2 = omega((x2s - yr) / W, beta);
+                double temp3 = omega((x3s - zr) / L, beta);
+                const double sourc = 1.0 / T * omegap((x1s - xr) / T, beta) * temp2 * temp3;
+                const double dblcp = 1.0 / W * temp1 * omegap((x2s - yr) / W, beta) * temp3;
+                const double dipcs = 1.0 / L * temp1 * temp2 * omegap((x3s - zr) / L, beta);
+                temp1 = omega((x1i - xr) / T, beta);
+                temp3 = omega((x3i + zr) / L, beta);
+                const double image = 1.0 / T * omegap((x1i - xr) / T, beta) * temp2 * temp3;
+                const double cplei = 1.0 / W * temp1 * omegap((x2s - yr) / W, beta) * temp3;
+                const double dipci = 1.0 / L * temp1 * temp2 * omegap((x3i + zr) / L, beta);
+                (void)dipci;
+                const size_t o = (size_t)(i1 - 1) + (size_t)sx1p * ((size_t)(i2 - 1) + (size_t)sx2 * (i3 - 1));
+                const double s11 = lambda * ekk + 2.0 * mu * e11, s22 = lambda * ekk + 2.0 * mu * e22;
+                const double s33 = lambda * ekk + 2.0 * mu * e33;
+                if (2.01 * DEG2RAD > dip) {
+                    /* method of images for subvertical sources */
+                    f1[o] = (real)(f1[o] + 2.0 * mu * e12 * sstrike * (sourc + image) +
+                                   2.0 * mu * e12 * cdip * cstrike * (dblcp + cplei) -
+                                   s11 * sstrike * (dblcp + cplei) - s22 * cdip * cstrike * (sourc + image));
+                    f2[o] = (real)(f2[o] + 2.0 * mu * e12 * cstrike * (sourc + image) -
+                                   2.0 * mu * e12 * cdip * sstrike * (dblcp + cplei) -
+                                   s11 * cstrike * (dblcp + cplei) + s22 * cdip * sstrike * (sourc + image));
+                    f3[o] = (real)(f3[o] - 2.0 * mu * e12 * sdip * (dblcp - cplei) + s22 * sdip * (sourc - image));
+                } else {
+                    f1[o] = (real)(f1[o] + 2.0 * mu * e12 * sstrike * sourc + 2.0 * mu * e12 * cdip * cstrike * dblcp -
+                                   s11 * sstrike * dblcp - s22 * cdip * cstrike * sourc);
+                    f2[o] = (real)(f2[o] + 2.0 * mu * e12 * cstrike * sourc - 2.0 * mu * e12 * cdip * sstrike * dblcp -
+                                   s11 * cstrike * dblcp + s22 * cdip * sstrike * sourc);
+                    f3[o] = (real)(f3[o] - 2.0 * mu * e12 * sdip * dblcp + s22 * sdip * sourc);
+                }
+                /* vertical shear components */
+                f1[o] = (real)(f1[o] + 2.0 * mu * e13 * cdip * sstrike * dipcs + 2.0 * mu * e13 * sdip * cstrike * dblcp -
+                               2.0 * mu * e23 * cdip * cstrike * dipcs - 2.0 * mu * e23 * sdip * cstrike * sourc -
+                               s33 * sdip * dipcs * cstrike);
+                f2[o] = (real)(f2[o] + 2.0 * mu * e13 * cdip * cstrike * dipcs - 2.0 * mu * e13 * sdip * sstrike * dblcp +
+                               2.0 * mu * e23 * cdip * sstrike * dipcs + 2.0 * mu * e23 * sdip * sstrike * sourc +
+                               s33 * sdip * dipcs * sstrike);
+                f3[o] = (real)(f3[o] + 2.0 * mu * e13 * cdip * dblcp - 2.0 * mu * e23 * cdip * sourc -
+                               s33 * cdip * dipcs);
+            }
+        }
+    }
+}
+
+/* the outward unit normals of a tetrahedron's faces BCD, CDA, DAB, ABC and
+ * the faces' centroids (tetrahedronSource / momentDensityTetrahedron,
+ * src/elastic3d.f90:1946-1980, :2816-2848); 0 for a tetrahedron without
+ * volume */
+static int tet_faces(const double A[3], const double B[3], const double C[3], const double D[3], double n[4][3],
+                     double cen[4][3])
+{
+    const double *P[4] = {A, B, C, D};
+    /* nA = (C-B) x (D-B), nB = (D-C) x (A-C), nC = (A-D) x (B-D), nD = (B-A) x (C-A) */
+    const int tri[4][3] = {{1, 2, 3}, {2, 3, 0}, {3, 0, 1}, {0, 1, 2}};
+    for (int f = 0; f < 4; f++) {
+        const double *p = P[tri[f][0]], *q = P[tri[f][1]], *r = P[tri[f][2]];
+        const double u[3] = {q[0] - p[0], q[1] - p[1], q[2] - p[2]};
+        const double v[3] = {r[0] - p[0], r[1] - p[1], r[2] - p[2]};
+        n[f][0] = u[1] * v[2] - u[2] * v[1];
+        n[f][1] = u[2] * v[0] - u[0] * v[2];
+        n[f][2] = u[0] * v[1] - u[1] * v[0];
+    }
+    for (int f = 0; f < 4; f++)
+        if (0.0 == sqrt(n[f][0] * n[f][0] + n[f][1] * n[f][1] + n[f][2] * n[f][2])) return 0;
+    for (int f = 0; f < 4; f++) {
+        const double nn = sqrt(n[f][0] * n[f][0] + n[f][1] * n[f][1] + n[f][2] * n[f][2]);
+        for (int k = 0; k < 3; k++) n[f][k] = n[f][k] / nn;
+    }
+    for (int f = 0; f < 4; f++) {
+        const double *p = P[tri[f][0]], *q = P[tri[f][1]], *r = P[tri[f][2]];
+        for (int k = 0; k < 3; k++) cen[f][k] = (p[k] + q[k] + r[k]) / 3;
+        /* outward: the opposite vertex lies behind the face */
+        const double *o = P[f];
+        const double d = n[f][0] * (o[0] - cen[f][0]) + n[f][1] * (o[1] - cen[f][1]) + n[f][2] * (o[2] - cen[f][2]);
+        if (d > 0) for (int k = 0; k < 3; k++) n[f][k] = -n[f][k];
+    }
+    return 1;
+}
+
+/* tetrahedronSource, src/elastic3d.f90:1916-2039: body force of an
+ * eigenstrain e in a tetrahedron ABCD, the faces smoothed with Gaussians of
+ * width dx1, physical layers of the (sx1+2, sx2, sx3) box. */
+void orc_tetrahedronsource(double lambda, double mu, const relax_tensor *e, const double A[3], const double B[3],
+                           const double C[3], const double D[3], int sx1, int sx2, int sx3, double dx1, double dx2,
+                           double dx3, real *f1, real *f2, real *f3)
+{
+    otensor m = {e->s11, e->s12, e->s13, e->s22, e->s23, e->s33};
+    isotropic(&m, lambda, mu);
+    double n[4][3], cen[4][3];
+    if (!tet_faces(A, B, C, D, n, cen)) return;
+    double tr[4][3];
+    for (int f = 0; f < 4; f++) tdot(&m, n[f], tr[f]);
+    const int sx1p = sx1 + 2;
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3 / 2; i3++) {
+        double x[3];
+        x[2] = (double)(i3 - 1) * dx3;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                double dum;
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x[0], &x[1], &dum);
+                double d[4];
+                for (int f = 0; f < 4; f++)
+                    d[f] = (cen[f][0] - x[0]) * n[f][0] + (cen[f][1] - x[1]) * n[f][1] + (cen[f][2] - x[2]) * n[f][2];
+                if (fabs(d[0]) > 7.0 * dx1 && fabs(d[1]) > 7.0 * dx1 && fabs(d[2]) > 7.0 * dx1 &&
+                    fabs(d[3]) > 7.0 * dx1)
+                    continue;
+                double H[4], G[4];
+                for (int f = 0; f < 4; f++) H[f] = gaussi(d[f], dx1);
+                for (int f = 0; f < 4; f++) G[f] = gauss(d[f], dx1);
+                const size_t o = (size_t)(i1 - 1) + (size_t)sx1p * ((size_t)(i2 - 1) + (size_t)sx2 * (i3 - 1));
+                real *fk[3] = {f1, f2, f3};
+                for (int k = 0; k < 3; k++)
+                    fk[k][o] = (real)(fk[k][o] + tr[0][k] * G[0] * H[1] * H[2] * H[3] +
+                                      tr[1][k] * H[0] * G[1] * H[2] * H[3] + tr[2][k] * H[0] * H[1] * G[2] * H[3] +
+                                      tr[3][k] * H[0] * H[1] * H[2] * G[3]);
+            }
+        }
+    }
+}
+
+/* momentDensityCuboid, src/elastic3d.f90:2927-3029: moment density of the
+ * eigenstrain e (strike, normal, dip frame) in a cuboid, physical layers
+ * (sx3 of them); the image term is computed but not used there */
+void orc_momentdensitycuboid(double mu, double lambda, const relax_tensor *e, double x, double y, double z,
+                             double L, double W, double T, double strike, double dip, double beta, int sx1, int sx2,
+                             int sx3, double dx1, double dx2, double dx3, otensor *sig)
+{
+    const otensor lamdij = {(real)lambda, 0, 0, (real)lambda, 0, (real)lambda};
+    const real rmu = (real)2 * (real)mu;
+    const double cstrike = cos(strike), sstrike = sin(strike), cdip = cos(dip), sdip = sin(dip);
+    const double Wp = W * (1.0 + 2.0 * beta) / 2.0, Lp = L * (1.0 + 2.0 * beta) / 2.0,
+                 Tp = T * (1.0 + 2.0 * beta) / 2.0;
+    double mx = Wp > Lp ? Wp : Lp;
+    if (Tp > mx) mx = Tp;
+    const double r2 = (double)sqrtf(2.0f) * mx;
+    const double x2r0 = cstrike * x - sstrike * y;
+    const double xr = cdip * x2r0 - sdip * z, yr = sstrike * x + cstrike * y, zr = sdip * x2r0 + cdip * z;
+    const double n[3] = {+cdip * cstrike, -cdip * sstrike, -sdip};
+    const double s[3] = {-sstrike, -cstrike, 0};
+    const double d[3] = {+cstrike * sdip, -sstrike * sdip, +cdip};
+    const otensor ss = sdyad(s, s), ns = sdyad(n, s), sd = sdyad(s, d), nn = sdyad(n, n), nd = sdyad(n, d),
+                  dd = sdyad(d, d);
+    const otensor et = {e->s11, e->s12, e->s13, e->s22, e->s23, e->s33};
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3; i3++) {
+        const double x3 = (double)(i3 - 1) * dx3;
+        if (fabs(x3 - z) > r2) continue;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                double x1, x2, dum;
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x1, &x2, &dum);
+                if (fabs(x1 - x) > r2 || fabs(x2 - y) > r2 || fabs(x3 - z) > r2) continue;
+                const double x2r = cstrike * x1 - sstrike * x2;
+                const double x1s = cdip * x2r - sdip * x3;
+                const double x2s = sstrike * x1 + cstrike * x2;
+                const double x3s = sdip * x2r + cdip * x3;
+                const real aperture = (real)(omega((x1s - xr) / T, beta) * omega((x2s - yr) / W, beta) *
+                                             omega((x3s - zr) / L, beta));
+                const otensor ea = ttimes(aperture, et);
+                otensor Ei = ttimes(ea.s11, ss);
+                Ei = tplus(Ei, ttimes((real)2 * ea.s12, ns));
+                Ei = tplus(Ei, ttimes((real)2 * ea.s13, sd));
+                Ei = tplus(Ei, ttimes(ea.s22, nn));
+                Ei = tplus(Ei, ttimes((real)2 * ea.s23, nd));
+                Ei = tplus(Ei, ttimes(ea.s33, dd));
+                const real ekk = (real)ttrace(&Ei);
+                const size_t o = IDX3(i1 - 1, i2 - 1, i3 - 1, sx1, sx2);
+                sig[o] = tplus(tplus(sig[o], ttimes(ekk, lamdij)), ttimes(rmu, Ei));
+            }
+        }
+    }
+}
+
+/* momentDensityTetrahedron, src/elastic3d.f90:2788-2873: moment density of
+ * the eigenstrain e in a tetrahedron ABCD (physical layers, sx3 of them).
+ * A point is left out when its signed distances to all four faces are
+ * below 7 dx1, as the reference's test reads. */
+void orc_momentdensitytetrahedron(double mu, double lambda, const relax_tensor *e, const double A[3],
+                                  const double B[3], const double C[3], const double D[3], int sx1, int sx2,
+                                  int sx3, double dx1, double dx2, double dx3, otensor *sig)
+{
+    const otensor lamdij = {(real)lambda, 0, 0, (real)lambda, 0, (real)lambda};
+    const real rmu = (real)2 * (real)mu;
+    double n[4][3], cen[4][3];
+    if (!tet_faces(A, B, C, D, n, cen)) return;
+    const otensor et = {e->s11, e->s12, e->s13, e->s22, e->s23, e->s33};
+#pragma omp parallel for schedule(static)
+    for (int i3 = 1; i3 <= sx3; i3++) {
+        double x[3];
+        x[2] = (double)(i3 - 1) * dx3;
+        for (int i2 = 1; i2 <= sx2; i2++) {
+            for (int i1 = 1; i1 <= sx1; i1++) {
+                double dum;
+                shiftedcoordinates(i1, i2, i3, sx1, sx2, sx3, dx1, dx2, dx3, &x[0], &x[1], &dum);
+                double d[4];
+                for (int f = 0; f < 4; f++)
+                    d[f] = (cen[f][0] - x[0]) * n[f][0] + (cen[f][1] - x[1]) * n[f][1] + (cen[f][2] - x[2]) * n[f][2];
+                if (d[0] < 7.0 * dx1 && d[1] < 7.0 * dx1 && d[2] < 7.0 * dx1 && d[3] < 7.0 * dx1) continue;
+                const double H = gaussi(d[0], dx1) * gaussi(d[1], dx1) * gaussi(d[2], dx1) * gaussi(d[3], dx1);
+                const otensor ea = ttimes((real)H, et);
+                const real ekk = (real)ttrace(&ea);
+                const size_t o = IDX3(i1 - 1, i2 - 1, i3 - 1, sx1, sx2);
+                sig[o] = tplus(tplus(sig[o], ttimes(ekk, lamdij)), ttimes(rmu, ea));
+            }
+        }
+    }
+}
+
+
+/* dislocations without eigenstress, src/relax.f90:1116-1289: shear,
+ * cuboid and tetrahedral eigenstrain, tensile and point sources */
 static int orc_dislocations(orc_state *S, const relax_event *ev)
 {
     const relax_config *c = &S->cfg;
@@ -1789,11 +2039,38 @@ static int orc_dislocations(orc_state *S, const relax_event *ev)
                        s->rake, s->beta, S->sx1, S->sx2, S->sx3, c->dx1, c->dx2, c->dx3,
                        S->v[0], S->v[1], S->v[2], S->t[0], S->t[1], S->t[2]);
     }
+    /* cuboid and tetrahedral eigenstrain (src/relax.f90:1154-1181): the
+     * cuboid's L = width, W = length, T = thickness, the global beta */
+    for (int i = 0; i < ev->nc; i++) {
+        const relax_weakzone *q = &ev->c[i];
+        orc_cuboidsource(c->lambda, c->mu, &q->e, q->x, q->y, q->z, q->width, q->length, q->thickness, q->strike,
+                         q->dip, c->beta, S->sx1, S->sx2, S->sx3, c->dx1, c->dx2, c->dx3, S->v[0], S->v[1],
+                         S->v[2]);
+    }
+    for (int i = 0; i < ev->ntet; i++) {
+        const relax_tetrahedron *q = &ev->tet[i];
+        orc_tetrahedronsource(c->lambda, c->mu, &q->e, ev->vert + 3 * (q->i1 - 1), ev->vert + 3 * (q->i2 - 1),
+                              ev->vert + 3 * (q->i3 - 1), ev->vert + 3 * (q->i4 - 1), S->sx1, S->sx2, S->sx3,
+                              c->dx1, c->dx2, c->dx3, S->v[0], S->v[1], S->v[2]);
+    }
     for (int i = 0; i < ev->ns; i++) {
         const relax_source *s = &ev->s[i];
         orc_momentdensityshear(c->mu, s->slip, s->x, s->y, s->z, s->width, s->length, s->strike,
                                s->dip, s->rake, s->beta, S->sx1, S->sx2, S->sx3h, c->dx1, c->dx2,
                                c->dx3, S->tau);
+    }
+    /* their moment densities into tau (src/relax.f90:1208-1224) */
+    for (int i = 0; i < ev->nc; i++) {
+        const relax_weakzone *q = &ev->c[i];
+        orc_momentdensitycuboid(c->mu, c->lambda, &q->e, q->x, q->y, q->z, q->width, q->length, q->thickness,
+                                q->strike, q->dip, c->beta, S->sx1, S->sx2, S->sx3h, c->dx1, c->dx2, c->dx3,
+                                S->tau);
+    }
+    for (int i = 0; i < ev->ntet; i++) {
+        const relax_tetrahedron *q = &ev->tet[i];
+        orc_momentdensitytetrahedron(c->mu, c->lambda, &q->e, ev->vert + 3 * (q->i1 - 1), ev->vert + 3 * (q->i2 - 1),
+                                     ev->vert + 3 * (q->i3 - 1), ev->vert + 3 * (q->i4 - 1), S->sx1, S->sx2,
+                                     S->sx3h, c->dx1, c->dx2, c->dx3, S->tau);
     }
     /* tensile cracks (src/relax.f90:1226-1260): L = width, W = length, the
      * global beta, the crack's opening */

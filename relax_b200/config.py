@@ -70,11 +70,18 @@ class relax_weakzone(C.Structure):
                [("e", relax_tensor)]
 
 
+class relax_tetrahedron(C.Structure):
+    _fields_ = [("e", relax_tensor), ("i1", C.c_int), ("i2", C.c_int), ("i3", C.c_int), ("i4", C.c_int)]
+
+
 class relax_event(C.Structure):
     _fields_ = [("time", C.c_double), ("ns", C.c_int), ("nt", C.c_int), ("nm", C.c_int),
                 ("nl", C.c_int), ("s", C.POINTER(relax_source)),
                 ("ts", C.POINTER(relax_source)), ("m", C.POINTER(relax_source)),
-                ("l", C.POINTER(relax_source))]
+                ("l", C.POINTER(relax_source)),
+                ("nc", C.c_int), ("ntet", C.c_int), ("nvert", C.c_int),
+                ("c", C.POINTER(relax_weakzone)), ("tet", C.POINTER(relax_tetrahedron)),
+                ("vert", C.POINTER(C.c_double))]
 
 
 class relax_config(C.Structure):
@@ -230,12 +237,39 @@ class Load:
 
 
 @dataclass
+class Cuboid:
+    """A cuboid of eigenstrain (--with-eigenstrain, src/input.f90:1496-1560):
+    strain (e11, e12, e13, e22, e23, e33) in the source's (strike, normal,
+    dip) frame, centre geometry as a fault's, thickness across it."""
+    e: Tuple[float, float, float, float, float, float]
+    x: float
+    y: float
+    z: float
+    length: float
+    width: float
+    thickness: float
+    strike: float
+    dip: float
+
+
+@dataclass
+class Tetrahedron:
+    """A tetrahedron of eigenstrain (--with-curvilinear, src/input.f90:
+    1588-1660): strain in the grid frame and four 1-based vertex numbers."""
+    e: Tuple[float, float, float, float, float, float]
+    vertices: Tuple[int, int, int, int]
+
+
+@dataclass
 class Event:
     time: float
     faults: List[Fault] = field(default_factory=list)
     tensile: List[Tensile] = field(default_factory=list)
     points: List[Point] = field(default_factory=list)
     loads: List[Load] = field(default_factory=list)
+    cuboids: List[Cuboid] = field(default_factory=list)
+    tetrahedra: List[Tetrahedron] = field(default_factory=list)
+    vertices: List[Tuple[float, float, float]] = field(default_factory=list)
 
 
 @dataclass
@@ -282,6 +316,9 @@ class Simulation:
     def skip(self) -> int:
         # src/input.f90:308-316: "T, -n, t_s" -> skip = ceiling(n), odt < 0
         return int(math.ceil(-self.odt)) if self.odt < 0 else 0
+
+    def has_eigenstrain(self) -> bool:
+        return any(ev.cuboids or ev.tetrahedra for ev in self.events)
 
     @property
     def npoints(self) -> int:
@@ -396,6 +433,27 @@ class Simulation:
                 keep.append(larr)
                 earr[e].nl = len(ev.loads)
                 earr[e].l = C.cast(larr, C.POINTER(relax_source))
+            if ev.cuboids:
+                carr = (relax_weakzone * len(ev.cuboids))()
+                for k, q in enumerate(ev.cuboids):
+                    # wangconvention on the weak-zone geometry (src/input.f90:1548-1558)
+                    _, x, y, z, strike, dip, _ = wang_convention(
+                        0.0, q.x, q.y, q.z, q.length, q.width, q.strike, q.dip, 0.0, self.x0, self.y0, self.rot)
+                    carr[k] = relax_weakzone(dgammadot0=0.0, x=x, y=y, z=z, width=q.width, length=q.length,
+                                             thickness=q.thickness, strike=strike, dip=dip, e=relax_tensor(*q.e))
+                keep.append(carr)
+                earr[e].nc = len(ev.cuboids)
+                earr[e].c = C.cast(carr, C.POINTER(relax_weakzone))
+            if ev.tetrahedra:
+                tarr = (relax_tetrahedron * len(ev.tetrahedra))()
+                for k, q in enumerate(ev.tetrahedra):
+                    tarr[k] = relax_tetrahedron(relax_tensor(*q.e), *q.vertices)
+                varr = (C.c_double * (3 * len(ev.vertices)))(*[c for v in ev.vertices for c in v])
+                keep += [tarr, varr]
+                earr[e].ntet = len(ev.tetrahedra)
+                earr[e].tet = C.cast(tarr, C.POINTER(relax_tetrahedron))
+                earr[e].nvert = len(ev.vertices)
+                earr[e].vert = C.cast(varr, C.POINTER(C.c_double))
         keep.append(earr)
         cfg.ne = len(self.events)
         cfg.events = C.cast(earr, C.POINTER(relax_event))
@@ -435,8 +493,13 @@ class Simulation:
         interfaces).  Numbers are written with repr, so reading them back
         gives the same doubles.  obsplanes: (x1, x2, x3, length, width,
         strike, dip) and segments: (x1, x2, x3, length, width, strike, dip,
-        friction), in the input file's convention (degrees)."""
+        friction), in the input file's convention (degrees).  Decks with
+        eigenstrain sources are written with the --with-eigenstrain sections
+        (and --with-curvilinear ones when a tetrahedron is present): read
+        them with those flags."""
         r = repr
+        eigen = self.has_eigenstrain()
+        curvilinear = any(ev.tetrahedra for ev in self.events)
         out = ["# grid dimension (sx1,sx2,sx3)", f"{self.sx1} {self.sx2} {self.sx3}",
                "# sampling (dx1,dx2,dx3), smoothing (beta, nyquist)",
                f"{r(self.dx1)} {r(self.dx2)} {r(self.dx3)} {r(self.beta)} {r(self.nyquist)}",
@@ -496,6 +559,18 @@ class Simulation:
                     f"{r(t.strike)} {r(t.dip)}" for k, t in enumerate(ev.tensile)]
             out += ["# number of dilatation sources", str(len(ev.points))]
             out += [f"{k + 1} {r(m.amplitude)} {r(m.x)} {r(m.y)} {r(m.z)}" for k, m in enumerate(ev.points)]
+            if eigen:
+                out += ["# number of cuboid eigenstrain sources", str(len(ev.cuboids))]
+                out += [f"{k + 1} " + " ".join(r(float(v)) for v in q.e) +
+                        f" {r(q.x)} {r(q.y)} {r(q.z)} {r(q.length)} {r(q.width)} {r(q.thickness)} {r(q.strike)} "
+                        f"{r(q.dip)}" for k, q in enumerate(ev.cuboids)]
+                if curvilinear:
+                    out += ["# number of tetrahedra", str(len(ev.tetrahedra))]
+                    out += [f"{k + 1} " + " ".join(r(float(v)) for v in q.e) + " " +
+                            " ".join(str(i) for i in q.vertices) for k, q in enumerate(ev.tetrahedra)]
+                    if ev.tetrahedra:
+                        out += ["# number of vertices", str(len(ev.vertices))]
+                        out += [f"{k + 1} {r(v[0])} {r(v[1])} {r(v[2])}" for k, v in enumerate(ev.vertices)]
             out += ["# number of surface loads", str(len(ev.loads))]
             out += [f"{k + 1} {r(ld.x)} {r(ld.y)} {r(ld.length)} {r(ld.width)} {r(ld.t3)} {r(ld.period)} "
                     f"{r(ld.phase)}" + ("" if ld.beta is None else f" {r(ld.beta)}")

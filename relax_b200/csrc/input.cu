@@ -259,9 +259,12 @@ struct relax_input {
     std::vector<float> dg[4];
     std::vector<relax_plane> planes;
     std::vector<std::vector<relax_source>> es, ets, em, el;
+    std::vector<std::vector<relax_weakzone>> ecub;        // cuboid eigenstrain sources
+    std::vector<std::vector<relax_tetrahedron>> etet;     // tetrahedral ones
+    std::vector<std::vector<double>> evert;               // their vertices
     std::vector<relax_event> events;
     std::vector<relax_source> is, its;
-    int ncuboid = 0, ntetra = 0;
+    int ncuboid = 0, ntetra = 0;      // totals over the events
     double minlength = 0, minwidth = 0;
 };
 
@@ -691,6 +694,7 @@ void parse(const char *text, relax_input &in)
         if (ne < 0) perr("input line %d: negative number of events", r.line);
     }
     in.es.resize(ne); in.ets.resize(ne); in.em.resize(ne); in.el.resize(ne);
+    in.ecub.resize(ne); in.etet.resize(ne); in.evert.resize(ne);
     in.events.assign(ne, relax_event{});
     for (int e = 0; e < ne; e++) {
         relax_event &ev = in.events[e];
@@ -800,21 +804,84 @@ void parse(const char *text, relax_input &in)
             Record r = rd.record("the number of cuboid eigenstrain sources");
             const int n = r.integer("number of cuboids");
             echo.line(iw(n, 5));
-            for (int k = 1; k <= n; k++) rd.record("a cuboid");
+            if (n < 0) perr("input line %d: negative number of cuboids", r.line);
+            if (n > 0) {
+                echo.text(RULE);
+                echo.text("#  n       e11       e12       e13       e22       e23       e33       x1       x2       "
+                          "x3  length   width thickness strike dip");
+                echo.text(RULE);
+            }
+            for (int k = 1; k <= n; k++) {
+                // src/input.f90:1510-1560: the strain, then the geometry of a weak zone
+                Record q = rd.record("a cuboid");
+                const int i = q.integer("index");
+                relax_weakzone w{};
+                const char *en[6] = {"e11", "e12", "e13", "e22", "e23", "e33"};
+                float *ep[6] = {&w.e.s11, &w.e.s12, &w.e.s13, &w.e.s22, &w.e.s23, &w.e.s33};
+                double ev[6];
+                for (int j = 0; j < 6; j++) {
+                    ev[j] = q.real(en[j]);
+                    *ep[j] = (float)ev[j];
+                }
+                w.x = q.real("x1"); w.y = q.real("x2"); w.z = q.real("x3");
+                w.length = q.real("length"); w.width = q.real("width"); w.thickness = q.real("thickness");
+                w.strike = q.real("strike"); w.dip = q.real("dip");
+                // echoed from the stored REAL*4 strain, as the reference prints its copy
+                const double v9[9] = {w.e.s11, w.e.s12, w.e.s13, w.e.s22, w.e.s23, w.e.s33, w.x, w.y, w.z};
+                const double v3[3] = {w.length, w.width, w.thickness}, v2[2] = {w.strike, w.dip};
+                echo.line(iw(k, 4, 4) + esn(v9, 9, 10, 2, 2) + esn(v3, 3, 8, 2, 1) + esn(v2, 2, 9, 2, 1));
+                if (i != k) perr("input line %d: source index misfit (%d, expected %d)", q.line, i, k);
+                double dummy = 0, rake = 0;
+                wang(dummy, w.x, w.y, w.z, w.length, w.width, w.strike, w.dip, rake, in.x0, in.y0, in.rot);
+                in.ecub[e].push_back(w);
+            }
+            if (n > 0) echo.text(RULE);
             in.ncuboid += n;
             if (in.flags & RELAX_INPUT_CURVILINEAR) {
                 echo.text("# number of distributed tetrahedral eigenstrain sources");
                 Record t = rd.record("the number of tetrahedra");
                 const int nt = t.integer("number of tetrahedra");
                 echo.line(iw(nt, 5));
+                if (nt < 0) perr("input line %d: negative number of tetrahedra", t.line);
                 if (nt > 0) {
-                    for (int k = 1; k <= nt; k++) rd.record("a tetrahedron");
+                    echo.text(RULE);
+                    echo.text("#  n       e11       e12       e13       e22       e23       e33       i1       i2       "
+                              "i3       i4");
+                    echo.text(RULE);
+                    for (int k = 1; k <= nt; k++) {
+                        Record q = rd.record("a tetrahedron");
+                        const int i = q.integer("index");
+                        relax_tetrahedron tt{};
+                        const char *en[6] = {"e11", "e12", "e13", "e22", "e23", "e33"};
+                        float *ep[6] = {&tt.e.s11, &tt.e.s12, &tt.e.s13, &tt.e.s22, &tt.e.s23, &tt.e.s33};
+                        for (int j = 0; j < 6; j++) *ep[j] = (float)q.real(en[j]);
+                        tt.i1 = q.integer("i1"); tt.i2 = q.integer("i2");
+                        tt.i3 = q.integer("i3"); tt.i4 = q.integer("i4");
+                        const double v6[6] = {tt.e.s11, tt.e.s12, tt.e.s13, tt.e.s22, tt.e.s23, tt.e.s33};
+                        echo.line(iw(k, 4, 4) + esn(v6, 6, 10, 2, 2) + " " + iw(tt.i1, 8) + " " + iw(tt.i2, 8) +
+                                  " " + iw(tt.i3, 8) + " " + iw(tt.i4, 8));
+                        if (i != k) perr("input line %d: source index misfit (%d, expected %d)", q.line, i, k);
+                        in.etet[e].push_back(tt);
+                    }
                     echo.text("# number of tetrahedron vertices");
                     Record v = rd.record("the number of tetrahedron vertices");
                     const int nv = v.integer("number of vertices");
                     echo.line(iw(nv, 5));
+                    echo.text(RULE);
+                    echo.text("#  n        x1        x2        x3");
+                    echo.text(RULE);
                     if (nv <= 0) perr("input line %d: must provide tetrahedra vertices", v.line);
-                    for (int k = 1; k <= nv; k++) rd.record("a vertex");
+                    for (int k = 1; k <= nv; k++) {
+                        Record q = rd.record("a vertex");
+                        const int i = q.integer("index");
+                        const double xyz[3] = {q.real("x1"), q.real("x2"), q.real("x3")};
+                        echo.line(iw(k, 4, 4) + esn(xyz, 3, 10, 2, 2));
+                        if (i != k) perr("input line %d: source index misfit (%d, expected %d)", q.line, i, k);
+                        for (int j = 0; j < 3; j++) in.evert[e].push_back(xyz[j]);
+                    }
+                    for (const auto &tt : in.etet[e])
+                        for (int vi : {tt.i1, tt.i2, tt.i3, tt.i4})
+                            if (vi < 1 || vi > nv) perr("tetrahedron vertex %d out of range (1..%d)", vi, nv);
                 }
                 in.ntetra += nt;
             }
@@ -856,8 +923,6 @@ void parse(const char *text, relax_input &in)
         in.ntetra == 0 && c.interval <= 0)
         perr("input: no input dislocations or dilatation point sources or surface tractions for first event");
     (void)e0;
-    if (in.ncuboid > 0 || in.ntetra > 0)
-        throw ParseError{RELAX_ERR_UNSUPPORTED, "cuboid and tetrahedral eigenstrain sources are not supported"};
     if (echo.on) printf("# max sampling size (hor.,vert.):%s%s\n", es(in.minlength / 2.5, 8, 2, 1).c_str(),
                         es(in.minwidth / 2.5, 8, 2, 1).c_str());
 }
@@ -895,6 +960,9 @@ int finish(relax_input &in)
         ev.nt = (int)in.ets[e].size(); ev.ts = ev.nt ? in.ets[e].data() : nullptr;
         ev.nm = (int)in.em[e].size(); ev.m = ev.nm ? in.em[e].data() : nullptr;
         ev.nl = (int)in.el[e].size(); ev.l = ev.nl ? in.el[e].data() : nullptr;
+        ev.nc = (int)in.ecub[e].size(); ev.c = ev.nc ? in.ecub[e].data() : nullptr;
+        ev.ntet = (int)in.etet[e].size(); ev.tet = ev.ntet ? in.etet[e].data() : nullptr;
+        ev.nvert = (int)(in.evert[e].size() / 3); ev.vert = ev.nvert ? in.evert[e].data() : nullptr;
     }
     c.ne = (int)in.events.size();
     c.events = in.events.data();

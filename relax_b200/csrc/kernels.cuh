@@ -2287,6 +2287,203 @@ __global__ void k_moment_mogi(SrcArgs a)
 }
 
 // ------------------------------------------------------------------------
+// eigenstrain sources (--with-eigenstrain, --with-curvilinear): body forces
+// into a.f (physical layers of the whole-box arrays) and moment densities
+// into a.tau (6 x nh)
+// ------------------------------------------------------------------------
+struct EigArgs {
+    Grid g;
+    double lambda, mu, beta;
+    float e[6];                          // the eigenstrain e11 e12 e13 e22 e23 e33
+    // cuboid: centre, L = width, W = length, T = thickness (as dislocations
+    // passes them, src/relax.f90:1157-1166), strike, dip (radians)
+    double x, y, z, L, W, T, strike, dip;
+    float sdy[6][6];                     // s.s, n.s, s.d, n.n, n.d, d.d (momentDensityCuboid)
+    // tetrahedron: outward unit normals and centroids of the faces BCD, CDA,
+    // DAB, ABC, and the tractions (c : e) n of each face
+    double n[4][3], cen[4][3], tr[4][3];
+    float *f[3];
+    float *tau;
+};
+
+__device__ __forceinline__ double d_gaussi(double x, double s) { return (1.0 + erf(x / sqrt(2.0) / s)) / 2.0; }
+
+// cuboidSource, src/elastic3d.f90:1680-1884 (the surface-traction loop there
+// stores nothing)
+__global__ void k_source_cuboid(EigArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = i3 * g.dx3;
+    const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0,
+                 Tp = a.T * (1.0 + 2.0 * a.beta) / 2.0;
+    const double r2 = (double)1.41421354f * fmax(Wp, fmax(Lp, Tp));   // SQRT(2.) of default kind
+    if (fabs(x3 - a.z) > r2 || fabs(x1 - a.x) > r2 || fabs(x2 - a.y) > r2) return;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double x2r0 = cs * a.x - ss * a.y;
+    const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+    const double x2r = cs * x1 - ss * x2;
+    const double x1s = cd * x2r - sd * x3, x1i = cd * x2r + sd * x3;
+    const double x2s = ss * x1 + cs * x2;
+    const double x3s = sd * x2r + cd * x3, x3i = -sd * x2r + cd * x3;
+    const double T = a.T, W = a.W, L = a.L, b = a.beta;
+    double t1 = d_omega((x1s - xr) / T, b);
+    const double t2 = d_omega((x2s - yr) / W, b);
+    double t3 = d_omega((x3s - zr) / L, b);
+    const double sourc = 1.0 / T * d_omegap((x1s - xr) / T, b) * t2 * t3;
+    const double dblcp = 1.0 / W * t1 * d_omegap((x2s - yr) / W, b) * t3;
+    const double dipcs = 1.0 / L * t1 * t2 * d_omegap((x3s - zr) / L, b);
+    t1 = d_omega((x1i - xr) / T, b);
+    t3 = d_omega((x3i + zr) / L, b);
+    const double image = 1.0 / T * d_omegap((x1i - xr) / T, b) * t2 * t3;
+    const double cplei = 1.0 / W * t1 * d_omegap((x2s - yr) / W, b) * t3;
+    const double mu = a.mu;
+    const double ekk = (double)(a.e[0] + a.e[3] + a.e[5]);
+    const double e12 = a.e[1], e13 = a.e[2], e23 = a.e[4];
+    const double s11 = a.lambda * ekk + 2.0 * mu * a.e[0], s22 = a.lambda * ekk + 2.0 * mu * a.e[3],
+                 s33 = a.lambda * ekk + 2.0 * mu * a.e[5];
+    double f1, f2, f3;
+    if (2.01 * 0.01745329251994329547437168059786927 > a.dip) {
+        // method of images for subvertical sources
+        f1 = 2.0 * mu * e12 * ss * (sourc + image) + 2.0 * mu * e12 * cd * cs * (dblcp + cplei) -
+             s11 * ss * (dblcp + cplei) - s22 * cd * cs * (sourc + image);
+        f2 = 2.0 * mu * e12 * cs * (sourc + image) - 2.0 * mu * e12 * cd * ss * (dblcp + cplei) -
+             s11 * cs * (dblcp + cplei) + s22 * cd * ss * (sourc + image);
+        f3 = -2.0 * mu * e12 * sd * (dblcp - cplei) + s22 * sd * (sourc - image);
+    } else {
+        f1 = 2.0 * mu * e12 * ss * sourc + 2.0 * mu * e12 * cd * cs * dblcp - s11 * ss * dblcp - s22 * cd * cs * sourc;
+        f2 = 2.0 * mu * e12 * cs * sourc - 2.0 * mu * e12 * cd * ss * dblcp - s11 * cs * dblcp + s22 * cd * ss * sourc;
+        f3 = -2.0 * mu * e12 * sd * dblcp + s22 * sd * sourc;
+    }
+    float *p1 = a.f[0] + q, *p2 = a.f[1] + q, *p3 = a.f[2] + q;
+    *p1 = (float)(*p1 + f1);
+    *p2 = (float)(*p2 + f2);
+    *p3 = (float)(*p3 + f3);
+    // vertical shear components
+    *p1 = (float)(*p1 + 2.0 * mu * e13 * cd * ss * dipcs + 2.0 * mu * e13 * sd * cs * dblcp -
+                  2.0 * mu * e23 * cd * cs * dipcs - 2.0 * mu * e23 * sd * cs * sourc - s33 * sd * dipcs * cs);
+    *p2 = (float)(*p2 + 2.0 * mu * e13 * cd * cs * dipcs - 2.0 * mu * e13 * sd * ss * dblcp +
+                  2.0 * mu * e23 * cd * ss * dipcs + 2.0 * mu * e23 * sd * ss * sourc + s33 * sd * dipcs * ss);
+    *p3 = (float)(*p3 + 2.0 * mu * e13 * cd * dblcp - 2.0 * mu * e23 * cd * sourc - s33 * cd * dipcs);
+}
+
+// the signed distances of a point to the four faces (positive inside)
+__device__ __forceinline__ void tet_dist(const EigArgs &a, double x1, double x2, double x3, double d[4])
+{
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+        d[f] = (a.cen[f][0] - x1) * a.n[f][0] + (a.cen[f][1] - x2) * a.n[f][1] + (a.cen[f][2] - x3) * a.n[f][2];
+}
+
+// tetrahedronSource, src/elastic3d.f90:1916-2039: face tractions times a
+// Gaussian across the face and error-function steps across the others
+__global__ void k_source_tetra(EigArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = i3 * g.dx3;
+    double d[4];
+    tet_dist(a, x1, x2, x3, d);
+    const double lim = 7.0 * g.dx1;
+    if (fabs(d[0]) > lim && fabs(d[1]) > lim && fabs(d[2]) > lim && fabs(d[3]) > lim) return;
+    double H[4], G[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        H[f] = d_gaussi(d[f], g.dx1);
+        G[f] = d_gauss(d[f], g.dx1);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float *p = a.f[k] + q;
+        *p = (float)(*p + a.tr[0][k] * G[0] * H[1] * H[2] * H[3] + a.tr[1][k] * H[0] * G[1] * H[2] * H[3] +
+                     a.tr[2][k] * H[0] * H[1] * G[2] * H[3] + a.tr[3][k] * H[0] * H[1] * H[2] * G[3]);
+    }
+}
+
+// tau += trace(E) lambda delta + 2 mu E for an eigenstrain E (FP32 as the
+// reference's REAL*4 tensors)
+__device__ __forceinline__ void tau_add_eigen(float *tau, size_t nh, size_t q, const float E[6], float lambda,
+                                              float rmu)
+{
+    const float ekk = (float)(double)(E[0] + E[3] + E[5]);
+    const float lam[6] = {lambda, 0.f, 0.f, lambda, 0.f, lambda};
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        const float t = __fadd_rn(tau[c * nh + q], __fmul_rn(ekk, lam[c]));
+        tau[c * nh + q] = __fadd_rn(t, __fmul_rn(rmu, E[c]));
+    }
+}
+
+// momentDensityCuboid, src/elastic3d.f90:2927-3029 (the image term is not
+// used there)
+__global__ void k_moment_cuboid(EigArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = i3 * g.dx3;
+    const double Wp = a.W * (1.0 + 2.0 * a.beta) / 2.0, Lp = a.L * (1.0 + 2.0 * a.beta) / 2.0,
+                 Tp = a.T * (1.0 + 2.0 * a.beta) / 2.0;
+    const double r2 = (double)1.41421354f * fmax(Wp, fmax(Lp, Tp));
+    if (fabs(x3 - a.z) > r2 || fabs(x1 - a.x) > r2 || fabs(x2 - a.y) > r2) return;
+    const double cs = cos(a.strike), ss = sin(a.strike), cd = cos(a.dip), sd = sin(a.dip);
+    const double x2r0 = cs * a.x - ss * a.y;
+    const double xr = cd * x2r0 - sd * a.z, yr = ss * a.x + cs * a.y, zr = sd * x2r0 + cd * a.z;
+    const double x2r = cs * x1 - ss * x2;
+    const double x1s = cd * x2r - sd * x3, x2s = ss * x1 + cs * x2, x3s = sd * x2r + cd * x3;
+    const float ap = (float)(d_omega((x1s - xr) / a.T, a.beta) * d_omega((x2s - yr) / a.W, a.beta) *
+                             d_omega((x3s - zr) / a.L, a.beta));
+    float ea[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) ea[c] = __fmul_rn(ap, a.e[c]);
+    // E = e11 s.s + 2 e12 n.s + 2 e13 s.d + e22 n.n + 2 e23 n.d + e33 d.d
+    const float w[6] = {ea[0], __fmul_rn(2.f, ea[1]), __fmul_rn(2.f, ea[2]), ea[3], __fmul_rn(2.f, ea[4]), ea[5]};
+    float E[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        float v = __fmul_rn(w[0], a.sdy[0][c]);
+#pragma unroll
+        for (int k = 1; k < 6; k++) v = __fadd_rn(v, __fmul_rn(w[k], a.sdy[k][c]));
+        E[c] = v;
+    }
+    tau_add_eigen(a.tau, g.nh, q, E, (float)a.lambda, __fmul_rn(2.f, (float)a.mu));
+}
+
+// momentDensityTetrahedron, src/elastic3d.f90:2788-2873; a point is left
+// out when all four signed distances are below 7 dx1, as the source reads
+__global__ void k_moment_tetra(EigArgs a)
+{
+    const Grid &g = a.g;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nh) return;
+    const int i1 = (int)(q % g.sx1), i2 = (int)((q / g.sx1) % g.sx2), i3 = (int)(q / g.plane);
+    const double x1 = (i1 < g.sx1 / 2 ? i1 : i1 - g.sx1) * g.dx1;
+    const double x2 = (i2 < g.sx2 / 2 ? i2 : i2 - g.sx2) * g.dx2;
+    const double x3 = i3 * g.dx3;
+    double d[4];
+    tet_dist(a, x1, x2, x3, d);
+    const double lim = 7.0 * g.dx1;
+    if (d[0] < lim && d[1] < lim && d[2] < lim && d[3] < lim) return;
+    const double H = d_gaussi(d[0], g.dx1) * d_gaussi(d[1], g.dx1) * d_gaussi(d[2], g.dx1) * d_gaussi(d[3], g.dx1);
+    const float h = (float)H;
+    float E[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) E[c] = __fmul_rn(h, a.e[c]);
+    tau_add_eigen(a.tau, g.nh, q, E, (float)a.lambda, __fmul_rn(2.f, (float)a.mu));
+}
+
+// ------------------------------------------------------------------------
 // layout conversion between RELAX's arrays and the device layout
 // ------------------------------------------------------------------------
 // AoS TENSOR (sx1, sx2, sx3h) <-> SoA

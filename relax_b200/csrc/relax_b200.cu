@@ -466,13 +466,14 @@ static bool reg_shape(const Grid &g)
 // boxes, pruned transform (the time step's Green's functions)
 static bool zspec_tc_ok(const ZArgs &za) { return za.g.sx3 == 128 && za.nin == 64 && za.nout == 64; }
 
-static cudaError_t launch_zspec_tc(const ZArgs &za, int nsm, int *err, cudaStream_t st)
+static cudaError_t launch_zspec_tc(const ZArgs &za, int nsm, int *err, const uint4 *tab, cudaStream_t st)
 {
     ZtcArgs t{};
     t.z = za;
     t.ncol = za.g.sx2 * za.g.K1;
     t.ntiles = (t.ncol + ZT_COLS - 1) / ZT_COLS;
     t.err = err;
+    t.tab = tab;
     set_smem(k_zspec_tc, ZT_SMEM);
     k_zspec_tc<<<std::min(t.ntiles, std::max(1, nsm)), ZT_THREADS, ZT_SMEM, st>>>(t);
     return cudaGetLastError();
@@ -483,7 +484,21 @@ struct Spectral {
     bool use_reg = true;   // register-resident y/z passes where instantiated
     int mixed = 0;         // 1: the x3 pass on the tensor cores where zspec_tc_ok
     int *tc_err = nullptr; // device flag of k_zspec_tc (the context's error word)
+    uint4 *ztab = nullptr; // constant operands of k_zspec_tc (set_mixed)
     int nsm = 0;           // SMs of the device (persistent x3 pass)
+
+    // switches the tensor-core x3 pass on (its constant table built once) or off
+    int set_mixed(int on, int *err, cudaStream_t st)
+    {
+        if (on && !ztab) {
+            TRY(dalloc(&ztab, ZT_TAB_BYTES / 16));
+            k_ztc_tables<<<8, 256, 0, st>>>(ztab);
+            CKL();
+        }
+        mixed = on;
+        tc_err = err;
+        return RELAX_OK;
+    }
     bool yreg = false;
     Grid g{};
     float2 *S = nullptr;
@@ -553,8 +568,10 @@ struct Spectral {
     {
         if (S) dfree(S, idle);
         if (tw) dfree(tw, idle);
+        if (ztab) dfree(ztab, idle);
         S = nullptr;
         tw = nullptr;
+        ztab = nullptr;
     }
 
     // arguments of the five passes (the caller's parts of `xa` and `xi`
@@ -613,8 +630,8 @@ struct Spectral {
         }
         ZArgs za = zargs(nin, nout, lambda, mu, gam, twz);
         bool zr = false;
-        if (mixed && tc_err && zspec_tc_ok(za)) {
-            TIMED(prof, ST_ZSPEC, st, (re = launch_zspec_tc(za, nsm, tc_err, st)));
+        if (mixed && tc_err && ztab && zspec_tc_ok(za)) {
+            TIMED(prof, ST_ZSPEC, st, (re = launch_zspec_tc(za, nsm, tc_err, ztab, st)));
             if (re != cudaSuccess) return fail(RELAX_ERR_CUDA, "k_zspec_tc: %s", cudaGetErrorString(re));
             zr = true;
         }
@@ -808,6 +825,9 @@ static void prestress_terms(const relax_tensor_layer *pre, int nz, double mu, co
 struct EventCopy {
     double time;
     std::vector<relax_source> s, ts, m, l;
+    std::vector<relax_weakzone> cub;       // cuboid eigenstrain sources
+    std::vector<relax_tetrahedron> tet;    // tetrahedral ones, over `vert`
+    std::vector<double> vert;
 };
 
 struct relax_ctx {
@@ -966,10 +986,18 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
         if (e.nt > 0 && e.ts) o.ts.assign(e.ts, e.ts + e.nt);
         if (e.nm > 0 && e.m) o.m.assign(e.m, e.m + e.nm);
         if (e.nl > 0 && e.l) o.l.assign(e.l, e.l + e.nl);
+        if (e.nc > 0 && e.c) o.cub.assign(e.c, e.c + e.nc);
+        if (e.ntet > 0 && e.tet) o.tet.assign(e.tet, e.tet + e.ntet);
+        if (e.nvert > 0 && e.vert) o.vert.assign(e.vert, e.vert + 3 * (size_t)e.nvert);
     };
     c->events.resize(cfg->ne);
     for (int k = 0; k < cfg->ne; k++) copye(cfg->events[k], c->events[k]);
     copye(cfg->inter, c->inter);
+    for (size_t k = 0; k < c->events.size(); k++)
+        for (const auto &q : c->events[k].tet)
+            for (int v : {q.i1, q.i2, q.i3, q.i4})
+                if (v < 1 || (size_t)v > c->events[k].vert.size() / 3)
+                    return fail(RELAX_ERR_ARG, "event %zu: tetrahedron vertex %d out of range", k, v);
     for (const auto *v : {&c->lin, &c->non, &c->lt, &c->nlt})
         for (const auto &l : *v)
             if (l.stressexponent < 0.999999)
@@ -1264,6 +1292,73 @@ static int upload_loads(relax_ctx *c, const EventCopy &ev, double t, double Dt, 
 // tensile and point sources also their images below the surface), the
 // surface traction into c->twork, and the moment densities into tau.
 // *full: the lower half of the box is non-zero.
+// the arguments of the eigenstrain kernels for one cuboid or tetrahedron
+static EigArgs eig_args(relax_ctx *c, const relax_tensor &e)
+{
+    EigArgs a{};
+    a.g = c->g; a.lambda = c->cfg.lambda; a.mu = c->cfg.mu; a.beta = c->cfg.beta;
+    const float ev[6] = {e.s11, e.s12, e.s13, e.s22, e.s23, e.s33};
+    for (int k = 0; k < 6; k++) a.e[k] = ev[k];
+    const size_t nb = 2 * c->g.nh;
+    for (int k = 0; k < 3; k++) a.f[k] = c->work + k * nb;
+    a.tau = c->tau;
+    return a;
+}
+
+// tensorsymmetricdyadprod (src/elastic3d.f90:206-218) in the reference's
+// REAL*4 result
+static void sdyad6(const double u[3], const double v[3], float out[6])
+{
+    out[0] = (float)(u[0] * v[0]);
+    out[1] = (float)((u[0] * v[1] + u[1] * v[0]) / 2.0);
+    out[2] = (float)((u[0] * v[2] + u[2] * v[0]) / 2.0);
+    out[3] = (float)(u[1] * v[1]);
+    out[4] = (float)((u[1] * v[2] + u[2] * v[1]) / 2.0);
+    out[5] = (float)(u[2] * v[2]);
+}
+
+// outward unit normals, centroids and tractions (c : e) n of the faces BCD,
+// CDA, DAB, ABC (src/elastic3d.f90:1946-1985); false without volume
+static bool tet_setup(EigArgs &a, const double *A, const double *B, const double *C, const double *D)
+{
+    const double *P[4] = {A, B, C, D};
+    const int tri[4][3] = {{1, 2, 3}, {2, 3, 0}, {3, 0, 1}, {0, 1, 2}};
+    double nrm[4];
+    for (int f = 0; f < 4; f++) {
+        const double *p = P[tri[f][0]], *q = P[tri[f][1]], *r = P[tri[f][2]];
+        const double u[3] = {q[0] - p[0], q[1] - p[1], q[2] - p[2]}, v[3] = {r[0] - p[0], r[1] - p[1], r[2] - p[2]};
+        a.n[f][0] = u[1] * v[2] - u[2] * v[1];
+        a.n[f][1] = u[2] * v[0] - u[0] * v[2];
+        a.n[f][2] = u[0] * v[1] - u[1] * v[0];
+        nrm[f] = sqrt(a.n[f][0] * a.n[f][0] + a.n[f][1] * a.n[f][1] + a.n[f][2] * a.n[f][2]);
+    }
+    for (int f = 0; f < 4; f++)
+        if (nrm[f] == 0.0) return false;
+    // isotropicstressstrain (src/elastic3d.f90:129-142) of the eigenstrain
+    float m[6];
+    const double epskk = (double)(a.e[0] + a.e[3] + a.e[5]);
+    const float mu2 = (float)(2.0 * a.mu);
+    for (int k = 0; k < 6; k++) m[k] = mu2 * a.e[k];
+    m[0] = (float)(m[0] + a.lambda * epskk);
+    m[3] = (float)(m[3] + a.lambda * epskk);
+    m[5] = (float)(m[5] + a.lambda * epskk);
+    for (int f = 0; f < 4; f++) {
+        for (int k = 0; k < 3; k++) a.n[f][k] = a.n[f][k] / nrm[f];
+        const double *p = P[tri[f][0]], *q = P[tri[f][1]], *r = P[tri[f][2]];
+        for (int k = 0; k < 3; k++) a.cen[f][k] = (p[k] + q[k] + r[k]) / 3;
+        const double *o = P[f];
+        const double dd = a.n[f][0] * (o[0] - a.cen[f][0]) + a.n[f][1] * (o[1] - a.cen[f][1]) +
+                          a.n[f][2] * (o[2] - a.cen[f][2]);
+        if (dd > 0)
+            for (int k = 0; k < 3; k++) a.n[f][k] = -a.n[f][k];
+        const double *n = a.n[f];
+        a.tr[f][0] = m[0] * n[0] + m[1] * n[1] + m[2] * n[2];
+        a.tr[f][1] = m[1] * n[0] + m[3] * n[1] + m[4] * n[2];
+        a.tr[f][2] = m[2] * n[0] + m[4] * n[1] + m[5] * n[2];
+    }
+    return true;
+}
+
 static int event_sources(relax_ctx *c, const EventCopy &ev, bool *any, bool *full)
 {
     const Grid &g = c->g;
@@ -1288,9 +1383,48 @@ static int event_sources(relax_ctx *c, const EventCopy &ev, bool *any, bool *ful
             CKL();
         }
     }
+    // cuboid and tetrahedral eigenstrain (src/relax.f90:1154-1181): the
+    // cuboid's L = width, W = length, T = thickness, the global beta
+    for (const auto &q : ev.cub) {
+        EigArgs a = eig_args(c, q.e);
+        a.x = q.x; a.y = q.y; a.z = q.z; a.L = q.width; a.W = q.length; a.T = q.thickness;
+        a.strike = q.strike; a.dip = q.dip;
+        k_source_cuboid<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
+    }
+    for (const auto &q : ev.tet) {
+        EigArgs a = eig_args(c, q.e);
+        const double *V = ev.vert.data();
+        if (!tet_setup(a, V + 3 * (q.i1 - 1), V + 3 * (q.i2 - 1), V + 3 * (q.i3 - 1), V + 3 * (q.i4 - 1))) continue;
+        k_source_tetra<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
+    }
     for (const auto &s : ev.s) {
         SrcArgs a = args(s);
         k_moment_shear<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
+    }
+    // their moment densities into tau (src/relax.f90:1208-1224)
+    for (const auto &q : ev.cub) {
+        EigArgs a = eig_args(c, q.e);
+        a.x = q.x; a.y = q.y; a.z = q.z; a.L = q.width; a.W = q.length; a.T = q.thickness;
+        a.strike = q.strike; a.dip = q.dip;
+        const double cs = cos(q.strike), ss = sin(q.strike), cd = cos(q.dip), sd = sin(q.dip);
+        const double n[3] = {+cd * cs, -cd * ss, -sd}, sv[3] = {-ss, -cs, 0}, d[3] = {+cs * sd, -ss * sd, +cd};
+        sdyad6(sv, sv, a.sdy[0]);
+        sdyad6(n, sv, a.sdy[1]);
+        sdyad6(sv, d, a.sdy[2]);
+        sdyad6(n, n, a.sdy[3]);
+        sdyad6(n, d, a.sdy[4]);
+        sdyad6(d, d, a.sdy[5]);
+        k_moment_cuboid<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
+        CKL();
+    }
+    for (const auto &q : ev.tet) {
+        EigArgs a = eig_args(c, q.e);
+        const double *V = ev.vert.data();
+        if (!tet_setup(a, V + 3 * (q.i1 - 1), V + 3 * (q.i2 - 1), V + 3 * (q.i3 - 1), V + 3 * (q.i4 - 1))) continue;
+        k_moment_tetra<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
         CKL();
     }
     // tensile cracks: the opening, the global beta (src/relax.f90:1226-1260)
@@ -1319,7 +1453,8 @@ static int event_sources(relax_ctx *c, const EventCopy &ev, bool *any, bool *ful
         k_moment_mogi<<<nblocks(g.nh), RELAX_NTHREADS, 0, c->st>>>(a);
         CKL();
     }
-    *any = !ev.s.empty() || !ev.ts.empty() || !ev.m.empty() || !ev.l.empty();
+    *any = !ev.s.empty() || !ev.ts.empty() || !ev.m.empty() || !ev.l.empty() || !ev.cub.empty() ||
+           !ev.tet.empty();
     *full = !ev.ts.empty() || !ev.m.empty();
     return RELAX_OK;
 }
@@ -2418,8 +2553,8 @@ extern "C" int relax_set_precision(relax_ctx *c, int mode)
         return fail(RELAX_ERR_UNSUPPORTED, "the mixed-precision x3 pass needs a 128-deep box (sx3 = %d)", c->g.sx3);
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->st));
-    c->sp.mixed = mode;
-    c->sp.tc_err = c->err;
+    TRY(c->sp.set_mixed(mode, c->err, c->st));
+    CK(cudaStreamSynchronize(c->st));
     drop_graph(c);
     return RELAX_OK;
 }
@@ -2970,8 +3105,12 @@ extern "C" int relax_op_green_mixed(float *c1, float *c2, float *c3, float *t1, 
         return rc;
     }
     cudaMemsetAsync(err, 0, sizeof(int), st);
-    sp.mixed = 1;
-    sp.tc_err = err;
+    rc = sp.set_mixed(1, err, st);
+    if (rc != RELAX_OK) {
+        sp.release();
+        dfree(err);
+        return rc;
+    }
     XfArgs xa{};
     float *cs[3] = {c1, c2, c3}, *ts[3] = {t1, t2, t3};
     for (int k = 0; k < 3; k++) { xa.in[k] = cs[k]; xa.tin[k] = ts[k]; }

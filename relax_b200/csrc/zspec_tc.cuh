@@ -179,6 +179,7 @@ struct ZtcArgs {
     int ncol;         // sx2 * K1 columns
     int ntiles;       // ceil(ncol / 64)
     int *err;         // raised (1 << RELAX_ERR_CUDA) when a wait on the tensor cores times out
+    const uint4 *tab; // k_ztc_tables: the DFT-64 matrix (hi, lo) in operand layout, then W128^n
 };
 
 constexpr int ZT_COLS = 64;
@@ -190,8 +191,41 @@ constexpr uint32_t ZT_OP = 65536;                    // operand buffers [2][hi, 
 constexpr uint32_t ZT_TW = ZT_OP + 4 * 32768;        // W128^n, n < 128 (float2)
 constexpr uint32_t ZT_RED = ZT_TW + 128 * 8;         // FP32 partial sums [4 parts][12][64 columns]
 constexpr uint32_t ZT_CC = ZT_RED + 4 * 12 * 64 * 4; // per-column coefficients [14][64]
-constexpr uint32_t ZT_BAR = ZT_CC + 14 * 64 * 4;     // 2 mbarriers, TMEM base
+constexpr uint32_t ZT_COLC = ZT_CC + 14 * 64 * 4;   // per-column FP64 constants [12][64]
+constexpr uint32_t ZT_BAR = ZT_COLC + 12 * 64 * 8;   // 2 mbarriers, TMEM base
 constexpr uint32_t ZT_SMEM = ZT_BAR + 64;
+constexpr uint32_t ZT_TAB_BYTES = 65536 + 128 * 8;   // the table k_ztc_tables writes
+
+// The constant operands of k_zspec_tc, computed once per device buffer: the
+// BF16 hi / lo parts of the DFT-64 matrix B[nn][kq] (nn = 2k + ro: output k,
+// Re / Im; kq = 2n + ri: input n, Re / Im; e^{-i 2 pi n k / 64}) in the
+// kernel's shared-memory operand layout, followed by W128^n, n < 128.
+__global__ void k_ztc_tables(uint4 *tab)
+{
+    unsigned char *dst = reinterpret_cast<unsigned char *>(tab);
+    const int ch = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ch < 128 * 16) {
+        const int nn = ch >> 4, kb = ch & 15;
+        const int k = nn >> 1, ro = nn & 1;
+        uint32_t hv[4], lv[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int n = kb * 4 + e;
+            double sn, cs;
+            sincospi((double)((n * k) & 63) / 32.0, &sn, &cs);
+            const float w0 = ro == 0 ? (float)cs : (float)(-sn), w1 = ro == 0 ? (float)sn : (float)cs;
+            tc::split2(w0, w1, hv[e], lv[e]);
+        }
+        const uint32_t o = tc::opoff(nn, kb);
+        *reinterpret_cast<uint4 *>(dst + o) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+        *reinterpret_cast<uint4 *>(dst + 32768 + o) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+    }
+    if (ch < 128) {
+        double sn, cs;
+        sincospi(-(double)ch / 64.0, &sn, &cs);           // W128^n = e^{-2 pi i n / 128}
+        reinterpret_cast<float2 *>(dst + 65536)[ch] = make_float2((float)cs, (float)sn);
+    }
+}
 
 __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constant__ ZtcArgs t)
 {
@@ -205,32 +239,12 @@ __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constan
     float2 *tw = reinterpret_cast<float2 *>(zsm + ZT_TW);
     float *red = reinterpret_cast<float *>(zsm + ZT_RED);
     float *ccs = reinterpret_cast<float *>(zsm + ZT_CC);
+    double *colc = reinterpret_cast<double *>(zsm + ZT_COLC);   // [12][64]
 
-    // ---- set-up: DFT-64 matrix (hi/lo), twiddles, barriers, tensor memory
-    // B[nn][kq], nn = 2k + ro (output k, Re/Im), kq = 2n + ri (input n, Re/Im):
-    // e^{-i theta} with theta = 2 pi n k / 64
-    for (int ch = tid; ch < 128 * 16; ch += ZT_THREADS) {
-        const int nn = ch >> 4, kb = ch & 15;
-        const int k = nn >> 1, ro = nn & 1;
-        uint32_t hv[4], lv[4];
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int n = kb * 4 + e;                       // input n of the pair (2n, 2n+1)
-            double s, c;
-            sincospi((double)((n * k) & 63) / 32.0, &s, &c);
-            // (Re in, Im in) weights of output Re (ro = 0) or Im (ro = 1)
-            const float w0 = ro == 0 ? (float)c : (float)(-s), w1 = ro == 0 ? (float)s : (float)c;
-            tc::split2(w0, w1, hv[e], lv[e]);
-        }
-        const uint32_t o = tc::opoff(nn, kb);
-        *reinterpret_cast<uint4 *>(zsm + ZT_BH + o) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
-        *reinterpret_cast<uint4 *>(zsm + ZT_BL + o) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
-    }
-    if (tid < 128) {
-        double s, c;
-        sincospi(-(double)tid / 64.0, &s, &c);              // W128^n = e^{-2 pi i n / 128}
-        tw[tid] = make_float2((float)c, (float)s);
-    }
+    // ---- set-up: DFT-64 matrix (hi/lo) and twiddles from the table,
+    // barriers, tensor memory
+    for (int q = tid; q < 4096; q += ZT_THREADS) reinterpret_cast<uint4 *>(zsm + ZT_BH)[q] = t.tab[q];
+    if (tid < 64) reinterpret_cast<uint4 *>(zsm + ZT_TW)[tid] = t.tab[4096 + tid];
     if (tid == 0) {
         tc::mbar_init(bar[0], 1);
         tc::mbar_init(bar[1], 1);
@@ -293,20 +307,58 @@ __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constan
     const int row = 32 * lq + lane, par = row >> 6, rcol = row & 63;
     const uint32_t trow = tmem + ((uint32_t)(32 * lq) << 16);
 
+    // the loader's share of a tile: one column, a quarter of the 64 planes
+    const int lcol = tid & 63, zq = tid >> 6;
+    float2 x[16];
+    auto load_tile = [&](int tl, int comp) {
+        const int q0 = tl * ZT_COLS, nq = min(ZT_COLS, t.ncol - q0);
+        const float2 *src = a.S + sidx(g, comp, 0, 0, 0) + q0 + lcol;
+#pragma unroll
+        for (int i = 0; i < 16; i++)
+            x[i] = lcol < nq ? src[(size_t)(16 * zq + i) * PS] : make_float2(0.f, 0.f);
+    };
+    if (blockIdx.x < t.ntiles) load_tile(blockIdx.x, 0);
+
 #pragma unroll 1
     for (int tile = blockIdx.x; tile < t.ntiles && !aborted; tile += gridDim.x) {
         const int p0 = tile * ZT_COLS;
         const int np = min(ZT_COLS, t.ncol - p0);
+        auto load = [&](int comp) { load_tile(tile, comp); };
+
+        // the columns' constants of the traction solve, ahead of their sums
+        // (src/green.f90:356-366, :578-609): wavenumbers, beta, 1/(2 mu
+        // beta^3), 1/(2 alpha mu beta^4 (1 + gamma/beta)), the surface traction
+        if (tid < 64) {
+            const int c = tid, pc = p0 + c;
+            double v[12];
+#pragma unroll
+            for (int q = 0; q < 12; q++) v[q] = 0.0;
+            if (c < np) {
+                const int ck2 = pc / g.K1, ck1 = pc % g.K1;
+                const double ck1v = (double)ck1 / (g.sx1 * g.dx1);
+                const double ck2v = (ck2 < g.sx2 / 2) ? (double)ck2 / (g.sx2 * g.dx2)
+                                                      : -(double)(g.sx2 - ck2) / (g.sx2 * g.dx2);
+                if (!(ck1v == 0.0 && ck2v == 0.0)) {
+                    const double PI2 = 6.28318530717958623199592693708837032318;
+                    const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
+                    const double beta = PI2 * sqrt(ck1v * ck1v + ck2v * ck2v);
+                    const double h = a.gam / beta;
+                    v[0] = ck1v; v[1] = ck2v; v[2] = beta;
+                    v[3] = 1.0 / (2.0 * a.mu * beta * beta * beta);
+                    v[4] = 1.0 / (2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h));
+                    for (int cp = 0; cp < 3; cp++) {
+                        const float2 tcv = a.S[sidx(g, cp, g.sx3, ck2, ck1)];
+                        v[5 + 2 * cp] = tcv.x;
+                        v[6 + 2 * cp] = tcv.y;
+                    }
+                    v[11] = 1.0;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 12; q++) colc[q * 64 + c] = v[q];
+        }
 
         // ---- forward products of the three components ----------------
-        const int lcol = tid & 63, zq = tid >> 6;           // loader: column, quarter of the planes
-        float2 x[16];
-        auto load = [&](int comp) {
-            const float2 *src = a.S + sidx(g, comp, 0, 0, 0) + p0 + lcol;
-#pragma unroll
-            for (int i = 0; i < 16; i++)
-                x[i] = lcol < np ? src[(size_t)(16 * zq + i) * PS] : make_float2(0.f, 0.f);
-        };
         auto build_fwd = [&](int buf) {
             unsigned char *hi = zsm + ZT_OP + buf * 65536, *lo = hi + 32768;
 #pragma unroll
@@ -328,8 +380,7 @@ __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constan
             }
             tc::fence_async_smem();
         };
-        load(0);
-        build_fwd(0);
+        build_fwd(0);                                       // comp 0 was loaded ahead
         __syncthreads();
         issue(0, 0, true);
         load(1);
@@ -407,16 +458,13 @@ __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constan
         // per-column FP64 combination (fixed order), surface traction, and the
         // Cerruti coefficients of k_zspec_sm (src/green.f90:356-366, :578-609)
         if (tid < 64) {
-            const int c = tid, pc = p0 + c;
+            const int c = tid;
             float cc[14];
 #pragma unroll
             for (int q = 0; q < 14; q++) cc[q] = 0.f;
-            if (c < np) {
-                const int ck2 = pc / g.K1, ck1 = pc % g.K1;
-                const double ck1v = (double)ck1 / (g.sx1 * g.dx1);
-                const double ck2v = (ck2 < g.sx2 / 2) ? (double)ck2 / (g.sx2 * g.dx2)
-                                                      : -(double)(g.sx2 - ck2) / (g.sx2 * g.dx2);
-                if (!(ck1v == 0.0 && ck2v == 0.0)) {
+            {
+                const double ck1v = colc[0 * 64 + c], ck2v = colc[1 * 64 + c];
+                if (colc[11 * 64 + c] != 0.0) {
                     const double PI2 = 6.28318530717958623199592693708837032318;
                     double s[12];
                     for (int q = 0; q < 12; q++) {
@@ -433,22 +481,15 @@ __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constan
                     const double a3i = modulus * s[5] + a.lambda * (ck1v * s[7] + ck2v * s[9]);
                     const double sum[6] = {-PI2 * a1i, PI2 * a1r, -PI2 * a2i, PI2 * a2r,
                                            -PI2 * a3i - grav * s[10], PI2 * a3r - grav * s[11]};
-                    const double d = 128.0 * g.dx3;
+                    const double id = 1.0 / (128.0 * g.dx3);
                     double p[6];
-                    for (int cp = 0; cp < 3; cp++) {
-                        const float2 tcv = a.S[sidx(g, cp, g.sx3, ck2, ck1)];
-                        p[2 * cp] = (double)tcv.x - sum[2 * cp] / d;
-                        p[2 * cp + 1] = (double)tcv.y - sum[2 * cp + 1] / d;
-                    }
-                    const double beta = PI2 * sqrt(ck1v * ck1v + ck2v * ck2v);
-                    const double h = a.gam / beta;
-                    const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
+                    for (int q = 0; q < 6; q++) p[q] = colc[(5 + q) * 64 + c] - sum[q] * id;
+                    const double beta = colc[2 * 64 + c], c0 = colc[3 * 64 + c], iden = colc[4 * 64 + c];
                     const double b1r = p[0] * c0, b1i = p[1] * c0, b2r = p[2] * c0, b2i = p[3] * c0;
                     const double qr = PI2 * ck1v * p[0] + PI2 * ck2v * p[2];
                     const double qi = PI2 * ck1v * p[1] + PI2 * ck2v * p[3];
-                    const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
-                    const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
-                    const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
+                    const double b3r = (beta * p[4] + (1.0 - alpha) * qi) * iden;
+                    const double b3i = (beta * p[5] - (1.0 - alpha) * qr) * iden;
                     const double Qr = b1r * ck1v + b2r * ck2v, Qi = b1i * ck1v + b2i * ck2v;
                     const double ab = alpha * beta * PI2, er = 1.0 - 1.0 / alpha, ab2 = -alpha * beta * beta;
                     const double ap = alpha * PI2 * PI2, bb = 2.0 * beta * beta;
@@ -474,6 +515,8 @@ __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constan
         __syncthreads();
 
         // ---- inverse operands (response + Cerruti), products, epilogues --
+        // the next tile's first component is read while this one finishes
+        if (tile + (int)gridDim.x < t.ntiles) load_tile(tile + gridDim.x, 0);
         float cc[14];
 #pragma unroll
         for (int q = 0; q < 14; q++) cc[q] = ccs[q * 64 + rcol];

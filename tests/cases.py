@@ -127,3 +127,21 @@ def loads_small(periodic=True, second_event=True, sx=64, sz=32):
         s.events.append(Event(1.0, [Fault(0.5, -5.0, 8.0, 0.0, 10.0, 5.0, 30.0, 60.0, 45.0)],
                               loads=[Load(2.0, 2.0, 8.0, 6.0, -0.25, period=1.5, phase=-0.4)]))
     return s
+
+
+def eigenstrain_small(sx=64, sz=32, tetra=True):
+    """Linear Maxwell below 6 km with coseismic eigenstrain sources
+    (--with-eigenstrain): a dipping cuboid with a full strain tensor, a
+    vertical one (the method of images, src/elastic3d.f90:1810-1826) and,
+    with --with-curvilinear, a tetrahedron of 4 listed vertices."""
+    from relax_b200.config import Cuboid, Tetrahedron
+    s = linear_small(sx, sz, steps=4)
+    s.name = "eigenstrain-small"
+    ev = s.events[0]
+    ev.faults = []
+    ev.cuboids = [Cuboid((1e-2, 4e-3, -3e-3, -5e-3, 2e-3, 6e-3), -6.0, 4.0, 3.0, 12.0, 6.0, 4.0, 30.0, 60.0),
+                  Cuboid((0.0, 8e-3, 0.0, 0.0, 0.0, 0.0), 6.0, -6.0, 0.0, 10.0, 5.0, 3.0, 0.0, 90.0)]
+    if tetra:
+        ev.vertices = [(8.0, 8.0, 2.0), (14.0, 8.0, 3.0), (9.0, 15.0, 2.5), (10.0, 10.0, 9.0)]
+        ev.tetrahedra = [Tetrahedron((5e-3, 0.0, 2e-3, -4e-3, 0.0, 1e-3), (1, 2, 3, 4))]
+    return s

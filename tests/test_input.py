@@ -13,7 +13,7 @@ from relax_b200 import _lib
 from relax_b200.api import Input
 from relax_b200.config import Event, Fault, Plane, Point, Tensile, relax_layer, relax_source
 
-from cases import linear_small, loads_small, powerlaw_small, sources_small, transient_small, two_events
+from cases import eigenstrain_small, linear_small, loads_small, powerlaw_small, sources_small, transient_small, two_events
 
 
 def _src_eq(a, b, what):
@@ -51,6 +51,21 @@ def compare(got, want, nz):
             assert gn == n, (e, kind)
             for k in range(n):
                 _src_eq(getattr(ge, kind)[k], getattr(we, kind)[k], (e, kind, k))
+        # eigenstrain sources: cuboids (weak-zone geometry), tetrahedra, vertices
+        assert (ge.nc, ge.ntet, ge.nvert) == (we.nc, we.ntet, we.nvert), e
+        for k in range(we.nc):
+            for f, _ in ge.c[k]._fields_:
+                if f == "e":
+                    assert tuple(getattr(ge.c[k].e, n) for n, _ in ge.c[k].e._fields_) == \
+                        tuple(getattr(we.c[k].e, n) for n, _ in we.c[k].e._fields_), (e, k)
+                else:
+                    assert getattr(ge.c[k], f) == getattr(we.c[k], f), (e, k, f)
+        for k in range(we.ntet):
+            assert (ge.tet[k].i1, ge.tet[k].i2, ge.tet[k].i3, ge.tet[k].i4) == \
+                (we.tet[k].i1, we.tet[k].i2, we.tet[k].i3, we.tet[k].i4)
+            assert ge.tet[k].e.s13 == we.tet[k].e.s13
+        for k in range(3 * we.nvert):
+            assert ge.vert[k] == we.vert[k]
     for kind, n in (("s", want.inter.ns), ("ts", want.inter.nt)):
         assert (got.inter.ns if kind == "s" else got.inter.nt) == n
         for k in range(n):
@@ -62,6 +77,12 @@ def _rotated(sim):
     s.x0, s.y0, s.rot = 3.5, -2.25, 17.0
     s.events[0].faults[0].beta = 0.3
     s.events[0].points = [Point(0.2, 4.0, -3.0, 6.0)]
+    return s
+
+
+def _eigen_rotated():
+    s = eigenstrain_small(tetra=False)
+    s.x0, s.y0, s.rot = 2.0, -1.0, 35.0
     return s
 
 
@@ -80,6 +101,8 @@ CASES = {
     "rotated-origin": lambda: _rotated(None),
     "surface-loads": lambda: loads_small(),
     "surface-loads-rotated": lambda: _loads_rotated(),
+    "eigenstrain": lambda: eigenstrain_small(),
+    "eigenstrain-rotated": lambda: _eigen_rotated(),
 }
 
 
@@ -87,7 +110,8 @@ CASES = {
 def test_deck_reads_back_to_the_same_config(name):
     sim = CASES[name]()
     transient = bool(sim.ltransient or sim.nltransient)
-    inp = Input.parse(sim.to_input(), transient=transient)
+    inp = Input.parse(sim.to_input(), transient=transient, eigenstrain=sim.has_eigenstrain(),
+                      curvilinear=any(ev.tetrahedra for ev in sim.events))
     want, _keep = sim.to_c(_lib.structure_fn)
     compare(inp.config, want, sim.sx3h)
 
@@ -178,13 +202,27 @@ def test_event_times_must_increase():
         Input.parse(_deck(lines))
 
 
-def test_cuboids_are_rejected():
+def test_cuboid_records_and_tetrahedron_vertex_checks():
+    """A cuboid record (src/input.f90:1510-1558): the strain as REAL*4, the
+    geometry through wangconvention; a tetrahedron naming a vertex beyond
+    the list is an input error."""
     lines = list(BASE)
     lines.insert(-1, "1")
-    lines.insert(-1, "1 1 0 0 0 0 0 0 0 0 5 5 5 0 90")
+    lines.insert(-1, "1 1e-3 0 0 0 0 0 0 0 2 5 5 5 0 90")
+    inp = Input.parse(_deck(lines), eigenstrain=True)
+    ev = inp.config.events[0]
+    assert ev.nc == 1 and ev.c[0].e.s11 == pytest.approx(1e-3) and ev.c[0].thickness == 5.0
+    assert ev.c[0].dip == 0.0                      # 90 - 90 after the convention
+    bad = list(BASE)
+    bad.insert(-1, "0")                            # no cuboids
+    bad.insert(-1, "1")                            # one tetrahedron
+    bad.insert(-1, "1 1e-3 0 0 0 0 0 1 2 3 5")
+    bad.insert(-1, "4")
+    for k in range(4):
+        bad.insert(-1, f"{k + 1} {k} 0 1")
     with pytest.raises(_lib.RelaxError) as e:
-        Input.parse(_deck(lines), eigenstrain=True)
-    assert e.value.code == 4
+        Input.parse(_deck(bad), eigenstrain=True, curvilinear=True)
+    assert e.value.code == 1
 
 
 def test_weak_zones_in_internal_convention():
