@@ -326,8 +326,10 @@ int relax_segment_stress(relax_ctx *ctx, int n, const relax_segment *sop,
 /* of points, dilatation sources and loads), is read into a           */
 /* relax_config ready for relax_create.  Errors (index misfits,       */
 /* negative rates, missing values) return RELAX_ERR_ARG with the line */
-/* number in relax_last_error.  Cuboid and tetrahedral eigenstrain    */
-/* sources are read and rejected (RELAX_ERR_UNSUPPORTED).             */
+/* number in relax_last_error.  Cuboid eigenstrain sources (flag      */
+/* RELAX_INPUT_EIGENSTRAIN) and tetrahedral ones (with                */
+/* RELAX_INPUT_CURVILINEAR) are read into the events' nc/c and        */
+/* ntet/tet/nvert/vert.                                               */
 /* ------------------------------------------------------------------ */
 typedef struct relax_input relax_input;
 

@@ -56,6 +56,7 @@ def load(precision: int = 32) -> C.CDLL:
         "orc_source": (None, [D, D, D, D, D, D, D, D, D, D, D, I, I, I, D, D, D, P, P, P, P, P, P]),
         "orc_momentdensityshear": (None, [D, D, D, D, D, D, D, D, D, D, D, I, I, I, D, D, D, P]),
         "orc_okada": (None, [D] * 15 + [C.POINTER(D)]),
+        "orc_okada_dc3d": (None, [D] * 15 + [C.POINTER(D)]),
         "orc_cuboidsource": (None, [D, D, P] + [D] * 9 + [I, I, I, D, D, D, P, P, P]),
         "orc_momentdensitycuboid": (None, [D, D, P] + [D] * 9 + [I, I, I, D, D, D, P]),
         "orc_tetrahedronsource": (None, [D, D, P, P, P, P, P, I, I, I, D, D, D, P, P, P]),

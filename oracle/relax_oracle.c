@@ -1776,6 +1776,271 @@ static void integrationstep(double tm, double *Dt, double t, int oi, double odt,
 }
 
 /* ------------------------------------------------------------------ */
+/* DC3D of Okada (1992), src/okada/dc3d.f (displacement rows only), as */
+/* src/okada/green_space.f90:14-89 (okada) calls it: REAL*4 arguments, */
+/* REAL*8 arithmetic inside, REAL*4 results.  A second restatement of  */
+/* the half-space solution, from the reference's own routine, that     */
+/* checks the oracle's orc_okada and the library's okada.cuh.          */
+/* ------------------------------------------------------------------ */
+typedef struct dc3d_c0 { double alp1, alp2, alp3, alp4, alp5, sd, cd, sdsd, cdcd, sdcd; } dc3d_c0;
+typedef struct dc3d_c2 { double xi2, et2, q2, r, r2, r3, r5, y, d, tt, alx, ale, x11, y11, x32, y32; } dc3d_c2;
+
+/* DCCON0, dc3d.f:509-545 */
+static void dc3d_con0(double alpha, double dip, dc3d_c0 *c)
+{
+    const double pi2 = 6.283185307179586;
+    c->alp1 = (1.0 - alpha) / 2.0;
+    c->alp2 = alpha / 2.0;
+    c->alp3 = (1.0 - alpha) / alpha;
+    c->alp4 = 1.0 - alpha;
+    c->alp5 = alpha;
+    const double p18 = pi2 / 360.0;
+    c->sd = sin(dip * p18);
+    c->cd = cos(dip * p18);
+    if (fabs(c->cd) < 1e-6) {
+        c->cd = 0.0;
+        if (c->sd > 0.0) c->sd = 1.0;
+        if (c->sd < 0.0) c->sd = -1.0;
+    }
+    c->sdsd = c->sd * c->sd;
+    c->cdcd = c->cd * c->cd;
+    c->sdcd = c->sd * c->cd;
+}
+
+/* DCCON2, dc3d.f:596-665 (the quantities the displacement rows read) */
+static void dc3d_con2(double xi, double et, double q, double sd, double cd, int kxi, int ket, dc3d_c2 *c)
+{
+    if (fabs(xi) < 1e-6) xi = 0.0;
+    if (fabs(et) < 1e-6) et = 0.0;
+    if (fabs(q) < 1e-6) q = 0.0;
+    c->xi2 = xi * xi;
+    c->et2 = et * et;
+    c->q2 = q * q;
+    c->r2 = c->xi2 + c->et2 + c->q2;
+    c->r = sqrt(c->r2);
+    if (c->r == 0.0) return;
+    c->r3 = c->r * c->r2;
+    c->r5 = c->r3 * c->r2;
+    c->y = et * cd + q * sd;
+    c->d = et * sd - q * cd;
+    c->tt = (q == 0.0) ? 0.0 : atan(xi * et / (q * c->r));
+    if (kxi == 1) {
+        c->alx = -log(c->r - xi);
+        c->x11 = 0.0;
+        c->x32 = 0.0;
+    } else {
+        const double rxi = c->r + xi;
+        c->alx = log(rxi);
+        c->x11 = 1.0 / (c->r * rxi);
+        c->x32 = (c->r + rxi) * c->x11 * c->x11 / c->r;
+    }
+    if (ket == 1) {
+        c->ale = -log(c->r - et);
+        c->y11 = 0.0;
+        c->y32 = 0.0;
+    } else {
+        const double ret = c->r + et;
+        c->ale = log(ret);
+        c->y11 = 1.0 / (c->r * ret);
+        c->y32 = (c->r + ret) * c->y11 * c->y11 / c->r;
+    }
+}
+
+/* UA, UB, UC, dc3d.f:200-508: the displacement rows u(1..3) */
+static void dc3d_ua(double xi, double et, double q, const double disl[3], const dc3d_c0 *k, const dc3d_c2 *c,
+                    double u[3])
+{
+    const double pi2 = 6.283185307179586;
+    const double qx = q * c->x11, qy = q * c->y11;
+    double du[3];
+    u[0] = u[1] = u[2] = 0.0;
+    if (disl[0] != 0.0) {
+        du[0] = c->tt / 2.0 + k->alp2 * xi * qy;
+        du[1] = k->alp2 * q / c->r;
+        du[2] = k->alp1 * c->ale - k->alp2 * q * qy;
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[0] / pi2 * du[i];
+    }
+    if (disl[1] != 0.0) {
+        du[0] = k->alp2 * q / c->r;
+        du[1] = c->tt / 2.0 + k->alp2 * et * qx;
+        du[2] = k->alp1 * c->alx - k->alp2 * q * qx;
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[1] / pi2 * du[i];
+    }
+    if (disl[2] != 0.0) {
+        du[0] = -k->alp1 * c->ale - k->alp2 * q * qy;
+        du[1] = -k->alp1 * c->alx - k->alp2 * q * qx;
+        du[2] = c->tt / 2.0 - k->alp2 * (et * qx + xi * qy);
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[2] / pi2 * du[i];
+    }
+}
+
+static void dc3d_ub(double xi, double et, double q, const double disl[3], const dc3d_c0 *k, const dc3d_c2 *c,
+                    double u[3])
+{
+    const double pi2 = 6.283185307179586;
+    const double rd = c->r + c->d, sd = k->sd, cd = k->cd;
+    double ai3, ai4;
+    if (cd != 0.0) {
+        if (xi == 0.0) {
+            ai4 = 0.0;
+        } else {
+            const double x = sqrt(c->xi2 + c->q2);
+            ai4 = 1.0 / k->cdcd *
+                  (xi / rd * k->sdcd + 2.0 * atan((et * (x + q * cd) + x * (c->r + x) * sd) / (xi * (c->r + x) * cd)));
+        }
+        ai3 = (c->y * cd / rd - c->ale + sd * log(rd)) / k->cdcd;
+    } else {
+        const double rd2 = rd * rd;
+        ai3 = (et / rd + c->y * q / rd2 - c->ale) / 2.0;
+        ai4 = xi * c->y / rd2 / 2.0;
+    }
+    const double ai1 = -xi / rd * cd - ai4 * sd;
+    const double ai2 = log(rd) + ai3 * sd;
+    const double qx = q * c->x11, qy = q * c->y11;
+    double du[3];
+    u[0] = u[1] = u[2] = 0.0;
+    if (disl[0] != 0.0) {
+        du[0] = -xi * qy - c->tt - k->alp3 * ai1 * sd;
+        du[1] = -q / c->r + k->alp3 * c->y / rd * sd;
+        du[2] = q * qy - k->alp3 * ai2 * sd;
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[0] / pi2 * du[i];
+    }
+    if (disl[1] != 0.0) {
+        du[0] = -q / c->r + k->alp3 * ai3 * k->sdcd;
+        du[1] = -et * qx - c->tt - k->alp3 * xi / rd * k->sdcd;
+        du[2] = q * qx + k->alp3 * ai4 * k->sdcd;
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[1] / pi2 * du[i];
+    }
+    if (disl[2] != 0.0) {
+        du[0] = q * qy - k->alp3 * ai3 * k->sdsd;
+        du[1] = q * qx + k->alp3 * xi / rd * k->sdsd;
+        du[2] = et * qx + xi * qy - c->tt - k->alp3 * ai4 * k->sdsd;
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[2] / pi2 * du[i];
+    }
+}
+
+static void dc3d_uc(double xi, double et, double q, double z, const double disl[3], const dc3d_c0 *k,
+                    const dc3d_c2 *c, double u[3])
+{
+    const double pi2 = 6.283185307179586;
+    const double sd = k->sd, cd = k->cd;
+    const double cc = c->d + z;
+    const double h = q * cd - z;
+    const double z32 = sd / c->r3 - h * c->y32;
+    const double xy = xi * c->y11, qy = q * c->y11;
+    double du[3];
+    u[0] = u[1] = u[2] = 0.0;
+    if (disl[0] != 0.0) {
+        du[0] = k->alp4 * xy * cd - k->alp5 * xi * q * z32;
+        du[1] = k->alp4 * (cd / c->r + 2.0 * qy * sd) - k->alp5 * cc * q / c->r3;
+        du[2] = k->alp4 * qy * cd - k->alp5 * (cc * et / c->r3 - z * c->y11 + c->xi2 * z32);
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[0] / pi2 * du[i];
+    }
+    if (disl[1] != 0.0) {
+        du[0] = k->alp4 * cd / c->r - qy * sd - k->alp5 * cc * q / c->r3;
+        du[1] = k->alp4 * c->y * c->x11 - k->alp5 * cc * et * q * c->x32;
+        du[2] = -c->d * c->x11 - xy * sd - k->alp5 * cc * (c->x11 - c->q2 * c->x32);
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[1] / pi2 * du[i];
+    }
+    if (disl[2] != 0.0) {
+        du[0] = -k->alp4 * (sd / c->r + qy * cd) - k->alp5 * (z * c->y11 - c->q2 * z32);
+        du[1] = k->alp4 * 2.0 * xy * sd + c->d * c->x11 - k->alp5 * cc * (c->x11 - c->q2 * c->x32);
+        du[2] = k->alp4 * (c->y * c->x11 + xy * cd) + k->alp5 * q * (cc * et * c->x32 + xi * z32);
+        for (int i = 0; i < 3; i++) u[i] = u[i] + disl[2] / pi2 * du[i];
+    }
+}
+
+/* DC3D, dc3d.f:1-199 (displacement only); float arguments as the routine
+ * declares them.  Returns 0, or 1 for a point on a fault edge (zero). */
+static int dc3d_disp(float alpha, float x, float y, float z, float depth, float dip, float al1, float al2, float aw1,
+                     float aw2, float disl1, float disl2, float disl3, float out[3])
+{
+    const double eps = 1e-6;
+    dc3d_c0 k;
+    dc3d_c2 c;
+    memset(&c, 0, sizeof c);
+    double u[3] = {0, 0, 0};
+    dc3d_con0(alpha, dip, &k);
+    const double zz = z, dd[3] = {disl1, disl2, disl3};
+    double xi[2] = {(double)x - al1, (double)x - al2};
+    for (int j = 0; j < 2; j++)
+        if (fabs(xi[j]) < eps) xi[j] = 0.0;
+    for (int part = 0; part < 2; part++) {
+        /* part 0: the real source at d = depth + z; part 1: the image at depth - z */
+        const double d = part == 0 ? (double)depth + z : (double)depth - z;
+        const double p = y * k.cd + d * k.sd;
+        double q = y * k.sd - d * k.cd;
+        double et[2] = {p - aw1, p - aw2};
+        if (fabs(q) < eps) q = 0.0;
+        for (int j = 0; j < 2; j++)
+            if (fabs(et[j]) < eps) et[j] = 0.0;
+        if (q == 0.0 && ((xi[0] * xi[1] <= 0.0 && et[0] * et[1] == 0.0) ||
+                         (et[0] * et[1] <= 0.0 && xi[0] * xi[1] == 0.0))) {
+            out[0] = out[1] = out[2] = 0.0f;
+            return 1;
+        }
+        int kxi[2] = {0, 0}, ket[2] = {0, 0};
+        const double r12 = sqrt(xi[0] * xi[0] + et[1] * et[1] + q * q);
+        const double r21 = sqrt(xi[1] * xi[1] + et[0] * et[0] + q * q);
+        const double r22 = sqrt(xi[1] * xi[1] + et[1] * et[1] + q * q);
+        if (xi[0] < 0.0 && r21 + xi[1] < eps) kxi[0] = 1;
+        if (xi[0] < 0.0 && r22 + xi[1] < eps) kxi[1] = 1;
+        if (et[0] < 0.0 && r12 + et[1] < eps) ket[0] = 1;
+        if (et[0] < 0.0 && r22 + et[1] < eps) ket[1] = 1;
+        for (int kk = 0; kk < 2; kk++) {
+            for (int j = 0; j < 2; j++) {
+                /* the loop indices as DC3D passes them: KXI(K), KET(J) */
+                dc3d_con2(xi[j], et[kk], q, k.sd, k.cd, kxi[kk], ket[j], &c);
+                double xj = fabs(xi[j]) < eps ? 0.0 : xi[j], ek = fabs(et[kk]) < eps ? 0.0 : et[kk];
+                double du[3], ua[3];
+                dc3d_ua(xj, ek, q, dd, &k, &c, ua);
+                if (part == 0) {
+                    du[0] = -ua[0];
+                    du[1] = -ua[1] * k.cd + ua[2] * k.sd;
+                    du[2] = -ua[1] * k.sd - ua[2] * k.cd;
+                } else {
+                    double ub[3], uc[3];
+                    dc3d_ub(xj, ek, q, dd, &k, &c, ub);
+                    dc3d_uc(xj, ek, q, zz, dd, &k, &c, uc);
+                    du[0] = ua[0] + ub[0] + z * uc[0];
+                    du[1] = (ua[1] + ub[1] + z * uc[1]) * k.cd - (ua[2] + ub[2] + z * uc[2]) * k.sd;
+                    du[2] = (ua[1] + ub[1] - z * uc[1]) * k.sd + (ua[2] + ub[2] - z * uc[2]) * k.cd;
+                }
+                for (int i = 0; i < 3; i++) u[i] = (j + kk != 1) ? u[i] + du[i] : u[i] - du[i];
+            }
+        }
+    }
+    for (int i = 0; i < 3; i++) out[i] = (float)u[i];
+    return 0;
+}
+
+/* okada, src/okada/green_space.f90:14-89: a source in RELAX's input
+ * convention (degrees; x3 the depth of the top edge's reference point)
+ * at a receiver (xrec, yrec, zrec >= 0 depth) */
+void orc_okada_dc3d(double lambda, double mu, double slip, double opening, double x1, double x2, double x3,
+                    double width, double length, double strike, double dipd, double rake, double xrec, double yrec,
+                    double zrec, double *disp)
+{
+    const double degtorad = (double)1.745329252E-02f;        /* a default-real literal */
+    const float alpha = (float)((lambda + mu) / (lambda + 2.0 * mu));
+    const float z = (float)(-zrec);
+    disp[0] = disp[1] = disp[2] = 0.0;
+    const double st = strike * degtorad, csst = cos(st), ssst = sin(st);
+    const double ra = rake * degtorad, csra = cos(ra), ssra = sin(ra);
+    const float x = (float)((xrec - x1) * csst + (yrec - x2) * ssst);
+    const float y = (float)((xrec - x1) * ssst - (yrec - x2) * csst);
+    float u[3];
+    const int iret = dc3d_disp(alpha, x, y, z, (float)x3, (float)dipd, 0.0f, (float)length, -(float)width, 0.0f,
+                               (float)(slip * csra), (float)(slip * ssra), (float)opening, u);
+    if (iret == 0) {
+        disp[0] = disp[0] + (double)u[0] * csst + (double)u[1] * ssst;
+        disp[1] = disp[1] + (double)u[0] * ssst - (double)u[1] * csst;
+        disp[2] = disp[2] - (double)u[2];
+    }
+    (void)mu;
+}
+
+/* ------------------------------------------------------------------ */
 /* eigenstrain sources (--with-eigenstrain, --with-curvilinear)        */
 /* ------------------------------------------------------------------ */
 
