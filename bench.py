@@ -224,6 +224,17 @@ def accuracy_vs_fp64(sim, nsteps: int, device: int, mixed: bool):
     return out
 
 
+def max_over_ranks(v: float, dist=None, device: str = "cpu") -> float:
+    """The largest value over the ranks of the process group (every rank
+    takes the same collective step); v itself without a group."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args, rank, world):
     sim = workload()
     if rank != 0:
@@ -272,11 +283,7 @@ def run_gpu(args, rank, world, local_rank):
         torch.cuda.synchronize()
 
     def allmax(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(v, dist, "cuda")
 
     import ctypes as C
 
