@@ -2486,7 +2486,7 @@ int orc_coseismic(orc_state *S, relax_step_log *log)
     if (err) return err;
     orc_traction(c->mu, &c->events[0], S->sx1, S->sx2, c->dx1, c->dx2, 0.0, 0.0, S->t[2], 0);
     const relax_event *ev = &c->events[0];
-    if (ev->nt || ev->ns || ev->nm || ev->nl) {
+    if (ev->nt || ev->ns || ev->nm || ev->nl || ev->nc || ev->ntet) {   /* src/relax.f90:344-350 */
         if ((err = green(S))) return err;
         /* dislocations_disp: the sources smaller than the Nyquist length
          * (src/relax.f90:355-360, :1320-1347) */

@@ -17,10 +17,11 @@ The logs come from older builds of the reference than its current source:
   The current source builds the zone with beta = 0 (src/relax.f90:487),
   which gives the full 1 at that edge and tm(ve) = 0.5.  The test runs
   both: the log with the zone built at beta = 0.2 (Dt, tm(ve) and t then
-  agree with every line to 0.05 %, C:E^i to 0.7 %), and the current
-  source's field, whose tm(ve) must be exactly 0.5.  The log's power (the
-  amplitude of the moment-density rate) decays 0.08 % per step faster than
-  here (0.14 % apart at step 1, 2.4 % at step 30): bound RTOL4_POWER.
+  agree with every line to 0.05 %), and the current source's field, whose
+  tm(ve) must be exactly 0.5.  The log's power (the amplitude of the
+  moment-density rate) decays 0.08 % per step faster than here (0.14 %
+  apart at step 1, 2.4 % at step 30) and its C:E^i grows 0.02 % per step
+  slower (0.6 % apart at step 30): bounds RTOL4_POWER and RTOL4_CEI.
 * output2 (an MKL build) differs from step 1 by 0.2 % in Dt and tm(pl) (a
   minimum over the grid of 1/gammadot, i.e. of the peak stress; the FP32
   and FP64 oracles agree with the GPU there to 1e-5).  With the adaptive
@@ -50,6 +51,7 @@ RTOL = 5e-3
 RTOL2_EARLY = 3e-3
 RTOL2 = 2.5e-2
 RTOL4_POWER = 3e-2
+RTOL4_CEI = 1e-2
 
 
 def _close(ours, ref, rtol):
@@ -131,7 +133,7 @@ def test_gpu_reproduces_output4_with_the_logs_weak_zone_smoothing():
     cfg.lineardgammadot0 = field.ctypes.data_as(C.POINTER(C.c_float))
     with Relax(inp.simulation(), config=cfg, keep=(inp, field)) as r:
         logs = _run(r, len(ref) - 1)
-    _compare("output4", logs, ref, None, lambda i, c: RTOL4_POWER if c == 6 else RTOL)
+    _compare("output4", logs, ref, None, lambda i, c: RTOL4_POWER if c == 6 else RTOL4_CEI if c == 7 else RTOL)
 
 
 def test_output4_current_source_weak_zone():
