@@ -299,6 +299,16 @@ int orc_tensor_structure(const relax_tensor_layer *layers, int nv, double dx3, i
 static const float FIR7[7] = {8.77856e-01f, -2.81913e-01f, +6.22696e-02f, +2.82441e-02f,
                               -5.09029e-02f, +4.20471e-02f, -1.59409e-02f};
 
+/* The periodic neighbour index.  The reference's mod(sx+i-1-l,sx)+1 keeps
+ * the dividend's sign (Fortran MOD), so for a 7-point filter on an axis of
+ * 5 or 6 samples it indexes outside the axis (i - 1 - l < -sx); here the
+ * index wraps, which is the periodic neighbour the filter means. */
+static inline int pmod(int a, int n)
+{
+    const int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
 static int optimalfilter(int sx1, int sx2, int sx3, double *k1, double *k2, double *k3,
                          int *l1, int *l2, int *l3)
 {
@@ -346,13 +356,13 @@ int orc_stressupdate(const real *v1, const real *v2, const real *v3, double lamb
                 otensor e = {0, 0, 0, 0, 0, 0};
 #define V(a, j1, j2, j3) (a)[IDX3((j1) - 1, (j2) - 1, (j3) - 1, n1, sx2)]
                 for (int l = 1; l <= len1; l++) {
-                    int i1m = (sx1 + i1 - 1 - l) % sx1 + 1, i1p = (i1 - 1 + l) % sx1 + 1;
+                    int i1m = pmod(sx1 + i1 - 1 - l, sx1) + 1, i1p = (i1 - 1 + l) % sx1 + 1;
                     e.s11 = (real)(e.s11 + (real)(V(v1, i1p, i2, i3) - V(v1, i1m, i2, i3)) * ker1[l - 1]);
                     e.s12 = (real)(e.s12 + (real)(V(v2, i1p, i2, i3) - V(v2, i1m, i2, i3)) * ker1[l - 1]);
                     e.s13 = (real)(e.s13 + (real)(V(v3, i1p, i2, i3) - V(v3, i1m, i2, i3)) * ker1[l - 1]);
                 }
                 for (int l = 1; l <= len2; l++) {
-                    int i2m = (sx2 + i2 - 1 - l) % sx2 + 1, i2p = (i2 - 1 + l) % sx2 + 1;
+                    int i2m = pmod(sx2 + i2 - 1 - l, sx2) + 1, i2p = (i2 - 1 + l) % sx2 + 1;
                     e.s12 = (real)(e.s12 + (real)(V(v1, i1, i2p, i3) - V(v1, i1, i2m, i3)) * ker2[l - 1]);
                     e.s22 = (real)(e.s22 + (real)(V(v2, i1, i2p, i3) - V(v2, i1, i2m, i3)) * ker2[l - 1]);
                     e.s23 = (real)(e.s23 + (real)(V(v3, i1, i2p, i3) - V(v3, i1, i2m, i3)) * ker2[l - 1]);
@@ -423,13 +433,13 @@ int orc_equivalentbodyforce(const otensor *sig, double dx1, double dx2, double d
             for (int i1 = 1; i1 <= sx1; i1++) {
                 double f1 = 0, f2 = 0, f3 = 0;
                 for (int l = 1; l <= len1; l++) {
-                    int i1m = (sx1 + i1 - 1 - l) % sx1 + 1, i1p = (i1 - 1 + l) % sx1 + 1;
+                    int i1m = pmod(sx1 + i1 - 1 - l, sx1) + 1, i1p = (i1 - 1 + l) % sx1 + 1;
                     f1 += (real)(S(i1p, i2, i3).s11 - S(i1m, i2, i3).s11) * ker1[l - 1];
                     f2 += (real)(S(i1p, i2, i3).s12 - S(i1m, i2, i3).s12) * ker1[l - 1];
                     f3 += (real)(S(i1p, i2, i3).s13 - S(i1m, i2, i3).s13) * ker1[l - 1];
                 }
                 for (int l = 1; l <= len2; l++) {
-                    int i2m = (sx2 + i2 - 1 - l) % sx2 + 1, i2p = (i2 - 1 + l) % sx2 + 1;
+                    int i2m = pmod(sx2 + i2 - 1 - l, sx2) + 1, i2p = (i2 - 1 + l) % sx2 + 1;
                     f1 += (real)(S(i1, i2p, i3).s12 - S(i1, i2m, i3).s12) * ker2[l - 1];
                     f2 += (real)(S(i1, i2p, i3).s22 - S(i1, i2m, i3).s22) * ker2[l - 1];
                     f3 += (real)(S(i1, i2p, i3).s23 - S(i1, i2m, i3).s23) * ker2[l - 1];

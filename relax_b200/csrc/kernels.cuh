@@ -69,6 +69,63 @@ __device__ __forceinline__ float4 ldc4(const float *p) { return *reinterpret_cas
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
 __device__ __forceinline__ float geti(const float4 &v, int j) { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
 
+// The derivative along x2.  optimalfilter (src/elastic3d.f90:846-907)
+// takes the central difference (w[i2+1] - w[i2-1]) / (2 dx2) for sx2 <= 4
+// and sx2 >= 15, and the 7-point FIR differentiator fir7 of
+// src/kernel7.inc for 5 <= sx2 <= 14: sum over l = 1..7 of
+// (w[i2+l] - w[i2-l]) fir7(l) / dx2, indexes periodic (localstrain_ani,
+// src/elastic3d.f90:1140-1178, and localdivergence_ani, :1431-1470).  n = 7
+// selects the filter, c[l-1] = fir7(l) / dx2; otherwise the central
+// difference runs.  Along x3, fir7 is selected for 5 <= sx3/2 <= 14, but
+// then every layer is a boundary layer of the filter ((i3 > 7) and
+// (i3 < sx3/2 - 6) is never true, stressupdate :975-976), so the finite
+// differences of localstrain_ani apply throughout; along x1 the grid needs
+// sx1 >= 16.
+struct FirY {
+    int n;
+    float c[7];
+};
+
+// sum_l (w[(i2+l) % sx2] - w[(i2-l) % sx2]) c[l-1] at 4 consecutive points
+// of rows of pitch sx1 (w points at x1 of the row i2 = 0 of the plane)
+__device__ __forceinline__ float4 fir_y4(const float *w, int i2, int sx2, int sx1, const FirY &f)
+{
+    float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int l = 1; l <= 7; l++) {
+        const float4 p = ld4(w + (size_t)((i2 + l) % sx2) * sx1);
+        const float4 m = ld4(w + (size_t)((i2 + 2 * sx2 - l) % sx2) * sx1);   // sx2 >= 5 > l / 2
+        d.x += (p.x - m.x) * f.c[l - 1];
+        d.y += (p.y - m.y) * f.c[l - 1];
+        d.z += (p.z - m.z) * f.c[l - 1];
+        d.w += (p.w - m.w) * f.c[l - 1];
+    }
+    return d;
+}
+
+// the x2 derivatives of the 3 components of w (3 x nh) by fir7, for
+// k_stress on grids of 5 <= sx2 <= 14 (the filter kept out of its registers)
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_fir_y(Grid g, const float *w, float *wy, FirY f)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 3 * (g.nh >> 2)) return;
+    const int c = (int)(q / (g.nh >> 2));
+    const size_t p = 4 * (q % (g.nh >> 2));
+    const int i1 = (int)(p % g.sx1), i2 = (int)((p / g.sx1) % g.sx2), i3 = (int)(p / g.plane);
+    const float4 d = fir_y4(w + c * g.nh + (size_t)i3 * g.plane + i1, i2, g.sx2, g.sx1, f);
+    *reinterpret_cast<float4 *>(wy + c * g.nh + p) = d;
+}
+
+__device__ __forceinline__ float fir_y1(const float *w, int i2, int sx2, int sx1, const FirY &f)
+{
+    float d = 0.f;
+#pragma unroll
+    for (int l = 1; l <= 7; l++)
+        d += (__ldg(w + (size_t)((i2 + l) % sx2) * sx1) - __ldg(w + (size_t)((i2 + 2 * sx2 - l) % sx2) * sx1)) *
+             f.c[l - 1];
+    return d;
+}
+
 // ------------------------------------------------------------------------
 // Fused stress / eigenstress kernel.
 //
@@ -103,6 +160,7 @@ struct StressArgs {
     const float *spdev;      // 6 x sx3h deviatoric prestress (or null)
     const StepState *st;
     float k1, k2, k3, k3b;   // 0.5/dx1, 0.5/dx2, 0.5/dx3, 1/dx3
+    const float *wy;         // FIRY: the x2 derivatives of w by fir7 (3 x nh, k_fir_y)
     float lam, mu2, muinv;   // lambda, 2 mu, 1/mu
     int store_sig;
     const unsigned char *sig_mask;   // store_sig: only groups of 4 points flagged here (null = all)
@@ -125,7 +183,9 @@ struct StressArgs {
 // minima), in CORR the predicted strain epsilonikdot = Dt/2 epsilonikdot +
 // epsilonik (:693-695), the corrector's calls on it (:764-787) and
 // epsilonik += Dt epsilonikdot (:789).
-template <int MODE, bool BATCH = false, bool TRANS = false>
+// FIRY: the x2 derivatives of w come from a.wy (k_fir_y, grids of the 7-point
+// x2 filter) instead of the central difference of rows i2 -+ 1.
+template <int MODE, bool BATCH = false, bool TRANS = false, bool FIRY = false>
 __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const __grid_constant__ StressArgs a0)
 {
     const StressArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
@@ -206,11 +266,16 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const 
                 dxw[c][1] = (cv.z - cv.x) * a.k1;
                 dxw[c][2] = (cv.w - cv.y) * a.k1;
                 dxw[c][3] = (rgt - cv.z) * a.k1;
-                const float4 ym = ld4(wc + rym), yp = ld4(wc + ryp);
-                dyw[c][0] = (yp.x - ym.x) * a.k2;
-                dyw[c][1] = (yp.y - ym.y) * a.k2;
-                dyw[c][2] = (yp.z - ym.z) * a.k2;
-                dyw[c][3] = (yp.w - ym.w) * a.k2;
+                if (FIRY) {
+                    const float4 d = ld4(a.wy + c * nh + idx);
+                    dyw[c][0] = d.x; dyw[c][1] = d.y; dyw[c][2] = d.z; dyw[c][3] = d.w;
+                } else {
+                    const float4 ym = ld4(wc + rym), yp = ld4(wc + ryp);
+                    dyw[c][0] = (yp.x - ym.x) * a.k2;
+                    dyw[c][1] = (yp.y - ym.y) * a.k2;
+                    dyw[c][2] = (yp.z - ym.z) * a.k2;
+                    dyw[c][3] = (yp.w - ym.w) * a.k2;
+                }
                 const float4 zm = ld4(wc + rzm), zp = ld4(wc + rzp);
                 dzw[c][0] = (zp.x - zm.x) * kz;
                 dzw[c][1] = (zp.y - zm.y) * kz;
@@ -1003,6 +1068,7 @@ struct XfArgs {
     int has_trac;            // blockIdx.y == nin is the traction plane
     const float *m;          // XIN_DIV: 6 x nh moment
     float k1, k2, k3, k3b;
+    FirY fy;                 // XIN_DIV: the x2 differentiator (n = 7: fir7, k_xfwd only)
     const float *in[3];      // XIN_REAL
     size_t rp, pp;           // row / plane pitch (elements)
     const float *tin[3];
@@ -1048,8 +1114,10 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xfwd(XfArgs a)
                     const float *mx = a.m + cx * g.nh + pl + rowo;
                     const float fx = (__ldg(mx + (i1 + 1) % g.sx1) - __ldg(mx + (i1 + g.sx1 - 1) % g.sx1)) * a.k1;
                     const float *my = a.m + cy * g.nh + pl + i1;
-                    const float fy = (__ldg(my + (size_t)((i2 + 1) % g.sx2) * g.sx1) -
-                                      __ldg(my + (size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1)) * a.k2;
+                    const float fy = a.fy.n == 7
+                                         ? fir_y1(my, i2, g.sx2, g.sx1, a.fy)
+                                         : (__ldg(my + (size_t)((i2 + 1) % g.sx2) * g.sx1) -
+                                            __ldg(my + (size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1)) * a.k2;
                     const float *mz = a.m + cz * g.nh + rowo + i1;
                     float fz;
                     if (i3 == 0) fz = (__ldg(mz + g.plane) - __ldg(mz)) * a.k3b;
@@ -1484,11 +1552,97 @@ __global__ void __launch_bounds__(CW *N2) k_ypass_reg(const __grid_constant__ YA
     (void)n;
 }
 
+// 8-byte asynchronous copy global -> shared (zero-filled when n = 0)
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, int n)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// pass 2 / 4, persistent form of k_ypass_reg: each block walks tiles of CW
+// columns (gridDim.x apart) and copies the next tile into the other half of
+// its shared memory (cp.async) while it transforms the current one, so the
+// loads of one tile overlap the butterflies of the previous.  A thread
+// transposes in place: it writes the rows N2 k1 + t it copied itself.
+template <int N1, int N2, int CW, int SIGN>
+__global__ void __launch_bounds__(CW *N2, 3) k_ypass_pst(const __grid_constant__ YArgs a)
+{
+    constexpr int n = N1 * N2, Q = N1 / N2;
+    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
+    extern __shared__ float2 smy[];   // [2][n][CW]
+    const Grid &g = a.g;
+    const int c = threadIdx.x % CW, t = threadIdx.x / CW;
+    const int np = a.nbody + a.traction;
+    const int ncol = 3 * np * g.K1;
+    const int ntiles = (ncol + CW - 1) / CW;
+    // column f = (cp np + pi) K1 + k1 of the flattened (component, plane, k1)
+    auto base_of = [&](int f) -> size_t {
+        const int cp = f / (np * g.K1), rem = f % (np * g.K1);
+        const int pi = rem / g.K1, k1c = rem % g.K1;
+        const int p = (a.traction && pi == a.nbody) ? g.sx3 : pi;
+        return sidx(g, cp, p, 0, k1c);
+    };
+    auto prefetch = [&](int tile, int buf) {
+        const int f = tile * CW + c;
+        const bool ok = f < ncol;
+        const size_t base = ok ? base_of(f) : 0;
+        float2 *B = smy + (size_t)buf * n * CW;
+#pragma unroll
+        for (int j1 = 0; j1 < N1; j1++) {
+            const int row = N2 * j1 + t;
+            cp_async8(B + row * CW + c, a.S + base + (size_t)row * g.K1, ok ? 8 : 0);
+        }
+        cp_async_commit();
+    };
+    int tile = blockIdx.x;
+    if (tile < ntiles) prefetch(tile, 0);
+    for (int it = 0; tile < ntiles; it++, tile += gridDim.x) {
+        const int buf = it & 1;
+        if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, buf ^ 1);
+        else cp_async_commit();   // an empty group: the wait below still leaves one
+        cp_async_wait<1>();
+        float2 *B = smy + (size_t)buf * n * CW;
+        const int f = tile * CW + c;
+        const bool ok = f < ncol;
+        float2 x[N1];
+#pragma unroll
+        for (int j1 = 0; j1 < N1; j1++) x[j1] = B[(N2 * j1 + t) * CW + c];
+        RDft<N1, SIGN>::run(x);
+#pragma unroll
+        for (int k1 = 1; k1 < N1; k1++)
+            if (t) x[k1] = cmul(x[k1], twn<SIGN>(a.py.tw, t * k1));
+#pragma unroll
+        for (int k1 = 0; k1 < N1; k1++) B[(k1 * N2 + t) * CW + c] = x[k1];
+        __syncthreads();
+        const size_t base = ok ? base_of(f) : 0;
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            float2 y[N2];
+            const int k1 = t + N2 * q;
+#pragma unroll
+            for (int jj = 0; jj < N2; jj++) y[jj] = B[(k1 * N2 + jj) * CW + c];
+            RDft<N2, SIGN>::run(y);
+            if (ok) {
+#pragma unroll
+                for (int k2 = 0; k2 < N2; k2++) a.S[base + (size_t)(k1 + N1 * k2) * g.K1] = y[k2];
+            }
+        }
+        __syncthreads();   // the buffer is refilled two tiles on
+    }
+    cp_async_wait<0>();
+    (void)n;
+}
+
 // pass 3, register/shared-memory version.  The three components of CW
 // columns stay in shared memory (U[cp][k1][j2][c]) between the phases, so a
 // thread holds one N1 or 3 x N2 group at a time.  PRUNED: input planes
 // [n/2, n) are zero and only output planes [0, n/2) are wanted (the step's
 // Green's functions); otherwise nin/nout are honoured.
+constexpr int ZCOL = 26;   // floats of per-column constants in k_zspec_sm
+
 template <int N1, int N2, int CW, bool PRUNED, bool BATCH = false>
 __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(const __grid_constant__ ZArgs a0)
 {
@@ -1498,7 +1652,9 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
     extern __shared__ float2 smz[];
     float2 *U = smz;                                                   // [3][N1][N2][CW]
     float *red = reinterpret_cast<float *>(smz + 3 * n * CW);          // [N2][12][CW]
-    float *colc = red + N2 * 12 * CW;                                  // [CW][17]
+    // per column, ZCOL floats: the Cerruti coefficients cc[14], the surface
+    // traction (6 floats), then beta, c0, 1/den as doubles (float offset 20)
+    float *colc = red + N2 * 12 * CW;                                  // [CW][ZCOL]
     const Grid &g = a.g;
     const int c = threadIdx.x % CW, t = threadIdx.x / CW;
     // columns (k1, k2) flattened over the plane: col = k2 K1 + k1
@@ -1520,6 +1676,32 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
             const bool ld = ok && (PRUNED || i3 < a.nin);
             x[cp][j1] = ld ? a.S[sidx(g, cp, i3, k2i, k1c)] : make_float2(0.f, 0.f);
         }
+    // while those loads are in flight, one thread per column reads the
+    // surface traction and forms the column's data-independent FP64
+    // constants of cerrutisolmodified (src/green.f90:578-609): beta =
+    // 2 pi |k|, c0 = 1/(2 mu beta^3), 1/den = 1/(2 alpha mu beta^4 (1 + gam/beta))
+    if (t == N2 - 1) {
+        float *cc = colc + c * ZCOL;
+        if (ok) {
+#pragma unroll
+            for (int cp = 0; cp < 3; cp++) {
+                const float2 tc = a.S[sidx(g, cp, g.sx3, k2i, k1c)];
+                cc[14 + 2 * cp] = tc.x;
+                cc[15 + 2 * cp] = tc.y;
+            }
+        }
+        double *cd = reinterpret_cast<double *>(cc + 20);
+        const double k1d = (double)k1c / (g.sx1 * g.dx1);
+        const double k2d = (k2i < g.sx2 / 2) ? (double)k2i / (g.sx2 * g.dx2) : -(double)(g.sx2 - k2i) / (g.sx2 * g.dx2);
+        if (ok && !(k1d == 0.0 && k2d == 0.0)) {
+            const double alpha = (a.lambda + a.mu) / (a.lambda + 2.0 * a.mu);
+            const double beta = PI2 * sqrt(k1d * k1d + k2d * k2d);
+            const double h = a.gam / beta;
+            cd[0] = beta;
+            cd[1] = 1.0 / (2.0 * a.mu * beta * beta * beta);
+            cd[2] = 1.0 / (2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h));
+        }
+    }
     {
         float2 tw[N1];   // W_n^(t k1), shared by the three components
 #pragma unroll
@@ -1545,6 +1727,7 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
     // B = ratio1 / r2^2 (src/green.f90:78-90 rearranged); surface traction
     // from the FP64 sums Sk_i = sum k3 u_i and S_i = sum u_i over k3
     const float ra = a.ratio1 * (1.f + a.ratio2);
+    const float il3f = (float)inv_l3;   // k3 = jw / (n dx3)
     // FP32 partial sums of jw u_i (k3 = jw / (n dx3)) and of u_i over this
     // thread's k3; the reference accumulates these in REAL*4 over all k3
     // (src/green.f90:365-367)
@@ -1563,8 +1746,8 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
         for (int k2 = 0; k2 < N2; k2++) {
             const int j = k1 + N1 * k2;
             const int jw = j < n / 2 ? j : j - n;
-            const double k3v = (double)jw * inv_l3;
-            const float k3f = (float)k3v;
+            const float w = (float)jw;
+            const float k3f = w * il3f;
             const float2 c1 = y[0][k2], c2 = y[1][k2], c3 = y[2][k2];
             const float r2 = k1f * k1f + k2f * k2f + k3f * k3f;
             float2 u1, u2, u3;
@@ -1582,7 +1765,6 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
             U[uidx(0, k1, k2)] = u1;
             U[uidx(1, k1, k2)] = u2;
             U[uidx(2, k1, k2)] = u3;
-            const float w = (float)jw;
             acc[0] += w * u1.x; acc[1] += w * u1.y; acc[2] += w * u2.x;
             acc[3] += w * u2.y; acc[4] += w * u3.x; acc[5] += w * u3.y;
             acc[6] += u1.x; acc[7] += u1.y; acc[8] += u2.x; acc[9] += u2.y; acc[10] += u3.x; acc[11] += u3.y;
@@ -1596,8 +1778,13 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
         for (int tt = 0; tt < N2; tt++)
             for (int qq = 0; qq < 12; qq++) s[qq] += (double)red[(tt * 12 + qq) * CW + c];
         for (int qq = 0; qq < 6; qq++) s[qq] *= inv_l3;
-        float *cc = colc + c * 17;
-        for (int qq = 0; qq < 16; qq++) cc[qq] = 0.f;
+        float *cc = colc + c * ZCOL;
+        const double *cd = reinterpret_cast<const double *>(cc + 20);
+        float tr[6];
+#pragma unroll
+        for (int qq = 0; qq < 6; qq++) tr[qq] = cc[14 + qq];
+#pragma unroll
+        for (int qq = 0; qq < 14; qq++) cc[qq] = 0.f;
         if (ok && !(k1v == 0.0 && k2v == 0.0)) {
             // surfacetractioncowling (src/green.f90:356-366): i 2pi (...) - grav u3
             const double modulus = a.lambda + 2.0 * a.mu;
@@ -1608,25 +1795,20 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
             const double a3i = modulus * s[5] + a.lambda * (k1v * s[7] + k2v * s[9]);
             const double sum[6] = {-PI2 * a1i, PI2 * a1r, -PI2 * a2i, PI2 * a2r,
                                    -PI2 * a3i - grav * s[10], PI2 * a3r - grav * s[11]};
-            const double d = (double)n * g.dx3;
+            const double id = inv_l3;   // 1 / (n dx3)
             double p[6];
-            for (int cp = 0; cp < 3; cp++) {
-                const float2 tc = a.S[sidx(g, cp, g.sx3, k2i, k1c)];
-                p[2 * cp] = (double)tc.x - sum[2 * cp] / d;
-                p[2 * cp + 1] = (double)tc.y - sum[2 * cp + 1] / d;
-            }
+#pragma unroll
+            for (int qq = 0; qq < 6; qq++) p[qq] = (double)tr[qq] - sum[qq] * id;
             // cerrutisolmodified (src/green.f90:578-609) written as
             // u_i += fi (P_i + g R_i), g = 2 pi k3 fi, with per-column P_i, R_i
-            const double beta = PI2 * sqrt(k1v * k1v + k2v * k2v);
-            const double h = a.gam / beta;
-            const double c0 = 1.0 / (2.0 * a.mu * beta * beta * beta);
+            const double beta = cd[0], c0 = cd[1], iden = cd[2];
             const double b1r = p[0] * c0, b1i = p[1] * c0, b2r = p[2] * c0, b2i = p[3] * c0;
             const double qr = PI2 * k1v * p[0] + PI2 * k2v * p[2], qi = PI2 * k1v * p[1] + PI2 * k2v * p[3];
-            const double den = 2.0 * alpha * a.mu * beta * beta * beta * beta * (1 + h);
-            const double b3r = (beta * p[4] + (1.0 - alpha) * qi) / den;
-            const double b3i = (beta * p[5] - (1.0 - alpha) * qr) / den;
+            const double b3r = (beta * p[4] + (1.0 - alpha) * qi) * iden;
+            const double b3i = (beta * p[5] - (1.0 - alpha) * qr) * iden;
             const double Qr = b1r * k1v + b2r * k2v, Qi = b1i * k1v + b2i * k2v;
-            const double ab = alpha * beta * PI2, er = 1.0 - 1.0 / alpha, ab2 = -alpha * beta * beta;
+            const double ialpha = (a.lambda + 2.0 * a.mu) / (a.lambda + a.mu);   // 1 / alpha
+            const double ab = alpha * beta * PI2, er = 1.0 - ialpha, ab2 = -alpha * beta * beta;
             const double ap = alpha * PI2 * PI2, bb = 2.0 * beta * beta;
             // P_1 = i k1 ab er b3 - 2 beta^2 b1' + ap k1 Q ; R_1 = k1 ab b3 - i ap k1 Q
             cc[0] = (float)(-k1v * ab * er * b3i - bb * b1r + ap * k1v * Qr);
@@ -1638,8 +1820,8 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
             cc[6] = (float)(k2v * ab * b3r + ap * k2v * Qi);
             cc[7] = (float)(k2v * ab * b3i - ap * k2v * Qr);
             // P_3 = ab2 b3 / alpha ; R_3 = -i ab2 b3 + alpha beta 2pi Q
-            cc[8] = (float)(ab2 * b3r / alpha);
-            cc[9] = (float)(ab2 * b3i / alpha);
+            cc[8] = (float)(ab2 * b3r * ialpha);
+            cc[9] = (float)(ab2 * b3i * ialpha);
             cc[10] = (float)(ab2 * b3i + alpha * beta * PI2 * Qr);
             cc[11] = (float)(-ab2 * b3r + alpha * beta * PI2 * Qi);
             cc[12] = (float)beta;
@@ -1652,7 +1834,7 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
     {
         float cc[14];
 #pragma unroll
-        for (int qq = 0; qq < 14; qq++) cc[qq] = colc[c * 17 + qq];
+        for (int qq = 0; qq < 14; qq++) cc[qq] = colc[c * ZCOL + qq];
         const bool cerr = cc[13] != 0.f;
         const float pi2 = 6.28318530717958623f;
         const float beta = cc[12], b2 = beta * beta;
@@ -2532,7 +2714,7 @@ __global__ void k_repad(const float *src, float *dst, int sx1, size_t nrows)
 // standalone equivalentbodyforce (for the operator API): c_i -= div(sig),
 // t_i += sig_i3(x3=0) on padded arrays
 __global__ void k_bodyforce(Grid g, const float *m, float *c1, float *c2, float *c3, float *t1,
-                            float *t2, float *t3, float k1, float k2, float k3, float k3b)
+                            float *t2, float *t3, float k1, float k2, float k3, float k3b, FirY fir)
 {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.nh) return;
@@ -2547,7 +2729,9 @@ __global__ void k_bodyforce(Grid g, const float *m, float *c1, float *c2, float 
         const float *mx = m + cx * g.nh + pl + rowo;
         const float fx = (mx[(i1 + 1) % g.sx1] - mx[(i1 + g.sx1 - 1) % g.sx1]) * k1;
         const float *my = m + cy * g.nh + pl + i1;
-        const float fy = (my[(size_t)((i2 + 1) % g.sx2) * g.sx1] - my[(size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1]) * k2;
+        const float fy = fir.n == 7 ? fir_y1(my, i2, g.sx2, g.sx1, fir)
+                                    : (my[(size_t)((i2 + 1) % g.sx2) * g.sx1] -
+                                       my[(size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1]) * k2;
         const float *mz = m + cz * g.nh + rowo + i1;
         float fz;
         if (i3 == 0) fz = (mz[g.plane] - mz[0]) * k3b;

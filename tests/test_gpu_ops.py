@@ -51,6 +51,10 @@ def tensors_smooth(shape, scale=0.1, seed=0):
 
 
 GRIDS = [(32, 32, 32), (64, 48, 32), (96, 32, 36)]
+# grids of the 7-point FIR differentiator along x2 (5 <= sx2 <= 14: 6, 8, 9,
+# 12; sx2 = 6 wraps the 7 taps around the axis) and of shallow boxes
+# (5 <= sx3/2 <= 14, finite differences throughout), and sx2 = 4
+FIR_GRIDS = [(32, 8, 16), (32, 6, 12), (48, 12, 24), (64, 9, 18), (32, 4, 12)]
 
 
 @pytest.mark.parametrize("sx1,sx2,sx3", GRIDS + [(16, 12, 8), (128, 96, 64)])
@@ -73,7 +77,7 @@ def test_fft3_matches_oracle(oracle32, sx1, sx2, sx3):
     assert rel_l2(back, a[:, :, :sx1]) < 2e-6
 
 
-@pytest.mark.parametrize("sx1,sx2,sx3", GRIDS)
+@pytest.mark.parametrize("sx1,sx2,sx3", GRIDS + FIR_GRIDS)
 def test_stressupdate_matches_oracle(oracle32, sx1, sx2, sx3):
     lib = _lib.load()
     sx3h = sx3 // 2
@@ -93,7 +97,7 @@ def test_stressupdate_matches_oracle(oracle32, sx1, sx2, sx3):
     assert rel_l2(tensor_array(got), tensor_array(ref)) < 1e-6
 
 
-@pytest.mark.parametrize("sx1,sx2,sx3", GRIDS)
+@pytest.mark.parametrize("sx1,sx2,sx3", GRIDS + FIR_GRIDS)
 def test_bodyforce_matches_oracle(oracle32, sx1, sx2, sx3):
     lib = _lib.load()
     sx3h = sx3 // 2
@@ -271,9 +275,13 @@ def test_tensoramplitude_matches_oracle(oracle32):
 
 def test_unsupported_grid_is_rejected():
     lib = _lib.load()
-    d = dev(np.zeros((20, 10, 14), np.float32))
-    rc = lib.relax_op_fft3(ptr(d), 12, 10, 20, 1.0, 1.0, 1.0, -1, None)   # sx1/2 = 6 ok, sx2=10 no
+    d = dev(np.zeros((20, 10, 18), np.float32))
+    rc = lib.relax_op_fft3(ptr(d), 16, 10, 20, 1.0, 1.0, 1.0, -1, None)   # sx2 = 10 = 2 x 5
     assert rc == 4
+    u = dev(np.zeros((4, 8, 18), np.float32))
+    sig = dev(np.zeros((4, 8, 16, 6), np.float32))
+    rc = lib.relax_op_stressupdate(ptr(u), ptr(u), ptr(u), 1.0, 1.0, 1.0, 1.0, 1.0, 16, 8, 4, ptr(sig), None)
+    assert rc == 4                                                         # sx3/2 = 4 < 5
 
 
 @pytest.mark.parametrize("power", [1.0, 3.0])
