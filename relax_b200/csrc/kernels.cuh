@@ -1552,90 +1552,6 @@ __global__ void __launch_bounds__(CW *N2) k_ypass_reg(const __grid_constant__ YA
     (void)n;
 }
 
-// 8-byte asynchronous copy global -> shared (zero-filled when n = 0)
-__device__ __forceinline__ void cp_async8(void *dst, const void *src, int n)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// pass 2 / 4, persistent form of k_ypass_reg: each block walks tiles of CW
-// columns (gridDim.x apart) and copies the next tile into the other half of
-// its shared memory (cp.async) while it transforms the current one, so the
-// loads of one tile overlap the butterflies of the previous.  A thread
-// transposes in place: it writes the rows N2 k1 + t it copied itself.
-template <int N1, int N2, int CW, int SIGN>
-__global__ void __launch_bounds__(CW *N2, 3) k_ypass_pst(const __grid_constant__ YArgs a)
-{
-    constexpr int n = N1 * N2, Q = N1 / N2;
-    static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
-    extern __shared__ float2 smy[];   // [2][n][CW]
-    const Grid &g = a.g;
-    const int c = threadIdx.x % CW, t = threadIdx.x / CW;
-    const int np = a.nbody + a.traction;
-    const int ncol = 3 * np * g.K1;
-    const int ntiles = (ncol + CW - 1) / CW;
-    // column f = (cp np + pi) K1 + k1 of the flattened (component, plane, k1)
-    auto base_of = [&](int f) -> size_t {
-        const int cp = f / (np * g.K1), rem = f % (np * g.K1);
-        const int pi = rem / g.K1, k1c = rem % g.K1;
-        const int p = (a.traction && pi == a.nbody) ? g.sx3 : pi;
-        return sidx(g, cp, p, 0, k1c);
-    };
-    auto prefetch = [&](int tile, int buf) {
-        const int f = tile * CW + c;
-        const bool ok = f < ncol;
-        const size_t base = ok ? base_of(f) : 0;
-        float2 *B = smy + (size_t)buf * n * CW;
-#pragma unroll
-        for (int j1 = 0; j1 < N1; j1++) {
-            const int row = N2 * j1 + t;
-            cp_async8(B + row * CW + c, a.S + base + (size_t)row * g.K1, ok ? 8 : 0);
-        }
-        cp_async_commit();
-    };
-    int tile = blockIdx.x;
-    if (tile < ntiles) prefetch(tile, 0);
-    for (int it = 0; tile < ntiles; it++, tile += gridDim.x) {
-        const int buf = it & 1;
-        if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x, buf ^ 1);
-        else cp_async_commit();   // an empty group: the wait below still leaves one
-        cp_async_wait<1>();
-        float2 *B = smy + (size_t)buf * n * CW;
-        const int f = tile * CW + c;
-        const bool ok = f < ncol;
-        float2 x[N1];
-#pragma unroll
-        for (int j1 = 0; j1 < N1; j1++) x[j1] = B[(N2 * j1 + t) * CW + c];
-        RDft<N1, SIGN>::run(x);
-#pragma unroll
-        for (int k1 = 1; k1 < N1; k1++)
-            if (t) x[k1] = cmul(x[k1], twn<SIGN>(a.py.tw, t * k1));
-#pragma unroll
-        for (int k1 = 0; k1 < N1; k1++) B[(k1 * N2 + t) * CW + c] = x[k1];
-        __syncthreads();
-        const size_t base = ok ? base_of(f) : 0;
-#pragma unroll
-        for (int q = 0; q < Q; q++) {
-            float2 y[N2];
-            const int k1 = t + N2 * q;
-#pragma unroll
-            for (int jj = 0; jj < N2; jj++) y[jj] = B[(k1 * N2 + jj) * CW + c];
-            RDft<N2, SIGN>::run(y);
-            if (ok) {
-#pragma unroll
-                for (int k2 = 0; k2 < N2; k2++) a.S[base + (size_t)(k1 + N1 * k2) * g.K1] = y[k2];
-            }
-        }
-        __syncthreads();   // the buffer is refilled two tiles on
-    }
-    cp_async_wait<0>();
-    (void)n;
-}
-
 // pass 3, register/shared-memory version.  The three components of CW
 // columns stay in shared memory (U[cp][k1][j2][c]) between the phases, so a
 // thread holds one N1 or 3 x N2 group at a time.  PRUNED: input planes
@@ -1644,7 +1560,7 @@ __global__ void __launch_bounds__(CW *N2, 3) k_ypass_pst(const __grid_constant__
 constexpr int ZCOL = 26;   // floats of per-column constants in k_zspec_sm
 
 template <int N1, int N2, int CW, bool PRUNED, bool BATCH = false>
-__global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(const __grid_constant__ ZArgs a0)
+__global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 2 : 4) k_zspec_sm(const __grid_constant__ ZArgs a0)
 {
     const ZArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     constexpr int n = N1 * N2, Q = N1 / N2;
@@ -1735,12 +1651,21 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
 #pragma unroll
     for (int q = 0; q < Q; q++) {
         const int k1 = t + N2 * q;
-        float2 y[3][N2];
+        // SEQ (N2 >= 16): one component's DFT at a time, back to the
+        // thread's own slots of U, so that 3 N2 values never sit in
+        // registers together; otherwise the three stay in registers
+        constexpr bool SEQ = N2 >= 16;
+        float2 y[SEQ ? 1 : 3][N2];
 #pragma unroll
         for (int cp = 0; cp < 3; cp++) {
+            float2 *v = y[SEQ ? 0 : cp];
 #pragma unroll
-            for (int jj = 0; jj < N2; jj++) y[cp][jj] = U[uidx(cp, k1, jj)];
-            RDft<N2, -1>::run(y[cp]);
+            for (int jj = 0; jj < N2; jj++) v[jj] = U[uidx(cp, k1, jj)];
+            RDft<N2, -1>::run(v);
+            if (SEQ) {
+#pragma unroll
+                for (int jj = 0; jj < N2; jj++) U[uidx(cp, k1, jj)] = v[jj];
+            }
         }
 #pragma unroll
         for (int k2 = 0; k2 < N2; k2++) {
@@ -1748,7 +1673,9 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
             const int jw = j < n / 2 ? j : j - n;
             const float w = (float)jw;
             const float k3f = w * il3f;
-            const float2 c1 = y[0][k2], c2 = y[1][k2], c3 = y[2][k2];
+            const float2 c1 = SEQ ? U[uidx(0, k1, k2)] : y[0][k2];
+            const float2 c2 = SEQ ? U[uidx(1, k1, k2)] : y[SEQ ? 0 : 1][k2];
+            const float2 c3 = SEQ ? U[uidx(2, k1, k2)] : y[SEQ ? 0 : 2][k2];
             const float r2 = k1f * k1f + k2f * k2f + k3f * k3f;
             float2 u1, u2, u3;
             if (r2 > 0.f) {
@@ -1842,29 +1769,41 @@ __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 1 : 4) k_zspec_sm(c
 #pragma unroll
         for (int q = 0; q < Q; q++) {
             const int k1 = t + N2 * q;
-            float2 y[3][N2];
+            constexpr bool SEQ = N2 >= 16;   // as in stage B
+            float2 y[SEQ ? 1 : 3][N2];
+            if (!SEQ || cerr) {
 #pragma unroll
-            for (int k2 = 0; k2 < N2; k2++) {
-                float2 u1 = U[uidx(0, k1, k2)], u2 = U[uidx(1, k1, k2)], u3 = U[uidx(2, k1, k2)];
-                if (cerr) {
-                    const int j = k1 + N1 * k2;
-                    const float k3f = (float)(j < n / 2 ? j : j - n) * il3;
-                    const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + b2);
-                    const float gg = pi2 * k3f * fi;
-                    u1.x += fi * (cc[0] + gg * cc[2]); u1.y += fi * (cc[1] + gg * cc[3]);
-                    u2.x += fi * (cc[4] + gg * cc[6]); u2.y += fi * (cc[5] + gg * cc[7]);
-                    u3.x += fi * (cc[8] + gg * cc[10]); u3.y += fi * (cc[9] + gg * cc[11]);
+                for (int k2 = 0; k2 < N2; k2++) {
+                    float2 u1 = U[uidx(0, k1, k2)], u2 = U[uidx(1, k1, k2)], u3 = U[uidx(2, k1, k2)];
+                    if (cerr) {
+                        const int j = k1 + N1 * k2;
+                        const float k3f = (float)(j < n / 2 ? j : j - n) * il3;
+                        const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + b2);
+                        const float gg = pi2 * k3f * fi;
+                        u1.x += fi * (cc[0] + gg * cc[2]); u1.y += fi * (cc[1] + gg * cc[3]);
+                        u2.x += fi * (cc[4] + gg * cc[6]); u2.y += fi * (cc[5] + gg * cc[7]);
+                        u3.x += fi * (cc[8] + gg * cc[10]); u3.y += fi * (cc[9] + gg * cc[11]);
+                    }
+                    if (SEQ) {
+                        U[uidx(0, k1, k2)] = u1; U[uidx(1, k1, k2)] = u2; U[uidx(2, k1, k2)] = u3;
+                    } else {
+                        y[0][k2] = u1; y[SEQ ? 0 : 1][k2] = u2; y[SEQ ? 0 : 2][k2] = u3;
+                    }
                 }
-                y[0][k2] = u1; y[1][k2] = u2; y[2][k2] = u3;
             }
             float2 tw[N2];   // W_n^(-jj k1), shared by the three components
 #pragma unroll
             for (int jj = 0; jj < N2; jj++) tw[jj] = twn<+1>(a.pz.tw, jj * k1);
 #pragma unroll
             for (int cp = 0; cp < 3; cp++) {
-                RDft<N2, +1>::run(y[cp]);
+                float2 *v = y[SEQ ? 0 : cp];
+                if (SEQ) {
 #pragma unroll
-                for (int jj = 0; jj < N2; jj++) U[uidx(cp, k1, jj)] = jj ? cmul(y[cp][jj], tw[jj]) : y[cp][jj];
+                    for (int jj = 0; jj < N2; jj++) v[jj] = U[uidx(cp, k1, jj)];
+                }
+                RDft<N2, +1>::run(v);
+#pragma unroll
+                for (int jj = 0; jj < N2; jj++) U[uidx(cp, k1, jj)] = jj ? cmul(v[jj], tw[jj]) : v[jj];
             }
         }
     }

@@ -9,7 +9,9 @@ benchmark lines time, run against both oracle builds.
   Dt = 0.5 (<= 1e-4 after the run).
 * C3 shape -- three seeded faults with gravity and n = 3.5 below a 25 km lid
   on a box of the large instance's x1 length (sx1 = 512: the M = 256 x
-  passes), narrowed along x2 and x3 so that the oracle finishes in seconds.
+  passes), narrowed along x2 and x3 so that the oracle finishes in seconds;
+  and on a box of its depth (sx3 = 256: the pruned z pass with 16 x 16),
+  narrowed along x1 and x2.
 
 The GPU run is adaptive; the oracles replay its Dt sequence (a fixed dt
 schedule).  Tolerances: relative L2 of u, sig, tau (gamma 3x, see
@@ -55,4 +57,9 @@ def test_c1_full_run_matches_oracles(oracle32, oracle64):
 
 def test_c3_shape_matches_oracles(oracle32, oracle64):
     sim = random_faults(1, sx=512, sx2=64, sz=64, dx=1.0, lmax=40.0)
+    _replay(oracle32, oracle64, sim, 3, 1e-4)
+
+
+def test_c3_depth_matches_oracles(oracle32, oracle64):
+    sim = random_faults(1, sx=64, sx2=64, sz=256, dx=1.0, lmax=40.0)
     _replay(oracle32, oracle64, sim, 3, 1e-4)
