@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constan
                     const float2 c3 = make_float2(f2[2 * i], f2[2 * i + 1]);
                     float2 u1, u2, u3;
                     if (r2 > 0.f) {
-                        const float ir2 = 1.f / r2;
+                        const float ir2 = rcp_fast(r2);
                         const float A = ra * ir2, B = a.ratio1 * ir2 * ir2;
                         const float kcr = k1f * c1.x + k2f * c2.x + k3f * c3.x;
                         const float kci = k1f * c1.y + k2f * c2.y + k3f * c3.y;
@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(ZT_THREADS, 1) k_zspec_tc(const __grid_constan
                     for (int i = 0; i < 16; i++) {
                         const int j = 2 * (32 * hv + 16 * q + i) + par;
                         const float k3f = (float)(j < 64 ? j : j - 128) * il3;
-                        const float fi = (2.f * beta) / ((pi2 * pi2) * (k3f * k3f) + b2);
+                        const float fi = (2.f * beta) * rcp_fast((pi2 * pi2) * (k3f * k3f) + b2);
                         const float gg = pi2 * k3f * fi;
                         u[2 * i] += fi * (Pr + gg * Rr);
                         u[2 * i + 1] += fi * (Pi + gg * Ri);
