@@ -531,10 +531,14 @@ int relax_launch_count(relax_ctx *ctx, long long *n);
 /* members and one host synchronisation; members whose time reached   */
 /* the interval stay put and report i = 0.  Grids without the         */
 /* register-resident passes (lengths other than 64/128/256 along x1    */
-/* and x3, 64..512 along x2) step the members in turn.  Events with   */
-/* surface loads are rejected (RELAX_ERR_UNSUPPORTED).  Each member is */
-/* a relax_ctx owned by the batch (relax_batch_member) for field and   */
-/* patch access; do not destroy or step it directly.                  */
+/* and x3, 64..512 along x2) step the members in turn.  Otherwise the  */
+/* batch tunes itself on its first six steps: three batched (the third */
+/* timed), three with the members in turn (the sixth timed), and the   */
+/* faster form from then on (relax_batch_tuning); both forms give the  */
+/* same results.  Events with surface loads are rejected              */
+/* (RELAX_ERR_UNSUPPORTED).  Each member is a relax_ctx owned by the   */
+/* batch (relax_batch_member) for field and patch access; do not      */
+/* destroy or step it directly.                                       */
 /* ------------------------------------------------------------------ */
 typedef struct relax_batch relax_batch;
 
@@ -548,16 +552,20 @@ int relax_batch_coseismic(relax_batch *batch, relax_step_log *logs);
 int relax_batch_step(relax_batch *batch, relax_step_log *logs);
 int relax_batch_launch_count(relax_batch *batch, long long *n);
 int relax_batch_get_stream(relax_batch *batch, void **stream);
+/* The tuner's state: mode 0 while measuring, 1 batched launches, 2 the
+ * members in turn; the measured step times in ms (-1 until measured). */
+int relax_batch_tuning(relax_batch *batch, int *mode, double *batched_ms,
+                       double *in_turn_ms);
 
 /* An ensemble of members with uneven grids (no reference counterpart).
  * The members are grouped by shape (grid, spacing, elastic constants,
- * number of afterslip planes) into batches, each with its own stream;
- * relax_ensemble_step queues every group's step (one launch per stage per
- * group, replayed from a captured graph) and then waits once per group, so
- * that groups of different shapes run concurrently and the ensemble step
- * costs one host synchronisation.  Members keep their order: logs[k] and
- * relax_ensemble_member(k) are member k of `members`.  Members stepped in
- * an ensemble equal the same decks stepped alone, bit for bit. */
+ * number of afterslip planes) into batches, each with its own stream and
+ * its own tuning; relax_ensemble_step queues every group's step, each
+ * behind the previous group's (run concurrently, the groups competed for
+ * L2 and took longer), and then waits once per group.  Members keep their
+ * order: logs[k] and relax_ensemble_member(k) are member k of `members`.
+ * Members stepped in an ensemble equal the same decks stepped alone, bit
+ * for bit. */
 typedef struct relax_ensemble relax_ensemble;
 
 int relax_ensemble_create(const relax_config *members, int n, int device, relax_ensemble **ensemble);
@@ -568,6 +576,11 @@ int relax_ensemble_member(relax_ensemble *ensemble, int k, relax_ctx **member);
 int relax_ensemble_coseismic(relax_ensemble *ensemble, relax_step_log *logs);
 int relax_ensemble_step(relax_ensemble *ensemble, relax_step_log *logs);
 int relax_ensemble_launch_count(relax_ensemble *ensemble, long long *n);
+/* Group `group`'s grid (sx: 3 ints), member count and tuner state as
+ * relax_batch_tuning reports it (any output may be NULL). */
+int relax_ensemble_tuning(relax_ensemble *ensemble, int group, int *sx,
+                          int *nmembers, int *mode, double *batched_ms,
+                          double *in_turn_ms);
 
 /* ------------------------------------------------------------------ */
 /* stateless operators on device buffers (reference layout)           */

@@ -87,6 +87,7 @@ def load() -> C.CDLL:
         "relax_batch_step": (I, [P, C.POINTER(relax_step_log)]),
         "relax_batch_launch_count": (I, [P, C.POINTER(C.c_longlong)]),
         "relax_batch_get_stream": (I, [P, C.POINTER(P)]),
+        "relax_batch_tuning": (I, [P, C.POINTER(I), C.POINTER(D), C.POINTER(D)]),
         "relax_ensemble_create": (I, [C.POINTER(relax_config), I, I, C.POINTER(P)]),
         "relax_ensemble_destroy": (I, [P]),
         "relax_ensemble_size": (I, [P, C.POINTER(I), C.POINTER(I)]),
@@ -94,6 +95,8 @@ def load() -> C.CDLL:
         "relax_ensemble_coseismic": (I, [P, C.POINTER(relax_step_log)]),
         "relax_ensemble_step": (I, [P, C.POINTER(relax_step_log)]),
         "relax_ensemble_launch_count": (I, [P, C.POINTER(C.c_longlong)]),
+        "relax_ensemble_tuning": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(D),
+                                      C.POINTER(D)]),
         "relax_op_stressupdate": (I, [P, P, P, D, D, D, D, D, I, I, I, P, P]),
         "relax_op_bodyforce": (I, [P, D, D, D, I, I, I, P, P, P, P, P, P, P]),
         "relax_op_viscouseigenstress": (I, [D, P, P, P, I, I, I, P, C.POINTER(D), P, P, P]),

@@ -421,6 +421,9 @@ class _Member(Relax):
         self.h = None
 
 
+_MODES = {0: "measuring", 1: "batched", 2: "in turn"}
+
+
 class Batch:
     """Members sharing grid and elastic constants, stepped together.
 
@@ -487,10 +490,20 @@ class Batch:
         _lib.check(self.lib.relax_batch_get_stream(self.h, C.byref(s)))
         return s.value
 
+    def tuning(self) -> dict:
+        """The batch's choice between one launch per stage for all members
+        and the members stepped in turn, from its first six steps:
+        {"mode": "measuring" | "batched" | "in turn", "batched_ms", "in_turn_ms"}
+        (step times, -1 until measured)."""
+        m, tb, tt = C.c_int(), C.c_double(), C.c_double()
+        _lib.check(self.lib.relax_batch_tuning(self.h, C.byref(m), C.byref(tb), C.byref(tt)))
+        return {"mode": _MODES[m.value], "batched_ms": tb.value, "in_turn_ms": tt.value}
+
 
 class Ensemble(Batch):
-    """Members with uneven grids, grouped by shape into batches that run
-    concurrently; one host synchronisation per ensemble step.
+    """Members with uneven grids, grouped by shape into batches stepped one
+    after the other (each tuned on its own); one host synchronisation per
+    ensemble step.
 
         with Ensemble(ensemble_uneven(seed=4)) as e:
             e.coseismic()
@@ -544,3 +557,16 @@ class Ensemble(Batch):
 
     def stream(self) -> int:
         raise NotImplementedError("an ensemble runs one stream per shape group")
+
+    def tuning(self) -> List[dict]:
+        """Per shape group: {"grid": (sx1, sx2, sx3), "members", "mode",
+        "batched_ms", "in_turn_ms"} as Batch.tuning reports them."""
+        out = []
+        for q in range(self.groups()):
+            sx = (C.c_int * 3)()
+            nm, m, tb, tt = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+            _lib.check(self.lib.relax_ensemble_tuning(self.h, q, sx, C.byref(nm), C.byref(m), C.byref(tb),
+                                                      C.byref(tt)))
+            out.append({"grid": (sx[0], sx[1], sx[2]), "members": nm.value, "mode": _MODES[m.value],
+                        "batched_ms": tb.value, "in_turn_ms": tt.value})
+        return out

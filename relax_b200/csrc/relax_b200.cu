@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cmath>
 #include <cstdio>
@@ -3408,6 +3409,18 @@ struct relax_batch {
     long long glaunches = 0;
     bool graph_off = false;
     int plain_steps = 0;
+    // autotuning: whether one launch per stage for all members beats the
+    // members stepped in turn (each with its own captured step) is decided
+    // from the batch's own steps.  Steps 1-3 run batched (plain, capture,
+    // replay: the third is timed with CUDA events), steps 4-6 in turn (the
+    // sixth is timed on the host clock, the members' host tails included);
+    // the faster form runs from then on.  Both forms give the same
+    // results, bit for bit.
+    int mode = 0;                  // 0 measuring, 1 batched, 2 members in turn
+    int tune_steps = 0;
+    double tb_ms = -1.0, tt_ms = -1.0;
+    cudaEvent_t tev[2] = {nullptr, nullptr};
+    bool tev_pending = false;
 };
 
 static void free_batch(relax_batch *b)
@@ -3415,6 +3428,8 @@ static void free_batch(relax_batch *b)
     if (!b) return;
     for (auto *c : b->m) free_ctx(c);
     cudaDeviceSynchronize();
+    for (cudaEvent_t ev : b->tev)
+        if (ev) cudaEventDestroy(ev);
     if (b->tab.dev) dfree(b->tab.dev, true);
     if (b->dst) dfree(b->dst, true);
     if (b->hst) cudaFreeHost(b->hst);
@@ -3455,7 +3470,8 @@ extern "C" int relax_batch_create(const relax_config *members, int n, int device
                 return bail(fail(RELAX_ERR_UNSUPPORTED, "batch member %d: surface loads are evaluated on the host "
                                                         "at t + Dt; step such members alone", k));
     }
-    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->tev[0]) != cudaSuccess || cudaEventCreate(&b->tev[1]) != cudaSuccess)
         return bail(fail(RELAX_ERR_CUDA, "stream"));
     // member states in one array (one read-back per step)
     if (dalloc(&b->dst, (size_t)n) != RELAX_OK) return bail(RELAX_ERR_NOMEM);
@@ -3719,7 +3735,8 @@ static int batch_kernels(relax_batch *b)
 // of the members' states, all queued on the batch's stream.  *queued is
 // false when the members were stepped in turn (no batched instantiation)
 // or none is live; batch_step_finish then has nothing to collect.
-static int batch_step_begin(relax_batch *b, relax_step_log *logs, std::vector<char> &live, bool *queued)
+static int batch_step_begin(relax_batch *b, relax_step_log *logs, std::vector<char> &live, bool *queued,
+                            cudaEvent_t after = nullptr)
 {
     *queued = false;
     CK(cudaSetDevice(b->device));
@@ -3734,10 +3751,26 @@ static int batch_step_begin(relax_batch *b, relax_step_log *logs, std::vector<ch
         nlive += live[k];
     }
     if (!nlive) return RELAX_OK;
-    if (!b->batched || n == 1) {
-        // no batched instantiation for this grid: the members in turn
-        for (int k = 0; k < n; k++)
-            if (live[k]) TRY(do_step(b->m[k], nullptr, &logs[k]));
+    // no batched instantiation for this grid: the members in turn
+    if (!b->batched || n == 1) b->mode = 2;
+    bool turn = b->mode == 2, time_turn = false, time_batched = false;
+    if (b->mode == 0) {
+        turn = b->tune_steps >= 3;
+        time_turn = b->tune_steps == 5;
+        time_batched = b->tune_steps == 2;
+        b->tune_steps++;
+    }
+    if (turn) {
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int k = 0; k < n; k++) {
+            if (!live[k]) continue;
+            if (after) CK(cudaStreamWaitEvent(b->m[k]->st, after, 0));
+            TRY(do_step(b->m[k], nullptr, &logs[k]));
+        }
+        if (time_turn) {
+            b->tt_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            b->mode = (b->tb_ms > 0.0 && b->tb_ms <= b->tt_ms) ? 1 : 2;
+        }
         return RELAX_OK;
     }
     if (!b->tables_valid) TRY(build_tables(b));
@@ -3745,6 +3778,7 @@ static int batch_step_begin(relax_batch *b, relax_step_log *logs, std::vector<ch
     for (auto *c : b->m) CK(cudaStreamSynchronize(c->st));
     BatchTables &t = b->tab;
     cudaStream_t st = b->st;
+    if (after) CK(cudaStreamWaitEvent(st, after, 0));
     // ---- predictor
     for (int k = 0; k < n; k++) {
         relax_ctx *c = b->m[k];
@@ -3780,12 +3814,17 @@ static int batch_step_begin(relax_batch *b, relax_step_log *logs, std::vector<ch
         cudaGetLastError();
         b->launches = l0;
     }
+    if (time_batched) CK(cudaEventRecord(b->tev[0], st));
     if (b->gexec) {
         CK(cudaGraphLaunch(b->gexec, st));
         b->launches += b->glaunches;
     } else {
         TRY(batch_kernels(b));
         b->plain_steps++;
+    }
+    if (time_batched) {
+        CK(cudaEventRecord(b->tev[1], st));
+        b->tev_pending = true;
     }
     CK(cudaMemcpyAsync(b->hst, b->dst, n * sizeof(StepState), cudaMemcpyDeviceToHost, st));
     *queued = true;
@@ -3798,6 +3837,12 @@ static int batch_step_finish(relax_batch *b, relax_step_log *logs, const std::ve
 {
     CK(cudaSetDevice(b->device));
     CK(cudaStreamSynchronize(b->st));
+    if (b->tev_pending) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, b->tev[0], b->tev[1]));
+        b->tb_ms = ms;
+        b->tev_pending = false;
+    }
     for (int k = 0; k < (int)b->m.size(); k++) {
         if (!live[k]) continue;
         relax_ctx *c = b->m[k];
@@ -3821,19 +3866,24 @@ extern "C" int relax_batch_step(relax_batch *b, relax_step_log *logs)
 
 // ---------------------------------------------------------------------------
 // ensembles of uneven grids: one batch per grid shape, each on its own
-// stream, stepped together with one host synchronisation per step
+// stream, stepped with one host synchronisation per step.  The groups' steps
+// run one after the other (each stream waits for the previous group's step):
+// run concurrently they competed for L2 and took longer than in sequence.
 // ---------------------------------------------------------------------------
 struct relax_ensemble {
     std::vector<relax_batch *> groups;
     std::vector<std::vector<int>> index;   // member numbers of each group
     std::vector<std::pair<int, int>> where;   // group and slot of each member
     std::vector<std::vector<relax_step_log>> glog;
+    std::vector<cudaEvent_t> done;          // end of each group's queued step
     int device = 0;
 };
 
 static void free_ensemble(relax_ensemble *e)
 {
     if (!e) return;
+    for (cudaEvent_t ev : e->done)
+        if (ev) cudaEventDestroy(ev);
     for (auto *b : e->groups) free_batch(b);
     delete e;
 }
@@ -3867,6 +3917,13 @@ extern "C" int relax_ensemble_create(const relax_config *members, int n, int dev
         }
         e->groups.push_back(b);
         e->glog.emplace_back(idx.size());
+        cudaEvent_t ev = nullptr;
+        const cudaError_t ce = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (ce != cudaSuccess) {
+            free_ensemble(e);
+            return fail(RELAX_ERR_CUDA, "cudaEventCreate: %s", cudaGetErrorString(ce));
+        }
+        e->done.push_back(ev);
     }
     *out = e;
     return RELAX_OK;
@@ -3911,11 +3968,17 @@ extern "C" int relax_ensemble_step(relax_ensemble *e, relax_step_log *logs)
     const size_t ng = e->groups.size();
     std::vector<std::vector<char>> live(ng);
     std::vector<char> queued(ng, 0);
-    // every group's step queued on its own stream, then one wait per group
+    // every group's step queued on its own stream behind the previous
+    // group's, then one wait per group
+    cudaEvent_t prev = nullptr;
     for (size_t q = 0; q < ng; q++) {
         bool qd = false;
-        TRY(batch_step_begin(e->groups[q], e->glog[q].data(), live[q], &qd));
+        TRY(batch_step_begin(e->groups[q], e->glog[q].data(), live[q], &qd, prev));
         queued[q] = qd;
+        if (qd) {
+            CK(cudaEventRecord(e->done[q], e->groups[q]->st));
+            prev = e->done[q];
+        }
     }
     for (size_t q = 0; q < ng; q++)
         if (queued[q]) TRY(batch_step_finish(e->groups[q], e->glog[q].data(), live[q]));
@@ -3942,6 +4005,28 @@ extern "C" int relax_batch_launch_count(relax_batch *b, long long *n)
     *n = b->launches;
     for (auto *c : b->m) *n += c->prof.launches;
     return RELAX_OK;
+}
+
+extern "C" int relax_batch_tuning(relax_batch *b, int *mode, double *batched_ms, double *in_turn_ms)
+{
+    if (!b) return fail(RELAX_ERR_ARG, "null batch");
+    if (mode) *mode = b->mode;
+    if (batched_ms) *batched_ms = b->tb_ms;
+    if (in_turn_ms) *in_turn_ms = b->tt_ms;
+    return RELAX_OK;
+}
+
+extern "C" int relax_ensemble_tuning(relax_ensemble *e, int group, int *sx, int *nmembers, int *mode,
+                                     double *batched_ms, double *in_turn_ms)
+{
+    if (!e) return fail(RELAX_ERR_ARG, "null ensemble");
+    if (group < 0 || group >= (int)e->groups.size()) return fail(RELAX_ERR_ARG, "group %d out of range", group);
+    relax_batch *b = e->groups[group];
+    if (sx) {
+        sx[0] = b->m[0]->g.sx1; sx[1] = b->m[0]->g.sx2; sx[2] = b->m[0]->g.sx3;
+    }
+    if (nmembers) *nmembers = (int)b->m.size();
+    return relax_batch_tuning(b, mode, batched_ms, in_turn_ms);
 }
 
 extern "C" int relax_batch_get_stream(relax_batch *b, void **s)

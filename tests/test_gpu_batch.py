@@ -70,11 +70,12 @@ def _same(a, b):
 def test_batch_matches_members_alone():
     base = powerlaw_small(sx=128, sz=64, dx=1.0)
     sims = [_variant(base, k) for k in range(3)]
-    outs, launches = _batched(sims, 4)
+    outs, launches = _batched(sims, 3)
     for k, s in enumerate(sims):
-        _same(outs[k], _alone(s, 4))
+        _same(outs[k], _alone(s, 3))
     # one launch per stage for all members: 2 friction + dt + 5 + corr + friction + monitor + 5 + end
-    assert launches == 4 * 16
+    # (the tuner's first three steps are batched)
+    assert launches == 3 * 16
 
 
 def test_batch_linear_members_finish_at_their_interval():
@@ -155,3 +156,48 @@ def test_ensemble_of_uneven_grids_matches_members_alone():
             outs.append(o)
     for k, s in enumerate(sims):
         _same(outs[k], _alone(s, 3))
+
+
+def test_batch_tuner_chooses_a_form_and_keeps_members_exact():
+    """The batch's tuner: steps 1-3 batched (the third timed), 4-6 with the
+    members in turn (the sixth timed), then the faster form; every step of
+    either form leaves each member equal to its deck stepped alone."""
+    base = powerlaw_small(sx=64, sz=64, dx=1.0)
+    sims = [_variant(base, k) for k in range(3)]
+    with Batch(sims) as b:
+        logs = [[l] for l in b.coseismic()]
+        states = []
+        for step in range(8):
+            for k, l in enumerate(b.step()):
+                logs[k].append(l)
+            states.append(b.tuning())
+        outs = []
+        for k in range(len(sims)):
+            m = b.member(k)
+            o = {"logs": logs[k], "u": m.field("u"), "tau": m.field("tau"), "gamma": m.field("gamma"),
+                 "patches": np.array([(p.slip, p.v, p.taus) for p in m.patches(0)])}
+            outs.append(o)
+    assert [s["mode"] for s in states[:5]] == ["measuring"] * 5
+    assert states[2]["batched_ms"] > 0 and states[4]["in_turn_ms"] < 0
+    final = states[-1]
+    assert final["mode"] in ("batched", "in turn")
+    assert final["batched_ms"] > 0 and final["in_turn_ms"] > 0
+    assert final["mode"] == ("batched" if final["batched_ms"] <= final["in_turn_ms"] else "in turn")
+    for k, s in enumerate(sims):
+        _same(outs[k], _alone(s, 8))
+
+
+def test_ensemble_reports_each_group_tuning():
+    from relax_b200.api import Ensemble
+    a = powerlaw_small(sx=64, sz=64, dx=1.0, afterslip=False)
+    c = linear_small(sx=96, sz=64, steps=8)
+    sims = [_variant(a, 0), _variant(c, 0), _variant(a, 1)]
+    with Ensemble(sims) as e:
+        e.coseismic()
+        for _ in range(7):
+            e.step()
+        t = e.tuning()
+    assert [g["grid"] for g in t] == [(64, 64, 64), (96, 96, 64)]
+    assert [g["members"] for g in t] == [2, 1]
+    assert t[0]["mode"] in ("batched", "in turn") and t[0]["batched_ms"] > 0 and t[0]["in_turn_ms"] > 0
+    assert t[1]["mode"] == "in turn"   # one member: nothing to batch
