@@ -225,11 +225,11 @@ const char *relax_last_error(void);     /* thread-local message        */
 
 /* Allocates all device state for one RELAX instance on `device`.  The
  * configuration is deep-copied.  Replaces cuinflags_/cuinit_
- * (src/cuelastic.cu:736, :476).  Grids: sx1 >= 16 and a multiple of 4,
+ * (src/cuelastic.cu:736, :476).  Grids: sx1 >= 8 and a multiple of 4,
  * sx2 >= 2, even sx3 with sx3/2 >= 5, FFT lengths sx1/2, sx2, sx3
- * products of 2 and 3 (RELAX_ERR_UNSUPPORTED otherwise); the x2
+ * products of 2 and 3 (RELAX_ERR_UNSUPPORTED otherwise); the x1 and x2
  * derivatives take the 7-point FIR filter of src/kernel7.inc for
- * 5 <= sx2 <= 14 as optimalfilter (src/elastic3d.f90:846-907) does. */
+ * 5 <= sx <= 14 as optimalfilter (src/elastic3d.f90:846-907) does. */
 int relax_create(const relax_config *cfg, int device, relax_ctx **out);
 /* Replaces cudeinit_ (src/cuelastic.cu:1344).  The context's device
  * memory goes back to the library's own memory pool on that device, which

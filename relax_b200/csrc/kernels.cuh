@@ -82,26 +82,25 @@ __device__ __forceinline__ float rcp_fast(float x)
     return r;
 }
 
-// The derivative along x2.  optimalfilter (src/elastic3d.f90:846-907)
-// takes the central difference (w[i2+1] - w[i2-1]) / (2 dx2) for sx2 <= 4
-// and sx2 >= 15, and the 7-point FIR differentiator fir7 of
-// src/kernel7.inc for 5 <= sx2 <= 14: sum over l = 1..7 of
-// (w[i2+l] - w[i2-l]) fir7(l) / dx2, indexes periodic (localstrain_ani,
-// src/elastic3d.f90:1140-1178, and localdivergence_ani, :1431-1470).  n = 7
-// selects the filter, c[l-1] = fir7(l) / dx2; otherwise the central
-// difference runs.  Along x3, fir7 is selected for 5 <= sx3/2 <= 14, but
-// then every layer is a boundary layer of the filter ((i3 > 7) and
-// (i3 < sx3/2 - 6) is never true, stressupdate :975-976), so the finite
-// differences of localstrain_ani apply throughout; along x1 the grid needs
-// sx1 >= 16.
-struct FirY {
+// Derivatives along the periodic axes x1 and x2.  optimalfilter
+// (src/elastic3d.f90:846-907) takes the central difference
+// (w[i+1] - w[i-1]) / (2 dx) for sx <= 4 and sx >= 15, and the 7-point FIR
+// differentiator fir7 of src/kernel7.inc for 5 <= sx <= 14: sum over
+// l = 1..7 of (w[i+l] - w[i-l]) fir7(l) / dx, indexes periodic
+// (localstrain_ani, src/elastic3d.f90:1140-1178, and localdivergence_ani,
+// :1431-1470).  A Fir7 with n = 7 selects the filter, c[l-1] = fir7(l) / dx;
+// n = 0 the central difference.  Along x3, fir7 is selected for
+// 5 <= sx3/2 <= 14, but then every layer is a boundary layer of the filter
+// ((i3 > 7) and (i3 < sx3/2 - 6) is never true, stressupdate :975-976), so
+// the finite differences of localstrain_ani apply throughout.
+struct Fir7 {
     int n;
     float c[7];
 };
 
 // sum_l (w[(i2+l) % sx2] - w[(i2-l) % sx2]) c[l-1] at 4 consecutive points
 // of rows of pitch sx1 (w points at x1 of the row i2 = 0 of the plane)
-__device__ __forceinline__ float4 fir_y4(const float *w, int i2, int sx2, int sx1, const FirY &f)
+__device__ __forceinline__ float4 fir_y4(const float *w, int i2, int sx2, int sx1, const Fir7 &f)
 {
     float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
@@ -116,20 +115,52 @@ __device__ __forceinline__ float4 fir_y4(const float *w, int i2, int sx2, int sx
     return d;
 }
 
-// the x2 derivatives of the 3 components of w (3 x nh) by fir7, for
-// k_stress on grids of 5 <= sx2 <= 14 (the filter kept out of its registers)
-__global__ void __launch_bounds__(RELAX_NTHREADS) k_fir_y(Grid g, const float *w, float *wy, FirY f)
+// the same along x1 for the point i1 of a row (sx1 >= 5)
+__device__ __forceinline__ float fir_x1(const float *row, int i1, int sx1, const Fir7 &f)
+{
+    float d = 0.f;
+#pragma unroll
+    for (int l = 1; l <= 7; l++)
+        d += (__ldg(row + (i1 + l) % sx1) - __ldg(row + (i1 + 2 * sx1 - l) % sx1)) * f.c[l - 1];
+    return d;
+}
+
+// The x1 and x2 derivatives of the 3 components of w (3 x nh each) for
+// k_stress on grids where either axis takes fir7 (kept out of the stress
+// kernel's registers): by the filter where its Fir7 says so, else by the
+// central difference exactly as k_stress forms it ((right - left) * k).
+__global__ void __launch_bounds__(RELAX_NTHREADS) k_fir_xy(Grid g, const float *w, float *wx, float *wy, Fir7 fx,
+                                                           Fir7 fy, float k1, float k2)
 {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= 3 * (g.nh >> 2)) return;
     const int c = (int)(q / (g.nh >> 2));
     const size_t p = 4 * (q % (g.nh >> 2));
     const int i1 = (int)(p % g.sx1), i2 = (int)((p / g.sx1) % g.sx2), i3 = (int)(p / g.plane);
-    const float4 d = fir_y4(w + c * g.nh + (size_t)i3 * g.plane + i1, i2, g.sx2, g.sx1, f);
-    *reinterpret_cast<float4 *>(wy + c * g.nh + p) = d;
+    const float *wc = w + c * g.nh;
+    const float *row = wc + p - i1;
+    float4 dx;
+    if (fx.n == 7) {
+        dx = make_float4(fir_x1(row, i1, g.sx1, fx), fir_x1(row, i1 + 1, g.sx1, fx),
+                         fir_x1(row, i1 + 2, g.sx1, fx), fir_x1(row, i1 + 3, g.sx1, fx));
+    } else {
+        const float4 cv = ld4(wc + p);
+        const float lft = __ldg(row + (i1 + g.sx1 - 1) % g.sx1), rgt = __ldg(row + (i1 + 4) % g.sx1);
+        dx = make_float4((cv.y - lft) * k1, (cv.z - cv.x) * k1, (cv.w - cv.y) * k1, (rgt - cv.z) * k1);
+    }
+    float4 dy;
+    if (fy.n == 7) {
+        dy = fir_y4(wc + (size_t)i3 * g.plane + i1, i2, g.sx2, g.sx1, fy);
+    } else {
+        const float4 ym = ld4(wc + (size_t)i3 * g.plane + (size_t)((i2 + g.sx2 - 1) % g.sx2) * g.sx1 + i1);
+        const float4 yp = ld4(wc + (size_t)i3 * g.plane + (size_t)((i2 + 1) % g.sx2) * g.sx1 + i1);
+        dy = make_float4((yp.x - ym.x) * k2, (yp.y - ym.y) * k2, (yp.z - ym.z) * k2, (yp.w - ym.w) * k2);
+    }
+    *reinterpret_cast<float4 *>(wx + c * g.nh + p) = dx;
+    *reinterpret_cast<float4 *>(wy + c * g.nh + p) = dy;
 }
 
-__device__ __forceinline__ float fir_y1(const float *w, int i2, int sx2, int sx1, const FirY &f)
+__device__ __forceinline__ float fir_y1(const float *w, int i2, int sx2, int sx1, const Fir7 &f)
 {
     float d = 0.f;
 #pragma unroll
@@ -173,7 +204,7 @@ struct StressArgs {
     const float *spdev;      // 6 x sx3h deviatoric prestress (or null)
     const StepState *st;
     float k1, k2, k3, k3b;   // 0.5/dx1, 0.5/dx2, 0.5/dx3, 1/dx3
-    const float *wy;         // FIRY: the x2 derivatives of w by fir7 (3 x nh, k_fir_y)
+    const float *wx, *wy;    // FIR: the x1 and x2 derivatives of w (3 x nh each, k_fir_xy)
     float lam, mu2, muinv;   // lambda, 2 mu, 1/mu
     int store_sig;
     const unsigned char *sig_mask;   // store_sig: only groups of 4 points flagged here (null = all)
@@ -196,9 +227,9 @@ struct StressArgs {
 // minima), in CORR the predicted strain epsilonikdot = Dt/2 epsilonikdot +
 // epsilonik (:693-695), the corrector's calls on it (:764-787) and
 // epsilonik += Dt epsilonikdot (:789).
-// FIRY: the x2 derivatives of w come from a.wy (k_fir_y, grids of the 7-point
-// x2 filter) instead of the central difference of rows i2 -+ 1.
-template <int MODE, bool BATCH = false, bool TRANS = false, bool FIRY = false>
+// FIR: the x1 and x2 derivatives of w come from a.wx, a.wy (k_fir_xy, grids
+// where x1 or x2 takes the 7-point filter) instead of the central differences.
+template <int MODE, bool BATCH = false, bool TRANS = false, bool FIR = false>
 __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const __grid_constant__ StressArgs a0)
 {
     const StressArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
@@ -273,13 +304,18 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const 
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const float *wc = a.w + c * nh;
-                const float4 cv = ld4(wc + idx);
-                const float lft = __ldg(wc + row + i1m), rgt = __ldg(wc + row + i1p);
-                dxw[c][0] = (cv.y - lft) * a.k1;
-                dxw[c][1] = (cv.z - cv.x) * a.k1;
-                dxw[c][2] = (cv.w - cv.y) * a.k1;
-                dxw[c][3] = (rgt - cv.z) * a.k1;
-                if (FIRY) {
+                if (FIR) {
+                    const float4 d = ld4(a.wx + c * nh + idx);
+                    dxw[c][0] = d.x; dxw[c][1] = d.y; dxw[c][2] = d.z; dxw[c][3] = d.w;
+                } else {
+                    const float4 cv = ld4(wc + idx);
+                    const float lft = __ldg(wc + row + i1m), rgt = __ldg(wc + row + i1p);
+                    dxw[c][0] = (cv.y - lft) * a.k1;
+                    dxw[c][1] = (cv.z - cv.x) * a.k1;
+                    dxw[c][2] = (cv.w - cv.y) * a.k1;
+                    dxw[c][3] = (rgt - cv.z) * a.k1;
+                }
+                if (FIR) {
                     const float4 d = ld4(a.wy + c * nh + idx);
                     dyw[c][0] = d.x; dyw[c][1] = d.y; dyw[c][2] = d.z; dyw[c][3] = d.w;
                 } else {
@@ -1081,7 +1117,7 @@ struct XfArgs {
     int has_trac;            // blockIdx.y == nin is the traction plane
     const float *m;          // XIN_DIV: 6 x nh moment
     float k1, k2, k3, k3b;
-    FirY fy;                 // XIN_DIV: the x2 differentiator (n = 7: fir7, k_xfwd only)
+    Fir7 fx, fy;             // XIN_DIV: the x1, x2 differentiators (n = 7: fir7, k_xfwd only)
     const float *in[3];      // XIN_REAL
     size_t rp, pp;           // row / plane pitch (elements)
     const float *tin[3];
@@ -1125,7 +1161,9 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xfwd(XfArgs a)
                     const int cz = c == 0 ? 2 : c == 1 ? 4 : 5;
                     const size_t pl = (size_t)i3 * g.plane;
                     const float *mx = a.m + cx * g.nh + pl + rowo;
-                    const float fx = (__ldg(mx + (i1 + 1) % g.sx1) - __ldg(mx + (i1 + g.sx1 - 1) % g.sx1)) * a.k1;
+                    const float fx = a.fx.n == 7
+                                         ? fir_x1(mx, i1, g.sx1, a.fx)
+                                         : (__ldg(mx + (i1 + 1) % g.sx1) - __ldg(mx + (i1 + g.sx1 - 1) % g.sx1)) * a.k1;
                     const float *my = a.m + cy * g.nh + pl + i1;
                     const float fy = a.fy.n == 7
                                          ? fir_y1(my, i2, g.sx2, g.sx1, a.fy)
@@ -2666,7 +2704,8 @@ __global__ void k_repad(const float *src, float *dst, int sx1, size_t nrows)
 // standalone equivalentbodyforce (for the operator API): c_i -= div(sig),
 // t_i += sig_i3(x3=0) on padded arrays
 __global__ void k_bodyforce(Grid g, const float *m, float *c1, float *c2, float *c3, float *t1,
-                            float *t2, float *t3, float k1, float k2, float k3, float k3b, FirY fir)
+                            float *t2, float *t3, float k1, float k2, float k3, float k3b, Fir7 firx,
+                            Fir7 fir)
 {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.nh) return;
@@ -2679,7 +2718,8 @@ __global__ void k_bodyforce(Grid g, const float *m, float *c1, float *c2, float 
         const int cy = c == 0 ? 1 : c == 1 ? 3 : 4;
         const int cz = c == 0 ? 2 : c == 1 ? 4 : 5;
         const float *mx = m + cx * g.nh + pl + rowo;
-        const float fx = (mx[(i1 + 1) % g.sx1] - mx[(i1 + g.sx1 - 1) % g.sx1]) * k1;
+        const float fx = firx.n == 7 ? fir_x1(mx, i1, g.sx1, firx)
+                                     : (mx[(i1 + 1) % g.sx1] - mx[(i1 + g.sx1 - 1) % g.sx1]) * k1;
         const float *my = m + cy * g.nh + pl + i1;
         const float fy = fir.n == 7 ? fir_y1(my, i2, g.sx2, g.sx1, fir)
                                     : (my[(size_t)((i2 + 1) % g.sx2) * g.sx1] -

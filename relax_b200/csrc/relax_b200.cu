@@ -442,9 +442,10 @@ static cudaError_t launch_xfwd_reg(const XfArgs &xa, bool div, dim3 grid, int nm
 
 static bool xfwd_reg(const XfArgs &xa, bool div, int nplanes, cudaStream_t st, cudaError_t *e, int nm = 1)
 {
-    // rows of 16: never a grid of the x2 FIR differentiator (sx2 <= 14),
-    // which k_xfwd alone applies
-    if (xa.g.sx2 % 16 || (div && xa.fy.n)) return false;
+    // the 7-point filters are applied by k_xfwd alone (grids of the x2
+    // filter have no rows of 16 anyway, nor those of the x1 filter a register
+    // x pass)
+    if (xa.g.sx2 % 16 || (div && (xa.fx.n || xa.fy.n))) return false;
     const dim3 grid(xa.g.sx2 / 16, nplanes);
     switch (xa.g.M) {
     case 32: *e = launch_xfwd_reg<8, 4>(xa, div, grid, nm, st); return true;
@@ -672,8 +673,8 @@ struct Spectral {
 
 static int make_grid(Grid &g, int sx1, int sx2, int sx3, double dx1, double dx2, double dx3)
 {
-    if (sx1 < 16 || sx2 < 2 || sx3 < 4 || (sx1 % 4) || (sx3 % 2))
-        return fail(RELAX_ERR_UNSUPPORTED, "grid %dx%dx%d: need sx1 >= 16 and a multiple of 4, even sx3",
+    if (sx1 < 8 || sx2 < 2 || sx3 < 4 || (sx1 % 4) || (sx3 % 2))
+        return fail(RELAX_ERR_UNSUPPORTED, "grid %dx%dx%d: need sx1 >= 8 and a multiple of 4, even sx3",
                     sx1, sx2, sx3);
     // optimalfilter (src/elastic3d.f90:846-907) has no differentiator for a
     // depth sx3/2 below 5
@@ -690,21 +691,25 @@ static int make_grid(Grid &g, int sx1, int sx2, int sx3, double dx1, double dx2,
     return RELAX_OK;
 }
 
-// The x2 differentiator of optimalfilter (src/elastic3d.f90:846-907): the
-// 7-point FIR fir7 of src/kernel7.inc scaled by 1/dx2 for 5 <= sx2 <= 14
-// (the REAL*8 literals of kernel7.inc are single-precision constants),
-// else the central difference (n = 0, the kernels' k2 = 0.5/dx2).
-static FirY fir_y(const Grid &g)
+// The differentiator of optimalfilter (src/elastic3d.f90:846-907) along a
+// periodic axis of n samples: the 7-point FIR fir7 of src/kernel7.inc scaled
+// by 1/dx for 5 <= n <= 14 (the REAL*8 literals of kernel7.inc are
+// single-precision constants), else the central difference (n = 0, the
+// kernels' k = 0.5/dx).
+static Fir7 fir7_of(int n, double dx)
 {
     static const float fir7[7] = {8.77856e-01f, -2.81913e-01f, +6.22696e-02f, +2.82441e-02f,
                                   -5.09029e-02f, +4.20471e-02f, -1.59409e-02f};
-    FirY f{};
-    if (g.sx2 >= 5 && g.sx2 <= 14) {
+    Fir7 f{};
+    if (n >= 5 && n <= 14) {
         f.n = 7;
-        for (int l = 0; l < 7; l++) f.c[l] = (float)((double)fir7[l] / g.dx2);
+        for (int l = 0; l < 7; l++) f.c[l] = (float)((double)fir7[l] / dx);
     }
     return f;
 }
+static Fir7 fir_x(const Grid &g) { return fir7_of(g.sx1, g.dx1); }
+static Fir7 fir_y(const Grid &g) { return fir7_of(g.sx2, g.dx2); }
+static bool has_fir(const Grid &g) { return fir_x(g).n || fir_y(g).n; }
 
 // ---------------------------------------------------------------------------
 // host helpers: depth structures (src/elastic3d.f90:630-829)
@@ -865,7 +870,7 @@ struct relax_ctx {
     // device fields
     float *tau = nullptr, *m = nullptr, *sig = nullptr, *u = nullptr, *vp = nullptr, *gamma = nullptr;
     float *work = nullptr, *twork = nullptr, *tload = nullptr;
-    float *wy = nullptr;     // x2 derivatives of the strain source by fir7 (grids of 5 <= sx2 <= 14)
+    float *wxy = nullptr;    // x1 and x2 derivatives of the strain source (grids where x1 or x2 takes fir7)
     DepthVisc *visc[2] = {nullptr, nullptr};
     // transient (Burgers) rheology: structures, weak zones, epsilonik, epsilonikdot
     std::vector<relax_layer> lt, nlt;
@@ -926,7 +931,7 @@ static void free_ctx(relax_ctx *c)
     // one wait for the device, then every buffer goes back to the pool
     cudaDeviceSynchronize();
     const bool idle = true;
-    float *fs[] = {c->tau, c->m, c->sig, c->u, c->vp, c->wy, c->gamma, c->work, c->twork, c->tload, c->spdev,
+    float *fs[] = {c->tau, c->m, c->sig, c->u, c->vp, c->wxy, c->gamma, c->work, c->twork, c->tload, c->spdev,
                    c->dg0[0], c->dg0[1], c->tm_part, c->fr_part, c->vel, c->ur, c->urs};
     for (float *p : fs)
         if (p) dfree(p, idle);
@@ -1038,7 +1043,7 @@ static int create(const relax_config *cfg, int device, relax_ctx *c)
     TRY(dalloc(&c->work, 6 * nh));   // coseismic body force over the whole box (3 x sx3 layers)
     TRY(dalloc(&c->twork, 3 * g.plane));
     TRY(dalloc(&c->tload, g.plane));
-    if (fir_y(g).n) TRY(dalloc(&c->wy, 3 * nh));
+    if (has_fir(g)) TRY(dalloc(&c->wxy, 6 * nh));
     CK(cudaMemsetAsync(c->m, 0, 6 * nh * sizeof(float), c->st));
     CK(cudaMemsetAsync(c->sig, 0, 6 * nh * sizeof(float), c->st));
     CK(cudaMemsetAsync(c->u, 0, 3 * nh * sizeof(float), c->st));
@@ -1231,12 +1236,15 @@ static int launch_stress(relax_ctx *c, StressArgs a)
     const int stage = MODE == MODE_END ? ST_STRESS_END : MODE == MODE_CORR ? ST_STRESS_CORR
                       : MODE == MODE_INIT ? ST_STRESS_INIT : ST_OTHER;
     const bool trans = c->trans && MODE != MODE_OP && MODE != MODE_EIGEN;
-    if (c->wy && MODE != MODE_EIGEN) {
-        // grids of the 7-point x2 filter: its derivatives first, then the
-        // stress instantiation that reads them
+    if (c->wxy && MODE != MODE_EIGEN) {
+        // grids of the 7-point filter along x1 or x2: the derivatives first,
+        // then the stress instantiation that reads them
+        const Grid &g = c->g;
         TIMED(&c->prof, stage, c->st,
-              (k_fir_y<<<nblocks(3 * (c->g.nh / 4)), RELAX_NTHREADS, 0, c->st>>>(c->g, a.w, c->wy, fir_y(c->g))));
-        a.wy = c->wy;
+              (k_fir_xy<<<nblocks(3 * (g.nh / 4)), RELAX_NTHREADS, 0, c->st>>>(
+                  g, a.w, c->wxy, c->wxy + 3 * g.nh, fir_x(g), fir_y(g), a.k1, a.k2)));
+        a.wx = c->wxy;
+        a.wy = c->wxy + 3 * g.nh;
         if constexpr (MODE != MODE_OP && MODE != MODE_EIGEN) {
             if (trans) {
                 TIMED(&c->prof, stage, c->st,
@@ -1261,6 +1269,7 @@ static XfArgs xf_div(relax_ctx *c)
     x.m = c->m;
     x.k1 = (float)(0.5 / g.dx1); x.k2 = (float)(0.5 / g.dx2);
     x.k3 = (float)(0.5 / g.dx3); x.k3b = (float)(1.0 / g.dx3);
+    x.fx = fir_x(g);
     x.fy = fir_y(g);
     x.tload = nullptr;
     return x;
@@ -2872,11 +2881,13 @@ extern "C" int relax_op_stressupdate(const float *u1, const float *u2, const flo
     StressArgs a = op_args(g, lambda, mu);
     a.w = w;
     a.sig = s;
-    if (fir_y(g).n) {
-        float *wy;
-        TRY(sc.get(&wy, 3 * g.nh));
-        k_fir_y<<<nblocks(3 * (g.nh / 4)), RELAX_NTHREADS, 0, st>>>(g, w, wy, fir_y(g));
-        a.wy = wy;
+    if (has_fir(g)) {
+        float *wxy;
+        TRY(sc.get(&wxy, 6 * g.nh));
+        k_fir_xy<<<nblocks(3 * (g.nh / 4)), RELAX_NTHREADS, 0, st>>>(g, w, wxy, wxy + 3 * g.nh, fir_x(g),
+                                                                     fir_y(g), a.k1, a.k2);
+        a.wx = wxy;
+        a.wy = wxy + 3 * g.nh;
         k_stress<MODE_OP, false, false, true><<<nblocks(g.nh / 4), RELAX_NTHREADS, 0, st>>>(a);
     } else {
         k_stress<MODE_OP><<<nblocks(g.nh / 4), RELAX_NTHREADS, 0, st>>>(a);
@@ -2899,7 +2910,7 @@ extern "C" int relax_op_bodyforce(const relax_tensor *sig, double dx1, double dx
     k_aos_to_soa<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(sig, s, g.nh);
     k_bodyforce<<<nblocks(g.nh), RELAX_NTHREADS, 0, st>>>(g, s, c1, c2, c3, t1, t2, t3, (float)(0.5 / dx1),
                                                           (float)(0.5 / dx2), (float)(0.5 / dx3), (float)(1.0 / dx3),
-                                                          fir_y(g));
+                                                          fir_x(g), fir_y(g));
     CKL();
     return RELAX_OK;
 }
@@ -3555,7 +3566,7 @@ static int build_tables(relax_batch *b)
     for (int k = 0; k < n; k++) {
         relax_ctx *c = b->m[k];
         if (!c->m_valid) TRY(tail_init(c));
-        // batched shapes have sx2 % 32 == 0, never the x2 FIR (c->wy is null)
+        // batched shapes have sx2 % 32 == 0 and sx1 >= 64: no 7-point filter (c->wxy is null)
         corr[k] = stress_args(c, c->vp);
         end[k] = stress_args(c, c->u);
         xf[k] = c->sp.xargs(xf_div(c), g.sx3h);

@@ -52,9 +52,11 @@ def tensors_smooth(shape, scale=0.1, seed=0):
 
 GRIDS = [(32, 32, 32), (64, 48, 32), (96, 32, 36)]
 # grids of the 7-point FIR differentiator along x2 (5 <= sx2 <= 14: 6, 8, 9,
-# 12; sx2 = 6 wraps the 7 taps around the axis) and of shallow boxes
-# (5 <= sx3/2 <= 14, finite differences throughout), and sx2 = 4
-FIR_GRIDS = [(32, 8, 16), (32, 6, 12), (48, 12, 24), (64, 9, 18), (32, 4, 12)]
+# 12; sx2 = 6 wraps the 7 taps around the axis), along x1 (sx1 = 8, 12) or
+# both, and of shallow boxes (5 <= sx3/2 <= 14, finite differences
+# throughout), and sx2 = 4
+FIR_GRIDS = [(32, 8, 16), (32, 6, 12), (48, 12, 24), (64, 9, 18), (32, 4, 12), (8, 32, 16), (12, 16, 12),
+             (8, 6, 18), (12, 12, 24)]
 
 
 @pytest.mark.parametrize("sx1,sx2,sx3", GRIDS + [(16, 12, 8), (128, 96, 64)])

@@ -1,8 +1,9 @@
 """The oracle's differentiators against a numpy restatement, on grids where
 optimalfilter (src/elastic3d.f90:846-907) picks the 7-point FIR filter of
-src/kernel7.inc along x2 (5 <= sx2 <= 14) and along x3 (5 <= sx3/2 <= 14,
-where every layer is a boundary layer of the filter and the finite
-differences of localstrain_ani apply), and the central difference elsewhere.
+src/kernel7.inc along x1 (5 <= sx1 <= 14), x2 (5 <= sx2 <= 14) and x3
+(5 <= sx3/2 <= 14, where every layer is a boundary layer of the filter and
+the finite differences of localstrain_ani apply), and the central
+difference elsewhere.
 
 numpy's roll gives the periodic neighbours, so sx2 = 6 also checks the
 wrap-around of a 7-tap filter on an axis shorter than 2 x 7 + 1 samples.
@@ -40,7 +41,8 @@ def grad(a, dx, sx1, sx2):
     return (d_periodic(a, 2, sx1, dx[0]), d_periodic(a, 1, sx2, dx[1]), d_depth(a, dx[2]))
 
 
-GRIDS = [(32, 8, 8), (32, 6, 6), (48, 12, 12), (16, 9, 9), (32, 4, 6), (32, 16, 16), (16, 14, 5)]
+GRIDS = [(32, 8, 8), (32, 6, 6), (48, 12, 12), (16, 9, 9), (32, 4, 6), (32, 16, 16), (16, 14, 5),
+         (8, 32, 8), (12, 8, 6), (8, 6, 12), (12, 4, 9)]
 
 
 @pytest.mark.parametrize("sx1,sx2,sx3h", GRIDS)
