@@ -444,6 +444,14 @@ def run_gpu(args, rank, world, local_rank):
                          "coseismic solve and one untimed step), FP32 oracle restating the "
                          "reference CPU path"}
         accuracy = accuracy_vs_fp64(sim, args.steps, local_rank, mixed is not None)
+        # the other named single-instance configurations against the FP64
+        # oracle: the linear Maxwell box for its full 20 steps, and the large
+        # instance for one step (the oracle takes about a minute per step there)
+        from relax_b200.config import linear_maxwell, random_faults
+        accuracy["C1"] = accuracy_vs_fp64(linear_maxwell(sx=128, sz=128, dx=0.8, steps=20), 20, local_rank,
+                                          False)
+        if not args.no_large:
+            accuracy["C3"] = accuracy_vs_fp64(random_faults(1), 1, local_rank, False)
     b_alg = 536.0 * sim.npoints
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
