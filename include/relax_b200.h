@@ -701,11 +701,11 @@ int relax_op_dft64_tc(const float *in, float *out, int inverse, void *stream);
  * RELAX_ERR_ARG.  The first call on each device looks the array up
  * (cudaGetSymbolAddress) and sets kernel attributes: make that first call
  * before any stream capture.  All calls share the array; calls that overlap
- * on the GPU race on it, so order them on one stream.  Grid rules: sx1 >= 16
+ * on the GPU race on it, so order them on one stream.  Grid rules: sx1 >= 8
  * and a multiple of 4, even sx3 >= 4, sx2 >= 2, FFT lengths sx1/2, sx2, sx3
  * products of 2 and 3.  relax_op_green asks in addition what a context
- * needs (sx2 <= 4 or >= 15, sx3/2 >= 15, for the stencils of the step), so
- * this entry point also takes smaller grids. */
+ * needs (sx3/2 >= 5, where the step's differentiators stop), so this entry
+ * point also takes shallower grids. */
 int relax_op_green_noalloc(float *c1, float *c2, float *c3, float *t1,
                            float *t2, float *t3, int sx1, int sx2, int sx3,
                            double dx1, double dx2, double dx3, double lambda,

@@ -109,8 +109,8 @@ extern "C" int relax_op_green_noalloc(float *c1, float *c2, float *c3, float *t1
 {
     char msg[256];
     if (!c1 || !c2 || !c3 || !t1 || !t2 || !t3) return relax_noalloc_fail(RELAX_ERR_ARG, "null buffer");
-    if (sx1 < 16 || sx1 % 4 || sx2 < 2 || sx3 < 4 || sx3 % 2 || !(dx1 > 0 && dx2 > 0 && dx3 > 0))
-        return relax_noalloc_fail(RELAX_ERR_UNSUPPORTED, "grid: need sx1 >= 16, a multiple of 4, and even sx3");
+    if (sx1 < 8 || sx1 % 4 || sx2 < 2 || sx3 < 4 || sx3 % 2 || !(dx1 > 0 && dx2 > 0 && dx3 > 0))
+        return relax_noalloc_fail(RELAX_ERR_UNSUPPORTED, "grid: need sx1 >= 8, a multiple of 4, and even sx3");
     Grid g{};
     g.sx1 = sx1; g.sx2 = sx2; g.sx3 = sx3; g.sx3h = sx3 / 2; g.M = sx1 / 2; g.K1 = sx1 / 2 + 1;
     g.dx1 = dx1; g.dx2 = dx2; g.dx3 = dx3; g.plane = (size_t)sx1 * sx2; g.nh = g.plane * g.sx3h;

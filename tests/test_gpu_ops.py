@@ -221,7 +221,8 @@ def test_friction_abort_is_reported(oracle32):
 # sx1 = 256 and 512 take the x passes of the benchmarked boxes (M = 128, 256);
 # 256 x 256 x 128 is the C2 box itself
 GREEN_GRIDS = GRIDS + [(64, 64, 64), (64, 256, 128), (32, 512, 256), (128, 128, 128), (192, 192, 96),
-                       (64, 96, 96), (128, 32, 64), (256, 32, 64), (512, 32, 64), (256, 256, 128)]
+                       (64, 96, 96), (128, 32, 64), (256, 32, 64), (512, 32, 64), (256, 256, 128),
+                       (8, 32, 16), (12, 8, 12)]
 
 
 @pytest.mark.parametrize("sx1,sx2,sx3", GREEN_GRIDS)

@@ -79,12 +79,13 @@ def test_noalloc_green_rejects_a_grid_just_over_its_scratch():
         assert rc == want, (sx3, rc, lib.relax_last_error())
 
 
-def test_noalloc_green_small_grid_matches_oracle(oracle32):
-    """A grid that only this entry point takes (sx2 = 8, sx3/2 = 8: the
-    context's stencil rules do not apply to the Green's function alone),
-    against the oracle's greenfunctioncowling."""
+@pytest.mark.parametrize("sx1,sx2,sx3", [(32, 8, 16), (8, 12, 8)])
+def test_noalloc_green_small_grid_matches_oracle(oracle32, sx1, sx2, sx3):
+    """Small grids (sx2 = 8 or 12, sx1 = 8 with the generic x passes) and a
+    box shallower than a context takes (sx3/2 = 4: the step's
+    differentiators stop at 5, the Green's function alone does not), against
+    the oracle's greenfunctioncowling."""
     lib = _lib.load()
-    sx1, sx2, sx3 = 32, 8, 16
     c, t = _inputs(5, sx1, sx2, sx3)
     cr, tr = c.copy(), t.copy()
     oracle32.green(cr, tr, sx1, sx2, sx3, (0.5, 0.4, 0.25), 1.0, 1.0, 8.3e-4)
