@@ -372,6 +372,22 @@ def run_gpu(args, rank, world, local_rank):
                                    "frac": lb / (lstep / 1e3) / 1e9 / peaks()[0]},
                  "kernels": lk, "gpu_launches": llaunches, "clocks": lclocks}
 
+    # the linear Maxwell configuration (128^2 x 128 box, Dt = 0.5): 20 steps
+    # timed after 3 warm-up steps, plain form (the interval also holds the
+    # 10 profiled steps that follow)
+    from relax_b200.config import linear_maxwell
+    csim = linear_maxwell(sx=128, sz=128, dx=0.8, steps=33)
+    cms, claunches, cclocks, _, _ = timed_form("fp32", csim, 20, 3)
+    cstep = cms / 20
+    c1 = {"workload": "linear Maxwell below 30 km, vertical strike-slip fault, box 128x128x128, dx=0.8 km, "
+                      "Dt=0.5, 20 timed steps",
+          "grid_points": csim.npoints, "steps": 20, "warmup": 3,
+          "value": world * csim.npoints * 20 / (cms / 1e3), "unit": UNIT, "ms_per_step": cstep,
+          "step_roofline": {"alg_bytes_per_step": 536.0 * csim.npoints,
+                            "achieved_gbs": 536.0 * csim.npoints / (cstep / 1e3) / 1e9,
+                            "frac": 536.0 * csim.npoints / (cstep / 1e3) / 1e9 / peaks()[0]},
+          "gpu_launches": claunches, "clocks": cclocks}
+
     # the mixed-precision form beside the plain one (x3 transform's DFT-64
     # sub-transforms on the tensor cores), same workload, same timing
     mixed = None
@@ -475,6 +491,7 @@ def run_gpu(args, rank, world, local_rank):
         "accuracy": accuracy,
         "mixed": mixed,
         "large_instance": large,
+        "c1_instance": c1,
         "ensemble_c4": ens.get("c4"),
         "ensemble_c5": ens.get("c5"),
     }
