@@ -3775,8 +3775,11 @@ static int batch_step_begin(relax_batch *b, relax_step_log *logs, std::vector<ch
         const auto t0 = std::chrono::steady_clock::now();
         for (int k = 0; k < n; k++) {
             if (!live[k]) continue;
-            if (after) CK(cudaStreamWaitEvent(b->m[k]->st, after, 0));
-            TRY(do_step(b->m[k], nullptr, &logs[k]));
+            relax_ctx *c = b->m[k];
+            if (after) CK(cudaStreamWaitEvent(c->st, after, 0));
+            const int e0 = c->e;
+            TRY(do_step(c, nullptr, &logs[k]));
+            if (c->e != e0) b->tables_valid = false;   // as after a batched step's event branch
         }
         if (time_turn) {
             b->tt_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
