@@ -201,3 +201,15 @@ def test_ensemble_reports_each_group_tuning():
     assert [g["members"] for g in t] == [2, 1]
     assert t[0]["mode"] in ("batched", "in turn") and t[0]["batched_ms"] > 0 and t[0]["in_turn_ms"] > 0
     assert t[1]["mode"] == "in turn"   # one member: nothing to batch
+
+
+def test_batch_of_transient_members_matches_members_alone():
+    """Members with the transient (Burgers) rheology and a viscous layer:
+    the batched TRANS instantiations of the corrector and END passes (the
+    tuner's first three steps are batched, the fourth in turn)."""
+    from cases import transient_small
+    base = transient_small(linear=True, nonlinear=True, viscous=True, sx=64, sz=64)
+    sims = [_variant(base, k) for k in range(2)]
+    outs, _ = _batched(sims, 4)
+    for k, s in enumerate(sims):
+        _same(outs[k], _alone(s, 4))
