@@ -246,15 +246,19 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const 
     double amp_m = 0.0, amp_t = 0.0;
 
     if (live) {
-        const int i1 = (int)(q % q4) * 4;
-        const size_t r = q / q4;
-        const int i2 = (int)(r % g.sx2), i3 = (int)(r / g.sx2);
+        // point indexes by 32-bit division (nh / 4 < 2^32) and the periodic
+        // neighbours by selects: no 64-bit division on the device
+        const unsigned qq = (unsigned)q, q4u = (unsigned)q4, sx2u = (unsigned)g.sx2;
+        const unsigned r = qq / q4u, r3 = r / sx2u;
+        const int i1 = (int)(qq - r * q4u) * 4;
+        const int i2 = (int)(r - r3 * sx2u), i3 = (int)r3;
         const size_t nh = g.nh;
         const size_t row = ((size_t)i3 * g.sx2 + i2) * g.sx1;
         const size_t idx = row + i1;
-        const int i1m = (i1 + g.sx1 - 1) % g.sx1, i1p = (i1 + 4) % g.sx1;
-        const size_t rym = ((size_t)i3 * g.sx2 + (i2 + g.sx2 - 1) % g.sx2) * g.sx1 + i1;
-        const size_t ryp = ((size_t)i3 * g.sx2 + (i2 + 1) % g.sx2) * g.sx1 + i1;
+        const int i1m = i1 == 0 ? g.sx1 - 1 : i1 - 1, i1p = i1 + 4 == g.sx1 ? 0 : i1 + 4;
+        const int i2m = i2 == 0 ? g.sx2 - 1 : i2 - 1, i2p = i2 + 1 == g.sx2 ? 0 : i2 + 1;
+        const size_t rym = ((size_t)i3 * g.sx2 + i2m) * g.sx1 + i1;
+        const size_t ryp = ((size_t)i3 * g.sx2 + i2p) * g.sx1 + i1;
         size_t rzm, rzp;
         float kz;
         if (i3 == 0) { rzm = idx; rzp = idx + g.plane; kz = a.k3b; }
@@ -419,6 +423,10 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const 
             float4 gold = make_float4(0.f, 0.f, 0.f, 0.f);
             if ((MODE == MODE_CORR || MODE == MODE_EIGEN) && a.gamma) gold = ldc4(a.gamma + idx);
             float gacc[4] = {gold.x, gold.y, gold.z, gold.w};
+            // the largest gammadot per mechanism: its reciprocal is the
+            // minimum of the points' 1/gammadot (a correctly rounded
+            // reciprocal is monotonic), one division instead of four
+            float gmx[2] = {0.f, 0.f};
 #pragma unroll
             for (int mech = 0; mech < 2; mech++) {
                 if (!a.visc[mech]) continue;
@@ -452,7 +460,7 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const 
                     mo[3][j] += gd2 * d22 - gp2 * sp[3];
                     mo[4][j] += gd2 * s[4][j] - gp2 * sp[4];
                     mo[5][j] += gd2 * d33 - gp2 * sp[5];
-                    tmin[mech] = fminf(tmin[mech], 1.f / gd);
+                    gmx[mech] = fmaxf(gmx[mech], gd);
                     gsum[j] = gd * x;
                     if (MODE == MODE_EIGEN) gacc[j] = gsum[j];
                 }
@@ -461,6 +469,8 @@ __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const 
                     for (int j = 0; j < 4; j++) gacc[j] = gacc[j] + dtf * gsum[j];
                 }
             }
+#pragma unroll
+            for (int mech = 0; mech < 2; mech++) tmin[mech] = fminf(tmin[mech], 1.f / gmx[mech]);
             if (TRANS && (MODE == MODE_INIT || MODE == MODE_END || MODE == MODE_CORR) && a.eps) {
                 float ep[6][4], in[6][4], rate[6][4];
 #pragma unroll
