@@ -64,6 +64,20 @@ __device__ __forceinline__ float tnorm6(float a, float b, float c, float d, floa
     return sqrtf((a * a + 2.f * b * b + 2.f * c * c + d * d + 2.f * e * e + f * f) * 0.5f);
 }
 
+// Programmatic dependent launch.  A kernel launched with the
+// programmatic-serialization attribute may be scheduled while the kernel
+// before it in the stream still runs; pdl_wait (griddepcontrol.wait) blocks
+// until that kernel has completed and its memory operations are visible, and
+// returns at once in a launch without the attribute.  pdl_trigger
+// (griddepcontrol.launch_dependents) lets the next kernel be scheduled once
+// every block of this one has issued it.  The step's streaming kernels call
+// both first thing, wait before trigger, so that at most the next kernel's
+// blocks are placed during a kernel's last wave, and none reads memory
+// before its wait.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_enter() { pdl_wait(); }
+
 __device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
 __device__ __forceinline__ float4 ldc4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
@@ -232,6 +246,7 @@ struct StressArgs {
 template <int MODE, bool BATCH = false, bool TRANS = false, bool FIR = false>
 __global__ void __launch_bounds__(RELAX_NTHREADS, TRANS ? 2 : 3) k_stress(const __grid_constant__ StressArgs a0)
 {
+    pdl_enter();
     const StressArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     __shared__ float shf[32];
     __shared__ double shd[32];
@@ -848,6 +863,7 @@ struct FrictionPtsArgs {
 template <bool BATCH = false>
 __global__ void __launch_bounds__(RELAX_NTHREADS) k_friction_pts(const __grid_constant__ FrictionPtsArgs a0)
 {
+    pdl_enter();
     const FrictionPtsArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     __shared__ float shf[32];
     const Grid &g = a.g;
@@ -1227,6 +1243,7 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xfwd(XfArgs a)
 template <int XIN, int N1, int N2, int RW, bool BATCH = false>
 __global__ void __launch_bounds__(RW *N2, (RW * N2 <= 128) ? 8 : 4) k_xfwd_reg(const __grid_constant__ XfArgs a0)
 {
+    pdl_enter();
     const XfArgs &a = BATCH ? a0.tab[blockIdx.z] : a0;
     constexpr int M = N1 * N2, Q = N1 / N2, N2P = N2 + 1, NT = RW * N2;
     constexpr int RS0 = (N1 * N2P > M + 1 ? N1 * N2P : M + 1);
@@ -1573,6 +1590,7 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_zspec(ZArgs a)
 template <int N1, int N2, int CW, int SIGN, bool BATCH = false>
 __global__ void __launch_bounds__(CW *N2) k_ypass_reg(const __grid_constant__ YArgs a0)
 {
+    pdl_enter();
     const YArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     constexpr int n = N1 * N2, Q = N1 / N2;
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
@@ -1623,6 +1641,7 @@ constexpr int ZCOL = 26;   // floats of per-column constants in k_zspec_sm
 template <int N1, int N2, int CW, bool PRUNED, bool BATCH = false>
 __global__ void __launch_bounds__(CW *N2, (CW * N2 >= 256) ? 2 : 4) k_zspec_sm(const __grid_constant__ ZArgs a0)
 {
+    pdl_enter();
     const ZArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
     constexpr int n = N1 * N2, Q = N1 / N2;
     static_assert(N1 % N2 == 0, "N1 must be a multiple of N2");
@@ -1952,6 +1971,7 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
 template <int N1, int N2, int RW, int V, bool BATCH = false>
 __global__ void __launch_bounds__(RW *N2) k_xinv_reg(const __grid_constant__ XiArgs a0)
 {
+    pdl_enter();
     const XiArgs &a = BATCH ? a0.tab[blockIdx.z / 3] : a0;
     // RW rows of one plane and component per block, N2 threads per row.
     // (A) the block's spectrum rows, one contiguous run of RW*K1 values

@@ -297,15 +297,35 @@ static void set_smem(K kern, size_t sm)
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
 }
 
+// A launch with programmatic dependent launch allowed: the kernel (one that
+// enters through pdl_enter) may be scheduled while the previous kernel in the
+// stream finishes its last wave, and waits for it before touching memory.
+// Errors are left for cudaGetLastError, as with <<< >>>.
+template <typename... P, typename... A>
+static void launch_pdl(void (*kern)(P...), dim3 grid, dim3 block, size_t sm, cudaStream_t st, const A &...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <int N1, int N2, int SIGN>
 static void launch_ypass_sign(const YArgs &ya, dim3 grid, size_t sm, int nm, cudaStream_t st)
 {
     if (nm > 1) {
         set_smem(k_ypass_reg<N1, N2, kCW, SIGN, true>, sm);
-        k_ypass_reg<N1, N2, kCW, SIGN, true><<<dim3(grid.x, nm), kCW * N2, sm, st>>>(ya);
+        launch_pdl(k_ypass_reg<N1, N2, kCW, SIGN, true>, dim3(grid.x, nm), kCW * N2, sm, st, ya);
     } else {
         set_smem(k_ypass_reg<N1, N2, kCW, SIGN>, sm);
-        k_ypass_reg<N1, N2, kCW, SIGN><<<grid, kCW * N2, sm, st>>>(ya);
+        launch_pdl(k_ypass_reg<N1, N2, kCW, SIGN>, grid, kCW * N2, sm, st, ya);
     }
 }
 
@@ -340,10 +360,10 @@ static void launch_zspec_pr(const ZArgs &za, dim3 grid, size_t sm, int nm, cudaS
 {
     if (nm > 1) {
         set_smem(k_zspec_sm<N1, N2, kCW, PRUNED, true>, sm);
-        k_zspec_sm<N1, N2, kCW, PRUNED, true><<<dim3(grid.x, nm), kCW * N2, sm, st>>>(za);
+        launch_pdl(k_zspec_sm<N1, N2, kCW, PRUNED, true>, dim3(grid.x, nm), kCW * N2, sm, st, za);
     } else {
         set_smem(k_zspec_sm<N1, N2, kCW, PRUNED>, sm);
-        k_zspec_sm<N1, N2, kCW, PRUNED><<<grid, kCW * N2, sm, st>>>(za);
+        launch_pdl(k_zspec_sm<N1, N2, kCW, PRUNED>, grid, kCW * N2, sm, st, za);
     }
 }
 
@@ -375,10 +395,10 @@ static void launch_xinv_v(const XiArgs &xi, int nout, size_t sm, int nm, cudaStr
     constexpr int RW = 32;
     if (nm > 1) {
         set_smem(k_xinv_reg<N1, N2, RW, V, true>, sm);
-        k_xinv_reg<N1, N2, RW, V, true><<<dim3(xi.g.sx2 / RW, nout, 3 * nm), RW * N2, sm, st>>>(xi);
+        launch_pdl(k_xinv_reg<N1, N2, RW, V, true>, dim3(xi.g.sx2 / RW, nout, 3 * nm), RW * N2, sm, st, xi);
     } else {
         set_smem(k_xinv_reg<N1, N2, RW, V>, sm);
-        k_xinv_reg<N1, N2, RW, V><<<dim3(xi.g.sx2 / RW, nout, 3), RW * N2, sm, st>>>(xi);
+        launch_pdl(k_xinv_reg<N1, N2, RW, V>, dim3(xi.g.sx2 / RW, nout, 3), RW * N2, sm, st, xi);
     }
 }
 
@@ -422,10 +442,10 @@ static void launch_xfwd_in(const XfArgs &xa, dim3 grid, size_t sm, int nm, cudaS
     constexpr int RW = 16;
     if (nm > 1) {
         set_smem(k_xfwd_reg<XIN, N1, N2, RW, true>, sm);
-        k_xfwd_reg<XIN, N1, N2, RW, true><<<dim3(grid.x, grid.y, nm), RW * N2, sm, st>>>(xa);
+        launch_pdl(k_xfwd_reg<XIN, N1, N2, RW, true>, dim3(grid.x, grid.y, nm), RW * N2, sm, st, xa);
     } else {
         set_smem(k_xfwd_reg<XIN, N1, N2, RW>, sm);
-        k_xfwd_reg<XIN, N1, N2, RW><<<grid, RW * N2, sm, st>>>(xa);
+        launch_pdl(k_xfwd_reg<XIN, N1, N2, RW>, grid, RW * N2, sm, st, xa);
     }
 }
 
@@ -1248,17 +1268,17 @@ static int launch_stress(relax_ctx *c, StressArgs a)
         if constexpr (MODE != MODE_OP && MODE != MODE_EIGEN) {
             if (trans) {
                 TIMED(&c->prof, stage, c->st,
-                      (k_stress<MODE, false, true, true><<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(a)));
+                      (launch_pdl(k_stress<MODE, false, true, true>, c->nblk, RELAX_NTHREADS, 0, c->st, a)));
                 return RELAX_OK;
             }
         }
-        TIMED(&c->prof, stage, c->st, (k_stress<MODE, false, false, true><<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(a)));
+        TIMED(&c->prof, stage, c->st, (launch_pdl(k_stress<MODE, false, false, true>, c->nblk, RELAX_NTHREADS, 0, c->st, a)));
         return RELAX_OK;
     }
     if (trans)
-        TIMED(&c->prof, stage, c->st, (k_stress<MODE, false, true><<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(a)));
+        TIMED(&c->prof, stage, c->st, (launch_pdl(k_stress<MODE, false, true>, c->nblk, RELAX_NTHREADS, 0, c->st, a)));
     else
-        TIMED(&c->prof, stage, c->st, (k_stress<MODE><<<c->nblk, RELAX_NTHREADS, 0, c->st>>>(a)));
+        TIMED(&c->prof, stage, c->st, (launch_pdl(k_stress<MODE>, c->nblk, RELAX_NTHREADS, 0, c->st, a)));
     return RELAX_OK;
 }
 
@@ -1838,7 +1858,7 @@ static int friction_planes(relax_ctx *c, bool want_tm, int *nblk_out)
         FrictionPtsArgs a = friction_pts_args(c, k, want_tm);
         const int nb = (int)nblocks(a.npts);
         if (want_tm) a.tm_part = c->fr_part + blk_total;
-        TIMED(&c->prof, ST_FRICTION, c->st, (k_friction_pts<<<nb, RELAX_NTHREADS, 0, c->st>>>(a)));
+        TIMED(&c->prof, ST_FRICTION, c->st, (launch_pdl(k_friction_pts<false>, nb, RELAX_NTHREADS, 0, c->st, a)));
         blk_total += nb;
     }
     *nblk_out = blk_total;
@@ -3687,7 +3707,7 @@ static int batch_kernels(relax_batch *b)
     if (!c0->fc.empty())
         for (size_t q = 0; q < np; q++)
             if (t.frblk[q] > 0) {
-                k_friction_pts<true><<<dim3(t.frblk[q], n), RELAX_NTHREADS, 0, st>>>(t.frp0[q]);
+                launch_pdl(k_friction_pts<true>, dim3(t.frblk[q], n), RELAX_NTHREADS, 0, st, t.frp0[q]);
                 b->launches++;
             }
     k_dt_batch<<<n, RELAX_NTHREADS, 0, st>>>(t.dt);
@@ -3695,13 +3715,13 @@ static int batch_kernels(relax_batch *b)
     CKL();
     TRY(batch_green(b, t.xip0));
     // ---- corrector
-    if (b->trans) k_stress<MODE_CORR, true, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.corr0);
-    else k_stress<MODE_CORR, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.corr0);
+    if (b->trans) launch_pdl(k_stress<MODE_CORR, true, true>, dim3(c0->nblk, n), RELAX_NTHREADS, 0, st, t.corr0);
+    else launch_pdl(k_stress<MODE_CORR, true>, dim3(c0->nblk, n), RELAX_NTHREADS, 0, st, t.corr0);
     b->launches++;
     if (!c0->fc.empty())
         for (size_t q = 0; q < np; q++) {
             if (t.frblk[q] > 0) {
-                k_friction_pts<true><<<dim3(t.frblk[q], n), RELAX_NTHREADS, 0, st>>>(t.frc0[q]);
+                launch_pdl(k_friction_pts<true>, dim3(t.frblk[q], n), RELAX_NTHREADS, 0, st, t.frc0[q]);
                 b->launches++;
             }
             if (t.monblk[q] > 0) {
@@ -3734,8 +3754,8 @@ static int batch_kernels(relax_batch *b)
     }
     CKL();
     TRY(batch_green(b, t.xic0));
-    if (b->trans) k_stress<MODE_END, true, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.end0);
-    else k_stress<MODE_END, true><<<dim3(c0->nblk, n), RELAX_NTHREADS, 0, st>>>(t.end0);
+    if (b->trans) launch_pdl(k_stress<MODE_END, true, true>, dim3(c0->nblk, n), RELAX_NTHREADS, 0, st, t.end0);
+    else launch_pdl(k_stress<MODE_END, true>, dim3(c0->nblk, n), RELAX_NTHREADS, 0, st, t.end0);
     b->launches++;
     CKL();
     return RELAX_OK;
