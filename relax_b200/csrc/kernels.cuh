@@ -1586,11 +1586,13 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_zspec(ZArgs a)
 // length n = N1*N2, CW columns per block, N2 threads per column.
 // ------------------------------------------------------------------------
 
-// pass 2 / 4 along x2 (the 128-point transform, 128 threads a block, is given
-// the registers it asks for: 78 instead of 54-64, which measured faster on
-// 128 x 128 boxes)
+// pass 2 / 4 along x2.  Register budgets as measured fastest: the 128-point
+// transform (128 threads a block) takes the registers it asks for (78
+// instead of 54-64 on 128 x 128 boxes), the 256-point one 3 blocks of 256
+// threads per SM (85 registers instead of 64: forward pass 30.4 -> 27.4 us
+// on the 256 x 256 x 128 box)
 template <int N1, int N2, int CW, int SIGN, bool BATCH = false>
-__global__ void __launch_bounds__(CW *N2, (N1 == 16 && N2 == 8) ? 1 : 0) k_ypass_reg(const __grid_constant__ YArgs a0)
+__global__ void __launch_bounds__(CW *N2, (N1 == 16 && N2 == 8) ? 1 : (N1 == 16 && N2 == 16) ? 3 : 0) k_ypass_reg(const __grid_constant__ YArgs a0)
 {
     pdl_enter();
     const YArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
@@ -1969,9 +1971,11 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_xinv(XiArgs a)
 // values, RW rows of one plane and one component per block, N2 threads per
 // row, with the field update out = base + coef * w.  Shared-memory rows are
 // padded (N2+1 per k1 group, row stride = 8 mod 16 float2) so both transpose
-// access patterns are free of bank conflicts.
+// access patterns are free of bank conflicts.  Register budgets as measured:
+// 3 blocks per SM for M = 128 (33.6 -> 32.5 us on the 256 x 256 x 128 box),
+// the registers asked for at M = 64.
 template <int N1, int N2, int RW, int V, bool BATCH = false>
-__global__ void __launch_bounds__(RW *N2) k_xinv_reg(const __grid_constant__ XiArgs a0)
+__global__ void __launch_bounds__(RW *N2, (N1 * N2 == 128) ? 3 : (N1 * N2 == 64) ? 1 : 0) k_xinv_reg(const __grid_constant__ XiArgs a0)
 {
     pdl_enter();
     const XiArgs &a = BATCH ? a0.tab[blockIdx.z / 3] : a0;
