@@ -1590,9 +1590,11 @@ __global__ void __launch_bounds__(RELAX_NTHREADS) k_zspec(ZArgs a)
 // transform (128 threads a block) takes the registers it asks for (78
 // instead of 54-64 on 128 x 128 boxes), the 256-point one 3 blocks of 256
 // threads per SM (80 registers instead of 64: forward pass 30.4 -> 27.4 us
-// on the 256 x 256 x 128 box)
+// on the 256 x 256 x 128 box), the 512-point one 2 blocks per SM (128
+// registers instead of 85: 192 -> 187 us forward, 193 -> 185 us inverse on
+// the 512 x 512 x 256 box)
 template <int N1, int N2, int CW, int SIGN, bool BATCH = false>
-__global__ void __launch_bounds__(CW *N2, (N1 == 16 && N2 == 8) ? 1 : (N1 == 16 && N2 == 16) ? 3 : 0) k_ypass_reg(const __grid_constant__ YArgs a0)
+__global__ void __launch_bounds__(CW *N2, (N1 == 16 && N2 == 8) ? 1 : (N1 == 16 && N2 == 16) ? 3 : (N1 == 32) ? 2 : 0) k_ypass_reg(const __grid_constant__ YArgs a0)
 {
     pdl_enter();
     const YArgs &a = BATCH ? a0.tab[blockIdx.y] : a0;
